@@ -1,0 +1,351 @@
+/*
+ * rbmd_gpu.h -- C ABI of the B200 (sm_100a) per-step force-and-integrate path of RBMD.
+ *
+ * This header is the drop-in boundary.  It replaces the VTK-m execution objects and worklet
+ * launches that RBMD's NVT execution class drives (framework/run/ExecutionNVT.cpp:76-235), and the
+ * four Cont* and Exec* device objects:
+ *   - point locator      framework/locator/ContPointLocator.cxx:70-115, ExecPointLocator.h:38-382
+ *   - force function     framework/forceFunction/ContForceFunction.cpp:30-45, ExecForceFunction.h
+ *   - static erfc table  framework/staticTable/ContStaticTable.cpp:30-44 (replaced by analytic erfc)
+ *   - topology           framework/topology/ContTopology.cpp:31-42, ExecTopology.h:35-97
+ * and the worklet library framework/run/worklet/RunWorklet.h:40-502 plus the water constraint and
+ * bonded worklets of framework/run/worklet/MolecularWorklet.h.
+ *
+ * Plain C: pointers, sizes and status codes; no C++ or torch types cross this boundary.  Every
+ * function returns an int status (RBMD_OK == 0).  rbmd_last_error() gives the text of the last
+ * failure on a context.  The library never calls exit() (the reference's console::Error does,
+ * framework/Logging.h:44-51).
+ *
+ * Threading: one context per host thread, or external locking.  rbmd_step() only enqueues work on
+ * the context's CUDA stream; results are valid after rbmd_sync() (or any rbmd_get_* call, which
+ * synchronises first).
+ */
+#ifndef RBMD_GPU_H
+#define RBMD_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RBMD_ABI_VERSION 1
+
+/* ---------------------------------------------------------------- status codes */
+enum rbmd_status {
+  RBMD_OK = 0,
+  RBMD_ERR_ARG = 1,          /* bad argument (null pointer, size, unknown enum) */
+  RBMD_ERR_OOM = 2,          /* device allocation failed */
+  RBMD_ERR_NUMERIC = 3,      /* non-finite force / SHAKE or RATTLE singular / overflow */
+  RBMD_ERR_TIMEOUT = 4,      /* bounded device wait or serving wait expired */
+  RBMD_ERR_CUDA = 5,         /* CUDA runtime error */
+  RBMD_ERR_STATE = 6,        /* call out of order (unknown system id, serving not started ...) */
+  RBMD_ERR_BUDGET = 7,       /* request exceeds the HBM budget */
+  RBMD_ERR_UNSUPPORTED = 8,  /* configuration not implemented */
+  RBMD_ERR_IO = 9            /* file could not be read or parsed */
+};
+
+/* ---------------------------------------------------------------- enums (JSON strings in comments) */
+enum rbmd_force_field {      /* hyper_parameters.force_field.type */
+  RBMD_FF_LJ_CUT = 0,        /* "LJ/CUT" */
+  RBMD_FF_LJ_CUT_COUL_LONG = 1, /* "LJ/CUT/COUL/LONG" */
+  RBMD_FF_CVFF = 2,          /* "CVFF" (LJ + Coulomb + harmonic bond/angle + special bonds) */
+  RBMD_FF_EAM = 3            /* "EAM" (funcfl) */
+};
+enum rbmd_neighbor {         /* hyper_parameters.neighbor.type */
+  RBMD_NEIGH_RBL = 0,        /* "RBL" */
+  RBMD_NEIGH_VERLET = 1      /* "VERLETLIST" */
+};
+enum rbmd_coulomb {          /* hyper_parameters.coulomb.type (absent = NONE) */
+  RBMD_COUL_NONE = 0,
+  RBMD_COUL_RBE = 1,         /* "RBE" */
+  RBMD_COUL_EWALD = 2        /* "EWALD" */
+};
+enum rbmd_temp_ctrl {        /* execution.temp_ctrl_type */
+  RBMD_TC_NOSE_HOOVER = 0,   /* "NOSE_HOOVER" */
+  RBMD_TC_BERENDSEN = 1,     /* "BERENDSEN" */
+  RBMD_TC_RESCALE = 2,       /* "TEMP_RESCALE" */
+  RBMD_TC_NONE = 3           /* plain velocity Verlet (NVE) */
+};
+enum rbmd_units {            /* init_configuration.*.unit */
+  RBMD_UNITS_LJ = 0, RBMD_UNITS_REAL = 1, RBMD_UNITS_METAL = 2
+};
+enum rbmd_precision {
+  RBMD_PREC_FP64 = 0,        /* every kernel in FP64 */
+  RBMD_PREC_MIXED = 1        /* pair + RBE arithmetic FP32; positions, rho(k) sums, reductions,
+                                SHAKE, thermostat and barostat FP64 */
+};
+enum rbmd_rbl_mode {
+  RBMD_RBL_STRIDE = 0,       /* every pice-th shell atom in cell traversal order (reference) */
+  RBMD_RBL_PHILOX = 1        /* same stride, start offset drawn per (seed, step, atom) */
+};
+enum rbmd_random_mode {
+  RBMD_RANDOM_PHILOX = 0,    /* counter-based Philox4x32-10 keyed by (seed, step, index) */
+  RBMD_RANDOM_TEST = 1       /* every uniform is 0.5 (reference velocity_type "TEST") */
+};
+enum rbmd_shake_flag {       /* hyper_parameters.extend.fix_shake */
+  RBMD_SHAKE_NULL = -1,      /* key absent ("null") */
+  RBMD_SHAKE_FALSE = 0,
+  RBMD_SHAKE_TRUE = 1
+};
+enum rbmd_ensemble {
+  RBMD_ENS_NVT = 0, RBMD_ENS_NVE = 1, RBMD_ENS_NPT = 2
+};
+enum rbmd_press_ctrl {
+  RBMD_PC_BERENDSEN = 0      /* "Berendsen" isotropic volume rescale */
+};
+
+/* ---------------------------------------------------------------- run parameters */
+/* Mirrors the JSON keys that framework/hyperparameters/{ForceField,Neighbor,Coulomb,Extend}.cpp
+ * and ExecutionMD::SetParameters (framework/run/ExecutionMD.cpp:144-153) copy into Para. */
+typedef struct rbmd_params {
+  int32_t force_field;          /* enum rbmd_force_field */
+  int32_t neighbor;             /* enum rbmd_neighbor */
+  int32_t coulomb;              /* enum rbmd_coulomb */
+  int32_t ensemble;             /* enum rbmd_ensemble */
+  int32_t temp_ctrl;            /* enum rbmd_temp_ctrl */
+  int32_t units;                /* enum rbmd_units */
+  int32_t precision;            /* enum rbmd_precision */
+  int32_t rbl_mode;             /* enum rbmd_rbl_mode */
+  int32_t random_mode;          /* enum rbmd_random_mode */
+  int32_t fix_shake;            /* enum rbmd_shake_flag */
+  int32_t init_inbuild;         /* 1: system built by the inbuild lattice (temperature without kB) */
+  int32_t neighbor_sample_num;  /* RBL shell sample target */
+  double cut_off;               /* r_c */
+  double r_core;                /* r_s (VERLETLIST: ignored, r_s = r_c) */
+  int32_t coulomb_sample_num;   /* RBE P */
+  int32_t kmax[3];              /* Ewald k range (energy in RBE mode, force in EWALD mode) */
+  double alpha;                 /* Ewald splitting, reference convention: erfc(sqrt(alpha) r) */
+  double temperature[3];        /* T_start, T_stop, T_damp */
+  double pressure[3];           /* P_start, P_stop, P_damp (NPT) */
+  int32_t press_ctrl;           /* enum rbmd_press_ctrl */
+  int32_t pad0;
+  double timestep;
+  int64_t num_steps;            /* length of the run, used for temperature ramps */
+  double special_bonds[3];      /* 1-2, 1-3, 1-4 LJ weights */
+  uint64_t seed;                /* Philox key */
+} rbmd_params;
+
+/* Fill *p with the reference defaults (LJ units, RBL, NH, FP64, stride picks, seed 1). */
+void rbmd_params_default(rbmd_params* p);
+
+/* ---------------------------------------------------------------- system description */
+/* Host arrays; the library copies them at rbmd_system_add and the caller keeps ownership.
+ * Layout follows the Para fields of framework/FieldName.h:30-153: position Vec3[N], velocity
+ * Vec3[N], mass/charge Real[N], pts_type/molecule_id Id[N], epsilon/sigma Real[ntypes],
+ * position_flag Id3[N], special_ids/weights/offsets CSR, bond_atom_id Id[2nb], angle_atom_id
+ * Id[3na], {frho,rhor,z2r}_spline Vec7[n+1]. */
+typedef struct rbmd_system_desc {
+  int32_t n_atoms;
+  int32_t n_types;
+  double box_lo[3];
+  double box_hi[3];
+  const double* position;       /* [3*n_atoms] x0 y0 z0 x1 ... */
+  const double* velocity;       /* [3*n_atoms] or NULL (zero) */
+  const double* charge;         /* [n_atoms] or NULL (zero) */
+  const double* mass;           /* [n_atoms] per-atom mass */
+  const int32_t* type;          /* [n_atoms] 0-based type index */
+  const int32_t* molecule;      /* [n_atoms] or NULL (atom i is molecule i) */
+  const int32_t* image;         /* [3*n_atoms] or NULL (zero image flags) */
+  const double* epsilon;        /* [n_types] LJ epsilon per type */
+  const double* sigma;          /* [n_types] LJ sigma per type */
+  /* harmonic bonds (CVFF): E = k (r - r0)^2 */
+  int32_t n_bonds;
+  int32_t n_bond_types;
+  const int32_t* bond_atoms;    /* [2*n_bonds] */
+  const int32_t* bond_type;     /* [n_bonds] 0-based */
+  const double* bond_k;         /* [n_bond_types] */
+  const double* bond_r0;        /* [n_bond_types] */
+  /* harmonic angles (CVFF): E = k (theta - theta0)^2; also the SHAKE triples (H, O, H) */
+  int32_t n_angles;
+  int32_t n_angle_types;
+  const int32_t* angle_atoms;   /* [3*n_angles] */
+  const int32_t* angle_type;    /* [n_angles] */
+  const double* angle_k;        /* [n_angle_types] */
+  const double* angle_theta0;   /* [n_angle_types] degrees */
+  /* special-bond LJ weights, CSR over atoms (ModelFileInitCondition.cpp:843-923) */
+  const int32_t* special_offsets; /* [n_atoms+1] or NULL */
+  const int32_t* special_ids;
+  const double* special_weights;
+  /* EAM splines (ExecutionNVT.cpp:899-1104): Vec7 coefficient rows, index 0 unused */
+  int32_t eam_nrho;
+  int32_t eam_nr;
+  double eam_drho;
+  double eam_dr;
+  double eam_rhomax;
+  double eam_cut;
+  const double* eam_frho_spline; /* [(eam_nrho+1)*7] */
+  const double* eam_rhor_spline; /* [(eam_nr+1)*7] */
+  const double* eam_z2r_spline;  /* [(eam_nr+1)*7] */
+} rbmd_system_desc;
+
+/* ---------------------------------------------------------------- results */
+typedef struct rbmd_thermo {
+  int64_t step;                 /* Executioner current step of the system */
+  double temperature;           /* PARA_TEMPT after the last ComputeTempe */
+  double tempT_sum;             /* sum m v^2 mvv2e */
+  double kinetic_energy;        /* tempT_sum / N / 2 (ThermoOutput.cpp:180) */
+  double e_lj;                  /* per-atom averages, as ThermoOutput reports them */
+  double e_coul_near;
+  double e_coul_far;            /* Ewald k-space (kmax) + self energy */
+  double e_bond;
+  double e_angle;
+  double e_eam;
+  double potential_energy;
+  double total_energy;
+  double pressure;
+  double virial[6];             /* xx yy zz xy xz yz */
+  double nhc_eta[3];
+  double nhc_eta_dot[4];
+  double volume;
+  double box_lo[3];
+  double box_hi[3];
+  int32_t status;               /* device-side error word of the system (0 = ok) */
+  int32_t pad0;
+} rbmd_thermo;
+
+typedef struct rbmd_device_cfg {
+  int32_t device;               /* CUDA ordinal */
+  int32_t batched;              /* 1: one segment-indexed launch per kernel over all systems of a
+                                   rbmd_step call; 0: one launch per system (the plain path) */
+  int32_t use_graphs;           /* 1: capture the step of a fixed system set as a CUDA graph */
+  int32_t pad0;
+  int64_t hbm_budget_bytes;     /* admission budget for the serving loop (0 = free memory) */
+} rbmd_device_cfg;
+
+typedef struct rbmd_ctx rbmd_ctx;
+
+/* ---------------------------------------------------------------- context and systems */
+int rbmd_abi_version(void);
+int rbmd_ctx_create(const rbmd_device_cfg* cfg, rbmd_ctx** out);
+int rbmd_ctx_destroy(rbmd_ctx* ctx);
+const char* rbmd_last_error(const rbmd_ctx* ctx);
+
+/* Bytes of device memory a system with this description needs (admission by HBM budget). */
+int rbmd_system_bytes(const rbmd_system_desc* desc, const rbmd_params* params, int64_t* bytes);
+
+/* Upload a system (Para fields + JSON parameters; the InitCondition + SetForceFunction/SetTopology
+ * of ExecutionMD::Init, framework/run/ExecutionMD.cpp:117-134). */
+int rbmd_system_add(rbmd_ctx* ctx, const rbmd_system_desc* desc, const rbmd_params* params,
+                    int32_t* sys_id);
+int rbmd_system_remove(rbmd_ctx* ctx, int32_t sys_id);
+
+/* ExecutionNVT::Init's tail (framework/run/ExecutionNVT.cpp:60-74,139-187): thermostat set-up
+ * (ComputeTempe, ComputeTempTarget, NH chain masses) and the first ComputeForce. */
+int rbmd_init(rbmd_ctx* ctx, const int32_t* sys_ids, int32_t n);
+
+/* nsteps x Executioner::TakeStep -> ExecutionMD::Execute (PreSolve, Solve, PostSolve;
+ * framework/executioner/Executioner.cpp:112-117, framework/run/ExecutionNVT.cpp:76-135) for every
+ * listed system.  Enqueue only. */
+int rbmd_step(rbmd_ctx* ctx, const int32_t* sys_ids, int32_t n, int32_t nsteps);
+int rbmd_sync(rbmd_ctx* ctx);
+
+/* ComputeForce at the current positions without integrating (ExecutionNVT::ComputeForce,
+ * framework/run/ExecutionNVT.cpp:189-235); uses the system's current step for random draws. */
+int rbmd_compute_forces(rbmd_ctx* ctx, const int32_t* sys_ids, int32_t n);
+
+int rbmd_get_forces(rbmd_ctx* ctx, int32_t sys_id, double* force /* [3N] */);
+int rbmd_get_state(rbmd_ctx* ctx, int32_t sys_id, double* position, double* velocity,
+                   int32_t* image);
+int rbmd_set_state(rbmd_ctx* ctx, int32_t sys_id, const double* position, const double* velocity,
+                   const int32_t* image);
+/* Thermo quantities; energies are evaluated at the current positions on request (the reference
+ * recomputes them every step for ThermoOutput, framework/output/ThermoOutput.cpp:144-186). */
+int rbmd_get_thermo(rbmd_ctx* ctx, int32_t sys_id, rbmd_thermo* out);
+
+/* Cell list of the last binning (ContPointLocator::Build, framework/locator/ContPointLocator.cxx:70-92):
+ * dims[3]; per atom the reference flat cell id; atom ids sorted by cell (ascending id within a
+ * cell); per cell [lower, upper).  Any output pointer may be NULL. */
+int rbmd_get_cells(rbmd_ctx* ctx, int32_t sys_id, int32_t* dims, int32_t* cell_of_atom,
+                   int32_t* sorted_ids, int32_t* cell_lower, int32_t* cell_upper);
+
+/* Materialise the RBL lists of the current positions and step (ComputeRBLNeighboursOnceWorklet,
+ * framework/run/worklet/RunWorklet.cpp:906-980): per atom n_core, n_shell and the picked ids in
+ * traversal order, core first, in rows of `cap` ids.  Returns RBMD_ERR_ARG if a row exceeds cap. */
+int rbmd_get_rbl_lists(rbmd_ctx* ctx, int32_t sys_id, int32_t cap, int32_t* n_core,
+                       int32_t* n_shell, int32_t* ids);
+
+/* RBE k samples of the last force evaluation (integer m vectors, [3P]) and rho(k) ([2P]: Re, Im). */
+int rbmd_get_kspace(rbmd_ctx* ctx, int32_t sys_id, int32_t* m, double* rhok);
+
+/* Per-system parameters derived at upload: rs_num, rc_num, pice_num, num_cycles, dims[3],
+ * S (RBE normalisation), volume. */
+typedef struct rbmd_derived {
+  int32_t rs_num, rc_num, pice_num, num_cycles;
+  int32_t dims[3];
+  int32_t n_cells;
+  double rho_system;
+  double S_rbe;
+  double volume;
+  double cell_width[3];
+} rbmd_derived;
+int rbmd_get_derived(rbmd_ctx* ctx, int32_t sys_id, rbmd_derived* out);
+
+/* ---------------------------------------------------------------- EAM input helpers (host only) */
+/* funcfl file contents after the header lines (ExecutionNVT::ReadPotentialFile,
+ * framework/run/ExecutionNVT.cpp:899-931). */
+typedef struct rbmd_eam_file {
+  int32_t nrho, nr;
+  double drho, dr, cut_off;
+  const double* frho;   /* [nrho] */
+  const double* zr;     /* [nr] */
+  const double* rhor;   /* [nr] */
+} rbmd_eam_file;
+/* Number of rows the spline arrays need: (nrho+1) and (nr+1). */
+int rbmd_eam_spline_sizes(const rbmd_eam_file* in, int32_t* nrho_out, int32_t* nr_out);
+/* file2array + array2spline (framework/run/ExecutionNVT.cpp:933-1079): fills the three Vec7
+ * tables (caller allocates (nrho+1)*7, (nr+1)*7, (nr+1)*7 doubles) and rhomax. */
+int rbmd_eam_build_splines(const rbmd_eam_file* in, double* frho_spline, double* rhor_spline,
+                           double* z2r_spline, int32_t* nrho_out, double* drho_out,
+                           int32_t* nr_out, double* dr_out, double* rhomax_out);
+/* Read a funcfl file: first call with arrays NULL to get nrho/nr, second call to fill. */
+int rbmd_eam_read_funcfl(const char* path, rbmd_eam_file* out_sizes, double* frho, double* zr,
+                         double* rhor);
+
+/* ---------------------------------------------------------------- serving (continuous batching) */
+typedef struct rbmd_serve_cfg {
+  int64_t hbm_budget_bytes;     /* 0: use the context's budget */
+  int32_t max_systems;          /* slots (0 = unlimited) */
+  int32_t steps_per_round;      /* MD steps run per batched launch sequence between admissions */
+  int32_t use_graphs;
+  int32_t pad0;
+} rbmd_serve_cfg;
+
+typedef struct rbmd_request_stats {
+  double t_submit;              /* seconds, host monotonic clock */
+  double t_admit;
+  double t_done;
+  int64_t atom_steps;
+  int32_t n_atoms;
+  int32_t status;
+} rbmd_request_stats;
+
+enum rbmd_request_state {
+  RBMD_REQ_QUEUED = 0, RBMD_REQ_RUNNING = 1, RBMD_REQ_DONE = 2, RBMD_REQ_FAILED = 3
+};
+
+int rbmd_serve_start(rbmd_ctx* ctx, const rbmd_serve_cfg* cfg);
+/* Submit an independent MD system that should run nsteps; returns immediately. */
+int rbmd_serve_submit(rbmd_ctx* ctx, const rbmd_system_desc* desc, const rbmd_params* params,
+                      int32_t nsteps, int64_t* request_id);
+int rbmd_serve_poll(rbmd_ctx* ctx, int64_t request_id, int32_t* state);
+int rbmd_serve_wait(rbmd_ctx* ctx, int64_t request_id, double timeout_s);
+/* Final state and statistics; position/velocity [3N] may be NULL. Frees the request. */
+int rbmd_serve_result(rbmd_ctx* ctx, int64_t request_id, double* position, double* velocity,
+                      rbmd_thermo* thermo, rbmd_request_stats* stats);
+int rbmd_serve_stop(rbmd_ctx* ctx);
+
+/* ---------------------------------------------------------------- diagnostics */
+/* Number of kernel launches this context enqueued (graph replays count their nodes). */
+int rbmd_launch_count(rbmd_ctx* ctx, int64_t* launches);
+/* Average device time per launch of the named kernel family since the last reset, measured with
+ * CUDA events on the context stream when profiling is on ("pair", "rho", "final", ...). */
+int rbmd_profile_enable(rbmd_ctx* ctx, int32_t on);
+int rbmd_profile_get(rbmd_ctx* ctx, const char* kernel, double* avg_ms, int64_t* launches,
+                     double* units_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RBMD_GPU_H */

@@ -1,0 +1,257 @@
+"""rbmd_b200 -- B200-native (sm_100a) force-and-integrate path of RBMD behind a C ABI.
+
+The product is `rbmd_b200/_lib/librbmd_b200.so` (include/rbmd_gpu.h) and the `rbmd` host binary.
+This module is a thin ctypes binding of that ABI for Python callers (tests, bench, serving
+clients).  There is no CPU fallback: loading fails loudly when the library is missing.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi as A
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "librbmd_b200.so")
+
+_lib = None
+
+
+class RbmdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{A.STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load the sm_100a library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m rbmd_b200.build` (there is no CPU path)")
+        _lib = A.declare(C.CDLL(LIB_PATH))
+        if _lib.rbmd_abi_version() != A.RBMD_ABI_VERSION:
+            raise ImportError("ABI version mismatch between rbmd_b200/_abi.py and the library")
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(A.dptr)
+
+
+def _ip(a):
+    return a.ctypes.data_as(A.iptr)
+
+
+class Context:
+    """One CUDA device context: systems, batched steps, serving loop."""
+
+    def __init__(self, device=0, batched=True, graphs=True, hbm_budget_bytes=0):
+        L = lib()
+        cfg = A.DeviceCfg(device=device, batched=int(batched), use_graphs=int(graphs),
+                          hbm_budget_bytes=int(hbm_budget_bytes))
+        h = C.c_void_p()
+        rc = L.rbmd_ctx_create(C.byref(cfg), C.byref(h))
+        if rc:
+            raise RbmdError(rc, "rbmd_ctx_create failed (no CUDA device?)")
+        self.h = h
+        self._sizes = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().rbmd_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc):
+        if rc:
+            msg = lib().rbmd_last_error(self.h)
+            raise RbmdError(rc, msg.decode() if msg else "")
+        return rc
+
+    @staticmethod
+    def _ids(ids):
+        if isinstance(ids, int):
+            ids = [ids]
+        a = np.ascontiguousarray(ids, np.int32)
+        return a, len(a)
+
+    # ---- systems
+    def add_system(self, sd, params=None):
+        desc = sd.desc()
+        prm = params if params is not None else sd.params
+        sid = C.c_int32()
+        self._check(lib().rbmd_system_add(self.h, C.byref(desc), C.byref(prm), C.byref(sid)))
+        self._sizes[sid.value] = (sd.n, prm.coulomb_sample_num if prm.coulomb == A.COUL_RBE else 0)
+        return sid.value
+
+    def remove_system(self, sid):
+        self._check(lib().rbmd_system_remove(self.h, sid))
+        self._sizes.pop(sid, None)
+
+    def init(self, ids):
+        a, n = self._ids(ids)
+        self._check(lib().rbmd_init(self.h, _ip(a), n))
+
+    def step(self, ids, nsteps=1):
+        a, n = self._ids(ids)
+        self._check(lib().rbmd_step(self.h, _ip(a), n, nsteps))
+
+    def sync(self):
+        self._check(lib().rbmd_sync(self.h))
+
+    def compute_forces(self, ids):
+        a, n = self._ids(ids)
+        self._check(lib().rbmd_compute_forces(self.h, _ip(a), n))
+
+    def forces(self, sid):
+        n = self._sizes[sid][0]
+        f = np.zeros((n, 3))
+        self._check(lib().rbmd_get_forces(self.h, sid, _dp(f)))
+        return f
+
+    def state(self, sid):
+        n = self._sizes[sid][0]
+        x, v = np.zeros((n, 3)), np.zeros((n, 3))
+        img = np.zeros((n, 3), np.int32)
+        self._check(lib().rbmd_get_state(self.h, sid, _dp(x), _dp(v), _ip(img)))
+        return x, v, img
+
+    def set_state(self, sid, x=None, v=None, image=None):
+        x = None if x is None else np.ascontiguousarray(x, np.float64)
+        v = None if v is None else np.ascontiguousarray(v, np.float64)
+        image = None if image is None else np.ascontiguousarray(image, np.int32)
+        self._check(lib().rbmd_set_state(self.h, sid, None if x is None else _dp(x),
+                                         None if v is None else _dp(v), None if image is None else _ip(image)))
+
+    def thermo(self, sid):
+        t = A.Thermo()
+        self._check(lib().rbmd_get_thermo(self.h, sid, C.byref(t)))
+        return t.as_dict()
+
+    def derived(self, sid):
+        d = A.Derived()
+        self._check(lib().rbmd_get_derived(self.h, sid, C.byref(d)))
+        return {k: (list(getattr(d, k)) if hasattr(getattr(d, k), "__len__") else getattr(d, k))
+                for k, _ in d._fields_}
+
+    def cells(self, sid):
+        n = self._sizes[sid][0]
+        d = self.derived(sid)
+        nc = d["n_cells"]
+        dims = np.zeros(3, np.int32)
+        coa, srt = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        lo, up = np.zeros(nc, np.int32), np.zeros(nc, np.int32)
+        self._check(lib().rbmd_get_cells(self.h, sid, _ip(dims), _ip(coa), _ip(srt), _ip(lo), _ip(up)))
+        return dims, coa, srt, lo, up
+
+    def rbl_lists(self, sid, cap=1024):
+        n = self._sizes[sid][0]
+        nc, ns = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        ids = np.full((n, cap), -1, np.int32)
+        self._check(lib().rbmd_get_rbl_lists(self.h, sid, cap, _ip(nc), _ip(ns), _ip(ids)))
+        return nc, ns, ids
+
+    def kspace(self, sid):
+        P = self._sizes[sid][1]
+        m = np.zeros((P, 3), np.int32)
+        rk = np.zeros((P, 2))
+        self._check(lib().rbmd_get_kspace(self.h, sid, _ip(m), _dp(rk)))
+        return m, rk
+
+    # ---- diagnostics
+    def launch_count(self):
+        v = C.c_int64()
+        self._check(lib().rbmd_launch_count(self.h, C.byref(v)))
+        return v.value
+
+    def profile(self, on=True):
+        self._check(lib().rbmd_profile_enable(self.h, int(on)))
+
+    def profile_get(self, name):
+        ms, n, u = C.c_double(), C.c_int64(), C.c_double()
+        self._check(lib().rbmd_profile_get(self.h, name.encode(), C.byref(ms), C.byref(n), C.byref(u)))
+        return ms.value, n.value, u.value
+
+    # ---- serving
+    def serve_start(self, hbm_budget_bytes=0, max_systems=0, steps_per_round=10, graphs=True):
+        cfg = A.ServeCfg(hbm_budget_bytes=int(hbm_budget_bytes), max_systems=max_systems,
+                         steps_per_round=steps_per_round, use_graphs=int(graphs))
+        self._check(lib().rbmd_serve_start(self.h, C.byref(cfg)))
+
+    def serve_submit(self, sd, nsteps, params=None):
+        desc = sd.desc()
+        prm = params if params is not None else sd.params
+        rid = C.c_int64()
+        self._check(lib().rbmd_serve_submit(self.h, C.byref(desc), C.byref(prm), nsteps, C.byref(rid)))
+        self._sizes[("req", rid.value)] = sd.n
+        return rid.value
+
+    def serve_poll(self, rid):
+        st = C.c_int32()
+        self._check(lib().rbmd_serve_poll(self.h, rid, C.byref(st)))
+        return st.value
+
+    def serve_wait(self, rid, timeout=-1.0):
+        return lib().rbmd_serve_wait(self.h, rid, timeout)
+
+    def serve_result(self, rid, want_state=True):
+        n = self._sizes.pop(("req", rid))
+        x = np.zeros((n, 3)) if want_state else None
+        v = np.zeros((n, 3)) if want_state else None
+        th, st = A.Thermo(), A.RequestStats()
+        rc = lib().rbmd_serve_result(self.h, rid, None if x is None else _dp(x), None if v is None else _dp(v),
+                                     C.byref(th), C.byref(st))
+        self._check(rc)
+        stats = {k: getattr(st, k) for k, _ in st._fields_}
+        return x, v, th.as_dict(), stats
+
+    def serve_stop(self):
+        self._check(lib().rbmd_serve_stop(self.h))
+
+
+def eam_splines(file_dict):
+    """rbmd_eam_build_splines on a funcfl body given as a dict of numpy arrays."""
+    L = lib()
+    frho = np.ascontiguousarray(file_dict["frho"], np.float64)
+    zr = np.ascontiguousarray(file_dict["zr"], np.float64)
+    rhor = np.ascontiguousarray(file_dict["rhor"], np.float64)
+    f = A.EamFile(nrho=int(file_dict["nrho"]), nr=int(file_dict["nr"]), drho=float(file_dict["drho"]),
+                  dr=float(file_dict["dr"]), cut_off=float(file_dict["cut"]), frho=_dp(frho), zr=_dp(zr),
+                  rhor=_dp(rhor))
+    nrho, nr = C.c_int32(), C.c_int32()
+    if L.rbmd_eam_spline_sizes(C.byref(f), C.byref(nrho), C.byref(nr)):
+        raise RbmdError(A.ERR_ARG, "bad EAM table")
+    fs = np.zeros(7 * (nrho.value + 1))
+    rs = np.zeros(7 * (nr.value + 1))
+    zs = np.zeros(7 * (nr.value + 1))
+    o_nrho, o_nr = C.c_int32(), C.c_int32()
+    drho, dr, rhomax = C.c_double(), C.c_double(), C.c_double()
+    rc = L.rbmd_eam_build_splines(C.byref(f), _dp(fs), _dp(rs), _dp(zs), C.byref(o_nrho), C.byref(drho),
+                                  C.byref(o_nr), C.byref(dr), C.byref(rhomax))
+    if rc:
+        raise RbmdError(rc, "rbmd_eam_build_splines failed")
+    return dict(nrho=o_nrho.value, nr=o_nr.value, drho=drho.value, dr=dr.value, rhomax=rhomax.value,
+                cut=float(file_dict["cut"]), frho_spline=fs, rhor_spline=rs, z2r_spline=zs)
+
+
+def read_funcfl(path):
+    """rbmd_eam_read_funcfl: the body of a funcfl EAM file as a dict of numpy arrays."""
+    L = lib()
+    f = A.EamFile()
+    rc = L.rbmd_eam_read_funcfl(path.encode(), C.byref(f), None, None, None)
+    if rc:
+        raise RbmdError(rc, path)
+    frho, zr, rhor = np.zeros(f.nrho), np.zeros(f.nr), np.zeros(f.nr)
+    rc = L.rbmd_eam_read_funcfl(path.encode(), C.byref(f), _dp(frho), _dp(zr), _dp(rhor))
+    if rc:
+        raise RbmdError(rc, path)
+    return dict(nrho=f.nrho, nr=f.nr, drho=f.drho, dr=f.dr, cut=f.cut_off, frho=frho, zr=zr, rhor=rhor)

@@ -1,0 +1,202 @@
+// common.cuh -- device-side system record, random streams and warp/block helpers shared by the
+// sm_100a kernels of the RBMD force-and-integrate path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/rbmd_gpu.h"
+
+namespace rbmd {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kPif = 3.1415927410125732421875;  // float pi promoted, as the reference's Pif()
+
+constexpr int kWarp = 32;
+constexpr int kPairWarps = 8;          // atoms (warps) per block of the pair kernel
+constexpr int kAtomBlock = 256;        // atoms per block of the streaming kernels
+constexpr int kRhoChunk = 256;         // atoms per block of the structure-factor kernel
+constexpr int kCellBlock = 256;        // cells per block of the cell kernels
+constexpr int kRbeSlack = 64;          // extra Metropolis proposal slots beyond P
+constexpr int kQueue = 64;             // per-warp pair queue of the pair kernel
+
+// device error word bits (rbmd_thermo.status)
+enum : int {
+  kErrShakeOverflow = 1, kErrShakeSingular = 2, kErrShakeNoConverge = 4, kErrRattleSingular = 8,
+  kErrNonFinite = 16, kErrRbeSlots = 32, kErrCellRange = 64
+};
+
+// Random stream tags (third Philox counter word); must match the oracle's.
+enum : uint32_t {
+  kTagRbeGauss = 0x52424531u, kTagRbeAccept = 0x52424532u, kTagRblOffset = 0x52424c31u
+};
+
+// Per-system scalar state that kernels read and update on the device (thermostat chain,
+// reductions, step counter).  One record per system, in device memory.
+struct SysState {
+  double eta[3], eta_dot[4], eta_dotdot[3], eta_mass[3];
+  double t_target, ke_target, t_freq, tdrag, tdof;
+  double temperature;      // PARA_TEMPT
+  double tempT_sum;        // PARA_TEMPT_SUM
+  double vscale_pending;   // velocity factor not yet applied (end-of-step thermostat)
+  double vscale_pending_c; // same for atoms of constrained triples
+  double vscale_a;         // factor of the start-of-step half of the chain
+  double fmean[3];         // RBL mean near force of the last evaluation
+  double virial[6];        // last virial sum (when requested)
+  double shake_virial[6];  // sum of the last SHAKE virials
+  double energy[8];        // energy scratch: lj, coul, eam_embed, eam_pair, bond, angle, ewald, self
+  int64_t step;            // Executioner current step
+  int status;              // error word
+  int pad;
+  unsigned counter[8];     // last-block arrival counters
+};
+
+struct SysDev {
+  // sizes and switches
+  int n, ntypes, ff, neigh, coul, prec, rbl_mode, random_mode, temp_ctrl, fix_shake, inbuild;
+  int special, pice, nc, ncell, P, n_bonds, n_angles, nk_ewald;
+  int dims[3];
+  int eam_nrho, eam_nr;
+  int blocks_pair, blocks_atom, blocks_rho, blocks_tri, rbe_mmax, rbe_slots, has_triples, n_triples;
+  // geometry and physics
+  double lo[3], hi[3], L[3], d[3];
+  double rc, rs, rc2, rs2, alpha, volume, S;
+  double qqr2e, fmt2v, mvv2e, kB, boltz, nktv2p;
+  double dt, t_start, t_stop, t_damp;
+  int64_t num_steps;
+  double eam_dr, eam_drho, eam_rhomax, eam_cut;
+  double rbe_sigma[3];
+  uint32_t seed_lo, seed_hi;
+  // atom arrays (original order)
+  double4* x;          // x, y, z, charge
+  double4* v;          // vx, vy, vz, mass
+  double4* f;          // force
+  double4* xold;       // pre-drift positions (SHAKE)
+  double4* vold;       // pre-kick velocities (SHAKE first half)
+  double4* vold2;      // pre-kick velocities (RATTLE)
+  int4* meta;          // type, molecule, flags (bit0: in a constrained triple), unused
+  int* image;          // [3n]
+  // cells
+  int* cell_of_atom;   // reference flat cell id
+  int* cell_count;     // [ncell]
+  int* cell_start;     // [ncell + 1]
+  int* cell_fill;      // [ncell] scatter cursors
+  int* sorted;         // atom ids in cell order
+  double4* sx;         // sorted positions + charge (FP64)
+  float4* sxf;         // sorted positions + charge (FP32)
+  int4* smeta;         // sorted: atom id, type, molecule, unused
+  // per-type tables
+  double* eps;
+  double* sig;
+  // special-bond CSR and molecules
+  int* sp_off;
+  int* sp_ids;
+  double* sp_w;
+  int* mol_off;
+  int* mol_atoms;
+  // bonded terms
+  int* bond_atoms;
+  int* bond_type;
+  double* bond_k;
+  double* bond_r0;
+  int* angle_atoms;
+  int* angle_type;
+  double* angle_k;
+  double* angle_t0;
+  double4* term_force; // [2 n_bonds + 3 n_angles] per-term forces
+  int* aterm_off;      // [n + 1] atom -> term-force slots (CSR)
+  int* aterm;          // slots
+  double* term_energy; // [n_bonds + n_angles]
+  double* term_vir;    // [6 (n_bonds + n_angles)] per-term virials (pressure requests)
+  // k space
+  int* km;             // [3P] sampled m vectors
+  double4* kv;         // [P or nk] k vector + coefficient -4 pi / (V k^2) (Ewald: x exp(-k^2/4a))
+  double* rhok;        // [2P or 2nk]
+  double* rho_part;    // [blocks_rho * 2P]
+  double* rbe_tab;     // [3 * (2 mmax + 1) * 2]: P(m), q(m) per dimension
+  double4* kv_e;       // [nk_e] Ewald-energy k vectors (kmax grid), w = exp(-k^2/4a)/k^2
+  double* rhok_e;      // [2 nk_e]
+  int nk_e;
+  int pad_e;
+  // EAM
+  double* frho_s;
+  double* rhor_s;
+  double* z2r_s;
+  double* eam_fp;      // [n]
+  // reductions
+  double* pair_part;   // [blocks_pair * 4]
+  double* atom_part;   // [blocks_atom * 8]
+  double* vir_part;    // [blocks_pair * 9] pair-kernel partials
+  double* tri_part;    // [blocks_tri * 6] SHAKE virial partials
+  SysState* st;
+};
+
+// ------------------------------------------------------------------------------ Philox4x32-10
+// Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11.
+__host__ __device__ inline void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                              uint32_t k0, uint32_t k1, uint32_t out[4]) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+    uint32_t n1 = (uint32_t)p1;
+    uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+    uint32_t n3 = (uint32_t)p0;
+    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+__host__ __device__ inline double u01(uint32_t hi, uint32_t lo) {
+  uint64_t bits = ((uint64_t)(hi >> 5) << 26) | (uint64_t)(lo >> 6);
+  return (double)bits * (1.0 / 9007199254740992.0);
+}
+
+// ------------------------------------------------------------------------------ reductions
+template <typename T>
+__device__ inline T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ inline int warp_incl_scan(int v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+
+__device__ inline unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
+
+// Last-block-done pattern: every block of a system calls this after writing its partials; the
+// block that arrives last gets true and may reduce all partials of the system in a fixed order.
+// The counter is reset by the last block, so the pattern needs no host-side clearing.
+__device__ inline bool arrive_last(unsigned* counter, unsigned nblocks) {
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned t = atomicAdd(counter, 1u);
+    s_last = (t == nblocks - 1);
+    if (s_last) *counter = 0u;
+  }
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last;
+}
+
+// Orthorhombic minimum image (ExecPointLocator::MinDistanceVec).
+template <typename R>
+__device__ inline void min_image(R& x, R& y, R& z, R Lx, R Ly, R Lz) {
+  if (fabs(x) > Lx * R(0.5)) x -= (x > R(0) ? Lx : -Lx);
+  if (fabs(y) > Ly * R(0.5)) y -= (y > R(0) ? Ly : -Ly);
+  if (fabs(z) > Lz * R(0.5)) z -= (z > R(0) ? Lz : -Lz);
+}
+
+}  // namespace rbmd

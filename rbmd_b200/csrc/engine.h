@@ -1,0 +1,105 @@
+// engine.h -- host-side context, systems and step orchestration behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+namespace rbmd {
+
+struct Units {
+  double kB, fmt2v, mvv2e, qqr2e, boltz, nktv2p;
+};
+Units make_units(int units);
+
+// One system: its parameters, derived quantities and device allocations.
+struct System {
+  int id = -1;
+  int slot = -1;
+  rbmd_params p{};
+  rbmd_derived dv{};
+  SysDev dev{};                 // host mirror of the device record
+  std::vector<void*> allocs;    // device allocations owned by the system
+  int64_t bytes = 0;
+  double self_energy = 0.0;     // per-atom Ewald self energy (qqr2e applied)
+  int n_terms = 0;
+  int P = 0;
+  std::vector<double> charge;   // host copy (energies)
+};
+
+struct Profiler {
+  bool on = false;
+  struct Rec {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+    std::vector<double> units;
+    double ms = 0.0;
+    long long n = 0;
+    double units_sum = 0.0;
+  };
+  std::map<std::string, Rec> recs;
+};
+
+class Context {
+ public:
+  explicit Context(const rbmd_device_cfg& cfg);
+  ~Context();
+
+  int add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t* id);
+  int remove_system(int id);
+  int init(const int32_t* ids, int n);
+  int step(const int32_t* ids, int n, int nsteps);
+  int compute_forces(const int32_t* ids, int n);
+  int sync();
+  int get_forces(int id, double* f);
+  int get_state(int id, double* x, double* v, int32_t* image);
+  int set_state(int id, const double* x, const double* v, const int32_t* image);
+  int get_thermo(int id, rbmd_thermo* out);
+  int get_cells(int id, int32_t* dims, int32_t* coa, int32_t* sorted, int32_t* lo, int32_t* up);
+  int get_rbl_lists(int id, int cap, int32_t* nc, int32_t* ns, int32_t* ids);
+  int get_kspace(int id, int32_t* m, double* rhok);
+  int get_derived(int id, rbmd_derived* out);
+  int device_status(int id, int* status);
+
+  int fail(int code, const std::string& msg);
+  std::string last_error;
+  rbmd_device_cfg cfg{};
+  cudaStream_t stream = nullptr;
+  Profiler prof;
+  std::recursive_mutex mu;
+
+  System* find(int id);
+  static int64_t estimate_bytes(const rbmd_system_desc& d, const rbmd_params& p);
+
+ private:
+  struct BatchRec {
+    Batch b;
+    std::vector<void*> allocs;
+    std::vector<int> ids;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+  };
+  int ensure_slots(int need);
+  int upload_record(System* s);
+  std::vector<BatchRec*> batches_for(const int32_t* ids, int n, int& rc);
+  BatchRec* build_batch(const std::vector<System*>& group, int& rc);
+  void drop_batches_with(int id);
+  void enqueue_step(const Batch& b);
+  void enqueue_forces(const Batch& b, FinalMode mode, int virial);
+  template <class F> void timed(const char* name, double units, F&& fn);
+  int check_cuda(const char* where);
+
+  std::vector<System*> systems_;
+  std::vector<int> free_slots_;
+  SysDev* d_sys_ = nullptr;
+  int slot_cap_ = 0;
+  int next_id_ = 0;
+  std::map<std::vector<int>, BatchRec*> batch_cache_;
+};
+
+}  // namespace rbmd

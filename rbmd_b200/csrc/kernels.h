@@ -1,0 +1,53 @@
+// kernels.h -- host-side launchers of the sm_100a kernels.  A launch covers every system listed
+// in a Batch (segment-indexed work tables); the plain path builds one Batch per system.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace rbmd {
+
+// Work item of a segment-indexed launch: (system slot, first element of the block).
+struct Work {
+  int2* d = nullptr;
+  int n = 0;
+};
+
+struct Batch {
+  SysDev* sys = nullptr;     // device array of all system records (indexed by slot)
+  int* d_slots = nullptr;    // slots of this batch
+  int nsys = 0;
+  Work atom, pair, cell, rho, tri, term, kred, draw;
+  // uniform switches of the batch (a batch never mixes them)
+  int ff = 0, neigh = 0, coul = 0, prec = 0, temp_ctrl = 0, special = 0;
+  int has_shake = 0, has_bonded = 0;
+  int max_P = 0;             // largest P (or Ewald nk) in the batch
+};
+
+enum FinalMode { kFinalForceOnly = 0, kFinalKick = 1, kFinalInit = 2 };
+
+void launch_nhc_a(const Batch& b, cudaStream_t s);
+void launch_kick_drift(const Batch& b, cudaStream_t s);
+void launch_cells(const Batch& b, cudaStream_t s);
+void launch_shake(const Batch& b, cudaStream_t s);
+void launch_rattle(const Batch& b, cudaStream_t s);
+void launch_rbe_sample(const Batch& b, cudaStream_t s);
+void launch_rho(const Batch& b, cudaStream_t s, int ewald);
+void launch_bonded(const Batch& b, cudaStream_t s, int virial);
+void launch_pair(const Batch& b, cudaStream_t s, int virial);
+void launch_final(const Batch& b, cudaStream_t s, FinalMode mode, int virial);
+void launch_ke_thermostat(const Batch& b, cudaStream_t s);
+void launch_flush_vscale(const Batch& b, cudaStream_t s);
+void launch_energy(const Batch& b, cudaStream_t s);
+void launch_ewald_energy(const Batch& b, cudaStream_t s);
+
+// RBL list materialisation for parity checks (not on the step path).
+void launch_rbl_lists(const SysDev* sys, int slot, int n, int cap, int* n_core, int* n_shell,
+                      int* ids, cudaStream_t s);
+
+// number of kernel launches issued by the launchers so far (all threads)
+long long launches_issued();
+void note_launch(int k = 1);
+
+}  // namespace rbmd

@@ -1,0 +1,301 @@
+// serve.cpp -- continuous batching of independent MD systems on one GPU.
+//
+// Requests arrive at any time.  Between rounds of batched steps the loop admits queued requests
+// in arrival order while the HBM budget and the slot limit allow, runs `steps_per_round` steps
+// of every active system in one segment-indexed launch sequence (replayed as a CUDA graph while
+// the active set is unchanged), and retires systems whose step count is reached.  Positions,
+// velocities and thermostat state stay resident on the device for the whole request.  Each
+// system's arithmetic is independent of the others in the batch (per-system work tables and
+// per-system fixed-order reductions), so a result is the same alone and in the mix.
+#include "serve.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+
+namespace rbmd {
+
+double monotonic_seconds() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+template <class T>
+static void cp(std::vector<T>& dst, const T* src, size_t n) {
+  if (src && n) dst.assign(src, src + n);
+  else dst.clear();
+}
+
+void OwnedDesc::copy_from(const rbmd_system_desc& s) {
+  d = s;
+  const size_t n = (size_t)s.n_atoms;
+  cp(pos, s.position, 3 * n);
+  cp(vel, s.velocity, 3 * n);
+  cp(chg, s.charge, n);
+  cp(mass, s.mass, n);
+  cp(type, s.type, n);
+  cp(mol, s.molecule, n);
+  cp(img, s.image, 3 * n);
+  cp(eps, s.epsilon, (size_t)s.n_types);
+  cp(sig, s.sigma, (size_t)s.n_types);
+  cp(ba, s.bond_atoms, 2 * (size_t)s.n_bonds);
+  cp(bt, s.bond_type, (size_t)s.n_bonds);
+  cp(bk, s.bond_k, (size_t)s.n_bond_types);
+  cp(br0, s.bond_r0, (size_t)s.n_bond_types);
+  cp(aa, s.angle_atoms, 3 * (size_t)s.n_angles);
+  cp(at, s.angle_type, (size_t)s.n_angles);
+  cp(ak, s.angle_k, (size_t)s.n_angle_types);
+  cp(at0, s.angle_theta0, (size_t)s.n_angle_types);
+  cp(spo, s.special_offsets, s.special_offsets ? n + 1 : 0);
+  const size_t ns = s.special_offsets ? (size_t)s.special_offsets[n] : 0;
+  cp(spi, s.special_ids, ns);
+  cp(spw, s.special_weights, ns);
+  cp(frho, s.eam_frho_spline, s.eam_frho_spline ? 7 * (size_t)(s.eam_nrho + 1) : 0);
+  cp(rhor, s.eam_rhor_spline, s.eam_rhor_spline ? 7 * (size_t)(s.eam_nr + 1) : 0);
+  cp(z2r, s.eam_z2r_spline, s.eam_z2r_spline ? 7 * (size_t)(s.eam_nr + 1) : 0);
+  auto P = [](auto& v) { return v.empty() ? nullptr : v.data(); };
+  d.position = P(pos);
+  d.velocity = P(vel);
+  d.charge = P(chg);
+  d.mass = P(mass);
+  d.type = P(type);
+  d.molecule = P(mol);
+  d.image = P(img);
+  d.epsilon = P(eps);
+  d.sigma = P(sig);
+  d.bond_atoms = P(ba);
+  d.bond_type = P(bt);
+  d.bond_k = P(bk);
+  d.bond_r0 = P(br0);
+  d.angle_atoms = P(aa);
+  d.angle_type = P(at);
+  d.angle_k = P(ak);
+  d.angle_theta0 = P(at0);
+  d.special_offsets = P(spo);
+  d.special_ids = P(spi);
+  d.special_weights = P(spw);
+  d.eam_frho_spline = P(frho);
+  d.eam_rhor_spline = P(rhor);
+  d.eam_z2r_spline = P(z2r);
+}
+
+Server::Server(Context* c, const rbmd_serve_cfg& cfg) : ctx_(c), cfg_(cfg) {
+  if (cfg_.steps_per_round <= 0) cfg_.steps_per_round = 10;
+  budget_ = cfg_.hbm_budget_bytes > 0 ? cfg_.hbm_budget_bytes : c->cfg.hbm_budget_bytes;
+  if (budget_ <= 0) {
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    budget_ = (int64_t)(fr * 0.85);
+  }
+}
+
+Server::~Server() { stop(); }
+
+int Server::start() {
+  std::lock_guard<std::mutex> lk(mu_);
+  if (running_) return RBMD_OK;
+  stop_ = false;
+  running_ = true;
+  th_ = std::thread([this] { loop(); });
+  return RBMD_OK;
+}
+
+int Server::stop() {
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!running_) return RBMD_OK;
+    stop_ = true;
+  }
+  cv_.notify_all();
+  if (th_.joinable()) th_.join();
+  std::lock_guard<std::mutex> lk(mu_);
+  running_ = false;
+  // fail whatever is still queued or active
+  for (Request* r : queue_) {
+    r->state = RBMD_REQ_FAILED;
+    r->status = RBMD_ERR_STATE;
+  }
+  queue_.clear();
+  for (Request* r : active_) {
+    if (r->sys >= 0) ctx_->remove_system(r->sys);
+    r->state = RBMD_REQ_FAILED;
+    r->status = RBMD_ERR_STATE;
+  }
+  active_.clear();
+  done_cv_.notify_all();
+  return RBMD_OK;
+}
+
+int Server::submit(const rbmd_system_desc& d, const rbmd_params& p, int nsteps, int64_t* rid) {
+  if (d.n_atoms <= 0 || !d.position || !d.mass || !d.type) return ctx_->fail(RBMD_ERR_ARG, "incomplete system");
+  auto r = std::make_unique<Request>();
+  r->desc.copy_from(d);
+  r->params = p;
+  r->nsteps = r->remaining = nsteps;
+  r->bytes = Context::estimate_bytes(d, p);
+  r->t_submit = monotonic_seconds();
+  std::lock_guard<std::mutex> lk(mu_);
+  if (!running_) return ctx_->fail(RBMD_ERR_STATE, "serving loop not running");
+  if (r->bytes > budget_) return ctx_->fail(RBMD_ERR_BUDGET, "request larger than the HBM budget");
+  r->id = next_id_++;
+  *rid = r->id;
+  queue_.push_back(r.get());
+  all_[r->id] = std::move(r);
+  cv_.notify_all();
+  return RBMD_OK;
+}
+
+int Server::poll(int64_t rid, int32_t* state) {
+  std::lock_guard<std::mutex> lk(mu_);
+  auto it = all_.find(rid);
+  if (it == all_.end()) return ctx_->fail(RBMD_ERR_STATE, "unknown request");
+  if (state) *state = it->second->state;
+  return RBMD_OK;
+}
+
+int Server::wait(int64_t rid, double timeout_s) {
+  std::unique_lock<std::mutex> lk(mu_);
+  auto it = all_.find(rid);
+  if (it == all_.end()) return ctx_->fail(RBMD_ERR_STATE, "unknown request");
+  Request* r = it->second.get();
+  auto pred = [&] { return r->state == RBMD_REQ_DONE || r->state == RBMD_REQ_FAILED; };
+  if (timeout_s < 0) {
+    done_cv_.wait(lk, pred);
+  } else if (!done_cv_.wait_for(lk, std::chrono::duration<double>(timeout_s), pred)) {
+    return RBMD_ERR_TIMEOUT;
+  }
+  return r->state == RBMD_REQ_DONE ? RBMD_OK : r->status;
+}
+
+int Server::result(int64_t rid, double* x, double* v, rbmd_thermo* th, rbmd_request_stats* stats) {
+  std::lock_guard<std::mutex> lk(mu_);
+  auto it = all_.find(rid);
+  if (it == all_.end()) return ctx_->fail(RBMD_ERR_STATE, "unknown request");
+  Request* r = it->second.get();
+  if (r->state != RBMD_REQ_DONE && r->state != RBMD_REQ_FAILED) return RBMD_ERR_STATE;
+  const size_t n = (size_t)r->desc.d.n_atoms;
+  if (x && r->x.size() == 3 * n) std::memcpy(x, r->x.data(), sizeof(double) * 3 * n);
+  if (v && r->v.size() == 3 * n) std::memcpy(v, r->v.data(), sizeof(double) * 3 * n);
+  if (th) *th = r->thermo;
+  if (stats) {
+    stats->t_submit = r->t_submit;
+    stats->t_admit = r->t_admit;
+    stats->t_done = r->t_done;
+    stats->atom_steps = (int64_t)n * r->nsteps;
+    stats->n_atoms = (int32_t)n;
+    stats->status = r->status;
+  }
+  const int status = r->status;
+  all_.erase(it);
+  return status;
+}
+
+void Server::finish(Request* r, int status) {
+  r->status = status;
+  r->state = status == RBMD_OK ? RBMD_REQ_DONE : RBMD_REQ_FAILED;
+  r->t_done = monotonic_seconds();
+}
+
+void Server::admit_locked(std::vector<Request*>& admitted) {
+  while (!queue_.empty()) {
+    Request* r = queue_.front();
+    if (cfg_.max_systems > 0 && (int)active_.size() + (int)admitted.size() >= cfg_.max_systems) break;
+    if (used_ + r->bytes > budget_) break;  // admission strictly in arrival order
+    queue_.pop_front();
+    used_ += r->bytes;
+    admitted.push_back(r);
+  }
+}
+
+void Server::loop() {
+  while (!stop_) {
+    std::vector<Request*> admitted;
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      admit_locked(admitted);
+      if (admitted.empty() && active_.empty()) {
+        cv_.wait_for(lk, std::chrono::milliseconds(2), [&] { return stop_ || !queue_.empty(); });
+        continue;
+      }
+    }
+    // upload + Init of the admitted systems (outside the queue lock)
+    std::vector<int32_t> new_ids;
+    for (Request* r : admitted) {
+      int32_t sid = -1;
+      int rc = ctx_->add_system(r->desc.d, r->params, &sid);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (rc) {
+        used_ -= r->bytes;
+        finish(r, rc);
+        done_cv_.notify_all();
+        continue;
+      }
+      r->sys = sid;
+      r->state = RBMD_REQ_RUNNING;
+      r->t_admit = monotonic_seconds();
+      new_ids.push_back(sid);
+    }
+    if (!new_ids.empty()) {
+      int rc = ctx_->init(new_ids.data(), (int)new_ids.size());
+      if (rc) {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (Request* r : admitted)
+          if (r->sys >= 0) {
+            ctx_->remove_system(r->sys);
+            used_ -= r->bytes;
+            finish(r, rc);
+          }
+        done_cv_.notify_all();
+        continue;
+      }
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      for (Request* r : admitted)
+        if (r->state == RBMD_REQ_RUNNING) active_.push_back(r);
+    }
+    if (active_.empty()) continue;
+    // one round of batched steps over every active system
+    int k = cfg_.steps_per_round;
+    for (Request* r : active_) k = std::min(k, std::max(r->remaining, 0));
+    std::vector<int32_t> ids;
+    std::vector<Request*> stepping;
+    for (Request* r : active_)
+      if (r->remaining > 0) {
+        ids.push_back(r->sys);
+        stepping.push_back(r);
+      }
+    int rc = RBMD_OK;
+    if (!ids.empty() && k > 0) {
+      rc = ctx_->step(ids.data(), (int)ids.size(), k);
+      if (!rc) rc = ctx_->sync();
+      for (Request* r : stepping) r->remaining -= k;
+    }
+    // retire finished systems
+    std::vector<Request*> keep;
+    for (Request* r : active_) {
+      if (r->remaining > 0 && !rc) {
+        keep.push_back(r);
+        continue;
+      }
+      const int n = r->desc.d.n_atoms;
+      r->x.assign(3 * (size_t)n, 0.0);
+      r->v.assign(3 * (size_t)n, 0.0);
+      int st = rc;
+      if (!st) st = ctx_->get_state(r->sys, r->x.data(), r->v.data(), nullptr);
+      if (!st) st = ctx_->get_thermo(r->sys, &r->thermo);
+      if (!st && r->thermo.status != 0) st = RBMD_ERR_NUMERIC;
+      ctx_->remove_system(r->sys);
+      std::lock_guard<std::mutex> lk(mu_);
+      used_ -= r->bytes;
+      finish(r, st);
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      active_ = keep;
+    }
+    done_cv_.notify_all();
+  }
+}
+
+}  // namespace rbmd

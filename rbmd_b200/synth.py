@@ -1,0 +1,423 @@
+"""Seeded synthetic systems for the five benchmark workloads and the tests.
+
+Each builder returns a `SystemData` holding numpy arrays in the layout of `rbmd_system_desc`
+(include/rbmd_gpu.h) plus the matching `rbmd_params`.  No public dataset is involved: every system
+is generated from a seed (the reference ships no benchmark inputs, and its bundled data files are
+read by the data-file reader, not by these builders).
+
+Workloads (sizes exactly as named):
+  * lj_fcc        LJ fluid, 4000 atoms, fcc 10x10x10x4, rho* 0.8442, T* 1.44, rc 2.5, RBL rs 1.2
+  * nacl_melt     rock-salt melt, 20^3 simple-cubic alternating +1/-1, rho 0.6, RBE alpha 0.6 P 200
+  * spce_water    3000 SPC/E molecules, 1.0 g/cm^3, RBE alpha 0.09 (beta 0.3/A) P 100, SHAKE
+  * eam_cu        fcc Cu 20^3 x 4 = 32000 atoms, Johnson-form EAM tabulated to 5.0 A
+  * saline        SPC/E + 0.15 M NaCl (Joung-Cheatham 2008 SPC/E ion parameters)
+"""
+import math
+
+import numpy as np
+
+from . import _abi as A
+
+# physical constants for REAL units (g/mol, A, fs, kcal/mol)
+AVOGADRO = 6.02214076e23
+KB_REAL = 1.9872067e-3
+MVV2E_REAL = 1.0 / 4.186e-4
+
+M_O, M_H, M_NA, M_CL, M_CU = 15.9994, 1.008, 22.98977, 35.453, 63.546
+SPCE = dict(q_o=-0.8476, q_h=0.4238, sigma_o=3.166, eps_o=0.1553, r_oh=1.0, theta=109.47)
+# Joung & Cheatham, J. Phys. Chem. B 112, 9020 (2008), SPC/E set: sigma = Rmin / 2^(1/6)
+ION_NA = dict(sigma=2.1595, eps=0.3526418, q=1.0, mass=M_NA)
+ION_CL = dict(sigma=4.8305, eps=0.0127850, q=-1.0, mass=M_CL)
+
+
+class SystemData:
+    """Host-side arrays of one system; `desc()` returns an rbmd_system_desc pointing into them."""
+
+    def __init__(self, pos, mass, types, eps, sig, box_lo, box_hi, vel=None, charge=None,
+                 molecule=None, params=None, name="system"):
+        self.name = name
+        self.pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        n = self.pos.shape[0]
+        self.mass = np.ascontiguousarray(mass, dtype=np.float64).reshape(n)
+        self.types = np.ascontiguousarray(types, dtype=np.int32).reshape(n)
+        self.eps = np.ascontiguousarray(eps, dtype=np.float64)
+        self.sig = np.ascontiguousarray(sig, dtype=np.float64)
+        self.box_lo = np.asarray(box_lo, dtype=np.float64)
+        self.box_hi = np.asarray(box_hi, dtype=np.float64)
+        self.vel = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64).reshape(n, 3)
+        self.charge = None if charge is None else np.ascontiguousarray(charge, dtype=np.float64)
+        self.molecule = None if molecule is None else np.ascontiguousarray(molecule, dtype=np.int32)
+        self.image = None
+        self.bond_atoms = self.bond_type = self.bond_k = self.bond_r0 = None
+        self.angle_atoms = self.angle_type = self.angle_k = self.angle_theta0 = None
+        self.special_offsets = self.special_ids = self.special_weights = None
+        self.eam = None
+        self.params = params if params is not None else A.default_params()
+        self._desc = None
+
+    @property
+    def n(self):
+        return self.pos.shape[0]
+
+    def copy(self):
+        import copy
+        other = copy.copy(self)
+        for k, v in self.__dict__.items():
+            if isinstance(v, np.ndarray):
+                setattr(other, k, v.copy())
+        other.params = A.Params.from_buffer_copy(self.params)
+        other._desc = None
+        if self.eam is not None:
+            other.eam = dict(self.eam)
+        return other
+
+    def desc(self):
+        def dp(a):
+            return None if a is None else a.ctypes.data_as(A.dptr)
+
+        def ip(a):
+            return None if a is None else a.ctypes.data_as(A.iptr)
+
+        d = A.SystemDesc()
+        d.n_atoms = self.n
+        d.n_types = len(self.eps)
+        d.box_lo[:] = list(self.box_lo)
+        d.box_hi[:] = list(self.box_hi)
+        d.position = dp(self.pos)
+        d.velocity = dp(self.vel)
+        d.charge = dp(self.charge)
+        d.mass = dp(self.mass)
+        d.type = ip(self.types)
+        d.molecule = ip(self.molecule)
+        d.image = ip(self.image)
+        d.epsilon = dp(self.eps)
+        d.sigma = dp(self.sig)
+        if self.bond_atoms is not None:
+            d.n_bonds = len(self.bond_type)
+            d.n_bond_types = len(self.bond_k)
+            d.bond_atoms = ip(self.bond_atoms)
+            d.bond_type = ip(self.bond_type)
+            d.bond_k = dp(self.bond_k)
+            d.bond_r0 = dp(self.bond_r0)
+        if self.angle_atoms is not None:
+            d.n_angles = len(self.angle_atoms) // 3
+            d.angle_atoms = ip(self.angle_atoms)
+            if self.angle_type is not None:
+                d.n_angle_types = len(self.angle_k)
+                d.angle_type = ip(self.angle_type)
+                d.angle_k = dp(self.angle_k)
+                d.angle_theta0 = dp(self.angle_theta0)
+        if self.special_offsets is not None:
+            d.special_offsets = ip(self.special_offsets)
+            d.special_ids = ip(self.special_ids)
+            d.special_weights = dp(self.special_weights)
+        if self.eam is not None:
+            e = self.eam
+            d.eam_nrho, d.eam_nr = e["nrho"], e["nr"]
+            d.eam_drho, d.eam_dr = e["drho"], e["dr"]
+            d.eam_rhomax, d.eam_cut = e["rhomax"], e["cut"]
+            d.eam_frho_spline = dp(e["frho_spline"])
+            d.eam_rhor_spline = dp(e["rhor_spline"])
+            d.eam_z2r_spline = dp(e["z2r_spline"])
+        self._desc = d
+        return d
+
+
+def maxwell(mass, T, kB, mvv2e, rng):
+    """Maxwell-Boltzmann velocities at T with zero centre-of-mass momentum."""
+    n = len(mass)
+    sd = np.sqrt(kB * T / (mass * mvv2e))
+    v = rng.standard_normal((n, 3)) * sd[:, None]
+    p = (v * mass[:, None]).sum(0) / mass.sum()
+    return v - p[None, :]
+
+
+def special_lists(n, bonds, weights):
+    """special_ids/weights/offsets as ModelFileInitCondition::SetSpecialBonds builds them
+    (framework/InitCondition/ModelFileInitCondition.cpp:848-923): 1-2, 1-3 and 1-4 partners
+    through a symmetric multimap of the bond list, in insertion order; atoms without bonds carry
+    their own id with weight 1."""
+    links = [[] for _ in range(n)]
+    for a, b in bonds:
+        links[a].append(b)
+        links[b].append(a)
+    ids, ws, counts = [], [], []
+    for i in range(n):
+        if not links[i]:
+            ids.append(i)
+            ws.append(1.0)
+            counts.append(1)
+            continue
+        c = 0
+        for k1 in links[i]:
+            ids.append(k1)
+            ws.append(weights[0])
+            c += 1
+            for k2 in links[k1]:
+                if k2 == i:
+                    continue
+                ids.append(k2)
+                ws.append(weights[1])
+                c += 1
+                for k3 in links[k2]:
+                    if k3 == k1:
+                        continue
+                    ids.append(k3)
+                    ws.append(weights[2])
+                    c += 1
+        counts.append(c)
+    off = np.zeros(n + 1, dtype=np.int32)
+    off[1:] = np.cumsum(counts)
+    return off, np.asarray(ids, dtype=np.int32), np.asarray(ws, dtype=np.float64)
+
+
+# ---------------------------------------------------------------------------------- configs 1-4
+def lj_fcc(cells=10, rho=0.8442, T=1.44, seed=1, **kw):
+    """LJ fluid start: fcc cells^3 x 4 atoms, reduced density rho, Maxwell velocities at T."""
+    a = (4.0 / rho) ** (1.0 / 3.0)
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    g = np.arange(cells)
+    cell = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 1, 3)
+    pos = ((cell + base[None]) * a).reshape(-1, 3) + 0.25 * a
+    L = cells * a
+    rng = np.random.default_rng(seed)
+    n = pos.shape[0]
+    mass = np.ones(n)
+    vel = maxwell(mass, T, 1.0, 1.0, rng)
+    params = A.default_params(force_field=A.FF_LJ_CUT, neighbor=A.NEIGH_RBL, cut_off=2.5, r_core=1.2,
+                              neighbor_sample_num=100, units=A.UNITS_LJ, timestep=0.005,
+                              temp_ctrl=A.TC_NONE, ensemble=A.ENS_NVE, temperature=(T, T, 1.0),
+                              num_steps=1000, seed=seed)
+    for k, v in kw.items():
+        _set(params, k, v)
+    return SystemData(pos, mass, np.zeros(n), [1.0], [1.0], [0, 0, 0], [L, L, L], vel=vel,
+                      params=params, name=f"lj_fcc_{n}")
+
+
+def nacl_melt(n_side=20, rho=0.6, T=2.0, seed=1, P=200, alpha=0.6, **kw):
+    """Molten rock salt: n_side^3 simple cubic with alternating +1/-1 charges at reduced density."""
+    n = n_side ** 3
+    L = (n / rho) ** (1.0 / 3.0)
+    sp = L / n_side
+    g = np.arange(n_side)
+    ijk = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pos = (ijk + 0.5) * sp
+    charge = np.where(ijk.sum(1) % 2 == 0, 1.0, -1.0)
+    types = (charge < 0).astype(np.int32)
+    rng = np.random.default_rng(seed)
+    mass = np.ones(n)
+    vel = maxwell(mass, T, 1.0, 1.0, rng)
+    params = A.default_params(force_field=A.FF_LJ_CUT_COUL_LONG, neighbor=A.NEIGH_RBL, cut_off=3.0,
+                              r_core=1.5, neighbor_sample_num=100, coulomb=A.COUL_RBE,
+                              coulomb_sample_num=P, alpha=alpha, kmax=(6, 6, 6), units=A.UNITS_LJ,
+                              timestep=0.002, temp_ctrl=A.TC_NOSE_HOOVER, temperature=(T, T, 0.2),
+                              num_steps=500, seed=seed)
+    for k, v in kw.items():
+        _set(params, k, v)
+    return SystemData(pos, mass, types, [1.0, 1.0], [1.0, 1.0], [0, 0, 0], [L, L, L], vel=vel,
+                      charge=charge, params=params, name=f"nacl_{n}")
+
+
+def _rotations(rng, m):
+    q = rng.standard_normal((m, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    R = np.empty((m, 3, 3))
+    R[:, 0, 0] = 1 - 2 * (y * y + z * z)
+    R[:, 0, 1] = 2 * (x * y - z * w)
+    R[:, 0, 2] = 2 * (x * z + y * w)
+    R[:, 1, 0] = 2 * (x * y + z * w)
+    R[:, 1, 1] = 1 - 2 * (x * x + z * z)
+    R[:, 1, 2] = 2 * (y * z - x * w)
+    R[:, 2, 0] = 2 * (x * z - y * w)
+    R[:, 2, 1] = 2 * (y * z + x * w)
+    R[:, 2, 2] = 1 - 2 * (x * x + y * y)
+    return R
+
+
+def _water_block(n_sites, L, rng, water_sites, ion_sites=(), ions=()):
+    """Water molecules (H, O, H order per molecule) on the cubic-lattice sites `water_sites`, ions
+    on `ion_sites`.  Returns arrays in atom order: all waters first, then ions."""
+    side = int(round(n_sites ** (1.0 / 3.0)))
+    sp = L / side
+    def site_xyz(s):
+        i, r = divmod(s, side * side)
+        j, k = divmod(r, side)
+        return (np.array([i, j, k]) + 0.5) * sp
+    th = math.radians(SPCE["theta"])
+    r = SPCE["r_oh"]
+    h1 = np.array([r * math.sin(th / 2), 0.0, r * math.cos(th / 2)])
+    h2 = np.array([-r * math.sin(th / 2), 0.0, r * math.cos(th / 2)])
+    com = (M_H * h1 + M_H * h2) / (M_O + 2 * M_H)
+    R = _rotations(rng, len(water_sites))
+    pos, mass, types, charge, mol = [], [], [], [], []
+    for m, s in enumerate(water_sites):
+        c = site_xyz(s)
+        for vec, tp, ms, q in ((h1, 1, M_H, SPCE["q_h"]), (np.zeros(3), 0, M_O, SPCE["q_o"]),
+                               (h2, 1, M_H, SPCE["q_h"])):
+            pos.append(c + R[m] @ (vec - com))
+            types.append(tp)
+            mass.append(ms)
+            charge.append(q)
+            mol.append(m)
+    nw = len(water_sites)
+    for k, (s, ion) in enumerate(zip(ion_sites, ions)):
+        pos.append(site_xyz(s))
+        types.append(ion["type"])
+        mass.append(ion["mass"])
+        charge.append(ion["q"])
+        mol.append(nw + k)
+    pos = np.mod(np.asarray(pos), L)
+    return pos, np.asarray(mass), np.asarray(types, np.int32), np.asarray(charge), np.asarray(mol, np.int32)
+
+
+def _water_topology(sd, n_water, special=(0.0, 0.0, 0.0)):
+    """Harmonic O-H bonds and H-O-H angles (SPC/E geometry) and the SHAKE triples."""
+    bonds = []
+    angles = []
+    for m in range(n_water):
+        h1, o, h2 = 3 * m, 3 * m + 1, 3 * m + 2
+        bonds += [(o, h1), (o, h2)]
+        angles += [h1, o, h2]
+    sd.bond_atoms = np.asarray(bonds, np.int32).reshape(-1)
+    sd.bond_type = np.zeros(len(bonds), np.int32)
+    sd.bond_k = np.array([554.1349])
+    sd.bond_r0 = np.array([SPCE["r_oh"]])
+    sd.angle_atoms = np.asarray(angles, np.int32)
+    sd.angle_type = np.zeros(n_water, np.int32)
+    sd.angle_k = np.array([45.7696])
+    sd.angle_theta0 = np.array([SPCE["theta"]])
+    off, ids, ws = special_lists(sd.n, bonds, special)
+    sd.special_offsets, sd.special_ids, sd.special_weights = off, ids, ws
+
+
+def spce_water(n_mol=3000, density=1.0, T=300.0, seed=1, P=100, beta=0.3, **kw):
+    """SPC/E water: n_mol molecules at randomly rotated simple-cubic sites, density in g/cm^3."""
+    mass_tot = n_mol * (M_O + 2 * M_H) / AVOGADRO  # g
+    L = (mass_tot / density) ** (1.0 / 3.0) * 1e8  # A
+    side = int(math.ceil(n_mol ** (1.0 / 3.0) - 1e-9))
+    n_sites = side ** 3
+    rng = np.random.default_rng(seed)
+    sites = np.sort(rng.choice(n_sites, size=n_mol, replace=False))
+    pos, mass, types, charge, mol = _water_block(n_sites, L, rng, sites)
+    vel = maxwell(mass, T, KB_REAL, MVV2E_REAL, rng)
+    params = A.default_params(force_field=A.FF_CVFF, neighbor=A.NEIGH_RBL, cut_off=10.0, r_core=5.0,
+                              neighbor_sample_num=100, coulomb=A.COUL_RBE, coulomb_sample_num=P,
+                              alpha=beta * beta, kmax=(3, 3, 3), units=A.UNITS_REAL, timestep=1.0,
+                              temp_ctrl=A.TC_NOSE_HOOVER, temperature=(T, T, 100.0),
+                              fix_shake=A.SHAKE_TRUE, num_steps=1000, seed=seed,
+                              special_bonds=(0.0, 0.0, 0.0))
+    for k, v in kw.items():
+        _set(params, k, v)
+    sd = SystemData(pos, mass, types, [SPCE["eps_o"], 0.0], [SPCE["sigma_o"], 0.0], [0, 0, 0],
+                    [L, L, L], vel=vel, charge=charge, molecule=mol, params=params,
+                    name=f"spce_{3 * n_mol}")
+    _water_topology(sd, n_mol, tuple(params.special_bonds))
+    return sd
+
+
+def saline(n_atoms_target, T=300.0, seed=1, P=100, beta=0.3, molar=0.15, precision=A.PREC_MIXED, **kw):
+    """SPC/E water with `molar` NaCl at random lattice sites, close to n_atoms_target atoms."""
+    waters_per_pair = 55.5 / molar
+    n_pairs = max(1, int(round(n_atoms_target / (3 * waters_per_pair + 2))))
+    n_water = max(8, (n_atoms_target - 2 * n_pairs) // 3)
+    n_mol = n_water + 2 * n_pairs
+    mass_tot = (n_water * (M_O + 2 * M_H) + n_pairs * (M_NA + M_CL)) / AVOGADRO
+    L = (mass_tot / 1.0) ** (1.0 / 3.0) * 1e8
+    side = int(math.ceil(n_mol ** (1.0 / 3.0) - 1e-9))
+    n_sites = side ** 3
+    rng = np.random.default_rng(seed)
+    sites = rng.choice(n_sites, size=n_mol, replace=False)
+    water_sites = np.sort(sites[:n_water])
+    ion_sites = sites[n_water:]
+    ions = [dict(type=2, **ION_NA)] * n_pairs + [dict(type=3, **ION_CL)] * n_pairs
+    pos, mass, types, charge, mol = _water_block(n_sites, L, rng, water_sites, ion_sites, ions)
+    vel = maxwell(mass, T, KB_REAL, MVV2E_REAL, rng)
+    params = A.default_params(force_field=A.FF_CVFF, neighbor=A.NEIGH_RBL, cut_off=10.0, r_core=5.0,
+                              neighbor_sample_num=100, coulomb=A.COUL_RBE, coulomb_sample_num=P,
+                              alpha=beta * beta, kmax=(3, 3, 3), units=A.UNITS_REAL, timestep=1.0,
+                              temp_ctrl=A.TC_NOSE_HOOVER, temperature=(T, T, 100.0),
+                              fix_shake=A.SHAKE_TRUE, num_steps=1000, seed=seed,
+                              special_bonds=(0.0, 0.0, 0.0), precision=precision)
+    for k, v in kw.items():
+        _set(params, k, v)
+    eps = [SPCE["eps_o"], 0.0, ION_NA["eps"], ION_CL["eps"]]
+    sig = [SPCE["sigma_o"], 0.0, ION_NA["sigma"], ION_CL["sigma"]]
+    sd = SystemData(pos, mass, types, eps, sig, [0, 0, 0], [L, L, L], vel=vel, charge=charge,
+                    molecule=mol, params=params, name=f"saline_{len(mass)}")
+    _water_topology(sd, n_water, tuple(params.special_bonds))
+    return sd
+
+
+# Johnson-form analytic EAM for Cu (parameters as named by the benchmark configuration)
+JOHNSON_CU = dict(re=2.556, fe=1.0, beta=5.85, gamma=8.0, phi_e=0.59, E_c=3.54, rho_e=12.0)
+
+
+def johnson_functions(par=JOHNSON_CU):
+    re, fe, be, ga, phe, Ec, rhe = (par[k] for k in ("re", "fe", "beta", "gamma", "phi_e", "E_c", "rho_e"))
+    f = lambda r: fe * np.exp(-be * (r / re - 1.0))
+    phi = lambda r: phe * np.exp(-ga * (r / re - 1.0))
+    F = lambda rho: -Ec * np.sqrt(np.maximum(rho, 0.0) / rhe)
+    df = lambda r: -be / re * f(r)
+    dphi = lambda r: -ga / re * phi(r)
+    dF = lambda rho: -Ec * 0.5 / np.sqrt(np.maximum(rho, 1e-300) * rhe)
+    return f, phi, F, df, dphi, dF
+
+
+def johnson_funcfl(n=10000, cut=5.0, rho_max=None, par=JOHNSON_CU):
+    """Tabulate the Johnson functions as a funcfl file body: F on an nrho grid, Z(r) with
+    27.2*0.529*Z^2 = r*phi(r) (so the funcfl z2r conversion of the reader gives r*phi), rho(r)."""
+    f, phi, F, *_ = johnson_functions(par)
+    if rho_max is None:
+        rho_max = 3.0 * par["rho_e"]
+    dr = cut / (n - 1)
+    drho = rho_max / (n - 1)
+    r = np.arange(n) * dr
+    rr = np.where(r > 0, r, dr * 1e-3)
+    rhor = f(rr)
+    z = np.sqrt(rr * phi(rr) / (27.2 * 0.529))
+    frho = F(np.arange(n) * drho)
+    return dict(nrho=n, drho=drho, nr=n, dr=dr, cut=cut, frho=frho, zr=z, rhor=rhor)
+
+
+def eam_cu(cells=20, a=3.615, T=600.0, seed=1, build_splines=None, **kw):
+    """fcc Cu, cells^3 x 4 atoms, Johnson EAM; `build_splines(file_dict) -> eam dict` turns the
+    tabulated functions into the reference's Vec7 spline rows (rbmd_eam_build_splines)."""
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    g = np.arange(cells)
+    cell = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 1, 3)
+    pos = ((cell + base[None]) * a).reshape(-1, 3) + 0.25 * a
+    L = cells * a
+    n = pos.shape[0]
+    rng = np.random.default_rng(seed)
+    mass = np.full(n, M_CU)
+    kB, mvv2e = 8.617343e-5, 1.0364269e-4
+    vel = maxwell(mass, T, kB, mvv2e, rng)
+    params = A.default_params(force_field=A.FF_EAM, neighbor=A.NEIGH_RBL, cut_off=5.0, r_core=2.5,
+                              neighbor_sample_num=100, units=A.UNITS_METAL, timestep=0.002,
+                              temp_ctrl=A.TC_NOSE_HOOVER, temperature=(T, T, 0.1), num_steps=1000,
+                              seed=seed, precision=A.PREC_MIXED)
+    for k, v in kw.items():
+        _set(params, k, v)
+    sd = SystemData(pos, mass, np.zeros(n), [0.0], [0.0], [0, 0, 0], [L, L, L], vel=vel,
+                    params=params, name=f"eam_cu_{n}")
+    if build_splines is not None:
+        sd.eam = build_splines(johnson_funcfl())
+    return sd
+
+
+def _set(params, k, v):
+    cur = getattr(params, k)
+    if hasattr(cur, "__len__"):
+        cur[:] = v
+    else:
+        setattr(params, k, v)
+
+
+def serving_stream(n_requests=512, n_min=1000, n_max=64000, rate=50.0, seed=7):
+    """Request sizes log-uniform in [n_min, n_max] and Poisson arrival times at `rate` per s."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(math.log(n_min), math.log(n_max), n_requests)).astype(int)
+    gaps = rng.exponential(1.0 / rate, n_requests)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    return sizes, arrivals
