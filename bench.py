@@ -1,0 +1,423 @@
+#!/usr/bin/env python
+"""bench.py -- atom-steps/s of batched mixed-precision RBMD serving on B200, against the plain FP64
+one-system-per-launch path, with force error, p50/p99 latency, roofline and a CPU baseline.
+
+Workload (synthetic, seeded): the batched serving stream -- 512 independent SPC/E water systems
+with 0.15 M NaCl, atom counts log-uniform in [1k, 64k], Poisson arrivals at 50 req/s, each asking
+for 1000 RBE + RBL NVT steps at 300 K (RBE alpha 0.09 A^-2 [beta 0.3/A], P = 100; RBL rc 10 A, r_core
+5 A, 100 shell samples; SHAKE water; FP32 pair/RBE arithmetic with FP64 integration, rho(k) and
+reductions).
+
+Lines printed by rank 0 (one JSON line):
+  value  -- device-resident throughput: all 512 systems resident in HBM, K batched steps timed with
+            CUDA events on the library stream (max over ranks), atom-steps/s summed over ranks.
+  e2e    -- the same stream through the public serving API (rbmd_serve_submit with host arrays at
+            the Poisson arrival times; results read back to host), wall clock, with p50/p99
+            request latency.
+  plain_fp64 -- the same size distribution (every 32nd request) run FP64, one system per launch.
+  --impl reference -- the CPU restatement of the reference's algorithm (the reference itself needs
+            VTK-m, which this environment lacks) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s batched vs plain on 1 B200 at <=1e-3 force err; p50/p99 latency"
+UNIT = "atom-steps/s"
+WORKLOAD = ("saline serving stream: 512 SPC/E + 0.15 M NaCl systems, N log-uniform 1k-64k, Poisson 50 req/s, "
+            "1000 RBE(P=100)+RBL NVT steps each, mixed FP32/FP64")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20, help="timed batched steps of the resident batch")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--requests", type=int, default=512)
+    ap.add_argument("--request-steps", type=int, default=1000)
+    ap.add_argument("--rate", type=float, default=50.0)
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--out", default=None, help="also write the JSON line here")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------ utils
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.torch = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as td
+            torch.cuda.set_device(self.local)
+            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.torch = torch
+            self.td = td
+
+    def barrier(self):
+        if self.world > 1:
+            self.td.barrier()
+
+    def reduce(self, x, op="max"):
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([float(x)], device=f"cuda:{self.local}", dtype=self.torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX if op == "max" else self.td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.td.destroy_process_group()
+
+
+def build_stream(args, rank):
+    from rbmd_b200 import synth
+    sizes, arrivals = synth.serving_stream(n_requests=args.requests, rate=args.rate, seed=7 + 1000 * rank)
+    systems = [synth.saline(int(n), seed=100000 * rank + k) for k, n in enumerate(sizes)]
+    for k, sd in enumerate(systems):
+        sd.params.num_steps = args.request_steps
+        sd.params.seed = 1 + k + 100000 * rank
+    return systems, arrivals
+
+
+def desc_bytes(sd):
+    b = 0
+    for name in ("pos", "vel", "charge", "mass", "types", "molecule", "bond_atoms", "bond_type", "angle_atoms",
+                 "angle_type", "special_offsets", "special_ids", "special_weights", "eps", "sig"):
+        a = getattr(sd, name, None)
+        if a is not None:
+            b += a.nbytes
+    return b
+
+
+# ------------------------------------------------------------------------------------------ parts
+def measure_resident(ctx, systems, args, dist, clocks):
+    ids = [ctx.add_system(sd) for sd in systems]
+    ctx.init(ids)
+    ctx.step(ids, args.warmup)  # captures the batched step graph
+    ctx.sync()
+    launches0 = ctx.launch_count()
+    dist.barrier()
+    clocks.start()
+    ms = ctx.step_timed(ids, args.steps)
+    clk = clocks.stop()
+    launches = ctx.launch_count() - launches0
+    dist.barrier()
+    atoms = sum(sd.n for sd in systems)
+    ms_max = dist.reduce(ms, "max")
+    atoms_all = dist.reduce(atoms, "sum")
+    status = [ctx.thermo(i)["status"] for i in ids[:4]]
+    return ids, dict(ms=ms_max, atoms_rank=atoms, atoms_all=atoms_all, launches=launches, clocks=clk,
+                     value=atoms_all * args.steps / (ms_max * 1e-3), status=status)
+
+
+def kernel_profile(ctx, ids, systems):
+    """Per-kernel device time (CUDA events on the library stream) of two eager batched steps."""
+    ctx.profile(True)
+    ctx.step(ids, 2)
+    ctx.sync()
+    out = {}
+    for name in ("nhc", "kick_drift", "cells", "shake", "rbe_sample", "rho", "bonded", "pair", "final", "rattle"):
+        ms, n, units = ctx.profile_get(name)
+        if n:
+            out[name] = dict(avg_ms=ms, launches=n, units_per_launch=units)
+    ctx.profile(False)
+    return out
+
+
+def pair_stats(ctx, sid, n):
+    """Selected pairs per atom (core + sampled shell) of one representative system."""
+    nc, ns, _ = ctx.rbl_lists(sid, cap=1024)
+    return float((nc + ns).mean()), float(nc.mean()), float(ns.mean())
+
+
+def measure_plain(systems, args, device):
+    """FP64, one system per launch, eager: the plain path the batched mixed path is compared to."""
+    import rbmd_b200
+    from rbmd_b200 import _abi as A
+    sample = systems[::32]
+    ctx = rbmd_b200.Context(device=device, batched=False, graphs=False)
+    tot_ms, tot_as = 0.0, 0
+    steps = 5
+    for sd in sample:
+        s2 = sd.copy()
+        s2.params.precision = A.PREC_FP64
+        sid = ctx.add_system(s2)
+        ctx.init(sid)
+        ctx.step(sid, 1)
+        ms = ctx.step_timed(sid, steps)
+        tot_ms += ms
+        tot_as += s2.n * steps
+        ctx.remove_system(sid)
+    ctx.close()
+    return dict(value=tot_as / (tot_ms * 1e-3), systems=len(sample), steps_each=steps,
+                atoms=sum(sd.n for sd in sample))
+
+
+def measure_accuracy(device):
+    """(i) mixed vs FP64 on the same Philox stream; (ii) RBE vs full Ewald (FP64, converged kmax)."""
+    import rbmd_b200
+    from rbmd_b200 import _abi as A, synth
+    sd = synth.saline(4000, seed=11)
+    ctx = rbmd_b200.Context(device=device)
+    f = {}
+    for tag, prec, coul, km in (("mixed", A.PREC_MIXED, A.COUL_RBE, 3), ("fp64", A.PREC_FP64, A.COUL_RBE, 3),
+                                ("ewald", A.PREC_FP64, A.COUL_EWALD, 17)):
+        s2 = sd.copy()
+        s2.params.precision = prec
+        s2.params.coulomb = coul
+        s2.params.kmax[:] = (km, km, km)
+        sid = ctx.add_system(s2)
+        ctx.compute_forces(sid)
+        f[tag] = ctx.forces(sid)
+        ctx.remove_system(sid)
+    ctx.close()
+
+    def rr(a, b):
+        return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+    return dict(mixed_vs_fp64=rr(f["mixed"], f["fp64"]), rbe_vs_ewald_fp64=rr(f["fp64"], f["ewald"]),
+                mixed_vs_ewald=rr(f["mixed"], f["ewald"]), atoms=sd.n)
+
+
+def measure_e2e(systems, arrivals, args, device):
+    """The stream through rbmd_serve_*: submissions at the Poisson times, results back to host."""
+    import rbmd_b200
+    ctx = rbmd_b200.Context(device=device)
+    ctx.serve_start(steps_per_round=50)
+    rids = []
+    h2d = 0
+    t0 = time.monotonic()
+    for sd, ta in zip(systems, arrivals):
+        now = time.monotonic() - t0
+        if ta > now:
+            time.sleep(ta - now)
+        rids.append(ctx.serve_submit(sd, args.request_steps))
+        h2d += desc_bytes(sd)
+    lat, d2h, atom_steps = [], 0, 0
+    for rid, sd in zip(rids, systems):
+        rc = ctx.serve_wait(rid, 3600.0)
+        x, v, th, st = ctx.serve_result(rid)
+        if rc or st["status"]:
+            raise RuntimeError(f"request {rid} failed with {rc}/{st['status']}")
+        lat.append(st["t_done"] - st["t_submit"])
+        d2h += x.nbytes + v.nbytes
+        atom_steps += st["atom_steps"]
+    wall = time.monotonic() - t0
+    ctx.serve_stop()
+    ctx.close()
+    total_steps = len(systems) * args.request_steps
+    return dict(value=atom_steps / wall, wall_s=wall, p50_s=float(np.percentile(lat, 50)),
+                p99_s=float(np.percentile(lat, 99)), h2d=h2d / total_steps, d2h=d2h / total_steps,
+                atom_steps=atom_steps)
+
+
+def cpu_port_rate(seconds, threads=None):
+    """The FP64 CPU restatement of the reference algorithm on a sample of the workload: one 1000-atom
+    saline system stepped until `seconds` of CPU time."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_ffi
+    from rbmd_b200 import _abi as A, synth
+    if threads:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    sd = synth.saline(1000, seed=3)
+    sd.params.precision = A.PREC_FP64
+    o = oracle_ffi.Oracle(sd)
+    o.init()
+    o.step(1)
+    t0 = time.perf_counter()
+    steps = 0
+    while time.perf_counter() - t0 < seconds:
+        o.step(1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return dict(value=sd.n * steps / dt, unit=UNIT, cores=cores, kind="port",
+                sample=f"one {sd.n}-atom saline system of the stream's parameters, {steps} NVT steps in {dt:.1f} s")
+
+
+def roofline(prof, pairs_per_atom, peaks, fp32_peak):
+    p = prof.get("pair")
+    if not p:
+        return None, None
+    atoms = p["units_per_launch"]
+    secs = p["avg_ms"] * 1e-3
+    # algorithmic HBM bytes per atom of the pair kernel: its own position+charge (16 B FP32 copy),
+    # metadata (16 B), the force written (32 B); neighbour reuse is cache traffic, not counted
+    bytes_alg = 64.0 * atoms
+    flops = (26 + 14) * pairs_per_atom * atoms  # LJ + Coulomb pair convention (flops per pair)
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    achieved_gbs = bytes_alg / secs / 1e9
+    r_hbm = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s", "frac": achieved_gbs / hbm,
+             "traffic": None, "kernel": "k_pair (fused RBL traversal + LJ/erfc pair forces)",
+             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+    tf = flops / secs / 1e12
+    r_fp32 = {"bound": "fp32", "achieved": tf, "peak": fp32_peak, "unit": "TFLOP/s",
+              "frac": tf / fp32_peak if fp32_peak else None,
+              "peak_source": "FFMA-chain microbenchmark in this run (rbmd_fma_peak)",
+              "flops_per_pair": 40, "pairs_per_atom": pairs_per_atom}
+    return r_hbm, r_fp32
+
+
+def run_reference(args, dist):
+    """--impl reference: the CPU restatement of the reference algorithm on all host cores."""
+    if dist.rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    r = cpu_port_rate(max(5.0, args.cpu_seconds), threads=cores)
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "impl": "reference", "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": "cpu"},
+            "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference binary needs VTK-m 1.9 (absent); this is the FP64 C++ restatement of its algorithm"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    if args.impl == "reference":
+        run_reference(args, dist)
+        dist.close()
+        return
+    import rbmd_b200
+    device = dist.local
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    systems, arrivals = build_stream(args, dist.rank)
+    ctx = rbmd_b200.Context(device=device)
+    fp32_peak = ctx.fma_peak(False)
+    fp64_peak = ctx.fma_peak(True)
+    clocks = Clocks(device)
+    ids, res = measure_resident(ctx, systems, args, dist, clocks)
+    prof = kernel_profile(ctx, ids, systems)
+    rep = int(np.argsort([sd.n for sd in systems])[len(systems) // 2])
+    ppa, pcore, pshell = pair_stats(ctx, ids[rep], systems[rep].n)
+    for sid in ids:
+        ctx.remove_system(sid)
+    ctx.close()
+    r_hbm, r_fp32 = roofline(prof, ppa, peaks, fp32_peak)
+    extra = {}
+    if dist.rank == 0:
+        extra["accuracy"] = measure_accuracy(device)
+        if not args.skip_plain:
+            extra["plain_fp64"] = measure_plain(systems, args, device)
+    e2e = None
+    if not args.skip_e2e:
+        e2e = measure_e2e(systems, arrivals, args, device)
+        e2e_val = dist.reduce(e2e["value"], "sum")
+    dist.barrier()
+    if dist.rank == 0:
+        cpu = None if args.skip_cpu else cpu_port_rate(args.cpu_seconds, threads=1)
+        plain = extra.get("plain_fp64")
+        line = {
+            "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair/RBE + f64 integration/reductions",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_systems_per_gpu": len(systems), "atoms_per_gpu": res["atoms_rank"],
+                       "atoms_total": res["atoms_all"], "batched_step_per_launch": True, "parallelism": f"dp{dist.world} (independent systems)",
+                       "l2": "inputs larger than L2 (all systems resident, >1 GB)"},
+            "roofline": r_hbm, "roofline_fp32": r_fp32,
+            "pipe_peaks_tflops": {"fp32": fp32_peak, "fp64": fp64_peak},
+            "cpu_baseline": cpu,
+            "clocks": res["clocks"],
+            "gpu_launches": res["launches"],
+            "kernel_ms": prof,
+            "pairs_per_atom": {"total": ppa, "core": pcore, "shell_sampled": pshell},
+            "device_status": res["status"],
+        }
+        if plain:
+            line["plain_fp64"] = plain
+            line["speedup_vs_plain_fp64"] = res["value"] / dist.world / plain["value"]
+        if "accuracy" in extra:
+            line["force_rel_rms"] = extra["accuracy"]
+        if e2e is not None:
+            line["e2e"] = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"],
+                           "d2h_bytes_per_step": e2e["d2h"], "wall_s": e2e["wall_s"], "p50_latency_s": e2e["p50_s"],
+                           "p99_latency_s": e2e["p99_s"], "request_steps": args.request_steps,
+                           "step": "one MD step of one request; bytes averaged over all request-steps"}
+        s = json.dumps(line)
+        print(s, flush=True)
+        if args.out:
+            with open(args.out, "w") as fh:
+                fh.write(s + "\n")
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -343,6 +343,12 @@ int rbmd_launch_count(rbmd_ctx* ctx, int64_t* launches);
 int rbmd_profile_enable(rbmd_ctx* ctx, int32_t on);
 int rbmd_profile_get(rbmd_ctx* ctx, const char* kernel, double* avg_ms, int64_t* launches,
                      double* units_per_launch);
+/* rbmd_step bracketed by CUDA events recorded on the context stream; *ms is the device time of
+ * the nsteps steps (the call synchronises). */
+int rbmd_step_timed(rbmd_ctx* ctx, const int32_t* sys_ids, int32_t n, int32_t nsteps, double* ms);
+/* Non-tensor pipe peak of the device from a dependent FMA chain microbenchmark (fp64 = 0: FFMA,
+ * 1: DFMA); *tflops counts an FMA as 2 flops. */
+int rbmd_fma_peak(rbmd_ctx* ctx, int32_t fp64, double* tflops);
 
 #ifdef __cplusplus
 }

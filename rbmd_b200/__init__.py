@@ -173,6 +173,18 @@ class Context:
         self._check(lib().rbmd_launch_count(self.h, C.byref(v)))
         return v.value
 
+    def step_timed(self, ids, nsteps):
+        """Run nsteps and return their device time in ms (CUDA events on the library stream)."""
+        a, n = self._ids(ids)
+        ms = C.c_double()
+        self._check(lib().rbmd_step_timed(self.h, _ip(a), n, nsteps, C.byref(ms)))
+        return ms.value
+
+    def fma_peak(self, fp64=False):
+        v = C.c_double()
+        self._check(lib().rbmd_fma_peak(self.h, int(fp64), C.byref(v)))
+        return v.value
+
     def profile(self, on=True):
         self._check(lib().rbmd_profile_enable(self.h, int(on)))
 

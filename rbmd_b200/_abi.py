@@ -192,6 +192,8 @@ def declare(lib, prefix="rbmd"):
         "launch_count": ([ctx, P(C.c_int64)], C.c_int),
         "profile_enable": ([ctx, C.c_int32], C.c_int),
         "profile_get": ([ctx, C.c_char_p, dptr, P(C.c_int64), dptr], C.c_int),
+        "step_timed": ([ctx, iptr, C.c_int32, C.c_int32, dptr], C.c_int),
+        "fma_peak": ([ctx, C.c_int32, dptr], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, f"{prefix}_{name}")
@@ -208,5 +210,5 @@ HEADER_FUNCTIONS = [
     "rbmd_get_derived", "rbmd_eam_spline_sizes", "rbmd_eam_build_splines", "rbmd_eam_read_funcfl",
     "rbmd_serve_start", "rbmd_serve_submit", "rbmd_serve_poll", "rbmd_serve_wait",
     "rbmd_serve_result", "rbmd_serve_stop", "rbmd_launch_count", "rbmd_profile_enable",
-    "rbmd_profile_get",
+    "rbmd_profile_get", "rbmd_step_timed", "rbmd_fma_peak",
 ]

@@ -379,4 +379,29 @@ int rbmd_profile_get(rbmd_ctx* ctx, const char* kernel, double* avg_ms, int64_t*
   return RBMD_OK;
 }
 
+int rbmd_step_timed(rbmd_ctx* ctx, const int32_t* ids, int32_t n, int32_t nsteps, double* ms) {
+  CTX_CHECK(ctx);
+  if (!ids || n <= 0 || nsteps < 0 || !ms) return ctx->c->fail(RBMD_ERR_ARG, "bad step arguments");
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, ctx->c->stream);
+  int rc = ctx->c->step(ids, n, nsteps);
+  cudaEventRecord(b, ctx->c->stream);
+  cudaEventSynchronize(b);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = t;
+  return rc;
+}
+
+int rbmd_fma_peak(rbmd_ctx* ctx, int32_t fp64, double* tflops) {
+  CTX_CHECK(ctx);
+  if (!tflops) return RBMD_ERR_ARG;
+  *tflops = rbmd::fma_peak_tflops(fp64, ctx->c->stream);
+  return RBMD_OK;
+}
+
 }  // extern "C"

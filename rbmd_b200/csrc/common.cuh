@@ -57,6 +57,8 @@ struct SysDev {
   int special, pice, nc, ncell, P, n_bonds, n_angles, nk_ewald;
   int dims[3];
   int eam_nrho, eam_nr;
+  int lean;   // segment-table traversal usable (every dimension holds >= 2 nc + 1 cells)
+  int dense;  // pair kernel layout: warp per home cell (dense systems) or warp per atom
   int blocks_pair, blocks_atom, blocks_rho, blocks_tri, rbe_mmax, rbe_slots, has_triples, n_triples;
   // geometry and physics
   double lo[3], hi[3], L[3], d[3];
@@ -82,6 +84,7 @@ struct SysDev {
   int* cell_start;     // [ncell + 1]
   int* cell_fill;      // [ncell] scatter cursors
   int* sorted;         // atom ids in cell order
+  int* rank;           // [n] position of each atom in cell order (inverse of sorted)
   double4* sx;         // sorted positions + charge (FP64)
   float4* sxf;         // sorted positions + charge (FP32)
   int4* smeta;         // sorted: atom id, type, molecule, unused

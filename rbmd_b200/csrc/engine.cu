@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "engine.h"
@@ -276,7 +277,14 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   const bool shake = (p.fix_shake == RBMD_SHAKE_TRUE) && d.n_angles > 0 && d.angle_atoms;
   D.has_triples = shake ? 1 : 0;
   D.n_triples = shake ? d.n_angles : 0;
-  D.blocks_pair = (n + kPairWarps - 1) / kPairWarps;
+  // dense systems (tens of atoms per cell: water, saline) use the warp-per-home-cell pair kernel
+  D.lean = (D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1) ? 1 : 0;
+  D.dense = 0;
+  if (const char* lay = std::getenv("RBMD_PAIR_LAYOUT")) {  // tuning override: "atom" or "cell"
+    if (std::strcmp(lay, "atom") == 0) D.lean = 0;
+    else if (std::strcmp(lay, "cell") == 0) D.dense = 1;
+  }
+  D.blocks_pair = D.dense ? (D.ncell + kCellWarpsHost - 1) / kCellWarpsHost : (n + kPairWarps - 1) / kPairWarps;
   D.blocks_atom = (n + kAtomBlock - 1) / kAtomBlock;
   D.blocks_rho = (n + kRhoChunk - 1) / kRhoChunk;
   D.blocks_tri = (D.n_triples + 127) / 128;
@@ -423,6 +431,7 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   D.cell_start = (int*)dal(sizeof(int) * (D.ncell + 1));
   D.cell_fill = (int*)dal(sizeof(int) * D.ncell);
   D.sorted = (int*)dal(sizeof(int) * n);
+  D.rank = (int*)dal(sizeof(int) * n);
   D.sx = (double4*)dal(sizeof(double4) * n);
   D.sxf = (float4*)dal(sizeof(float4) * n);
   D.smeta = (int4*)dal(sizeof(int4) * n);
@@ -581,7 +590,8 @@ static bool same_group(const System* a, const System* b) {
   const SysDev &x = a->dev, &y = b->dev;
   return x.ff == y.ff && x.neigh == y.neigh && x.coul == y.coul && x.prec == y.prec &&
          x.temp_ctrl == y.temp_ctrl && x.special == y.special && x.has_triples == y.has_triples &&
-         ((x.n_bonds + x.n_angles) > 0) == ((y.n_bonds + y.n_angles) > 0);
+         ((x.n_bonds + x.n_angles) > 0) == ((y.n_bonds + y.n_angles) > 0) && x.dense == y.dense &&
+         x.lean == y.lean;
 }
 
 Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& rc) {
@@ -598,6 +608,8 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
   b.special = g.special;
   b.has_shake = g.has_triples;
   b.has_bonded = (g.n_bonds + g.n_angles) > 0;
+  b.dense = g.dense;
+  b.lean = g.lean;
   std::vector<int> slots;
   std::vector<int2> wa, wp, wc, wr, wt, wm;
   for (System* s : group) {
@@ -606,7 +618,10 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
     br->ids.push_back(s->id);
     b.max_P = std::max(b.max_P, std::max(D.P, D.nk_ewald));
     for (int k = 0; k < D.n; k += kAtomBlock) wa.push_back(make_int2(s->slot, k));
-    for (int k = 0; k < D.n; k += kPairWarps) wp.push_back(make_int2(s->slot, k));
+    if (D.dense)
+      for (int k = 0; k < D.ncell; k += kCellWarpsHost) wp.push_back(make_int2(s->slot, k));
+    else
+      for (int k = 0; k < D.n; k += kPairWarps) wp.push_back(make_int2(s->slot, k));
     for (int k = 0; k < D.ncell; k += kCellBlock) wc.push_back(make_int2(s->slot, k));
     for (int k = 0; k < D.n; k += kRhoChunk) wr.push_back(make_int2(s->slot, k));
     for (int k = 0; k < D.n_triples; k += 128) wt.push_back(make_int2(s->slot, k));
@@ -990,16 +1005,32 @@ int Context::get_cells(int id, int32_t* dims, int32_t* coa, int32_t* sorted, int
   const SysDev& D = s->dev;
   if (dims)
     for (int k = 0; k < 3; ++k) dims[k] = D.dims[k];
-  std::vector<int> start(D.ncell + 1);
-  if (coa) cudaMemcpyAsync(coa, D.cell_of_atom, sizeof(int) * D.n, cudaMemcpyDeviceToHost, stream);
-  if (sorted) cudaMemcpyAsync(sorted, D.sorted, sizeof(int) * D.n, cudaMemcpyDeviceToHost, stream);
+  std::vector<int> start(D.ncell + 1), icell(D.n), isorted(D.n);
+  cudaMemcpyAsync(icell.data(), D.cell_of_atom, sizeof(int) * D.n, cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(isorted.data(), D.sorted, sizeof(int) * D.n, cudaMemcpyDeviceToHost, stream);
   cudaMemcpyAsync(start.data(), D.cell_start, sizeof(int) * (D.ncell + 1), cudaMemcpyDeviceToHost, stream);
   rc = sync();
   if (rc) return rc;
-  for (int c = 0; c < D.ncell; ++c) {
-    if (lo) lo[c] = start[c];
-    if (up) up[c] = start[c + 1];
-  }
+  // internal id = z + dz (y + dy x); reference id = x + dx (y + dy z)
+  const int dx = D.dims[0], dy = D.dims[1], dz = D.dims[2];
+  auto to_ref = [&](int ic) {
+    const int x = ic / (dz * dy), y = (ic / dz) % dy, z = ic % dz;
+    return x + dx * (y + dy * z);
+  };
+  if (coa)
+    for (int i = 0; i < D.n; ++i) coa[i] = to_ref(icell[i]);
+  int run = 0;
+  for (int z = 0; z < dz; ++z)
+    for (int y = 0; y < dy; ++y)
+      for (int x = 0; x < dx; ++x) {
+        const int c = x + dx * (y + dy * z), ic = z + dz * (y + dy * x);
+        if (lo) lo[c] = run;
+        for (int k = start[ic]; k < start[ic + 1]; ++k) {
+          if (sorted) sorted[run] = isorted[k];
+          ++run;
+        }
+        if (up) up[c] = run;
+      }
   return RBMD_OK;
 }
 
@@ -1025,7 +1056,7 @@ int Context::get_rbl_lists(int id, int cap, int32_t* nc, int32_t* ns, int32_t* i
     cudaFree(d_ns);
     return fail(RBMD_ERR_OOM, "list buffers");
   }
-  launch_rbl_lists(d_sys_, s->slot, n, cap, d_nc, d_ns, d_ids, stream);
+  launch_rbl_lists(d_sys_, s->slot, n, s->dev.ncell, s->dev.dense, cap, d_nc, d_ns, d_ids, stream);
   std::vector<int> core((size_t)n * cap), shell((size_t)n * cap);
   cudaMemcpyAsync(nc, d_nc, sizeof(int) * n, cudaMemcpyDeviceToHost, stream);
   cudaMemcpyAsync(ns, d_ns, sizeof(int) * n, cudaMemcpyDeviceToHost, stream);

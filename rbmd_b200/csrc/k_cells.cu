@@ -30,7 +30,9 @@ __global__ void k_cells_count(const SysDev* __restrict__ S, const int2* __restri
     c = c > s.dims[k] - 1 ? s.dims[k] - 1 : c;
     ijk[k] = (int)c;
   }
-  const int cell = ijk[0] + ijk[1] * s.dims[0] + ijk[2] * s.dims[0] * s.dims[1];
+  // internal numbering is z fastest so that the 2 nc + 1 cells of a traversal row (fixed x and y
+  // offsets) are contiguous in cell order; get_cells reports the reference's x-fastest ids
+  const int cell = ijk[2] + s.dims[2] * (ijk[1] + s.dims[1] * ijk[0]);
   s.cell_of_atom[i] = cell;
   atomicAdd(&s.cell_count[cell], 1);
 }
@@ -93,6 +95,7 @@ __global__ void k_cells_sort_gather(const SysDev* __restrict__ S, const int2* __
   }
   for (int k = b; k < e; ++k) {
     const int i = ids[k];
+    s.rank[i] = k;
     const double4 p = s.x[i];
     s.sx[k] = p;
     s.sxf[k] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);

@@ -600,7 +600,13 @@ __global__ void k_shake(const SysDev* __restrict__ S, const int2* __restrict__ w
         s.image[3 * ii + k] = img;
       }
       s.v[ii] = make_double4(nv[0], nv[1], nv[2], ms[t]);
-      s.x[ii] = make_double4(nx[0], nx[1], nx[2], s.x[ii].w);
+      const double q = s.x[ii].w;
+      s.x[ii] = make_double4(nx[0], nx[1], nx[2], q);
+      // the cell list was built before the constraint (as the reference's locator is); refresh
+      // the cell-ordered copies the pair kernel streams
+      const int k = s.rank[ii];
+      s.sx[k] = make_double4(nx[0], nx[1], nx[2], q);
+      s.sxf[k] = make_float4((float)nx[0], (float)nx[1], (float)nx[2], (float)q);
     }
     const double dtfsq = 0.5 * dt * dt * fm;
     l01 = l01 / dtfsq;

@@ -336,7 +336,7 @@ k_pair(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int
         ox = (R)(s.d[0] * (double)(w0 - n0));
         oy = (R)(s.d[1] * (double)(w1 - n1));
         oz = (R)(s.d[2] * (double)(w2 - n2));
-        const int cell = w0 + w1 * s.dims[0] + w2 * s.dims[0] * s.dims[1];
+        const int cell = w2 + s.dims[2] * (w1 + s.dims[1] * w0);
         clo = __ldg(&s.cell_start[cell]);
         cnt = __ldg(&s.cell_start[cell + 1]) - clo;
       }
@@ -516,10 +516,677 @@ k_pair(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int
   }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Lean warp-per-atom traversal (boxes with at least 2 nc + 1 cells per dimension).  Per atom i the
+// warp first builds a segment table: every traversal row (fixed x and y cell offsets) is one or two
+// contiguous ranges of the cell-ordered arrays (z-fastest cell numbering; the split is the
+// periodic wrap), trimmed to the cells that can hold an atom within rc of i (cells entirely beyond
+// rc can never hold a core or shell atom, so dropping them keeps every shell rank unchanged).
+// Lanes then walk the flattened candidate sequence with a per-lane segment cursor; the stride pick
+// uses a precomputed bit mask instead of a modulo per candidate; selected pairs go through a
+// 64-entry ring queue and are evaluated 32 at a time.
+
+// Abramowitz & Stegun 7.1.26: erfc(x) = t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2),
+// t = 1 / (1 + p x), |error| <= 1.5e-7; used by the FP32 path only, sharing the exponential with
+// the second term of the real-space Coulomb kernel.
+__device__ inline float erfc_as_times(float x, float e) {
+  const float t = __frcp_rn(1.0f + 0.3275911f * x);
+  return t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f)))) * e;
+}
+
+template <int MODE, bool SPECIAL>
+__device__ inline void eval_pair_f32(const SysDev& s, int moli, float qi, int js, bool core, float rx, float ry,
+                                     float rz, int ti, const int* spi, const double* spw, int nsp, float pice,
+                                     float rc2, float rs2, float sa, float alpha, const float* tab, int ntypes,
+                                     float Lx, float Ly, float Lz, float& fx, float& fy, float& fz, float& gx,
+                                     float& gy, float& gz) {
+  const int4 mj = __ldg(&s.smeta[js]);
+  if (MODE == kLJ_RBL && moli == mj.z) return;
+  min_image(rx, ry, rz, Lx, Ly, Lz);
+  const float d2 = rx * rx + ry * ry + rz * rz;
+  float w = 1.0f;
+  if (SPECIAL)
+    for (int k = 0; k < nsp; ++k)
+      if (spi[k] == mj.x) w = (float)spw[k];
+  const int tp = ti * ntypes + mj.y;
+  const float clj = tab[2 * tp], s6 = tab[2 * tp + 1];
+  const float inv_r = rsqrtf(d2);
+  const float inv_d2 = inv_r * inv_r;
+  const float sd6 = s6 * inv_d2 * inv_d2 * inv_d2;
+  const float ljf = clj * (2.0f * sd6 - 1.0f) * sd6 * inv_d2;  // force / r_vector
+  float fl = 0.0f;
+  if (MODE == kLJ_RBL) {
+    if (core) fl = (d2 < rc2 && d2 > 0.0001f) ? ljf : 0.0f;
+    else fl = (d2 < rc2 && d2 > rs2) ? pice * ljf : 0.0f;
+  } else {
+    if (core) fl = (d2 < rs2 && d2 > 0.0001f) ? w * ljf : 0.0f;
+    else fl = (d2 < rc2 && d2 > rs2) ? w * (pice * ljf) : 0.0f;
+  }
+  fx += fl * rx;
+  fy += fl * ry;
+  fz += fl * rz;
+  if (MODE == kCOUL_RBL) {
+    const bool in = core ? (d2 < rc2 && d2 > 0.0001f)
+                         : (SPECIAL ? (d2 < rc2 && d2 > rs2) : (d2 < rc2 && d2 > 0.0001f));
+    if (in) {
+      const float qj = __ldg(&s.sxf[js].w);
+      const float r = d2 * inv_r;
+      const float x = sa * r;
+      const float e = __expf(-alpha * d2);
+      const float g = erfc_as_times(x, e) * inv_d2 + 1.1283791671f * sa * e * inv_r;  // 2/sqrt(pi)
+      float fc = -qi * qj * g * inv_r;
+      if (!core) fc *= pice;
+      gx += fc * rx;
+      gy += fc * ry;
+      gz += fc * rz;
+    }
+  }
+}
+
+template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
+__global__ void __launch_bounds__(kPairWarps * 32, 3)
+k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
+  using R4 = typename Vec4<R>::T;
+  constexpr bool F32 = sizeof(R) == 4 && (MODE == kLJ_RBL || MODE == kCOUL_RBL);
+  __shared__ int s_qj[kPairWarps][64];
+  __shared__ R s_qr[kPairWarps][3][64];
+  __shared__ int s_sa[kPairWarps][64];   // segment first sorted index
+  __shared__ int s_sb[kPairWarps][64];   // segment begin in the flattened sequence
+  __shared__ int s_se[kPairWarps][64];   // segment end in the flattened sequence
+  __shared__ R s_so[kPairWarps][3][64];  // segment coordinate offsets
+  __shared__ float s_tab[2 * 64];        // FP32 LJ pair table: -24 sqrt(eps_i eps_j), sigma_ij^6
+  __shared__ double s_red[kPairWarps][9];
+
+  const int2 wk = work[blockIdx.x];
+  const SysDev& s = S[wk.x];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  const int n = s.n, ntypes = s.ntypes;
+  if (F32) {
+    for (int t = threadIdx.x; t < ntypes * ntypes && t < 64; t += blockDim.x) {
+      const int a = t / ntypes, b = t % ntypes;
+      const double sg = (s.sig[a] + s.sig[b]) / 2;
+      s_tab[2 * t] = (float)(-24.0 * sqrt(s.eps[a] * s.eps[b]));
+      s_tab[2 * t + 1] = (float)(sg * sg * sg * sg * sg * sg);
+    }
+    __syncthreads();
+  }
+  const int sidx = wk.y + wid;
+  PairAcc a;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) a.f[k] = a.g[k] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) a.vir[k] = 0.0;
+  a.rho = a.e0 = a.e1 = 0.0;
+  float ffx = 0.f, ffy = 0.f, ffz = 0.f, fgx = 0.f, fgy = 0.f, fgz = 0.f;
+  int i = -1;
+
+  if (sidx < n) {
+    const int dx = s.dims[0], dy = s.dims[1], dz = s.dims[2];
+    const double d0 = s.d[0], d1 = s.d[1], d2c = s.d[2];
+    const int4 mi = __ldg(&s.smeta[sidx]);
+    i = mi.x;
+    const int ti = mi.y, moli = mi.z;
+    const double4 xi = ldg4(&s.sx[sidx]);
+    const R4 pi4 = load_sorted<R>(s, sidx);
+    const R pix = pi4.x, piy = pi4.y, piz = pi4.z;
+    const int c0 = (int)((xi.x - s.lo[0]) / d0);
+    const int c1 = (int)((xi.y - s.lo[1]) / d1);
+    const int c2 = (int)((xi.z - s.lo[2]) / d2c);
+    const double fpi = (MODE == kEAM_FORCE) ? s.eam_fp[i] : 0.0;
+    int nsp = 0;
+    const int* spi = nullptr;
+    const double* spw = nullptr;
+    if (SPECIAL) {
+      const int b = s.sp_off[i];
+      nsp = s.sp_off[i + 1] - b;
+      spi = s.sp_ids + b;
+      spw = s.sp_w + b;
+    }
+    const bool rbl = (MODE == kLJ_RBL || MODE == kCOUL_RBL ||
+                      ((MODE == kEAM_RHO || MODE == kEAM_FORCE) && s.neigh == RBMD_NEIGH_RBL));
+    const int pice = rbl ? s.pice : 1;
+    int nsh_mod = 0;  // running shell index modulo pice
+    if (rbl && s.rbl_mode == RBMD_RBL_PHILOX && pice > 1) {
+      uint32_t o[4];
+      philox4x32_10((uint32_t)i, 0u, (uint32_t)s.st->step, kTagRblOffset, s.seed_lo, s.seed_hi, o);
+      nsh_mod = (int)(o[0] % (uint32_t)pice);
+    }
+    uint32_t base_mask = 0;  // bits 0, pice, 2 pice, ... below 32
+    for (int k = 0; k < 32; k += pice) base_mask |= (1u << k);
+    const R rc2 = (R)s.rc2, rs2 = (R)s.rs2;
+    const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
+    // conservative culling radius: cells farther than rc from i (with a margin for atoms that
+    // moved since binning) cannot hold a core or shell atom
+    const double margin = 0.1 * fmin(d0, fmin(d1, d2c));
+    const double cut2 = s.rc2;
+    const double lo0 = s.lo[0], lo1 = s.lo[1], lo2 = s.lo[2];
+    const float spice = (float)pice;
+    const float fsa = (float)sqrt(s.alpha), falpha = (float)s.alpha;
+    const float fLx = (float)s.L[0], fLy = (float)s.L[1], fLz = (float)s.L[2];
+    const float frc2 = (float)s.rc2, frs2 = (float)s.rs2;
+    int head = 0, qn = 0;
+
+    auto flush = [&](int cnt) {
+      if (lane < cnt) {
+        const int slot = (head + lane) & 63;
+        int js = s_qj[wid][slot];
+        const bool core = js >= 0;
+        if (!core) js = ~js;
+        if (F32) {
+          eval_pair_f32<MODE, SPECIAL>(s, moli, (float)xi.w, js, core, (float)s_qr[wid][0][slot],
+                                       (float)s_qr[wid][1][slot], (float)s_qr[wid][2][slot], ti, spi, spw, nsp,
+                                       spice, frc2, frs2, fsa, falpha, s_tab, ntypes, fLx, fLy, fLz, ffx, ffy, ffz,
+                                       fgx, fgy, fgz);
+        } else {
+          eval_pair<R, MODE, SPECIAL, VIRIAL>(s, i, ti, moli, xi.w, fpi, js, core, s_qr[wid][0][slot],
+                                              s_qr[wid][1][slot], s_qr[wid][2][slot], spi, spw, nsp, (R)pice, a);
+        }
+      }
+      head = (head + cnt) & 63;
+      qn -= cnt;
+    };
+
+    for (int r0 = 0; r0 < nrows; r0 += 32) {
+      // ---- segment table of rows r0 .. r0 + 31 (one row per lane)
+      const int r = r0 + lane;
+      int nseg = 0, cnt = 0;
+      int sa0 = 0, sa1 = 0, n0c = 0, n1c = 0;
+      R oxv = R(0), oyv = R(0), oz0 = R(0), oz1 = R(0);
+      if (r < nrows) {
+        const int da = r / side - nc, db = r % side - nc;
+        int n0 = c0 + da, n1 = c1 + db;
+        int w0 = n0 < 0 ? n0 + dx : (n0 >= dx ? n0 - dx : n0);
+        int w1 = n1 < 0 ? n1 + dy : (n1 >= dy ? n1 - dy : n1);
+        const double ox = d0 * (double)(w0 - n0), oy = d1 * (double)(w1 - n1);
+        oxv = (R)ox;
+        oyv = (R)oy;
+        // squared gap between i and the column of cells (unwrapped frame), shrunk by the margin
+        const double bx0 = lo0 + n0 * d0 - margin, bx1 = lo0 + (n0 + 1) * d0 + margin;
+        const double by0 = lo1 + n1 * d1 - margin, by1 = lo1 + (n1 + 1) * d1 + margin;
+        const double gx = fmax(0.0, fmax(bx0 - xi.x, xi.x - bx1));
+        const double gy = fmax(0.0, fmax(by0 - xi.y, xi.y - by1));
+        const double gxy = gx * gx + gy * gy;
+        if (gxy < cut2) {
+          int elo = nc + 1, ehi = -nc - 1;
+          for (int de = -nc; de <= nc; ++de) {
+            const int n2 = c2 + de;
+            const double bz0 = lo2 + n2 * d2c - margin, bz1 = lo2 + (n2 + 1) * d2c + margin;
+            const double gz = fmax(0.0, fmax(bz0 - xi.z, xi.z - bz1));
+            if (gxy + gz * gz < cut2) {
+              elo = min(elo, de);
+              ehi = max(ehi, de);
+            }
+          }
+          if (elo <= ehi) {
+            const int base = dz * (w1 + dy * w0);
+            const int z0 = c2 + elo, z1 = c2 + ehi;
+            if (z0 < 0) {  // wrapped part first (traversal order: most negative offset first)
+              const int a0 = base + z0 + dz, a1 = base + dz;  // cells [z0 + dz, dz)
+              sa0 = __ldg(&s.cell_start[a0]);
+              n0c = __ldg(&s.cell_start[a1]) - sa0;
+              oz0 = (R)(d2c * (double)dz);
+              if (z1 >= 0) {
+                sa1 = __ldg(&s.cell_start[base]);
+                n1c = __ldg(&s.cell_start[base + z1 + 1]) - sa1;
+                oz1 = R(0);
+                nseg = 2;
+              } else {
+                nseg = 1;
+              }
+            } else if (z1 >= dz) {
+              sa0 = __ldg(&s.cell_start[base + z0]);
+              n0c = __ldg(&s.cell_start[base + dz]) - sa0;
+              oz0 = R(0);
+              if (z0 < dz) {
+                sa1 = __ldg(&s.cell_start[base]);
+                n1c = __ldg(&s.cell_start[base + z1 - dz + 1]) - sa1;
+                oz1 = (R)(-d2c * (double)dz);
+                nseg = 2;
+              } else {
+                sa0 = sa1;
+                nseg = 1;
+              }
+            } else {
+              sa0 = __ldg(&s.cell_start[base + z0]);
+              n0c = __ldg(&s.cell_start[base + z1 + 1]) - sa0;
+              oz0 = R(0);
+              nseg = 1;
+            }
+            cnt = n0c + (nseg == 2 ? n1c : 0);
+          }
+        }
+      }
+      const int seg_incl = warp_incl_scan(nseg, lane);
+      const int cnt_incl = warp_incl_scan(cnt, lane);
+      const int nsegs = __shfl_sync(FULL, seg_incl, 31);
+      const int total = __shfl_sync(FULL, cnt_incl, 31);
+      {
+        int slot = seg_incl - nseg, beg = cnt_incl - cnt;
+        if (nseg >= 1) {
+          s_sa[wid][slot] = sa0;
+          s_sb[wid][slot] = beg;
+          s_se[wid][slot] = beg + n0c;
+          s_so[wid][0][slot] = oxv;
+          s_so[wid][1][slot] = oyv;
+          s_so[wid][2][slot] = oz0;
+        }
+        if (nseg == 2) {
+          s_sa[wid][slot + 1] = sa1;
+          s_sb[wid][slot + 1] = beg + n0c;
+          s_se[wid][slot + 1] = beg + n0c + n1c;
+          s_so[wid][0][slot + 1] = oxv;
+          s_so[wid][1][slot + 1] = oyv;
+          s_so[wid][2][slot + 1] = oz1;
+        }
+      }
+      __syncwarp();
+      // ---- candidates of the flattened sequence, 32 per iteration
+      int seg = 0;
+      for (int base = 0; base < total; base += 32) {
+        const int p = base + lane;
+        const bool valid = p < total;
+        bool core = false, shell = false;
+        R rx = R(0), ry = R(0), rz = R(0);
+        int js = 0;
+        if (valid) {
+          while (p >= s_se[wid][seg]) ++seg;
+          js = s_sa[wid][seg] + (p - s_sb[wid][seg]);
+          const R4 pj = load_sorted<R>(s, js);
+          rx = (pj.x - s_so[wid][0][seg]) - pix;
+          ry = (pj.y - s_so[wid][1][seg]) - piy;
+          rz = (pj.z - s_so[wid][2][seg]) - piz;
+          const R dd = add_rn(add_rn(mul_rn(rx, rx), mul_rn(ry, ry)), mul_rn(rz, rz));
+          if (rbl) {
+            shell = (rc2 - dd > R(0.0001) && dd - rs2 > R(0.0001));
+            core = !shell && (rs2 - dd > R(0.0001) && dd > R(0.0001));
+          } else {
+            core = (rc2 - dd > R(0.0001) && dd > R(0.0001));
+          }
+        }
+        bool sel = core;
+        if (rbl) {
+          if (pice == 1) {
+            sel = core || shell;
+          } else {
+            const unsigned sm = __ballot_sync(FULL, shell);
+            const int phase = nsh_mod == 0 ? 0 : pice - nsh_mod;
+            const uint32_t mask = phase < 32 ? (base_mask << phase) : 0u;
+            const int pre = __popc(sm & lanemask_lt(lane));
+            sel = core || (shell && ((mask >> pre) & 1u));
+            nsh_mod += __popc(sm);
+            nsh_mod -= pice * (int)((unsigned)nsh_mod / (unsigned)pice);
+          }
+        }
+        const unsigned selm = __ballot_sync(FULL, sel);
+        if (sel) {
+          const int slot = (head + qn + __popc(selm & lanemask_lt(lane))) & 63;
+          s_qj[wid][slot] = core ? js : ~js;
+          s_qr[wid][0][slot] = rx;
+          s_qr[wid][1][slot] = ry;
+          s_qr[wid][2][slot] = rz;
+        }
+        qn += __popc(selm);
+        __syncwarp();
+        if (qn >= 32) {
+          flush(32);
+          __syncwarp();
+        }
+      }
+      __syncwarp();
+    }
+    if (qn > 0) flush(qn);
+    __syncwarp();
+  }
+
+  double r9[9];
+  if (F32) {
+    r9[0] = warp_sum((double)ffx);
+    r9[1] = warp_sum((double)ffy);
+    r9[2] = warp_sum((double)ffz);
+    if (MODE == kCOUL_RBL) {
+      const double q0 = warp_sum((double)fgx), q1 = warp_sum((double)fgy), q2 = warp_sum((double)fgz);
+      r9[0] = r9[0] + s.qqr2e * q0;
+      r9[1] = r9[1] + s.qqr2e * q1;
+      r9[2] = r9[2] + s.qqr2e * q2;
+    }
+  } else {
+    r9[0] = warp_sum(a.f[0]);
+    r9[1] = warp_sum(a.f[1]);
+    r9[2] = warp_sum(a.f[2]);
+    if (MODE == kCOUL_RBL) {
+      const double q0 = warp_sum(a.g[0]), q1 = warp_sum(a.g[1]), q2 = warp_sum(a.g[2]);
+      r9[0] = r9[0] + s.qqr2e * q0;
+      r9[1] = r9[1] + s.qqr2e * q1;
+      r9[2] = r9[2] + s.qqr2e * q2;
+    }
+  }
+  if (MODE == kEAM_RHO || MODE == kEAM_ENERGY) r9[0] = warp_sum(a.rho);
+  if (MODE == kEAM_ENERGY) r9[1] = warp_sum(a.e1);
+  if (MODE == kENERGY) {
+    r9[0] = warp_sum(a.e0);
+    r9[1] = warp_sum(a.e1);
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) r9[3 + k] = VIRIAL ? warp_sum(a.vir[k]) : 0.0;
+
+  if (lane == 0 && i >= 0) {
+    if (MODE == kEAM_RHO || MODE == kEAM_ENERGY) {
+      const double rho = r9[0];
+      double p = rho * (1.0 / s.eam_drho) + 1.0;
+      int m = (int)p;
+      m = max(1, min(m, s.eam_nrho - 1));
+      p -= m;
+      p = fmin(p, 1.0);
+      const double* c = s.frho_s + 7 * m;
+      if (MODE == kEAM_RHO) {
+        s.eam_fp[i] = (c[0] * p + c[1]) * p + c[2];
+      } else {
+        const double fpv = (c[0] * p + c[1]) * p + c[2];
+        double phi = ((c[3] * p + c[4]) * p + c[5]) * p + c[6];
+        if (rho > s.eam_rhomax) phi += fpv * (rho - s.eam_rhomax);
+        r9[0] = phi;
+      }
+    } else if (MODE != kENERGY) {
+      s.f[i] = make_double4(r9[0], r9[1], r9[2], 0.0);
+    }
+  }
+  const bool need_red = (MODE == kLJ_RBL || MODE == kCOUL_RBL || MODE == kENERGY ||
+                         MODE == kEAM_ENERGY || VIRIAL ||
+                         (MODE == kEAM_FORCE && s.neigh == RBMD_NEIGH_RBL));
+  if (!need_red) return;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s_red[wid][k] = (i >= 0) ? r9[k] : 0.0;
+  }
+  __syncthreads();
+  const int blk = wk.y / kPairWarps;
+  if (threadIdx.x < 9) {
+    double t = 0.0;
+    for (int w = 0; w < kPairWarps; ++w) t += s_red[w][threadIdx.x];
+    s.vir_part[(size_t)blk * 9 + threadIdx.x] = t;
+  }
+  if (arrive_last(&s.st->counter[0], (unsigned)s.blocks_pair)) {
+    if (threadIdx.x < 9) {
+      double t = 0.0;
+      for (int b = 0; b < s.blocks_pair; ++b) t += __ldcg(&s.vir_part[(size_t)b * 9 + threadIdx.x]);
+      const int k = threadIdx.x;
+      if (MODE == kENERGY) {
+        if (k < 2) s.st->energy[k] = t;
+      } else if (MODE == kEAM_ENERGY) {
+        if (k < 2) s.st->energy[2 + k] = t;
+      } else {
+        if (k < 3) s.st->fmean[k] = (MODE == kLJ_VERLET || MODE == kCOUL_VERLET) ? 0.0 : t / s.n;
+        if (k >= 3 && VIRIAL) s.st->virial[k - 3] = t;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Dense variant: one warp per home cell, one lane per atom of that cell.  Every atom of a cell has
+// the same neighbour cells in the same order, so the warp streams each traversal row (fixed x and
+// y offsets: 2 nc + 1 consecutive z cells, contiguous in the z-fastest internal numbering) through
+// shared memory 32 candidates at a time and every lane classifies each broadcast candidate for its
+// own atom.  The shell rank is a per-lane sequential counter, exactly the reference's index_shell.
+// Selected pairs go to a per-lane shared-memory queue that the warp evaluates in lock step.
+constexpr int kCellWarps = 4;
+template <typename R> struct QDepth { static constexpr int v = 16; };
+template <> struct QDepth<double> { static constexpr int v = 8; };
+
+__device__ inline int pmod(int a, int m) { return ((a % m) + m) % m; }
+
+template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
+__global__ void __launch_bounds__(kCellWarps * 32)
+k_pair_cells(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int* out_nc,
+             int* out_ns, int* out_core, int* out_shell) {
+  constexpr int Q = QDepth<R>::v;
+  using R4 = typename Vec4<R>::T;
+  __shared__ R4 s_c[kCellWarps][32];
+  __shared__ int s_cj[kCellWarps][32];
+  __shared__ int s_qj[kCellWarps][Q][32];
+  __shared__ R s_qr[kCellWarps][3][Q][32];
+  __shared__ double s_red[kCellWarps][9];
+
+  const int2 wk = work[blockIdx.x];
+  const SysDev& s = S[wk.x];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  const int hc = wk.y + wid;
+  const int dx = s.dims[0], dy = s.dims[1], dz = s.dims[2];
+  double red[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) red[k] = 0.0;
+
+  if (hc < s.ncell) {
+    const int hx = hc / (dz * dy), hy = (hc / dz) % dy, hz = hc % dz;
+    const int hs = __ldg(&s.cell_start[hc]), he = __ldg(&s.cell_start[hc + 1]);
+    const bool rbl = (MODE == kLJ_RBL || MODE == kCOUL_RBL || MODE == kLIST ||
+                      ((MODE == kEAM_RHO || MODE == kEAM_FORCE) && s.neigh == RBMD_NEIGH_RBL));
+    const int pice = rbl ? s.pice : 1;
+    const R rc2 = (R)s.rc2, rs2 = (R)s.rs2;
+    const int nc = s.nc;
+    for (int g0 = hs; g0 < he; g0 += 32) {
+      const int si = g0 + lane;
+      const bool act = si < he;
+      int i = -1, ti = 0, moli = 0, nsp = 0;
+      double qi = 0.0, fpi = 0.0;
+      R pix = R(0), piy = R(0), piz = R(0);
+      const int* spi = nullptr;
+      const double* spw = nullptr;
+      int nmod = 0;
+      if (act) {
+        const int4 mi = __ldg(&s.smeta[si]);
+        i = mi.x;
+        ti = mi.y;
+        moli = mi.z;
+        const R4 p4 = load_sorted<R>(s, si);
+        pix = p4.x;
+        piy = p4.y;
+        piz = p4.z;
+        qi = __ldg(reinterpret_cast<const double*>(&s.sx[si]) + 3);
+        if (MODE == kEAM_FORCE) fpi = s.eam_fp[i];
+        if (SPECIAL) {
+          const int b = s.sp_off[i];
+          nsp = s.sp_off[i + 1] - b;
+          spi = s.sp_ids + b;
+          spw = s.sp_w + b;
+        }
+        if (rbl && s.rbl_mode == RBMD_RBL_PHILOX && pice > 1) {
+          uint32_t o[4];
+          philox4x32_10((uint32_t)i, 0u, (uint32_t)s.st->step, kTagRblOffset, s.seed_lo, s.seed_hi, o);
+          nmod = (int)(o[0] % (uint32_t)pice);
+        }
+      }
+      PairAcc a;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a.f[k] = a.g[k] = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) a.vir[k] = 0.0;
+      a.rho = a.e0 = a.e1 = 0.0;
+      int qc = 0, n_core = 0, n_shell = 0;
+
+      auto flush = [&]() {
+        const int maxq = __reduce_max_sync(FULL, qc);
+        for (int q = 0; q < maxq; ++q) {
+          if (q < qc) {
+            int js = s_qj[wid][q][lane];
+            const bool core = js >= 0;
+            if (!core) js = ~js;
+            eval_pair<R, MODE, SPECIAL, VIRIAL>(s, i, ti, moli, qi, fpi, js, core, s_qr[wid][0][q][lane],
+                                                s_qr[wid][1][q][lane], s_qr[wid][2][q][lane], spi, spw, nsp,
+                                                (R)pice, a);
+          }
+        }
+        qc = 0;
+      };
+
+      for (int da = -nc; da <= nc; ++da) {
+        const int n0 = hx + da, w0 = pmod(n0, dx);
+        const R ox = (R)(s.d[0] * (double)(w0 - n0));
+        for (int db = -nc; db <= nc; ++db) {
+          const int n1 = hy + db, w1 = pmod(n1, dy);
+          const R oy = (R)(s.d[1] * (double)(w1 - n1));
+          int de = -nc;
+          while (de <= nc) {
+            const int n2 = hz + de, w2 = pmod(n2, dz);
+            int len = 1;
+            while (de + len <= nc && w2 + len < dz) ++len;  // consecutive cells, same z offset
+            const R oz = (R)(s.d[2] * (double)(w2 - n2));
+            const int c0 = w2 + dz * (w1 + dy * w0);
+            const int cs = __ldg(&s.cell_start[c0]), ce = __ldg(&s.cell_start[c0 + len]);
+            for (int k0 = cs; k0 < ce; k0 += 32) {
+              const int kk = k0 + lane;
+              if (kk < ce) {
+                const R4 pj = load_sorted<R>(s, kk);
+                R4 c;
+                c.x = pj.x - ox;
+                c.y = pj.y - oy;
+                c.z = pj.z - oz;
+                c.w = R(0);
+                s_c[wid][lane] = c;
+                s_cj[wid][lane] = kk;
+              }
+              __syncwarp();
+              const int nk = min(32, ce - k0);
+              for (int k = 0; k < nk; ++k) {
+                if (act) {
+                  const R4 c = s_c[wid][k];
+                  const R rx = c.x - pix, ry = c.y - piy, rz = c.z - piz;
+                  const R d2 = add_rn(add_rn(mul_rn(rx, rx), mul_rn(ry, ry)), mul_rn(rz, rz));
+                  bool core, sel;
+                  if (rbl) {
+                    const bool shell = (rc2 - d2 > R(0.0001) && d2 - rs2 > R(0.0001));
+                    core = !shell && (rs2 - d2 > R(0.0001) && d2 > R(0.0001));
+                    sel = core;
+                    if (shell) {
+                      sel = (nmod == 0);
+                      nmod = (nmod + 1 == pice) ? 0 : nmod + 1;
+                    }
+                  } else {
+                    core = (rc2 - d2 > R(0.0001) && d2 > R(0.0001));
+                    sel = core;
+                  }
+                  if (sel) {
+                    const int js = s_cj[wid][k];
+                    if (MODE == kLIST) {
+                      const int id = __ldg(&s.smeta[js]).x;
+                      if (core) {
+                        if (n_core < cap) out_core[(size_t)i * cap + n_core] = id;
+                        ++n_core;
+                      } else {
+                        if (n_shell < cap) out_shell[(size_t)i * cap + n_shell] = id;
+                        ++n_shell;
+                      }
+                    } else {
+                      s_qj[wid][qc][lane] = core ? js : ~js;
+                      s_qr[wid][0][qc][lane] = rx;
+                      s_qr[wid][1][qc][lane] = ry;
+                      s_qr[wid][2][qc][lane] = rz;
+                      ++qc;
+                    }
+                  }
+                }
+                if (MODE != kLIST && __any_sync(FULL, qc == Q)) flush();
+              }
+              __syncwarp();
+            }
+            de += len;
+          }
+        }
+      }
+      if (MODE == kLIST) {
+        if (act) {
+          out_nc[i] = n_core;
+          out_ns[i] = n_shell;
+        }
+        continue;
+      }
+      flush();
+      if (act) {
+        double r9[9];
+        r9[0] = a.f[0];
+        r9[1] = a.f[1];
+        r9[2] = a.f[2];
+        if (MODE == kCOUL_RBL) {
+          r9[0] = r9[0] + s.qqr2e * a.g[0];
+          r9[1] = r9[1] + s.qqr2e * a.g[1];
+          r9[2] = r9[2] + s.qqr2e * a.g[2];
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) r9[3 + k] = VIRIAL ? a.vir[k] : 0.0;
+        if (MODE == kEAM_RHO || MODE == kEAM_ENERGY) {
+          const double rho = a.rho;
+          double p = rho * (1.0 / s.eam_drho) + 1.0;
+          int m = (int)p;
+          m = max(1, min(m, s.eam_nrho - 1));
+          p -= m;
+          p = fmin(p, 1.0);
+          const double* c = s.frho_s + 7 * m;
+          if (MODE == kEAM_RHO) {
+            s.eam_fp[i] = (c[0] * p + c[1]) * p + c[2];
+          } else {
+            const double fpv = (c[0] * p + c[1]) * p + c[2];
+            double phi = ((c[3] * p + c[4]) * p + c[5]) * p + c[6];
+            if (rho > s.eam_rhomax) phi += fpv * (rho - s.eam_rhomax);
+            r9[0] = phi;
+            r9[1] = a.e1;
+          }
+        } else if (MODE == kENERGY) {
+          r9[0] = a.e0;
+          r9[1] = a.e1;
+        } else {
+          s.f[i] = make_double4(r9[0], r9[1], r9[2], 0.0);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) red[k] += r9[k];
+      }
+    }
+  }
+  if (MODE == kLIST || MODE == kEAM_RHO) return;
+  const bool need_red = (MODE == kLJ_RBL || MODE == kCOUL_RBL || MODE == kENERGY ||
+                         MODE == kEAM_ENERGY || VIRIAL ||
+                         (MODE == kEAM_FORCE && s.neigh == RBMD_NEIGH_RBL));
+  if (!need_red) return;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const double w = warp_sum(red[k]);
+    if (lane == 0) s_red[wid][k] = w;
+  }
+  __syncthreads();
+  const int blk = wk.y / kCellWarps;
+  if (threadIdx.x < 9) {
+    double t = 0.0;
+    for (int w = 0; w < kCellWarps; ++w) t += s_red[w][threadIdx.x];
+    s.vir_part[(size_t)blk * 9 + threadIdx.x] = t;
+  }
+  if (arrive_last(&s.st->counter[0], (unsigned)s.blocks_pair)) {
+    if (threadIdx.x < 9) {
+      double t = 0.0;
+      for (int b = 0; b < s.blocks_pair; ++b) t += __ldcg(&s.vir_part[(size_t)b * 9 + threadIdx.x]);
+      const int k = threadIdx.x;
+      if (MODE == kENERGY) {
+        if (k < 2) s.st->energy[k] = t;
+      } else if (MODE == kEAM_ENERGY) {
+        if (k < 2) s.st->energy[2 + k] = t;
+      } else {
+        if (k < 3) s.st->fmean[k] = (MODE == kLJ_VERLET || MODE == kCOUL_VERLET) ? 0.0 : t / s.n;
+        if (k >= 3 && VIRIAL) s.st->virial[k - 3] = t;
+      }
+    }
+  }
+}
+
 template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
 static void go(const Batch& b, cudaStream_t st) {
-  k_pair<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kPairWarps * 32, 0, st>>>(b.sys, b.pair.d, 0, nullptr,
-                                                                        nullptr, nullptr, nullptr);
+  if (b.dense)
+    k_pair_cells<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kCellWarps * 32, 0, st>>>(b.sys, b.pair.d, 0, nullptr,
+                                                                                nullptr, nullptr, nullptr);
+  else if (b.lean)
+    k_pair2<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kPairWarps * 32, 0, st>>>(b.sys, b.pair.d);
+  else
+    k_pair<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kPairWarps * 32, 0, st>>>(b.sys, b.pair.d, 0, nullptr,
+                                                                          nullptr, nullptr, nullptr);
   note_launch();
 }
 
@@ -562,17 +1229,22 @@ void launch_energy(const Batch& b, cudaStream_t st) {
   }
 }
 
-void launch_rbl_lists(const SysDev* sys, int slot, int n, int cap, int* n_core, int* n_shell,
-                      int* ids, cudaStream_t st) {
+void launch_rbl_lists(const SysDev* sys, int slot, int n, int ncell, int dense, int cap, int* n_core,
+                      int* n_shell, int* ids, cudaStream_t st) {
   // ids holds 2 * n * cap ints: core rows then shell rows
-  int nb = (n + kPairWarps - 1) / kPairWarps;
+  const int per = dense ? kCellWarps : kPairWarps;
+  const int nb = ((dense ? ncell : n) + per - 1) / per;
   int2* d_work = nullptr;
   cudaMallocAsync(&d_work, sizeof(int2) * nb, st);
   int2* h = new int2[nb];
-  for (int k = 0; k < nb; ++k) h[k] = make_int2(slot, k * kPairWarps);
+  for (int k = 0; k < nb; ++k) h[k] = make_int2(slot, k * per);
   cudaMemcpyAsync(d_work, h, sizeof(int2) * nb, cudaMemcpyHostToDevice, st);
-  k_pair<double, kLIST, false, false><<<nb, kPairWarps * 32, 0, st>>>(sys, d_work, cap, n_core, n_shell,
-                                                                     ids, ids + (size_t)n * cap);
+  if (dense)
+    k_pair_cells<double, kLIST, false, false><<<nb, kCellWarps * 32, 0, st>>>(sys, d_work, cap, n_core, n_shell,
+                                                                             ids, ids + (size_t)n * cap);
+  else
+    k_pair<double, kLIST, false, false><<<nb, kPairWarps * 32, 0, st>>>(sys, d_work, cap, n_core, n_shell,
+                                                                       ids, ids + (size_t)n * cap);
   note_launch();
   cudaStreamSynchronize(st);
   delete[] h;

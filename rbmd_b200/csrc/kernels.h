@@ -22,6 +22,8 @@ struct Batch {
   // uniform switches of the batch (a batch never mixes them)
   int ff = 0, neigh = 0, coul = 0, prec = 0, temp_ctrl = 0, special = 0;
   int has_shake = 0, has_bonded = 0;
+  int dense = 0;             // pair kernel: 1 = warp per home cell, 0 = warp per atom
+  int lean = 0;              // warp per atom with segment tables (dims >= 2 nc + 1 everywhere)
   int max_P = 0;             // largest P (or Ewald nk) in the batch
 };
 
@@ -43,8 +45,12 @@ void launch_energy(const Batch& b, cudaStream_t s);
 void launch_ewald_energy(const Batch& b, cudaStream_t s);
 
 // RBL list materialisation for parity checks (not on the step path).
-void launch_rbl_lists(const SysDev* sys, int slot, int n, int cap, int* n_core, int* n_shell,
-                      int* ids, cudaStream_t s);
+void launch_rbl_lists(const SysDev* sys, int slot, int n, int ncell, int dense, int cap, int* n_core,
+                      int* n_shell, int* ids, cudaStream_t s);
+
+constexpr int kCellWarpsHost = 4;  // home cells per block of the dense pair kernel
+
+double fma_peak_tflops(int fp64, cudaStream_t s);
 
 // number of kernel launches issued by the launchers so far (all threads)
 long long launches_issued();

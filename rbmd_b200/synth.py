@@ -240,55 +240,73 @@ def _water_block(n_sites, L, rng, water_sites, ion_sites=(), ions=()):
     on `ion_sites`.  Returns arrays in atom order: all waters first, then ions."""
     side = int(round(n_sites ** (1.0 / 3.0)))
     sp = L / side
+    water_sites = np.asarray(water_sites, dtype=np.int64)
+    ion_sites = np.asarray(ion_sites, dtype=np.int64)
+
     def site_xyz(s):
-        i, r = divmod(s, side * side)
-        j, k = divmod(r, side)
-        return (np.array([i, j, k]) + 0.5) * sp
+        i, r = np.divmod(s, side * side)
+        j, k = np.divmod(r, side)
+        return (np.stack([i, j, k], -1) + 0.5) * sp
+
     th = math.radians(SPCE["theta"])
     r = SPCE["r_oh"]
-    h1 = np.array([r * math.sin(th / 2), 0.0, r * math.cos(th / 2)])
-    h2 = np.array([-r * math.sin(th / 2), 0.0, r * math.cos(th / 2)])
-    com = (M_H * h1 + M_H * h2) / (M_O + 2 * M_H)
-    R = _rotations(rng, len(water_sites))
-    pos, mass, types, charge, mol = [], [], [], [], []
-    for m, s in enumerate(water_sites):
-        c = site_xyz(s)
-        for vec, tp, ms, q in ((h1, 1, M_H, SPCE["q_h"]), (np.zeros(3), 0, M_O, SPCE["q_o"]),
-                               (h2, 1, M_H, SPCE["q_h"])):
-            pos.append(c + R[m] @ (vec - com))
-            types.append(tp)
-            mass.append(ms)
-            charge.append(q)
-            mol.append(m)
+    local = np.array([[r * math.sin(th / 2), 0.0, r * math.cos(th / 2)], [0.0, 0.0, 0.0],
+                      [-r * math.sin(th / 2), 0.0, r * math.cos(th / 2)]])
+    com = (M_H * local[0] + M_H * local[2]) / (M_O + 2 * M_H)
     nw = len(water_sites)
-    for k, (s, ion) in enumerate(zip(ion_sites, ions)):
-        pos.append(site_xyz(s))
-        types.append(ion["type"])
-        mass.append(ion["mass"])
-        charge.append(ion["q"])
-        mol.append(nw + k)
-    pos = np.mod(np.asarray(pos), L)
-    return pos, np.asarray(mass), np.asarray(types, np.int32), np.asarray(charge), np.asarray(mol, np.int32)
+    R = _rotations(rng, nw)
+    centers = site_xyz(water_sites)
+    wpos = centers[:, None, :] + np.einsum("mij,aj->mai", R, local - com[None, :])
+    pos = [wpos.reshape(-1, 3)]
+    types = [np.tile(np.array([1, 0, 1], np.int32), nw)]
+    mass = [np.tile(np.array([M_H, M_O, M_H]), nw)]
+    charge = [np.tile(np.array([SPCE["q_h"], SPCE["q_o"], SPCE["q_h"]]), nw)]
+    mol = [np.repeat(np.arange(nw, dtype=np.int32), 3)]
+    if len(ion_sites):
+        pos.append(site_xyz(ion_sites))
+        types.append(np.array([ion["type"] for ion in ions], np.int32))
+        mass.append(np.array([ion["mass"] for ion in ions]))
+        charge.append(np.array([ion["q"] for ion in ions]))
+        mol.append(nw + np.arange(len(ion_sites), dtype=np.int32))
+    pos = np.mod(np.concatenate(pos), L)
+    return (pos, np.concatenate(mass), np.concatenate(types), np.concatenate(charge),
+            np.concatenate(mol).astype(np.int32))
+
+
+def water_special_lists(n_water, n_other, weights):
+    """special_lists() of the water topology built by _water_topology, vectorised: O carries its two
+    H (1-2), each H carries its O (1-2) and the other H (1-3); other atoms carry themselves."""
+    w12, w13 = float(weights[0]), float(weights[1])
+    m = np.arange(n_water, dtype=np.int32)
+    h1, o, h2 = 3 * m, 3 * m + 1, 3 * m + 2
+    ids = np.stack([o, h2, h1, h2, o, h1], -1)  # rows: H1 (o, h2), O (h1, h2), H2 (o, h1)
+    ws = np.tile(np.array([w12, w13, w12, w12, w12, w13]), (n_water, 1))
+    ids = ids.reshape(-1)
+    ws = ws.reshape(-1)
+    n = 3 * n_water + n_other
+    other = np.arange(3 * n_water, n, dtype=np.int32)
+    ids = np.concatenate([ids, other]).astype(np.int32)
+    ws = np.concatenate([ws, np.ones(n_other)])
+    counts = np.concatenate([np.full(3 * n_water, 2, np.int32), np.ones(n_other, np.int32)])
+    off = np.zeros(n + 1, dtype=np.int32)
+    off[1:] = np.cumsum(counts)
+    return off, ids, ws
 
 
 def _water_topology(sd, n_water, special=(0.0, 0.0, 0.0)):
     """Harmonic O-H bonds and H-O-H angles (SPC/E geometry) and the SHAKE triples."""
-    bonds = []
-    angles = []
-    for m in range(n_water):
-        h1, o, h2 = 3 * m, 3 * m + 1, 3 * m + 2
-        bonds += [(o, h1), (o, h2)]
-        angles += [h1, o, h2]
-    sd.bond_atoms = np.asarray(bonds, np.int32).reshape(-1)
-    sd.bond_type = np.zeros(len(bonds), np.int32)
+    m = np.arange(n_water, dtype=np.int32)
+    h1, o, h2 = 3 * m, 3 * m + 1, 3 * m + 2
+    sd.bond_atoms = np.stack([o, h1, o, h2], -1).reshape(-1).astype(np.int32)
+    sd.bond_type = np.zeros(2 * n_water, np.int32)
     sd.bond_k = np.array([554.1349])
     sd.bond_r0 = np.array([SPCE["r_oh"]])
-    sd.angle_atoms = np.asarray(angles, np.int32)
+    sd.angle_atoms = np.stack([h1, o, h2], -1).reshape(-1).astype(np.int32)
     sd.angle_type = np.zeros(n_water, np.int32)
     sd.angle_k = np.array([45.7696])
     sd.angle_theta0 = np.array([SPCE["theta"]])
-    off, ids, ws = special_lists(sd.n, bonds, special)
-    sd.special_offsets, sd.special_ids, sd.special_weights = off, ids, ws
+    sd.special_offsets, sd.special_ids, sd.special_weights = water_special_lists(
+        n_water, sd.n - 3 * n_water, special)
 
 
 def spce_water(n_mol=3000, density=1.0, T=300.0, seed=1, P=100, beta=0.3, **kw):

@@ -31,7 +31,7 @@ def nacl_small(**kw):
 
 
 def water_small(**kw):
-    return synth.spce_water(n_mol=512, **kw)
+    return synth.spce_water(n_mol=1000, **kw)
 
 
 def eam_small(oracle_mod, **kw):
@@ -39,11 +39,26 @@ def eam_small(oracle_mod, **kw):
     return _jiggle(sd, 0.05)
 
 
-def pair(ctx_factory, oracle_mod, sd, **ctxkw):
+def pair(ctx_factory, oracle_mod, sd, layout="auto", **ctxkw):
+    """GPU context + system and the oracle twin.  `layout` selects the pair kernel: "auto" (lean
+    segment-table traversal when the box allows it), "atom" (general warp-per-atom traversal),
+    "cell" (warp per home cell)."""
+    import os
     ctx = ctx_factory(**ctxkw)
-    sid = ctx.add_system(sd)
+    old = os.environ.get("RBMD_PAIR_LAYOUT")
+    os.environ["RBMD_PAIR_LAYOUT"] = layout
+    try:
+        sid = ctx.add_system(sd)
+    finally:
+        if old is None:
+            os.environ.pop("RBMD_PAIR_LAYOUT", None)
+        else:
+            os.environ["RBMD_PAIR_LAYOUT"] = old
     o = oracle_mod.Oracle(sd)
     return ctx, sid, o
+
+
+LAYOUTS = ["auto", "atom", "cell"]
 
 
 CASES = {
@@ -68,13 +83,14 @@ def test_cells_bit_exact(ctx_factory, oracle_mod, case):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("layout", ["auto", "cell"])
 @pytest.mark.parametrize("case,mode", [("lj_rbl", A.RBL_STRIDE), ("nacl_rbe_rbl", A.RBL_STRIDE),
                                        ("water_cvff_rbe_rbl", A.RBL_STRIDE),
                                        ("water_cvff_rbe_rbl", A.RBL_PHILOX), ("eam_rbl", A.RBL_STRIDE)])
-def test_rbl_lists_bit_exact(ctx_factory, oracle_mod, case, mode):
+def test_rbl_lists_bit_exact(ctx_factory, oracle_mod, case, mode, layout):
     sd = CASES[case](oracle_mod)
     sd.params.rbl_mode = mode
-    ctx, sid, o = pair(ctx_factory, oracle_mod, sd)
+    ctx, sid, o = pair(ctx_factory, oracle_mod, sd, layout=layout)
     gn, gs, gi = ctx.rbl_lists(sid, cap=1024)
     on, os_, oi = o.rbl_lists(cap=1024)
     assert np.array_equal(gn, on)
@@ -108,22 +124,24 @@ def test_rbe_samples_test_mode(ctx_factory, oracle_mod):
     assert np.array_equal(m, om)
 
 
+@pytest.mark.parametrize("layout", LAYOUTS)
 @pytest.mark.parametrize("case", sorted(CASES))
-def test_forces_fp64(ctx_factory, oracle_mod, case):
+def test_forces_fp64(ctx_factory, oracle_mod, case, layout):
     sd = CASES[case](oracle_mod)
     sd.params.precision = A.PREC_FP64
-    ctx, sid, o = pair(ctx_factory, oracle_mod, sd)
+    ctx, sid, o = pair(ctx_factory, oracle_mod, sd, layout=layout)
     ctx.compute_forces(sid)
     f = ctx.forces(sid)
     o.compute_forces()
     assert rel_rms(f, o.forces()) < FP64_TOL
 
 
+@pytest.mark.parametrize("layout", LAYOUTS)
 @pytest.mark.parametrize("case", ["lj_rbl", "nacl_rbe_rbl", "water_cvff_rbe_rbl", "eam_rbl"])
-def test_forces_mixed_vs_fp64_oracle(ctx_factory, oracle_mod, case):
+def test_forces_mixed_vs_fp64_oracle(ctx_factory, oracle_mod, case, layout):
     sd = CASES[case](oracle_mod)
     sd.params.precision = A.PREC_MIXED
-    ctx, sid, o = pair(ctx_factory, oracle_mod, sd)
+    ctx, sid, o = pair(ctx_factory, oracle_mod, sd, layout=layout)
     ctx.compute_forces(sid)
     f = ctx.forces(sid)
     o.compute_forces()
