@@ -200,9 +200,20 @@ typedef struct rbmd_thermo {
   double volume;
   double box_lo[3];
   double box_hi[3];
-  int32_t status;               /* device-side error word of the system (0 = ok) */
+  int32_t status;               /* device-side error word of the system (0 = ok), bits below */
   int32_t pad0;
 } rbmd_thermo;
+
+/* Bits of rbmd_thermo.status, sticky until the system is removed. */
+enum rbmd_status_bit {
+  RBMD_STATUS_SHAKE_OVERFLOW = 1,    /* SHAKE multipliers became NaN or exceeded 1e20 */
+  RBMD_STATUS_SHAKE_SINGULAR = 2,    /* SHAKE 3x3 system with |det| < 1e-4 */
+  RBMD_STATUS_SHAKE_NO_CONVERGE = 4, /* SHAKE iteration hit its 5000-step limit */
+  RBMD_STATUS_RATTLE_SINGULAR = 8,   /* RATTLE 3x3 system with |det| < 1e-4 */
+  RBMD_STATUS_NON_FINITE = 16,       /* a force component was Inf or NaN */
+  RBMD_STATUS_RBE_SLOTS = 32,        /* Metropolis chain ran out of proposal slots */
+  RBMD_STATUS_CELL_RANGE = 64        /* an atom outside the box met the warp-per-cell layout */
+};
 
 typedef struct rbmd_device_cfg {
   int32_t device;               /* CUDA ordinal */

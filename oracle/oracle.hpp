@@ -28,12 +28,38 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../include/rbmd_gpu.h"
 
 namespace oracle {
+
+// Parallel loop over [0, n) in contiguous chunks on std::threads (RBMD_ORACLE_THREADS, default all
+// cores).  Every index writes only its own outputs, so results do not depend on the thread count.
+template <class Fn>
+inline void par_for(long n, Fn&& fn) {
+  static int nt = [] {
+    const char* e = std::getenv("RBMD_ORACLE_THREADS");
+    int v = e ? std::atoi(e) : (int)std::thread::hardware_concurrency();
+    return v > 0 ? v : 1;
+  }();
+  const long T = std::min<long>(nt, std::max<long>(1, n / 16));
+  if (T <= 1) {
+    for (long i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve(T);
+  for (long t = 0; t < T; ++t)
+    th.emplace_back([&, t] {
+      const long a = n * t / T, b = n * (t + 1) / T;
+      for (long i = a; i < b; ++i) fn(i);
+    });
+  for (auto& x : th) x.join();
+}
 
 constexpr double kPi = 3.14159265358979323846;          // vtkm::Pi()
 constexpr double kPif = 3.1415927410125732421875;        // (double)vtkm::Pif(), the float pi

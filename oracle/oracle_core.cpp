@@ -403,7 +403,8 @@ void System::structure_factor() {
   // (framework/run/ExecutionMD.cpp:469-501): rho_l = sum_j q_j (cos, sin)(k_l . r_j)
   const int P = p.coulomb_sample_num;
   rhok.assign(2 * P, 0.0);
-  for (int l = 0; l < P; ++l) {
+  par_for((long)(P), [&](long l_l) {
+    const int l = (int)l_l;
     double kl[3];
     for (int d = 0; d < 3; ++d) kl[d] = 2 * kPi * kspace_m[3 * l + d] / L[d];
     double re = 0, im = 0;
@@ -414,7 +415,7 @@ void System::structure_factor() {
     }
     rhok[2 * l] = re;
     rhok[2 * l + 1] = im;
-  }
+  });
 }
 
 static void kspace_virial(const double K[3], const double r[3], double F, double v[6]) {
@@ -434,7 +435,9 @@ void System::rbe_force(std::vector<double>& F, double vir[6]) const {
   const int P = p.coulomb_sample_num;
   F.assign(3 * N, 0.0);
   for (int k = 0; k < 6; ++k) vir[k] = 0;
-  for (int i = 0; i < N; ++i) {
+  std::vector<double> vir_atom(6 * (size_t)N, 0.0);
+  par_for((long)(N), [&](long i_l) {
+    const int i = (int)i_l;
     const double* ri = &x[3 * i];
     double fi[3] = {0, 0, 0}, vi[6] = {0, 0, 0, 0, 0, 0};
     for (int l = 0; l < P; ++l) {
@@ -450,8 +453,10 @@ void System::rbe_force(std::vector<double>& F, double vir[6]) const {
       kspace_virial(kl, ri, Fs, vi);
     }
     for (int d = 0; d < 3; ++d) F[3 * i + d] = fi[d] * dv.S / P;
-    for (int k = 0; k < 6; ++k) vir[k] += vi[k] * dv.S / P;
-  }
+    for (int k = 0; k < 6; ++k) vir_atom[6 * (size_t)i + k] = vi[k] * dv.S / P;
+  });
+  for (int i = 0; i < N; ++i)
+    for (int k = 0; k < 6; ++k) vir[k] += vir_atom[6 * (size_t)i + k];
 }
 
 // ------------------------------------------------------------------ a14: full Ewald
@@ -460,26 +465,33 @@ void System::ewald_force(std::vector<double>& F, double vir[6]) const {
   // ComputeNewFarElectrostaticsWorklet + Computekspace_fix (RunWorklet.cpp:2492-2540,
   // ExecForceFunction.h:712-727); k order i, j, k nested, origin skipped.
   const int* km = p.kmax;
-  std::vector<double> K, rk;
+  std::vector<double> K;
   for (int a = -km[0]; a <= km[0]; ++a)
     for (int b = -km[1]; b <= km[1]; ++b)
       for (int c = -km[2]; c <= km[2]; ++c) {
         if (a == 0 && b == 0 && c == 0) continue;
         double kv[3] = {2 * kPi * a / L[0], 2 * kPi * b / L[1], 2 * kPi * c / L[2]};
-        double re = 0, im = 0;
-        for (int j = 0; j < N; ++j) {
-          double dot = kv[0] * x[3 * j] + kv[1] * x[3 * j + 1] + kv[2] * x[3 * j + 2];
-          re += q[j] * std::cos(dot);
-          im += q[j] * std::sin(dot);
-        }
         K.insert(K.end(), kv, kv + 3);
-        rk.push_back(re);
-        rk.push_back(im);
       }
-  const size_t nk = rk.size() / 2;
+  const size_t nk = K.size() / 3;
+  std::vector<double> rk(2 * nk, 0.0);
+  par_for((long)((long)nk), [&](long l_l) {
+    const long l = (long)l_l;
+    const double* kv = &K[3 * l];
+    double re = 0, im = 0;
+    for (int j = 0; j < N; ++j) {
+      double dot = kv[0] * x[3 * j] + kv[1] * x[3 * j + 1] + kv[2] * x[3 * j + 2];
+      re += q[j] * std::cos(dot);
+      im += q[j] * std::sin(dot);
+    }
+    rk[2 * l] = re;
+    rk[2 * l + 1] = im;
+  });
   F.assign(3 * N, 0.0);
   for (int k = 0; k < 6; ++k) vir[k] = 0;
-  for (int i = 0; i < N; ++i) {
+  std::vector<double> vir_atom(6 * (size_t)N, 0.0);
+  par_for((long)(N), [&](long i_l) {
+    const int i = (int)i_l;
     const double* ri = &x[3 * i];
     double fi[3] = {0, 0, 0}, vi[6] = {0, 0, 0, 0, 0, 0};
     for (size_t l = 0; l < nk; ++l) {
@@ -493,17 +505,23 @@ void System::ewald_force(std::vector<double>& F, double vir[6]) const {
       kspace_virial(kv, ri, Fs, vi);
     }
     for (int d = 0; d < 3; ++d) F[3 * i + d] = fi[d];
-    for (int k = 0; k < 6; ++k) vir[k] += vi[k];
-  }
+    for (int k = 0; k < 6; ++k) vir_atom[6 * (size_t)i + k] = vi[k];
+  });
+  for (int i = 0; i < N; ++i)
+    for (int k = 0; k < 6; ++k) vir[k] += vir_atom[6 * (size_t)i + k];
 }
 
 double System::ewald_energy_total(const int kmax[3]) const {
   // ExecutionMD::ComputeEwaldEnergy, framework/run/ExecutionMD.cpp:405-443
-  double total = 0.0;
+  std::vector<std::array<int, 3>> ks;
   for (int a = -kmax[0]; a <= kmax[0]; ++a)
     for (int b = -kmax[1]; b <= kmax[1]; ++b)
-      for (int c = -kmax[2]; c <= kmax[2]; ++c) {
-        if (a == 0 && b == 0 && c == 0) continue;
+      for (int c = -kmax[2]; c <= kmax[2]; ++c)
+        if (!(a == 0 && b == 0 && c == 0)) ks.push_back({a, b, c});
+  std::vector<double> terms(ks.size(), 0.0);
+  par_for((long)((long)ks.size()), [&](long t_l) {
+    const long t = (long)t_l;
+        const int a = ks[t][0], b = ks[t][1], c = ks[t][2];
         double kv[3] = {2 * kPi * a / L[0], 2 * kPi * b / L[1], 2 * kPi * c / L[2]};
         double Range_K = std::sqrt(kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2]);
         double re = 0, im = 0;
@@ -513,8 +531,10 @@ double System::ewald_energy_total(const int kmax[3]) const {
           im += q[j] * std::sin(dot);
         }
         double rd2 = re * re + im * im;
-        total += std::exp(-Range_K * Range_K / (4 * p.alpha)) * rd2 / (Range_K * Range_K);
-      }
+        terms[t] = std::exp(-Range_K * Range_K / (4 * p.alpha)) * rd2 / (Range_K * Range_K);
+  });
+  double total = 0.0;
+  for (double v : terms) total += v;
   return total;
 }
 

@@ -109,7 +109,8 @@ void System::near_force(std::vector<double>& F) {
     const double rdr = 1.0 / eam_dr, rdrho = 1.0 / eam_drho;
     std::vector<double> fp(N, 0.0);
     const bool rbl = (p.neighbor == RBMD_NEIGH_RBL);
-    for (int i = 0; i < N; ++i) {
+    par_for((long)(N), [&](long i_l) {
+      const int i = (int)i_l;
       double rho = 0.0;
       int index_shell = rbl_offset(i);
       traverse(i, [&](int, const double*, const double* r0, double d2) {
@@ -143,8 +144,9 @@ void System::near_force(std::vector<double>& F) {
       pp = std::min(pp, 1.0);
       const double* c = &frho_spline[7 * mm];
       fp[i] = (c[0] * pp + c[1]) * pp + c[2];
-    }
-    for (int i = 0; i < N; ++i) {
+    });
+    par_for((long)(N), [&](long i_l) {
+      const int i = (int)i_l;
       double fc[3] = {0, 0, 0}, fs[3] = {0, 0, 0};
       int index_shell = rbl_offset(i);
       traverse(i, [&](int j, const double*, const double* r0, double d2) {
@@ -189,7 +191,7 @@ void System::near_force(std::vector<double>& F) {
         for (int k = 0; k < 3; ++k) acc[k] += scale * (r[k] * fpair);
       });
       for (int k = 0; k < 3; ++k) F[3 * i + k] = fc[k] + fs[k];
-    }
+    });
     if (rbl) {
       double mean[3] = {0, 0, 0};
       for (int i = 0; i < N; ++i)
@@ -206,7 +208,8 @@ void System::near_force(std::vector<double>& F) {
     // LJ/CUT: ComputeLJForceRBLWorklet (RunWorklet.cpp:1817-1909), same-molecule pairs skipped.
     // Coulomb force fields: ComputeNearForceRBLERFWorklet (RunWorklet.cpp:982-1093) and its
     // special-bond variant (RunWorklet.cpp:1095-1266); core LJ uses cutoff rs there.
-    for (int i = 0; i < N; ++i) {
+    par_for((long)(N), [&](long i_l) {
+      const int i = (int)i_l;
       double lj_c[3] = {0, 0, 0}, lj_s[3] = {0, 0, 0}, el_c[3] = {0, 0, 0}, el_s[3] = {0, 0, 0};
       const int ti = type[i];
       int index_shell = rbl_offset(i);
@@ -250,7 +253,7 @@ void System::near_force(std::vector<double>& F) {
       });
       for (int k = 0; k < 3; ++k)
         F[3 * i + k] = (lj_c[k] + lj_s[k]) + u.qqr2e * (el_c[k] + el_s[k]);
-    }
+    });
     // SumRBLCorrForce with the mean, ExecutionMD.cpp:663-667 / 820-826
     double mean[3] = {0, 0, 0};
     for (int i = 0; i < N; ++i)
@@ -264,9 +267,12 @@ void System::near_force(std::vector<double>& F) {
   }
 
   // VERLETLIST: LJForceVerlet (RunWorklet.cpp:498-575), NearForceVerletVirial (:2890-2985),
-  // NearForceVerletWeightVirial (:2767-2888)
-  for (int i = 0; i < N; ++i) {
+  // NearForceVerletWeightVirial (:2767-2888).  Per-atom virials, summed in atom order afterwards.
+  std::vector<double> vir_atom(6 * (size_t)N, 0.0);
+  par_for((long)(N), [&](long i_l) {
+    const int i = (int)i_l;
     double fi[3] = {0, 0, 0};
+    double* virial = &vir_atom[6 * (size_t)i];
     const int ti = type[i];
     traverse(i, [&](int j, const double*, const double* r0, double d2) {
       if (!(rc_2 - d2 > 0.0001 && d2 > 0.0001)) return;
@@ -300,7 +306,9 @@ void System::near_force(std::vector<double>& F) {
       add_virial(virial, r, fpair, vscale);
     });
     for (int k = 0; k < 3; ++k) F[3 * i + k] = fi[k];
-  }
+  });
+  for (int i = 0; i < N; ++i)
+    for (int k = 0; k < 6; ++k) virial[k] += vir_atom[6 * (size_t)i + k];
 }
 
 // ------------------------------------------------------------------ a9 / a19
@@ -798,9 +806,11 @@ void System::energies(double& e_lj, double& e_coul, double& e_eam) const {
   const bool special = !special_offsets.empty();
   if (p.force_field == RBMD_FF_EAM) {
     const double cut = eam_cut, rdr = 1.0 / eam_dr, rdrho = 1.0 / eam_drho;
-    double emb = 0, pair = 0;
-    for (int i = 0; i < N; ++i) {
+    std::vector<double> emb_i(N, 0.0), pair_i(N, 0.0);
+    par_for((long)(N), [&](long i_l) {
+      const int i = (int)i_l;
       double rho = 0;
+      double& pair = pair_i[i];
       traverse(i, [&](int, const double*, const double* r0, double d2) {
         if (!(rc_2 - d2 > 0.0001 && d2 > 0.0001)) return;
         double r[3] = {-r0[0], -r0[1], -r0[2]};
@@ -826,15 +836,23 @@ void System::energies(double& e_lj, double& e_coul, double& e_eam) const {
       double fpv = (c[0] * pp + c[1]) * pp + c[2];
       double phi = ((c[3] * pp + c[4]) * pp + c[5]) * pp + c[6];
       if (rho > eam_rhomax) phi += fpv * (rho - eam_rhomax);
-      emb += phi;
+      emb_i[i] = phi;
+    });
+    double emb = 0, pair = 0;
+    for (int i = 0; i < N; ++i) {
+      emb += emb_i[i];
+      pair += pair_i[i];
     }
     e_eam = (emb + pair) / N;
     return;
   }
   const bool coul = (p.force_field != RBMD_FF_LJ_CUT);
-  double sl = 0, sc = 0;
-  for (int i = 0; i < N; ++i) {
+  std::vector<double> el(N, 0.0), ecl(N, 0.0);
+  par_for((long)(N), [&](long i_l) {
+    const int i = (int)i_l;
     const int ti = type[i];
+    double& sl = el[i];
+    double& sc = ecl[i];
     traverse(i, [&](int j, const double*, const double* r0, double d2) {
       if (!(rc_2 - d2 > 0.0001 && d2 > 0.0001)) return;
       double r[3] = {r0[0], r0[1], r0[2]};
@@ -850,6 +868,11 @@ void System::energies(double& e_lj, double& e_coul, double& e_eam) const {
         sc += u.qqr2e * (ec - (special ? (1 - w) * ef : 0.0));
       }
     });
+  });
+  double sl = 0, sc = 0;
+  for (int i = 0; i < N; ++i) {
+    sl += el[i];
+    sc += ecl[i];
   }
   e_lj = sl / N;
   e_coul = sc / N;

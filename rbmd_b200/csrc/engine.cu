@@ -277,8 +277,11 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   const bool shake = (p.fix_shake == RBMD_SHAKE_TRUE) && d.n_angles > 0 && d.angle_atoms;
   D.has_triples = shake ? 1 : 0;
   D.n_triples = shake ? d.n_angles : 0;
-  // dense systems (tens of atoms per cell: water, saline) use the warp-per-home-cell pair kernel
-  D.lean = (D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1) ? 1 : 0;
+  // pair traversal: the lean segment-table kernel when every dimension holds the 2 nc + 1 cells
+  // of a stencil without repeats, else the general warp-per-atom kernel.  The warp-per-home-cell
+  // kernel is an opt-in tuning layout (RBMD_PAIR_LAYOUT=cell); it needs every atom inside the box
+  // and sets the cell-range status bit otherwise.
+  D.lean =(D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1) ? 1 : 0;
   D.dense = 0;
   if (const char* lay = std::getenv("RBMD_PAIR_LAYOUT")) {  // tuning override: "atom" or "cell"
     if (std::strcmp(lay, "atom") == 0) D.lean = 0;

@@ -630,6 +630,9 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
     const double4 xi = ldg4(&s.sx[sidx]);
     const R4 pi4 = load_sorted<R>(s, sidx);
     const R pix = pi4.x, piy = pi4.y, piz = pi4.z;
+    // home cell by truncation and NOT clamped (InWhichCell, ExecPointLocator.h:271-274): an atom
+    // that a step left outside the box walks the neighbourhood of its unclamped cell, every
+    // neighbour cell wrapped by a true modulo below
     const int c0 = (int)((xi.x - s.lo[0]) / d0);
     const int c1 = (int)((xi.y - s.lo[1]) / d1);
     const int c2 = (int)((xi.z - s.lo[2]) / d2c);
@@ -696,8 +699,8 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
       if (r < nrows) {
         const int da = r / side - nc, db = r % side - nc;
         int n0 = c0 + da, n1 = c1 + db;
-        int w0 = n0 < 0 ? n0 + dx : (n0 >= dx ? n0 - dx : n0);
-        int w1 = n1 < 0 ? n1 + dy : (n1 >= dy ? n1 - dy : n1);
+        int w0 = ((n0 % dx) + dx) % dx;
+        int w1 = ((n1 % dy) + dy) % dy;
         const double ox = d0 * (double)(w0 - n0), oy = d1 * (double)(w1 - n1);
         oxv = (R)ox;
         oyv = (R)oy;
@@ -719,39 +722,25 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
             }
           }
           if (elo <= ehi) {
+            // unwrapped z cells [z0, z1] (at most dz of them, since dz >= 2 nc + 1) start in the
+            // periodic copy q = floor(z0 / dz); they map to wrapped cells [zw, zw + len) when that
+            // stays below dz, else to [zw, dz) then [0, zw + len - dz) of the next copy.  The
+            // shift of a cell is d * (wrapped - unwrapped) = -d dz q (first part), -d dz (q + 1).
             const int base = dz * (w1 + dy * w0);
-            const int z0 = c2 + elo, z1 = c2 + ehi;
-            if (z0 < 0) {  // wrapped part first (traversal order: most negative offset first)
-              const int a0 = base + z0 + dz, a1 = base + dz;  // cells [z0 + dz, dz)
-              sa0 = __ldg(&s.cell_start[a0]);
-              n0c = __ldg(&s.cell_start[a1]) - sa0;
-              oz0 = (R)(d2c * (double)dz);
-              if (z1 >= 0) {
-                sa1 = __ldg(&s.cell_start[base]);
-                n1c = __ldg(&s.cell_start[base + z1 + 1]) - sa1;
-                oz1 = R(0);
-                nseg = 2;
-              } else {
-                nseg = 1;
-              }
-            } else if (z1 >= dz) {
-              sa0 = __ldg(&s.cell_start[base + z0]);
-              n0c = __ldg(&s.cell_start[base + dz]) - sa0;
-              oz0 = R(0);
-              if (z0 < dz) {
-                sa1 = __ldg(&s.cell_start[base]);
-                n1c = __ldg(&s.cell_start[base + z1 - dz + 1]) - sa1;
-                oz1 = (R)(-d2c * (double)dz);
-                nseg = 2;
-              } else {
-                sa0 = sa1;
-                nseg = 1;
-              }
-            } else {
-              sa0 = __ldg(&s.cell_start[base + z0]);
-              n0c = __ldg(&s.cell_start[base + z1 + 1]) - sa0;
-              oz0 = R(0);
+            const int z0 = c2 + elo, len = ehi - elo + 1;
+            const int zw = ((z0 % dz) + dz) % dz;
+            const int q = (z0 - zw) / dz;
+            sa0 = __ldg(&s.cell_start[base + zw]);
+            oz0 = (R)(-d2c * (double)dz * (double)q);
+            if (zw + len <= dz) {
+              n0c = __ldg(&s.cell_start[base + zw + len]) - sa0;
               nseg = 1;
+            } else {
+              n0c = __ldg(&s.cell_start[base + dz]) - sa0;
+              sa1 = __ldg(&s.cell_start[base]);
+              n1c = __ldg(&s.cell_start[base + zw + len - dz]) - sa1;
+              oz1 = (R)(-d2c * (double)dz * (double)(q + 1));
+              nseg = 2;
             }
             cnt = n0c + (nseg == 2 ? n1c : 0);
           }
@@ -985,6 +974,14 @@ k_pair_cells(const SysDev* __restrict__ S, const int2* __restrict__ work, int ca
         piy = p4.y;
         piz = p4.z;
         qi = __ldg(reinterpret_cast<const double*>(&s.sx[si]) + 3);
+        {
+          // the reference walks the neighbourhood of the UNCLAMPED cell of a position outside
+          // the box; this layout walks the home cell's, so it reports such an atom instead
+          const double4 xd = ldg4(&s.sx[si]);
+          const int u0 = (int)((xd.x - s.lo[0]) / s.d[0]), u1 = (int)((xd.y - s.lo[1]) / s.d[1]);
+          const int u2 = (int)((xd.z - s.lo[2]) / s.d[2]);
+          if (u0 != hx || u1 != hy || u2 != hz) atomicOr(&s.st->status, kErrCellRange);
+        }
         if (MODE == kEAM_FORCE) fpi = s.eam_fp[i];
         if (SPECIAL) {
           const int b = s.sp_off[i];
@@ -1235,7 +1232,10 @@ void launch_rbl_lists(const SysDev* sys, int slot, int n, int ncell, int dense, 
   const int per = dense ? kCellWarps : kPairWarps;
   const int nb = ((dense ? ncell : n) + per - 1) / per;
   int2* d_work = nullptr;
-  cudaMallocAsync(&d_work, sizeof(int2) * nb, st);
+  if (cudaMallocAsync(&d_work, sizeof(int2) * nb, st) != cudaSuccess || !d_work) {
+    cudaGetLastError();
+    return;  // the caller's sync reports the missing lists
+  }
   int2* h = new int2[nb];
   for (int k = 0; k < nb; ++k) h[k] = make_int2(slot, k * per);
   cudaMemcpyAsync(d_work, h, sizeof(int2) * nb, cudaMemcpyHostToDevice, st);

@@ -21,7 +21,7 @@ def oracle_mod():
     return oracle_ffi
 
 
-@pytest.fixture(scope="session")
+@pytest.fixture
 def ctx_factory():
     """Builds rbmd_b200 contexts; the library must be present (no CPU path)."""
     import rbmd_b200

@@ -173,6 +173,38 @@ def test_one_step_and_thermo(ctx_factory, oracle_mod, case):
         assert tg["nhc_eta"][k] == pytest.approx(to["nhc_eta"][k], rel=1e-8, abs=1e-14)
 
 
+def _push_outside(sd):
+    """Moves a few atoms outside [lo, hi): one exactly onto hi, one a whole box length past it, one
+    below lo.  The reference bins them clamped but walks the neighbourhood of the unclamped cell."""
+    L = sd.box_hi[0] - sd.box_lo[0]
+    sd.pos = sd.pos.copy()
+    sd.pos[0, 0] = sd.box_hi[0]
+    sd.pos[7, 1] += L
+    sd.pos[11, 2] -= 0.3 * L
+    sd.pos[11, 2] = min(sd.pos[11, 2], sd.box_lo[2] - 0.05)
+    return sd
+
+
+@pytest.mark.parametrize("layout", ["auto", "atom"])
+@pytest.mark.parametrize("case", ["lj_rbl", "nacl_rbe_rbl", "eam_rbl", "lj_verlet"])
+def test_forces_atoms_outside_box(ctx_factory, oracle_mod, case, layout):
+    sd = _push_outside(CASES[case](oracle_mod))
+    sd.params.precision = A.PREC_FP64
+    ctx, sid, o = pair(ctx_factory, oracle_mod, sd, layout=layout)
+    ctx.compute_forces(sid)
+    f = ctx.forces(sid)
+    o.compute_forces()
+    assert rel_rms(f, o.forces()) < FP64_TOL
+    assert ctx.thermo(sid)["status"] == 0
+
+
+def test_cell_layout_reports_atoms_outside_box(ctx_factory, oracle_mod):
+    sd = _push_outside(lj_small())
+    ctx, sid, _ = pair(ctx_factory, oracle_mod, sd, layout="cell")
+    ctx.compute_forces(sid)
+    assert ctx.thermo(sid)["status"] & A.STATUS_CELL_RANGE
+
+
 @pytest.mark.parametrize("case", ["nacl_rbe_rbl", "water_cvff_rbe_rbl"])
 def test_ten_steps_track_oracle(ctx_factory, oracle_mod, case):
     sd = CASES[case](oracle_mod)
