@@ -276,6 +276,22 @@ int rbmd_get_cells(rbmd_ctx* ctx, int32_t sys_id, int32_t* dims, int32_t* cell_o
 int rbmd_get_rbl_lists(rbmd_ctx* ctx, int32_t sys_id, int32_t cap, int32_t* n_core,
                        int32_t* n_shell, int32_t* ids);
 
+/* The same lists as rbmd_get_rbl_lists, for callers that must not allocate device memory while
+ * systems run.  No counterpart in the reference (it keeps its lists in VTK-m arrays).  Who cannot
+ * allocate: an observer or monitoring thread beside running steps (cudaFree waits for the whole
+ * device, so it would stall every stream on the GPU), and a serving host whose HBM budget has
+ * already been handed to admitted systems (an allocation there can fail mid-run).
+ * Calls no cudaMalloc, cudaFree or allocating library routine.  Every temporary lives in one
+ * file-scope device array of 2^21 ints (8 MiB) that each GPU loading the library holds until the
+ * process exits.  The first call on a device looks up that array's address; make it before any
+ * stream capture on the device.  Limit: n_atoms * (2 cap + 2) plus small work tables must fit in
+ * the 2^21 ints, else RBMD_ERR_ARG is returned and nothing runs.  Rows: core ids, shell ids, then
+ * -1 up to cap.  The array keeps the last call's contents, and calls that overlap on the GPU (two
+ * host threads, on one context or on different contexts of one device) race on it: serialise
+ * them. */
+int rbmd_get_rbl_lists_static(rbmd_ctx* ctx, int32_t sys_id, int32_t cap, int32_t* n_core,
+                              int32_t* n_shell, int32_t* ids);
+
 /* RBE k samples of the last force evaluation (integer m vectors, [3P]) and rho(k) ([2P]: Re, Im). */
 int rbmd_get_kspace(rbmd_ctx* ctx, int32_t sys_id, int32_t* m, double* rhok);
 

@@ -160,6 +160,15 @@ class Context:
         self._check(lib().rbmd_get_rbl_lists(self.h, sid, cap, _ip(nc), _ip(ns), _ip(ids)))
         return nc, ns, ids
 
+    def rbl_lists_static(self, sid, cap=1024):
+        """rbl_lists without any device allocation, for callers that must not allocate while
+        systems run; one 8 MiB file-scope scratch per device, rows core ids, shell ids, then -1."""
+        n = self._sizes[sid][0]
+        nc, ns = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        ids = np.empty((n, cap), np.int32)
+        self._check(lib().rbmd_get_rbl_lists_static(self.h, sid, cap, _ip(nc), _ip(ns), _ip(ids)))
+        return nc, ns, ids
+
     def kspace(self, sid):
         P = self._sizes[sid][1]
         m = np.zeros((P, 3), np.int32)

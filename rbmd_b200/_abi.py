@@ -182,6 +182,7 @@ def declare(lib, prefix="rbmd"):
         "get_thermo": ([ctx, C.c_int32, P(Thermo)], C.c_int),
         "get_cells": ([ctx, C.c_int32, iptr, iptr, iptr, iptr, iptr], C.c_int),
         "get_rbl_lists": ([ctx, C.c_int32, C.c_int32, iptr, iptr, iptr], C.c_int),
+        "get_rbl_lists_static": ([ctx, C.c_int32, C.c_int32, iptr, iptr, iptr], C.c_int),
         "get_kspace": ([ctx, C.c_int32, iptr, dptr], C.c_int),
         "get_derived": ([ctx, C.c_int32, P(Derived)], C.c_int),
         "eam_spline_sizes": ([P(EamFile), iptr, iptr], C.c_int),
@@ -210,7 +211,8 @@ HEADER_FUNCTIONS = [
     "rbmd_abi_version", "rbmd_params_default", "rbmd_ctx_create", "rbmd_ctx_destroy",
     "rbmd_last_error", "rbmd_system_bytes", "rbmd_system_add", "rbmd_system_remove", "rbmd_init",
     "rbmd_step", "rbmd_sync", "rbmd_compute_forces", "rbmd_get_forces", "rbmd_get_state",
-    "rbmd_set_state", "rbmd_get_thermo", "rbmd_get_cells", "rbmd_get_rbl_lists", "rbmd_get_kspace",
+    "rbmd_set_state", "rbmd_get_thermo", "rbmd_get_cells", "rbmd_get_rbl_lists", "rbmd_get_rbl_lists_static",
+    "rbmd_get_kspace",
     "rbmd_get_derived", "rbmd_eam_spline_sizes", "rbmd_eam_build_splines", "rbmd_eam_read_funcfl",
     "rbmd_serve_start", "rbmd_serve_submit", "rbmd_serve_poll", "rbmd_serve_wait",
     "rbmd_serve_result", "rbmd_serve_stop", "rbmd_launch_count", "rbmd_profile_enable",

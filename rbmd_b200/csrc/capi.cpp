@@ -161,6 +161,12 @@ int rbmd_get_rbl_lists(rbmd_ctx* ctx, int32_t id, int32_t cap, int32_t* nc, int3
   return ctx->c->get_rbl_lists(id, cap, nc, ns, ids);
 }
 
+int rbmd_get_rbl_lists_static(rbmd_ctx* ctx, int32_t id, int32_t cap, int32_t* nc, int32_t* ns,
+                              int32_t* ids) {
+  CTX_CHECK(ctx);
+  return ctx->c->get_rbl_lists_static(id, cap, nc, ns, ids);
+}
+
 int rbmd_get_kspace(rbmd_ctx* ctx, int32_t id, int32_t* m, double* rhok) {
   CTX_CHECK(ctx);
   return ctx->c->get_kspace(id, m, rhok);

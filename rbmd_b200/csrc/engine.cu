@@ -1084,6 +1084,37 @@ int Context::get_rbl_lists(int id, int cap, int32_t* nc, int32_t* ns, int32_t* i
   return RBMD_OK;
 }
 
+// Allocation-free lists: every temporary in the file-scope scratch of k_pair.cu.  The first call
+// on a device looks the scratch address up (cudaGetSymbolAddress); later calls reuse it.
+int Context::get_rbl_lists_static(int id, int cap, int32_t* nc, int32_t* ns, int32_t* ids) {
+  std::lock_guard<std::recursive_mutex> lk(mu);
+  System* s = find(id);
+  if (!s) return fail(RBMD_ERR_STATE, "unknown system id");
+  if (cap <= 0 || !nc || !ns || !ids) return fail(RBMD_ERR_ARG, "bad list buffers");
+  if (s->dev.neigh != RBMD_NEIGH_RBL) return fail(RBMD_ERR_STATE, "system does not use RBL");
+  const SysDev& D = s->dev;
+  const long long need = static_list_ints(D.n, D.ncell, D.dense, cap);
+  if (need > kStaticListInts)
+    return fail(RBMD_ERR_ARG, "lists of " + std::to_string(D.n) + " atoms at cap " + std::to_string(cap) +
+                                  " need " + std::to_string(need) + " ints of scratch; the static scratch holds " +
+                                  std::to_string(kStaticListInts) + " (8 MiB)");
+  int* scratch = nullptr;
+  cudaSetDevice(cfg.device);
+  const int e = static_list_scratch(&scratch);
+  if (e) return fail(RBMD_ERR_CUDA, std::string("static list scratch: ") + cudaGetErrorString((cudaError_t)e));
+  StaticLists L;
+  launch_rbl_lists_static(d_sys_, s->slot, D.n, D.ncell, D.dense, cap, scratch, stream, &L);
+  int over = 0;
+  cudaMemcpyAsync(nc, L.n_core, sizeof(int) * D.n, cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(ns, L.n_shell, sizeof(int) * D.n, cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(ids, L.rows, sizeof(int) * (size_t)D.n * cap, cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(&over, L.flag, sizeof(int), cudaMemcpyDeviceToHost, stream);
+  const int rc = sync();
+  if (rc) return rc;
+  if (over) return fail(RBMD_ERR_ARG, "a list row exceeds cap");
+  return RBMD_OK;
+}
+
 int Context::get_kspace(int id, int32_t* m, double* rhok) {
   std::lock_guard<std::recursive_mutex> lk(mu);
   System* s = find(id);

@@ -62,6 +62,7 @@ class Context {
   int get_thermo(int id, rbmd_thermo* out);
   int get_cells(int id, int32_t* dims, int32_t* coa, int32_t* sorted, int32_t* lo, int32_t* up);
   int get_rbl_lists(int id, int cap, int32_t* nc, int32_t* ns, int32_t* ids);
+  int get_rbl_lists_static(int id, int cap, int32_t* nc, int32_t* ns, int32_t* ids);
   int get_kspace(int id, int32_t* m, double* rhok);
   int get_derived(int id, rbmd_derived* out);
   int device_status(int id, int* status);

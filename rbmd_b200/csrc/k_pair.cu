@@ -17,6 +17,9 @@
 // are compacted through a per-warp shared-memory queue and evaluated 32 at a time, so the force
 // arithmetic runs with full warps.  FP64 classification uses explicitly rounded products and
 // sums so that it makes the same decisions as the CPU oracle on the same positions.
+#include <algorithm>
+#include <mutex>
+
 #include "kernels.h"
 
 namespace rbmd {
@@ -1249,6 +1252,127 @@ void launch_rbl_lists(const SysDev* sys, int slot, int n, int ncell, int dense, 
   cudaStreamSynchronize(st);
   delete[] h;
   cudaFreeAsync(d_work, st);
+}
+
+
+// ---------------------------------------------------------------- allocation-free RBL lists
+// Every temporary of rbmd_get_rbl_lists_static lives in this one file-scope array: the work
+// tables of the binning and list kernels, the per-atom counts and the core and shell rows.  Each
+// GPU that loads the library holds its copy (kStaticListInts ints = 8 MiB) until the process
+// exits.  Host code must not pass the array's name to a kernel (on the host it is a stand-in, not
+// a device address): static_list_scratch() gives the device address.
+static __device__ __align__(256) int g_list_scratch[kStaticListInts];
+
+namespace {
+std::mutex g_scratch_mu;
+int* g_scratch_addr[64] = {};
+
+constexpr long long round64(long long v) { return (v + 63) / 64 * 64; }
+
+__global__ void k_static_work(int slot, int per, int2* atom, int na, int2* cell, int nc, int2* pair, int np,
+                              int* slot_flag) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < na) atom[t] = make_int2(slot, t * kAtomBlock);
+  if (t < nc) cell[t] = make_int2(slot, t * kCellBlock);
+  if (t < np) pair[t] = make_int2(slot, t * per);
+  if (t == 0) {
+    slot_flag[0] = slot;
+    slot_flag[1] = 0;  // overflow flag: the array keeps the last call's contents, so clear it
+  }
+}
+
+// warp per atom: shell ids moved behind the core ids of the same row, the rest of the row -1
+__global__ void k_static_pack(int n, int cap, const int* __restrict__ n_core, const int* __restrict__ n_shell,
+                              int* core_rows, const int* __restrict__ shell_rows, int* flag) {
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const int a = n_core[i], b = n_shell[i];
+  if (a + b > cap) {
+    if (lane == 0) atomicOr(flag, 1);
+    return;
+  }
+  int* row = core_rows + (size_t)i * cap;
+  const int* sh = shell_rows + (size_t)i * cap;
+  for (int k = lane; k < b; k += 32) row[a + k] = sh[k];
+  for (int k = a + b + lane; k < cap; k += 32) row[k] = -1;
+}
+}  // namespace
+
+int static_list_scratch(int** out) {
+  *out = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (dev < 0 || dev >= 64) return (int)cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_list_scratch);  // with `dev` current
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return (int)e;
+    }
+    g_scratch_addr[dev] = (int*)ptr;
+  }
+  *out = g_scratch_addr[dev];
+  return 0;
+}
+
+long long static_list_ints(int n, int ncell, int dense, int cap) {
+  const int per = dense ? kCellWarps : kPairWarps;
+  const long long na = (n + kAtomBlock - 1) / kAtomBlock, nc = (ncell + kCellBlock - 1) / kCellBlock;
+  const long long np = ((dense ? ncell : (long long)n) + per - 1) / per;
+  return round64(2 * na) + round64(2 * nc) + round64(2 * np) + 64 + round64(n) + round64(n) +
+         round64((long long)n * cap) + round64((long long)n * cap);
+}
+
+int launch_rbl_lists_static(const SysDev* sys, int slot, int n, int ncell, int dense, int cap, int* scratch,
+                            cudaStream_t st, StaticLists* out) {
+  if (!scratch || static_list_ints(n, ncell, dense, cap) > kStaticListInts) return 1;
+  const int per = dense ? kCellWarps : kPairWarps;
+  const int na = (n + kAtomBlock - 1) / kAtomBlock, nc = (ncell + kCellBlock - 1) / kCellBlock;
+  const int np = ((dense ? ncell : n) + per - 1) / per;
+  int* p = scratch;
+  int2* w_atom = (int2*)p;
+  p += round64(2LL * na);
+  int2* w_cell = (int2*)p;
+  p += round64(2LL * nc);
+  int2* w_pair = (int2*)p;
+  p += round64(2LL * np);
+  int* slot_flag = p;
+  p += 64;
+  out->n_core = p;
+  p += round64(n);
+  out->n_shell = p;
+  p += round64(n);
+  out->rows = p;
+  p += round64((long long)n * cap);
+  int* shell_rows = p;
+  out->flag = slot_flag + 1;
+
+  const int mx = std::max(na, std::max(nc, np));
+  k_static_work<<<(mx + 255) / 256, 256, 0, st>>>(slot, per, w_atom, na, w_cell, nc, w_pair, np, slot_flag);
+  note_launch();
+  Batch b;
+  b.sys = const_cast<SysDev*>(sys);
+  b.d_slots = slot_flag;
+  b.nsys = 1;
+  b.atom.d = w_atom;
+  b.atom.n = na;
+  b.cell.d = w_cell;
+  b.cell.n = nc;
+  launch_cells(b, st);
+  if (dense)
+    k_pair_cells<double, kLIST, false, false><<<np, kCellWarps * 32, 0, st>>>(sys, w_pair, cap, out->n_core,
+                                                                             out->n_shell, out->rows, shell_rows);
+  else
+    k_pair<double, kLIST, false, false><<<np, kPairWarps * 32, 0, st>>>(sys, w_pair, cap, out->n_core,
+                                                                       out->n_shell, out->rows, shell_rows);
+  note_launch();
+  k_static_pack<<<(n + 7) / 8, 256, 0, st>>>(n, cap, out->n_core, out->n_shell, out->rows, shell_rows,
+                                             out->flag);
+  note_launch();
+  return 0;
 }
 
 }  // namespace rbmd

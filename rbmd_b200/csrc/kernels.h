@@ -48,6 +48,23 @@ void launch_ewald_energy(const Batch& b, cudaStream_t s);
 void launch_rbl_lists(const SysDev* sys, int slot, int n, int ncell, int dense, int cap, int* n_core,
                       int* n_shell, int* ids, cudaStream_t s);
 
+// Allocation-free variant of the list materialisation: every temporary in one file-scope device
+// array of kStaticListInts ints (8 MiB) per device.  static_list_scratch() looks its device address
+// up once per device (the current one) and returns a cudaError_t; static_list_ints() is the number
+// of ints a call needs; the launcher returns 1 (and launches nothing) when that exceeds
+// kStaticListInts.  Calls that overlap on the GPU share the array and race.
+constexpr long long kStaticListInts = 1LL << 21;
+struct StaticLists {
+  int* n_core = nullptr;   // [n]
+  int* n_shell = nullptr;  // [n]
+  int* rows = nullptr;     // [n * cap]: core ids, then shell ids, then -1
+  int* flag = nullptr;     // nonzero: a row exceeded cap
+};
+int static_list_scratch(int** out);
+long long static_list_ints(int n, int ncell, int dense, int cap);
+int launch_rbl_lists_static(const SysDev* sys, int slot, int n, int ncell, int dense, int cap, int* scratch,
+                            cudaStream_t s, StaticLists* out);
+
 constexpr int kCellWarpsHost = 4;  // home cells per block of the dense pair kernel
 
 double fma_peak_tflops(int fp64, cudaStream_t s);
