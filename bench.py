@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--out", default=None, help="also write the JSON line here")
     return ap.parse_args()
@@ -287,8 +288,9 @@ def cpu_port_rate(seconds, threads=None):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_ffi
     from rbmd_b200 import _abi as A, synth
-    if threads:
-        os.environ["OMP_NUM_THREADS"] = str(threads)
+    # the oracle's loops run on RBMD_ORACLE_THREADS std::threads, fixed at its first parallel loop
+    threads = threads or (os.cpu_count() or 1)
+    os.environ["RBMD_ORACLE_THREADS"] = str(threads)
     sd = synth.saline(1000, seed=3)
     sd.params.precision = A.PREC_FP64
     o = oracle_ffi.Oracle(sd)
@@ -300,8 +302,7 @@ def cpu_port_rate(seconds, threads=None):
         o.step(1)
         steps += 1
     dt = time.perf_counter() - t0
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return dict(value=sd.n * steps / dt, unit=UNIT, cores=cores, kind="port",
+    return dict(value=sd.n * steps / dt, unit=UNIT, cores=threads, kind="port",
                 sample=f"one {sd.n}-atom saline system of the stream's parameters, {steps} NVT steps in {dt:.1f} s")
 
 
@@ -373,7 +374,8 @@ def main():
     r_hbm, r_fp32 = roofline(prof, ppa, peaks, fp32_peak)
     extra = {}
     if dist.rank == 0:
-        extra["accuracy"] = measure_accuracy(device)
+        if not args.skip_accuracy:
+            extra["accuracy"] = measure_accuracy(device)
         if not args.skip_plain:
             extra["plain_fp64"] = measure_plain(systems, args, device)
     e2e = None

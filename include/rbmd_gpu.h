@@ -211,8 +211,7 @@ enum rbmd_status_bit {
   RBMD_STATUS_SHAKE_NO_CONVERGE = 4, /* SHAKE iteration hit its 5000-step limit */
   RBMD_STATUS_RATTLE_SINGULAR = 8,   /* RATTLE 3x3 system with |det| < 1e-4 */
   RBMD_STATUS_NON_FINITE = 16,       /* a force component was Inf or NaN */
-  RBMD_STATUS_RBE_SLOTS = 32,        /* Metropolis chain ran out of proposal slots */
-  RBMD_STATUS_CELL_RANGE = 64        /* an atom outside the box met the warp-per-cell layout */
+  RBMD_STATUS_RBE_SLOTS = 32         /* Metropolis chain ran out of proposal slots */
 };
 
 typedef struct rbmd_device_cfg {

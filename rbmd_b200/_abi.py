@@ -14,7 +14,7 @@ STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_OOM", 3: "ERR_NUMERIC", 4: "ERR_T
 
 # bits of the device status word (rbmd_thermo.status), enum rbmd_status_bit
 (STATUS_SHAKE_OVERFLOW, STATUS_SHAKE_SINGULAR, STATUS_SHAKE_NO_CONVERGE, STATUS_RATTLE_SINGULAR,
- STATUS_NON_FINITE, STATUS_RBE_SLOTS, STATUS_CELL_RANGE) = (1, 2, 4, 8, 16, 32, 64)
+ STATUS_NON_FINITE, STATUS_RBE_SLOTS) = (1, 2, 4, 8, 16, 32)
 
 FF_LJ_CUT, FF_LJ_CUT_COUL_LONG, FF_CVFF, FF_EAM = 0, 1, 2, 3
 NEIGH_RBL, NEIGH_VERLET = 0, 1

@@ -19,11 +19,12 @@ constexpr int kRhoChunk = 256;         // atoms per block of the structure-facto
 constexpr int kCellBlock = 256;        // cells per block of the cell kernels
 constexpr int kRbeSlack = 64;          // extra Metropolis proposal slots beyond P
 constexpr int kQueue = 64;             // per-warp pair queue of the pair kernel
+constexpr int kMaxF32Types = 16;       // atom types of the FP32 (mixed) pair table
 
 // device error word bits (rbmd_thermo.status)
 enum : int {
   kErrShakeOverflow = 1, kErrShakeSingular = 2, kErrShakeNoConverge = 4, kErrRattleSingular = 8,
-  kErrNonFinite = 16, kErrRbeSlots = 32, kErrCellRange = 64
+  kErrNonFinite = 16, kErrRbeSlots = 32
 };
 
 // Random stream tags (third Philox counter word); must match the oracle's.
@@ -58,7 +59,7 @@ struct SysDev {
   int dims[3];
   int eam_nrho, eam_nr;
   int lean;   // segment-table traversal usable (every dimension holds >= 2 nc + 1 cells)
-  int dense;  // pair kernel layout: warp per home cell (dense systems) or warp per atom
+  int dense;  // pair kernel layout: tile (warp per home cell, dense systems) or warp per atom
   int blocks_pair, blocks_atom, blocks_rho, blocks_tri, rbe_mmax, rbe_slots, has_triples, n_triples;
   // geometry and physics
   double lo[3], hi[3], L[3], d[3];
@@ -68,6 +69,12 @@ struct SysDev {
   int64_t num_steps;
   double eam_dr, eam_drho, eam_rhomax, eam_cut;
   double rbe_sigma[3];
+  // Pair classification thresholds, exact equivalents of the reference's tests on d2 in each
+  // precision: d2 <= c[0]  <=>  rc2 - d2 > 1e-4;  d2 >= c[1]  <=>  d2 - rs2 > 1e-4;
+  // d2 <= c[2]  <=>  rs2 - d2 > 1e-4 (each side of the test rounded as the reference rounds it).
+  double cls_d[3];
+  float cls_f[3];
+  int cls_pad;
   uint32_t seed_lo, seed_hi;
   // atom arrays (original order)
   double4* x;          // x, y, z, charge

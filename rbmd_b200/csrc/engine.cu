@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <limits>
 #include <cstdlib>
 #include <cstring>
 
@@ -89,6 +90,28 @@ static void derive(const rbmd_system_desc& d, const rbmd_params& p, rbmd_derived
 }
 
 // ------------------------------------------------------------------------------ context
+namespace {
+// Exact thresholds for the reference's window tests.  fl(c - x) is non-increasing in x, so
+// {x : fl(c - x) > e} is a down-set of the floats and thr_below returns its largest element;
+// likewise {x : fl(x - c) > e} is an up-set and thr_above returns its smallest element.
+template <class T>
+T thr_below(T c, T e) {
+  const T inf = std::numeric_limits<T>::infinity();
+  T x = c - e;
+  while (!(c - x > e)) x = std::nextafter(x, -inf);
+  while (c - std::nextafter(x, inf) > e) x = std::nextafter(x, inf);
+  return x;
+}
+template <class T>
+T thr_above(T c, T e) {
+  const T inf = std::numeric_limits<T>::infinity();
+  T x = c + e;
+  while (!(x - c > e)) x = std::nextafter(x, inf);
+  while (std::nextafter(x, -inf) - c > e) x = std::nextafter(x, -inf);
+  return x;
+}
+}  // namespace
+
 Context::Context(const rbmd_device_cfg& c) : cfg(c) {
   cudaSetDevice(cfg.device);
   cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
@@ -195,6 +218,9 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   if (!(p.cut_off > 0) || (p.neighbor == RBMD_NEIGH_RBL && !(p.r_core > 0 && p.r_core <= p.cut_off)))
     return fail(RBMD_ERR_ARG, "cut_off must be > 0 and 0 < r_core <= cut_off");
   if (!(p.timestep > 0)) return fail(RBMD_ERR_ARG, "timestep must be > 0");
+  if (p.precision == RBMD_PREC_MIXED && d.n_types > kMaxF32Types)
+    return fail(RBMD_ERR_UNSUPPORTED, "mixed precision supports at most " + std::to_string(kMaxF32Types) +
+                                          " atom types");
   for (int k = 0; k < 3; ++k)
     if (!(d.box_hi[k] > d.box_lo[k])) return fail(RBMD_ERR_ARG, "box_hi must exceed box_lo");
   for (int i = 0; i < d.n_atoms; ++i) {
@@ -254,6 +280,12 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   D.rs = (p.neighbor == RBMD_NEIGH_RBL) ? p.r_core : p.cut_off;
   D.rc2 = D.rc * D.rc;
   D.rs2 = D.rs * D.rs;
+  D.cls_d[0] = thr_below<double>(D.rc2, 0.0001);
+  D.cls_d[1] = thr_above<double>(D.rs2, 0.0001);
+  D.cls_d[2] = thr_below<double>(D.rs2, 0.0001);
+  D.cls_f[0] = thr_below<float>((float)D.rc2, 0.0001f);
+  D.cls_f[1] = thr_above<float>((float)D.rs2, 0.0001f);
+  D.cls_f[2] = thr_below<float>((float)D.rs2, 0.0001f);
   D.alpha = p.alpha;
   D.volume = s->dv.volume;
   D.S = s->dv.S_rbe;
@@ -277,15 +309,26 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   const bool shake = (p.fix_shake == RBMD_SHAKE_TRUE) && d.n_angles > 0 && d.angle_atoms;
   D.has_triples = shake ? 1 : 0;
   D.n_triples = shake ? d.n_angles : 0;
-  // pair traversal: the lean segment-table kernel when every dimension holds the 2 nc + 1 cells
-  // of a stencil without repeats, else the general warp-per-atom kernel.  The warp-per-home-cell
-  // kernel is an opt-in tuning layout (RBMD_PAIR_LAYOUT=cell); it needs every atom inside the box
-  // and sets the cell-range status bit otherwise.
-  D.lean =(D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1) ? 1 : 0;
-  D.dense = 0;
-  if (const char* lay = std::getenv("RBMD_PAIR_LAYOUT")) {  // tuning override: "atom" or "cell"
-    if (std::strcmp(lay, "atom") == 0) D.lean = 0;
-    else if (std::strcmp(lay, "cell") == 0) D.dense = 1;
+  // Pair traversal.  Both segment-table kernels need every dimension to hold the 2 nc + 1 cells of
+  // a stencil without repeats; otherwise the general warp-per-atom kernel runs.  Of the two, the
+  // tile kernel (warp per home cell, candidates shared by the cell's atoms) pays off in mixed
+  // precision once cells hold a few atoms on average; the lean kernel (warp per atom) is faster
+  // below that and in FP64, where the tile kernel's per-lane FP64 state no longer fits in
+  // registers.  RBMD_PAIR_LAYOUT overrides the choice for tuning and tests: "atom" (general),
+  // "lean", "cell" (tile).
+  const bool stencil_ok = D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1;
+  D.lean = stencil_ok ? 1 : 0;
+  D.dense = (stencil_ok && p.precision == RBMD_PREC_MIXED && n < (1 << 25) &&
+             (double)n >= kTileMinPerCell * (double)D.ncell) ? 1 : 0;
+  if (const char* lay = std::getenv("RBMD_PAIR_LAYOUT")) {
+    if (std::strcmp(lay, "atom") == 0) {
+      D.lean = 0;
+      D.dense = 0;
+    } else if (std::strcmp(lay, "lean") == 0) {
+      D.dense = 0;
+    } else if (std::strcmp(lay, "cell") == 0) {
+      D.dense = (stencil_ok && n < (1 << 25)) ? 1 : 0;
+    }
   }
   D.blocks_pair = D.dense ? (D.ncell + kCellWarpsHost - 1) / kCellWarpsHost : (n + kPairWarps - 1) / kPairWarps;
   D.blocks_atom = (n + kAtomBlock - 1) / kAtomBlock;
@@ -620,6 +663,7 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
     slots.push_back(s->slot);
     br->ids.push_back(s->id);
     b.max_P = std::max(b.max_P, std::max(D.P, D.nk_ewald));
+    b.natoms += D.n;
     for (int k = 0; k < D.n; k += kAtomBlock) wa.push_back(make_int2(s->slot, k));
     if (D.dense)
       for (int k = 0; k < D.ncell; k += kCellWarpsHost) wp.push_back(make_int2(s->slot, k));
@@ -728,8 +772,8 @@ void Context::enqueue_forces(const Batch& b, FinalMode mode, int virial) {
   if (b.coul == RBMD_COUL_RBE) timed("rbe_sample", 0, [&] { launch_rbe_sample(b, stream); });
   if (b.coul != RBMD_COUL_NONE) timed("rho", 0, [&] { launch_rho(b, stream, b.coul == RBMD_COUL_EWALD); });
   if (b.has_bonded) timed("bonded", 0, [&] { launch_bonded(b, stream, virial); });
-  timed("pair", (double)b.pair.n * kPairWarps, [&] { launch_pair(b, stream, virial); });
-  timed("final", (double)b.atom.n * kAtomBlock, [&] { launch_final(b, stream, mode, virial); });
+  timed("pair", (double)b.natoms, [&] { launch_pair(b, stream, virial); });
+  timed("final", (double)b.natoms, [&] { launch_final(b, stream, mode, virial); });
 }
 
 void Context::enqueue_step(const Batch& b) {
@@ -740,8 +784,8 @@ void Context::enqueue_step(const Batch& b) {
   if (b.coul == RBMD_COUL_RBE) timed("rbe_sample", 0, [&] { launch_rbe_sample(b, stream); });
   if (b.coul != RBMD_COUL_NONE) timed("rho", 0, [&] { launch_rho(b, stream, b.coul == RBMD_COUL_EWALD); });
   if (b.has_bonded) timed("bonded", 0, [&] { launch_bonded(b, stream, 0); });
-  timed("pair", (double)b.pair.n * kPairWarps, [&] { launch_pair(b, stream, 0); });
-  timed("final", (double)b.atom.n * kAtomBlock, [&] { launch_final(b, stream, kFinalKick, 0); });
+  timed("pair", (double)b.natoms, [&] { launch_pair(b, stream, 0); });
+  timed("final", (double)b.natoms, [&] { launch_final(b, stream, kFinalKick, 0); });
   if (b.has_shake) {
     timed("rattle", 0, [&] { launch_rattle(b, stream); });
     if (b.temp_ctrl != RBMD_TC_NOSE_HOOVER) timed("ke", 0, [&] { launch_ke_thermostat(b, stream); });

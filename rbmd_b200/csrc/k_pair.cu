@@ -8,15 +8,19 @@
 //   ComputeEAMfp_Worklet / ComputeEAMRBLWorklet  RunWorklet.cpp:1651-1815             (EAM passes)
 //   LJ / Coulomb / EAM energy worklets           RunWorklet.cpp:2987-3221, ThermoOutput.cpp:293-356
 //
-// One warp per atom i, atoms taken in cell order so the warps of a block walk overlapping cells.
-// The (2 nc + 1)^3 neighbour cells are visited in the reference order (x offset outermost,
-// z innermost, ascending atom id inside a cell): 32 cells at a time, one per lane, their atom
-// counts prefix-summed so each lane then takes one candidate of the flattened sequence.  The
-// shell rank of every candidate is its warp-ballot prefix plus the running shell count, which
-// reproduces the reference's sequential "every pice-th shell atom" pick exactly.  Selected pairs
-// are compacted through a per-warp shared-memory queue and evaluated 32 at a time, so the force
-// arithmetic runs with full warps.  FP64 classification uses explicitly rounded products and
-// sums so that it makes the same decisions as the CPU oracle on the same positions.
+// Three traversals share the selection rule and the pair arithmetic:
+//   k_pair       one warp per atom, any box (cells may repeat in the stencil of a small box);
+//   k_pair2      one warp per atom with per-atom segment tables (every dimension holds 2 nc + 1
+//                cells), cells beyond rc of the atom culled;
+//   k_pair_tile  one warp per home cell: the cell's atoms share each batch of 32 candidates, the
+//                default for mixed precision once cells hold a few atoms.
+// All visit the (2 nc + 1)^3 neighbour cells in the reference order (x offset outermost, z
+// innermost, ascending atom id inside a cell).  The shell rank of every candidate is its position
+// among the shells of that order, which reproduces the reference's sequential "every pice-th shell
+// atom" pick exactly.  Selected pairs are queued in shared memory and evaluated with full warps.
+// FP64 classification uses explicitly rounded products and sums (or, in the tile kernel, exact
+// threshold equivalents of the reference's window tests) so that it makes the same decisions as
+// the CPU oracle on the same positions.
 #include <algorithm>
 #include <mutex>
 
@@ -531,27 +535,26 @@ k_pair(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int
 
 // Abramowitz & Stegun 7.1.26: erfc(x) = t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2),
 // t = 1 / (1 + p x), |error| <= 1.5e-7; used by the FP32 path only, sharing the exponential with
-// the second term of the real-space Coulomb kernel.
+// the second term of the real-space Coulomb kernel.  The reciprocal is the hardware approximation
+// (a few ulp), well inside the formula's own error.
 __device__ inline float erfc_as_times(float x, float e) {
-  const float t = __frcp_rn(1.0f + 0.3275911f * x);
+  const float t = __fdividef(1.0f, 1.0f + 0.3275911f * x);
   return t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f)))) * e;
 }
 
-template <int MODE, bool SPECIAL>
-__device__ inline void eval_pair_f32(const SysDev& s, int moli, float qi, int js, bool core, float rx, float ry,
-                                     float rz, int ti, const int* spi, const double* spw, int nsp, float pice,
-                                     float rc2, float rs2, float sa, float alpha, const float* tab, int ntypes,
-                                     float Lx, float Ly, float Lz, float& fx, float& fy, float& fz, float& gx,
-                                     float& gy, float& gz) {
-  const int4 mj = __ldg(&s.smeta[js]);
-  if (MODE == kLJ_RBL && moli == mj.z) return;
-  min_image(rx, ry, rz, Lx, Ly, Lz);
+// FP32 pair arithmetic of the RBL modes on preloaded data of j (type tj, molecule molj, charge qj)
+// and the special-bond weight w of the pair.  IMG applies the minimum image; callers whose
+// displacement is already the nearest image (|r| < rc < L / 2) skip it.
+template <int MODE, bool IMG = true>
+__device__ inline void eval_pair_f32_pre(int moli, float qi, bool core, float rx, float ry, float rz, int ti, int tj,
+                                         int molj, float qj, float w, float pice, float rc2, float rs2, float sa,
+                                         float alpha, const float* tab, int ntypes, float Lx, float Ly, float Lz,
+                                         float& fx, float& fy, float& fz, float& gx, float& gy, float& gz,
+                                         bool special) {
+  if (MODE == kLJ_RBL && moli == molj) return;
+  if (IMG) min_image(rx, ry, rz, Lx, Ly, Lz);
   const float d2 = rx * rx + ry * ry + rz * rz;
-  float w = 1.0f;
-  if (SPECIAL)
-    for (int k = 0; k < nsp; ++k)
-      if (spi[k] == mj.x) w = (float)spw[k];
-  const int tp = ti * ntypes + mj.y;
+  const int tp = ti * ntypes + tj;
   const float clj = tab[2 * tp], s6 = tab[2 * tp + 1];
   const float inv_r = rsqrtf(d2);
   const float inv_d2 = inv_r * inv_r;
@@ -570,9 +573,8 @@ __device__ inline void eval_pair_f32(const SysDev& s, int moli, float qi, int js
   fz += fl * rz;
   if (MODE == kCOUL_RBL) {
     const bool in = core ? (d2 < rc2 && d2 > 0.0001f)
-                         : (SPECIAL ? (d2 < rc2 && d2 > rs2) : (d2 < rc2 && d2 > 0.0001f));
+                         : (special ? (d2 < rc2 && d2 > rs2) : (d2 < rc2 && d2 > 0.0001f));
     if (in) {
-      const float qj = __ldg(&s.sxf[js].w);
       const float r = d2 * inv_r;
       const float x = sa * r;
       const float e = __expf(-alpha * d2);
@@ -586,6 +588,23 @@ __device__ inline void eval_pair_f32(const SysDev& s, int moli, float qi, int js
   }
 }
 
+template <int MODE, bool SPECIAL>
+__device__ inline void eval_pair_f32(const SysDev& s, int moli, float qi, int js, bool core, float rx, float ry,
+                                     float rz, int ti, const int* spi, const double* spw, int nsp, float pice,
+                                     float rc2, float rs2, float sa, float alpha, const float* tab, int ntypes,
+                                     float Lx, float Ly, float Lz, float& fx, float& fy, float& fz, float& gx,
+                                     float& gy, float& gz) {
+  const int4 mj = __ldg(&s.smeta[js]);
+  if (MODE == kLJ_RBL && moli == mj.z) return;
+  float w = 1.0f;
+  if (SPECIAL)
+    for (int k = 0; k < nsp; ++k)
+      if (spi[k] == mj.x) w = (float)spw[k];
+  const float qj = (MODE == kCOUL_RBL) ? __ldg(&s.sxf[js].w) : 0.0f;
+  eval_pair_f32_pre<MODE>(moli, qi, core, rx, ry, rz, ti, mj.y, mj.z, qj, w, pice, rc2, rs2, sa, alpha, tab, ntypes,
+                          Lx, Ly, Lz, fx, fy, fz, gx, gy, gz, SPECIAL);
+}
+
 template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
 __global__ void __launch_bounds__(kPairWarps * 32, 3)
 k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
@@ -597,7 +616,7 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
   __shared__ int s_sb[kPairWarps][64];   // segment begin in the flattened sequence
   __shared__ int s_se[kPairWarps][64];   // segment end in the flattened sequence
   __shared__ R s_so[kPairWarps][3][64];  // segment coordinate offsets
-  __shared__ float s_tab[2 * 64];        // FP32 LJ pair table: -24 sqrt(eps_i eps_j), sigma_ij^6
+  __shared__ float s_tab[2 * kMaxF32Types * kMaxF32Types];  // FP32 LJ table: -24 sqrt(eps eps), sigma^6
   __shared__ double s_red[kPairWarps][9];
 
   const int2 wk = work[blockIdx.x];
@@ -606,7 +625,7 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
   const unsigned FULL = 0xffffffffu;
   const int n = s.n, ntypes = s.ntypes;
   if (F32) {
-    for (int t = threadIdx.x; t < ntypes * ntypes && t < 64; t += blockDim.x) {
+    for (int t = threadIdx.x; t < ntypes * ntypes && t < kMaxF32Types * kMaxF32Types; t += blockDim.x) {
       const int a = t / ntypes, b = t % ntypes;
       const double sg = (s.sig[a] + s.sig[b]) / 2;
       s_tab[2 * t] = (float)(-24.0 * sqrt(s.eps[a] * s.eps[b]));
@@ -916,231 +935,627 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
 }
 
 // ------------------------------------------------------------------------------------------------
-// Dense variant: one warp per home cell, one lane per atom of that cell.  Every atom of a cell has
-// the same neighbour cells in the same order, so the warp streams each traversal row (fixed x and
-// y offsets: 2 nc + 1 consecutive z cells, contiguous in the z-fastest internal numbering) through
-// shared memory 32 candidates at a time and every lane classifies each broadcast candidate for its
-// own atom.  The shell rank is a per-lane sequential counter, exactly the reference's index_shell.
-// Selected pairs go to a per-lane shared-memory queue that the warp evaluates in lock step.
-constexpr int kCellWarps = 4;
-template <typename R> struct QDepth { static constexpr int v = 16; };
-template <> struct QDepth<double> { static constexpr int v = 8; };
+// Tile variant (dense systems: many atoms per cell).  One warp per home cell.  Every atom of a
+// home cell walks the same candidate sequence -- the (2 nc + 1)^2 traversal rows of the home cell,
+// each one or two contiguous ranges of the cell-ordered arrays -- so the warp streams that
+// sequence once, 32 candidates per batch (one per lane), and classifies each batch against every
+// atom of the cell in turn: two ballots (core, shell) per (atom, batch), the window tests done as
+// single compares against exact thresholds.  The lane that owns an atom then turns its masks into
+// picks -- every pice-th shell atom in traversal order, located with __fns from a running skip
+// count -- and queues the selected pairs as packed ints.  When any queue is nearly full the warp
+// evaluates all queues in lock step; with 16 or fewer atoms in the cell each queue is shared by
+// 2, 4, ... lanes whose partial sums are then added in a fixed order.  An atom outside the box
+// (its unclamped cell is not the home cell it is binned into) walks its own neighbourhood with
+// the whole warp before the cell's batches, as the reference's locator does.
+constexpr int kCellWarps = 4;    // home cells per block (kCellWarpsHost on the host side)
+// resident blocks per SM the tile kernel is compiled for (bounds its registers per thread)
+#ifndef RBMD_TILE_MIN_BLOCKS
+#define RBMD_TILE_MIN_BLOCKS 5
+#endif
+constexpr int kTileQ = 48;       // queued pairs per atom between evaluations (a batch adds <= 32)
+constexpr int kJsBits = 25;      // queue entry: sorted index | shift code << 25 | shell << 31
+constexpr int kJsMask = (1 << kJsBits) - 1;
+constexpr int kTileSp = 4;       // special partners per atom cached in shared memory
+constexpr int kTileHist = 16;    // batches of candidates kept for the queued pairs (power of 2)
 
-__device__ inline int pmod(int a, int m) { return ((a % m) + m) % m; }
+template <typename R> __device__ inline R cls_thr(const SysDev& s, int k);
+template <> __device__ inline double cls_thr<double>(const SysDev& s, int k) { return s.cls_d[k]; }
+template <> __device__ inline float cls_thr<float>(const SysDev& s, int k) { return s.cls_f[k]; }
+
+// Picked shells of one batch: the set bits of sm at ranks r, r + pice, ... where r is the number
+// of shells still to skip; r leaves as the skip count for the next batch.
+__device__ inline unsigned pick_shells(unsigned sm, int pice, int& r) {
+  if (pice == 1) return sm;
+  const int ns = __popc(sm);
+  unsigned pk = 0u;
+  while (r < ns) {
+    pk |= 1u << __fns(sm, 0u, r + 1);
+    r += pice;
+  }
+  r -= ns;
+  return pk;
+}
+
+// Per-atom result of a pair pass: forces written (or the EAM embedding derivative); r9 leaves as
+// the atom's nine reduction values.
+template <int MODE>
+__device__ inline void finish_atom(const SysDev& s, int i, double (&r9)[9]) {
+  if (MODE == kEAM_RHO || MODE == kEAM_ENERGY) {
+    const double rho = r9[0];
+    double p = rho * (1.0 / s.eam_drho) + 1.0;
+    int m = (int)p;
+    m = max(1, min(m, s.eam_nrho - 1));
+    p -= m;
+    p = fmin(p, 1.0);
+    const double* c = s.frho_s + 7 * m;
+    if (MODE == kEAM_RHO) {
+      s.eam_fp[i] = (c[0] * p + c[1]) * p + c[2];
+    } else {
+      const double fpv = (c[0] * p + c[1]) * p + c[2];
+      double phi = ((c[3] * p + c[4]) * p + c[5]) * p + c[6];
+      if (rho > s.eam_rhomax) phi += fpv * (rho - s.eam_rhomax);
+      r9[0] = phi;
+    }
+  } else if (MODE != kENERGY && MODE != kLIST) {
+    s.f[i] = make_double4(r9[0], r9[1], r9[2], 0.0);
+  }
+}
+
+// The nine per-atom values from the accumulators.
+template <int MODE, bool F32, bool VIRIAL>
+__device__ inline void acc_to_r9(const SysDev& s, const double (&c)[6], const PairAcc& a, double (&r9)[9]) {
+#pragma unroll
+  for (int k = 0; k < 9; ++k) r9[k] = 0.0;
+  if (F32) {
+    r9[0] = c[0];
+    r9[1] = c[1];
+    r9[2] = c[2];
+    if (MODE == kCOUL_RBL) {
+      r9[0] = r9[0] + s.qqr2e * c[3];
+      r9[1] = r9[1] + s.qqr2e * c[4];
+      r9[2] = r9[2] + s.qqr2e * c[5];
+    }
+    return;
+  }
+  r9[0] = a.f[0];
+  r9[1] = a.f[1];
+  r9[2] = a.f[2];
+  if (MODE == kCOUL_RBL) {
+    r9[0] = r9[0] + s.qqr2e * a.g[0];
+    r9[1] = r9[1] + s.qqr2e * a.g[1];
+    r9[2] = r9[2] + s.qqr2e * a.g[2];
+  }
+  if (VIRIAL) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) r9[3 + k] = a.vir[k];
+  }
+  if (MODE == kEAM_RHO || MODE == kEAM_ENERGY) r9[0] = a.rho;
+  if (MODE == kEAM_ENERGY) r9[1] = a.e1;
+  if (MODE == kENERGY) {
+    r9[0] = a.e0;
+    r9[1] = a.e1;
+  }
+}
+
+__device__ inline void acc_zero(float (&ff)[6], PairAcc& a) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k) ff[k] = 0.f;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) a.f[k] = a.g[k] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) a.vir[k] = 0.0;
+  a.rho = a.e0 = a.e1 = 0.0;
+}
+
+// Adds the accumulators of lanes (a, m), m = 0 .. k - 1 (lane = a + m nat), into lane (a, 0), in a
+// fixed tree order.  The FP32 partials are widened to FP64 first.
+template <bool F32>
+__device__ inline void acc_combine(float (&ff)[6], PairAcc& a, double (&c)[6], int k, int nat) {
+  const unsigned FULL = 0xffffffffu;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) c[j] = (double)ff[j];
+  for (int off = k >> 1; off >= 1; off >>= 1) {
+    const int d = off * nat;
+    if (F32) {
+#pragma unroll
+      for (int j = 0; j < 6; ++j) c[j] += __shfl_down_sync(FULL, c[j], d);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        a.f[j] += __shfl_down_sync(FULL, a.f[j], d);
+        a.g[j] += __shfl_down_sync(FULL, a.g[j], d);
+      }
+#pragma unroll
+      for (int j = 0; j < 6; ++j) a.vir[j] += __shfl_down_sync(FULL, a.vir[j], d);
+      a.rho += __shfl_down_sync(FULL, a.rho, d);
+      a.e0 += __shfl_down_sync(FULL, a.e0, d);
+      a.e1 += __shfl_down_sync(FULL, a.e1, d);
+    }
+  }
+}
+
+// Sum over all 32 lanes (every lane gets the total), same fields as acc_combine.
+template <bool F32>
+__device__ inline void acc_warp_total(float (&ff)[6], PairAcc& a, double (&c)[6]) {
+#pragma unroll
+  for (int j = 0; j < 6; ++j) c[j] = warp_sum((double)ff[j]);
+  if (!F32) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      a.f[j] = warp_sum(a.f[j]);
+      a.g[j] = warp_sum(a.g[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 6; ++j) a.vir[j] = warp_sum(a.vir[j]);
+    a.rho = warp_sum(a.rho);
+    a.e0 = warp_sum(a.e0);
+    a.e1 = warp_sum(a.e1);
+  }
+}
+
+// One atom whose position lies outside the box, walked by the whole warp over the (2 nc + 1)^3
+// cells around its unclamped cell, each wrapped by a true modulo (ExecPointLocator::InWhichCell
+// and PeriodicIndexOffset), candidates 32 at a time.  Selected pairs are evaluated in place into
+// the lanes' accumulators (zero on entry); list mode writes the rows directly.
+template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
+__device__ void tile_stray(const SysDev& s, int si, int skip, int pice, bool rbl, const float* s_tab, int cap,
+                           int* out_nc, int* out_ns, int* out_core, int* out_shell, float (&ff)[6],
+                           PairAcc& acc) {
+  using R4 = typename Vec4<R>::T;
+  constexpr bool F32 = sizeof(R) == 4 && (MODE == kLJ_RBL || MODE == kCOUL_RBL);
+  const int lane = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  const int4 mi = __ldg(&s.smeta[si]);
+  const int i = mi.x, ti = mi.y, moli = mi.z;
+  const double4 xd = ldg4(&s.sx[si]);
+  const R4 p4 = load_sorted<R>(s, si);
+  const double fpi = (MODE == kEAM_FORCE) ? s.eam_fp[i] : 0.0;
+  int nsp = 0;
+  const int* spi = nullptr;
+  const double* spw = nullptr;
+  if (SPECIAL) {
+    const int b = s.sp_off[i];
+    nsp = s.sp_off[i + 1] - b;
+    spi = s.sp_ids + b;
+    spw = s.sp_w + b;
+  }
+  const R t_rc = cls_thr<R>(s, 0), t_rs_hi = cls_thr<R>(s, 1), t_rs_lo = cls_thr<R>(s, 2);
+  const R far = R(1e30);
+  const float spice = (float)pice, fsa = (float)sqrt(s.alpha), falpha = (float)s.alpha;
+  const int dx = s.dims[0], dy = s.dims[1], dz = s.dims[2];
+  const int u0 = (int)((xd.x - s.lo[0]) / s.d[0]), u1 = (int)((xd.y - s.lo[1]) / s.d[1]);
+  const int u2 = (int)((xd.z - s.lo[2]) / s.d[2]);
+  const int nc = s.nc;
+  int n_core = 0, n_shell = 0;
+  for (int da = -nc; da <= nc; ++da)
+    for (int db = -nc; db <= nc; ++db)
+      for (int de = -nc; de <= nc; ++de) {
+        const int n0 = u0 + da, n1 = u1 + db, n2 = u2 + de;
+        const int w0 = ((n0 % dx) + dx) % dx, w1 = ((n1 % dy) + dy) % dy, w2 = ((n2 % dz) + dz) % dz;
+        const R ox = (R)(s.d[0] * (double)(w0 - n0)), oy = (R)(s.d[1] * (double)(w1 - n1));
+        const R oz = (R)(s.d[2] * (double)(w2 - n2));
+        const int cell = w2 + dz * (w1 + dy * w0);
+        const int cs = __ldg(&s.cell_start[cell]), ce = __ldg(&s.cell_start[cell + 1]);
+        for (int k0 = cs; k0 < ce; k0 += 32) {
+          const int kk = k0 + lane;
+          R rx = far, ry = far, rz = far;
+          if (kk < ce) {
+            const R4 pj = load_sorted<R>(s, kk);
+            rx = (pj.x - ox) - p4.x;
+            ry = (pj.y - oy) - p4.y;
+            rz = (pj.z - oz) - p4.z;
+          }
+          const R dd = add_rn(add_rn(mul_rn(rx, rx), mul_rn(ry, ry)), mul_rn(rz, rz));
+          const bool shell = rbl && dd >= t_rs_hi && dd <= t_rc;
+          const bool core = rbl ? (dd <= t_rs_lo && dd > R(0.0001)) : (dd <= t_rc && dd > R(0.0001));
+          const unsigned cm = __ballot_sync(FULL, core), sm = __ballot_sync(FULL, shell);
+          const unsigned pk = rbl ? pick_shells(sm, pice, skip) : 0u;
+          const bool sel = ((cm | pk) >> lane) & 1u;
+          if (MODE == kLIST) {
+            if (sel) {
+              const int id = __ldg(&s.smeta[kk]).x;
+              if (core) {
+                const int pos = n_core + __popc(cm & lanemask_lt(lane));
+                if (pos < cap) out_core[(size_t)i * cap + pos] = id;
+              } else {
+                const int pos = n_shell + __popc(pk & lanemask_lt(lane));
+                if (pos < cap) out_shell[(size_t)i * cap + pos] = id;
+              }
+            }
+            n_core += __popc(cm);
+            n_shell += __popc(pk);
+          } else if (sel) {
+            if (F32)
+              eval_pair_f32<MODE, SPECIAL>(s, moli, (float)xd.w, kk, core, (float)rx, (float)ry, (float)rz, ti, spi,
+                                           spw, nsp, spice, (float)s.rc2, (float)s.rs2, fsa, falpha, s_tab,
+                                           s.ntypes, (float)s.L[0], (float)s.L[1], (float)s.L[2], ff[0], ff[1],
+                                           ff[2], ff[3], ff[4], ff[5]);
+            else
+              eval_pair<R, MODE, SPECIAL, VIRIAL>(s, i, ti, moli, xd.w, fpi, kk, core, rx, ry, rz, spi, spw, nsp,
+                                                  (R)pice, acc);
+          }
+        }
+      }
+  if (MODE == kLIST && lane == 0) {
+    out_nc[i] = n_core;
+    out_ns[i] = n_shell;
+  }
+}
 
 template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
-__global__ void __launch_bounds__(kCellWarps * 32)
-k_pair_cells(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int* out_nc,
-             int* out_ns, int* out_core, int* out_shell) {
-  constexpr int Q = QDepth<R>::v;
+__global__ void __launch_bounds__(kCellWarps * 32, RBMD_TILE_MIN_BLOCKS)
+k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int* out_nc, int* out_ns,
+            int* out_core, int* out_shell) {
   using R4 = typename Vec4<R>::T;
-  __shared__ R4 s_c[kCellWarps][32];
-  __shared__ int s_cj[kCellWarps][32];
-  __shared__ int s_qj[kCellWarps][Q][32];
-  __shared__ R s_qr[kCellWarps][3][Q][32];
+  constexpr bool F32 = sizeof(R) == 4 && (MODE == kLJ_RBL || MODE == kCOUL_RBL);
+  constexpr bool QUEUE = MODE != kLIST;
+  // per-atom pair queues (column = atom of the chunk); an entry is (history slot << 5 | lane) with
+  // bit 15 set for a shell pair
+  __shared__ unsigned short s_q[kCellWarps][kTileQ][32];
+  __shared__ R4 s_pi[kCellWarps][32];          // chunk atom positions (far away for box-outside atoms)
+  __shared__ int s_hist[kCellWarps][kTileHist][32];  // packed candidates of the batches since the
+                                                     // last evaluation; queue entries index it
+  __shared__ int s_sa[kCellWarps][64];         // segment first sorted index
+  __shared__ int s_sb[kCellWarps][64];         // segment begin in the flattened sequence
+  __shared__ int s_se[kCellWarps][64];         // segment end in the flattened sequence
+  __shared__ int s_code[kCellWarps][64];       // segment shift code (<< kJsBits)
+  __shared__ R s_shift[3][3];                  // per dimension: d (w - n) for w - n = -dims, 0, +dims
+  __shared__ float s_tab[2 * kMaxF32Types * kMaxF32Types];
   __shared__ double s_red[kCellWarps][9];
+  __shared__ int s_spi[kCellWarps][kTileSp][32];  // first special partners of each chunk atom
+  __shared__ float s_spw[kCellWarps][kTileSp][32];
 
   const int2 wk = work[blockIdx.x];
   const SysDev& s = S[wk.x];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
-  const int hc = wk.y + wid;
   const int dx = s.dims[0], dy = s.dims[1], dz = s.dims[2];
-  double red[9];
-#pragma unroll
-  for (int k = 0; k < 9; ++k) red[k] = 0.0;
+  const int ntypes = s.ntypes;
+  if (threadIdx.x < 9) {
+    const int dim = threadIdx.x / 3, t = threadIdx.x % 3;
+    s_shift[dim][t] = (R)(s.d[dim] * (double)((t - 1) * s.dims[dim]));
+  }
+  if (F32) {
+    for (int t = threadIdx.x; t < ntypes * ntypes && t < kMaxF32Types * kMaxF32Types; t += blockDim.x) {
+      const int a = t / ntypes, b = t % ntypes;
+      const double sg = (s.sig[a] + s.sig[b]) / 2;
+      s_tab[2 * t] = (float)(-24.0 * sqrt(s.eps[a] * s.eps[b]));
+      s_tab[2 * t + 1] = (float)(sg * sg * sg * sg * sg * sg);
+    }
+  }
+  __syncthreads();
 
+  const bool rbl = (MODE == kLJ_RBL || MODE == kCOUL_RBL || MODE == kLIST ||
+                    ((MODE == kEAM_RHO || MODE == kEAM_FORCE) && s.neigh == RBMD_NEIGH_RBL));
+  const int pice = rbl ? s.pice : 1;
+  const R t_rc = cls_thr<R>(s, 0), t_rs_hi = cls_thr<R>(s, 1), t_rs_lo = cls_thr<R>(s, 2);
+  const R far = R(1e30);
+  const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
+  const float spice = (float)pice, fsa = (float)sqrt(s.alpha), falpha = (float)s.alpha;
+  const float fLx = (float)s.L[0], fLy = (float)s.L[1], fLz = (float)s.L[2];
+  const float frc2 = (float)s.rc2, frs2 = (float)s.rs2;
+  if (lane < 9) s_red[wid][lane] = 0.0;  // per-warp reduction values, added in a fixed order
+  // lane 0 adds the warp total of v (owner lanes' values, in lane order) to s_red[wid][k]
+  auto add_red = [&](const double (&v)[9], bool take) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const double w = warp_sum(take ? v[k] : 0.0);
+      if (lane == 0) s_red[wid][k] += w;
+    }
+  };
+
+  const int hc = wk.y + wid;
   if (hc < s.ncell) {
     const int hx = hc / (dz * dy), hy = (hc / dz) % dy, hz = hc % dz;
     const int hs = __ldg(&s.cell_start[hc]), he = __ldg(&s.cell_start[hc + 1]);
-    const bool rbl = (MODE == kLJ_RBL || MODE == kCOUL_RBL || MODE == kLIST ||
-                      ((MODE == kEAM_RHO || MODE == kEAM_FORCE) && s.neigh == RBMD_NEIGH_RBL));
-    const int pice = rbl ? s.pice : 1;
-    const R rc2 = (R)s.rc2, rs2 = (R)s.rs2;
-    const int nc = s.nc;
     for (int g0 = hs; g0 < he; g0 += 32) {
-      const int si = g0 + lane;
-      const bool act = si < he;
-      int i = -1, ti = 0, moli = 0, nsp = 0;
-      double qi = 0.0, fpi = 0.0;
-      R pix = R(0), piy = R(0), piz = R(0);
+      const int nat = min(32, he - g0);
+      int k = 1;
+      while (2 * k * nat <= 32) k *= 2;
+      const int a = lane % nat, m = lane / nat;
+      const bool member = m < k;  // lane (a, m) helps evaluate the queue of atom a
+      const bool owner = lane < nat;
+      const int si = g0 + a;
+      const int4 mi = __ldg(&s.smeta[si]);
+      const int i = mi.x, ti = mi.y, moli = mi.z;
+      const R4 p4 = load_sorted<R>(s, si);
+      const R pix = p4.x, piy = p4.y, piz = p4.z;
+      const double4 xd = ldg4(&s.sx[si]);
+      const double qi = xd.w;
+      const bool stray = (int)((xd.x - s.lo[0]) / s.d[0]) != hx || (int)((xd.y - s.lo[1]) / s.d[1]) != hy ||
+                         (int)((xd.z - s.lo[2]) / s.d[2]) != hz;
+      const double fpi = (MODE == kEAM_FORCE) ? s.eam_fp[i] : 0.0;
+      int nsp = 0;
       const int* spi = nullptr;
       const double* spw = nullptr;
-      int nmod = 0;
-      if (act) {
-        const int4 mi = __ldg(&s.smeta[si]);
-        i = mi.x;
-        ti = mi.y;
-        moli = mi.z;
-        const R4 p4 = load_sorted<R>(s, si);
-        pix = p4.x;
-        piy = p4.y;
-        piz = p4.z;
-        qi = __ldg(reinterpret_cast<const double*>(&s.sx[si]) + 3);
-        {
-          // the reference walks the neighbourhood of the UNCLAMPED cell of a position outside
-          // the box; this layout walks the home cell's, so it reports such an atom instead
-          const double4 xd = ldg4(&s.sx[si]);
-          const int u0 = (int)((xd.x - s.lo[0]) / s.d[0]), u1 = (int)((xd.y - s.lo[1]) / s.d[1]);
-          const int u2 = (int)((xd.z - s.lo[2]) / s.d[2]);
-          if (u0 != hx || u1 != hy || u2 != hz) atomicOr(&s.st->status, kErrCellRange);
-        }
-        if (MODE == kEAM_FORCE) fpi = s.eam_fp[i];
-        if (SPECIAL) {
-          const int b = s.sp_off[i];
-          nsp = s.sp_off[i + 1] - b;
-          spi = s.sp_ids + b;
-          spw = s.sp_w + b;
-        }
-        if (rbl && s.rbl_mode == RBMD_RBL_PHILOX && pice > 1) {
-          uint32_t o[4];
-          philox4x32_10((uint32_t)i, 0u, (uint32_t)s.st->step, kTagRblOffset, s.seed_lo, s.seed_hi, o);
-          nmod = (int)(o[0] % (uint32_t)pice);
+      if (SPECIAL) {
+        const int b = s.sp_off[i];
+        nsp = s.sp_off[i + 1] - b;
+        spi = s.sp_ids + b;
+        spw = s.sp_w + b;
+      }
+      int skip = 0;  // shells still to skip before the next pick (owner lanes)
+      if (rbl && s.rbl_mode == RBMD_RBL_PHILOX && pice > 1) {
+        uint32_t o[4];
+        philox4x32_10((uint32_t)i, 0u, (uint32_t)s.st->step, kTagRblOffset, s.seed_lo, s.seed_hi, o);
+        const int nm = (int)(o[0] % (uint32_t)pice);
+        skip = nm == 0 ? 0 : pice - nm;
+      }
+      __syncwarp();  // the previous chunk has finished with s_pi
+      if (owner) {
+        R4 q = p4;
+        if (stray) q.x = q.y = q.z = far;
+        s_pi[wid][lane] = q;
+        if (SPECIAL && nsp <= kTileSp)
+          for (int t = 0; t < nsp; ++t) {
+            s_spi[wid][t][lane] = spi[t];
+            s_spw[wid][t][lane] = (float)spw[t];
+          }
+      }
+      float ff[6];
+      PairAcc acc;
+      acc_zero(ff, acc);
+      double cmb[6];
+      int qc = 0, n_core = 0, n_shell = 0;
+      int nh = 0;  // batches in the history ring since the last evaluation (warp-uniform)
+
+      // ---- atoms outside the box: the whole warp walks each one's own neighbourhood
+      unsigned strays = __ballot_sync(FULL, owner && stray);
+      while (strays) {
+        const int as = __ffs(strays) - 1;
+        strays &= strays - 1;
+        const int sk = __shfl_sync(FULL, skip, as);
+        tile_stray<R, MODE, SPECIAL, VIRIAL>(s, g0 + as, sk, pice, rbl, s_tab, cap, out_nc, out_ns, out_core,
+                                             out_shell, ff, acc);
+        if (MODE != kLIST) {
+          acc_warp_total<F32>(ff, acc, cmb);
+          double r9[9];
+          acc_to_r9<MODE, F32, VIRIAL>(s, cmb, acc, r9);
+          if (lane == as) finish_atom<MODE>(s, i, r9);
+          if (lane == 0) {  // r9 is the same in every lane (a warp total)
+#pragma unroll
+            for (int q = 0; q < 9; ++q) s_red[wid][q] += r9[q];
+          }
+          acc_zero(ff, acc);
         }
       }
-      PairAcc a;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) a.f[k] = a.g[k] = 0.0;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) a.vir[k] = 0.0;
-      a.rho = a.e0 = a.e1 = 0.0;
-      int qc = 0, n_core = 0, n_shell = 0;
 
       auto flush = [&]() {
-        const int maxq = __reduce_max_sync(FULL, qc);
-        for (int q = 0; q < maxq; ++q) {
-          if (q < qc) {
-            int js = s_qj[wid][q][lane];
-            const bool core = js >= 0;
-            if (!core) js = ~js;
-            eval_pair<R, MODE, SPECIAL, VIRIAL>(s, i, ti, moli, qi, fpi, js, core, s_qr[wid][0][q][lane],
-                                                s_qr[wid][1][q][lane], s_qr[wid][2][q][lane], spi, spw, nsp,
-                                                (R)pice, a);
+        const int qa = __shfl_sync(FULL, qc, a);
+        const int maxq = __reduce_max_sync(FULL, member ? qa : 0);
+        const int rounds = (maxq + k - 1) / k;
+        if (F32) {
+          // software pipelined: round t + 1's entry, position and metadata are loaded before
+          // round t is evaluated
+          int e_n = 0;
+          float4 pj_n = make_float4(0.f, 0.f, 0.f, 0.f);
+          int4 mj_n = make_int4(0, 0, 0, 0);
+          bool v_n = member && m < qa;
+          if (v_n) {
+            const int h = s_q[wid][m][a];
+            e_n = s_hist[wid][(h >> 5) & (kTileHist - 1)][h & 31] | (int)((unsigned)(h & 0x8000) << 16);
+            pj_n = __ldg(&s.sxf[e_n & kJsMask]);
+            mj_n = __ldg(&s.smeta[e_n & kJsMask]);
+          }
+          for (int t = 0; t < rounds; ++t) {
+            const int e = e_n;
+            const float4 pj = pj_n;
+            const int4 mj = mj_n;
+            const bool v = v_n;
+            const int q2 = (t + 1) * k + m;
+            v_n = member && q2 < qa;
+            if (v_n) {
+              const int h = s_q[wid][q2][a];
+              e_n = s_hist[wid][(h >> 5) & (kTileHist - 1)][h & 31] | (int)((unsigned)(h & 0x8000) << 16);
+              pj_n = __ldg(&s.sxf[e_n & kJsMask]);
+              mj_n = __ldg(&s.smeta[e_n & kJsMask]);
+            }
+            if (v) {
+              const float rx = (pj.x - (float)s_shift[0][(e >> kJsBits) & 3]) - (float)pix;
+              const float ry = (pj.y - (float)s_shift[1][(e >> (kJsBits + 2)) & 3]) - (float)piy;
+              const float rz = (pj.z - (float)s_shift[2][(e >> (kJsBits + 4)) & 3]) - (float)piz;
+              float w = 1.0f;
+              if (SPECIAL) {
+                if (nsp <= kTileSp) {
+                  for (int t2 = 0; t2 < nsp; ++t2)
+                    if (s_spi[wid][t2][a] == mj.x) w = s_spw[wid][t2][a];
+                } else {
+                  for (int t2 = 0; t2 < nsp; ++t2)
+                    if (spi[t2] == mj.x) w = (float)spw[t2];
+                }
+              }
+              eval_pair_f32_pre<MODE, false>(moli, (float)qi, e >= 0, rx, ry, rz, ti, mj.y, mj.z, pj.w, w, spice, frc2,
+                                      frs2, fsa, falpha, s_tab, ntypes, fLx, fLy, fLz, ff[0], ff[1], ff[2], ff[3],
+                                      ff[4], ff[5], SPECIAL);
+            }
+          }
+          qc = 0;
+          nh = 0;
+          __syncwarp();
+          return;
+        }
+        for (int t = 0; t < rounds; ++t) {
+          const int q = t * k + m;
+          if (member && q < qa) {
+            const int h = s_q[wid][q][a];
+            const int e = s_hist[wid][(h >> 5) & (kTileHist - 1)][h & 31] | (int)((unsigned)(h & 0x8000) << 16);
+            const int js = e & kJsMask;
+            const bool core = e >= 0;
+            const R4 pj = load_sorted<R>(s, js);
+            const R rx = (pj.x - s_shift[0][(e >> kJsBits) & 3]) - pix;
+            const R ry = (pj.y - s_shift[1][(e >> (kJsBits + 2)) & 3]) - piy;
+            const R rz = (pj.z - s_shift[2][(e >> (kJsBits + 4)) & 3]) - piz;
+            if (F32)
+              eval_pair_f32<MODE, SPECIAL>(s, moli, (float)qi, js, core, (float)rx, (float)ry, (float)rz, ti, spi,
+                                           spw, nsp, spice, frc2, frs2, fsa, falpha, s_tab, ntypes, fLx, fLy,
+                                           fLz, ff[0], ff[1], ff[2], ff[3], ff[4], ff[5]);
+            else
+              eval_pair<R, MODE, SPECIAL, VIRIAL>(s, i, ti, moli, qi, fpi, js, core, rx, ry, rz, spi, spw, nsp,
+                                                  (R)pice, acc);
           }
         }
         qc = 0;
+        nh = 0;
+        __syncwarp();
       };
 
-      for (int da = -nc; da <= nc; ++da) {
-        const int n0 = hx + da, w0 = pmod(n0, dx);
-        const R ox = (R)(s.d[0] * (double)(w0 - n0));
-        for (int db = -nc; db <= nc; ++db) {
-          const int n1 = hy + db, w1 = pmod(n1, dy);
-          const R oy = (R)(s.d[1] * (double)(w1 - n1));
-          int de = -nc;
-          while (de <= nc) {
-            const int n2 = hz + de, w2 = pmod(n2, dz);
-            int len = 1;
-            while (de + len <= nc && w2 + len < dz) ++len;  // consecutive cells, same z offset
-            const R oz = (R)(s.d[2] * (double)(w2 - n2));
-            const int c0 = w2 + dz * (w1 + dy * w0);
-            const int cs = __ldg(&s.cell_start[c0]), ce = __ldg(&s.cell_start[c0 + len]);
-            for (int k0 = cs; k0 < ce; k0 += 32) {
-              const int kk = k0 + lane;
-              if (kk < ce) {
-                const R4 pj = load_sorted<R>(s, kk);
-                R4 c;
-                c.x = pj.x - ox;
-                c.y = pj.y - oy;
-                c.z = pj.z - oz;
-                c.w = R(0);
-                s_c[wid][lane] = c;
-                s_cj[wid][lane] = kk;
-              }
-              __syncwarp();
-              const int nk = min(32, ce - k0);
-              for (int k = 0; k < nk; ++k) {
-                if (act) {
-                  const R4 c = s_c[wid][k];
-                  const R rx = c.x - pix, ry = c.y - piy, rz = c.z - piz;
-                  const R d2 = add_rn(add_rn(mul_rn(rx, rx), mul_rn(ry, ry)), mul_rn(rz, rz));
-                  bool core, sel;
-                  if (rbl) {
-                    const bool shell = (rc2 - d2 > R(0.0001) && d2 - rs2 > R(0.0001));
-                    core = !shell && (rs2 - d2 > R(0.0001) && d2 > R(0.0001));
-                    sel = core;
-                    if (shell) {
-                      sel = (nmod == 0);
-                      nmod = (nmod + 1 == pice) ? 0 : nmod + 1;
-                    }
-                  } else {
-                    core = (rc2 - d2 > R(0.0001) && d2 > R(0.0001));
-                    sel = core;
-                  }
-                  if (sel) {
-                    const int js = s_cj[wid][k];
-                    if (MODE == kLIST) {
-                      const int id = __ldg(&s.smeta[js]).x;
-                      if (core) {
-                        if (n_core < cap) out_core[(size_t)i * cap + n_core] = id;
-                        ++n_core;
-                      } else {
-                        if (n_shell < cap) out_shell[(size_t)i * cap + n_shell] = id;
-                        ++n_shell;
-                      }
-                    } else {
-                      s_qj[wid][qc][lane] = core ? js : ~js;
-                      s_qr[wid][0][qc][lane] = rx;
-                      s_qr[wid][1][qc][lane] = ry;
-                      s_qr[wid][2][qc][lane] = rz;
-                      ++qc;
-                    }
-                  }
-                }
-                if (MODE != kLIST && __any_sync(FULL, qc == Q)) flush();
-              }
-              __syncwarp();
-            }
-            de += len;
+      // ---- the home cell's candidate sequence, traversal rows in groups of 32 (one per lane)
+      for (int r0 = 0; r0 < nrows; r0 += 32) {
+        const int r = r0 + lane;
+        int nseg = 0, cnt = 0, sa0 = 0, sa1 = 0, n0c = 0, n1c = 0, code0 = 0, code1 = 0;
+        if (r < nrows) {
+          const int da = r / side - nc, db = r % side - nc;
+          const int n0 = hx + da, n1 = hy + db;  // the home cell is inside the grid and nc < dims
+          const int w0 = n0 < 0 ? n0 + dx : (n0 >= dx ? n0 - dx : n0);
+          const int w1 = n1 < 0 ? n1 + dy : (n1 >= dy ? n1 - dy : n1);
+          const int t0 = n0 < 0 ? 2 : (n0 >= dx ? 0 : 1), t1 = n1 < 0 ? 2 : (n1 >= dy ? 0 : 1);
+          const int cxy = (t0 << kJsBits) | (t1 << (kJsBits + 2));
+          const int base = dz * (w1 + dy * w0);
+          // unwrapped z cells hz - nc .. hz + nc: one range, or two around the periodic wrap
+          const int z0 = hz - nc;
+          const int zw = z0 < 0 ? z0 + dz : z0;
+          const int tz = z0 < 0 ? 2 : 1;
+          sa0 = __ldg(&s.cell_start[base + zw]);
+          code0 = cxy | (tz << (kJsBits + 4));
+          if (zw + side <= dz) {
+            n0c = __ldg(&s.cell_start[base + zw + side]) - sa0;
+            nseg = 1;
+          } else {
+            n0c = __ldg(&s.cell_start[base + dz]) - sa0;
+            sa1 = __ldg(&s.cell_start[base]);
+            n1c = __ldg(&s.cell_start[base + zw + side - dz]) - sa1;
+            code1 = cxy | ((tz - 1) << (kJsBits + 4));
+            nseg = 2;
+          }
+          cnt = n0c + (nseg == 2 ? n1c : 0);
+        }
+        const int seg_incl = warp_incl_scan(nseg, lane);
+        const int cnt_incl = warp_incl_scan(cnt, lane);
+        const int total = __shfl_sync(FULL, cnt_incl, 31);
+        {
+          const int slot = seg_incl - nseg, beg = cnt_incl - cnt;
+          if (nseg >= 1) {
+            s_sa[wid][slot] = sa0;
+            s_sb[wid][slot] = beg;
+            s_se[wid][slot] = beg + n0c;
+            s_code[wid][slot] = code0;
+          }
+          if (nseg == 2) {
+            s_sa[wid][slot + 1] = sa1;
+            s_sb[wid][slot + 1] = beg + n0c;
+            s_se[wid][slot + 1] = beg + n0c + n1c;
+            s_code[wid][slot + 1] = code1;
           }
         }
+        __syncwarp();
+        // candidate p of the flattened sequence: the load of batch b + 1 is issued before batch b
+        // is classified
+        int seg = 0, ent_n = 0;
+        bool val_n = false;
+        R4 pj_n;
+        pj_n.x = pj_n.y = pj_n.z = pj_n.w = R(0);
+        auto fetch = [&](int p) {
+          val_n = p < total;
+          if (val_n) {
+            while (p >= s_se[wid][seg]) ++seg;
+            const int js = s_sa[wid][seg] + (p - s_sb[wid][seg]);
+            ent_n = js | s_code[wid][seg];
+            pj_n = load_sorted<R>(s, js);
+          }
+        };
+        fetch(lane);
+        for (int base = 0; base < total; base += 32) {
+          const R4 pj = pj_n;
+          const int ent = ent_n;
+          const bool val = val_n;
+          if (base + 32 < total) fetch(base + 32 + lane);
+          R cx = far, cy = far, cz = far;
+          if (val) {
+            cx = pj.x - s_shift[0][(ent >> kJsBits) & 3];
+            cy = pj.y - s_shift[1][(ent >> (kJsBits + 2)) & 3];
+            cz = pj.z - s_shift[2][(ent >> (kJsBits + 4)) & 3];
+          }
+          s_hist[wid][nh][lane] = val ? ent : 0;
+          // every atom of the chunk against the batch: two ballots each, kept by the atom's lane
+          unsigned my_cm = 0u, my_sm = 0u;
+          for (int ii = 0; ii < nat; ++ii) {
+            const R4 q = s_pi[wid][ii];
+            const R rx = cx - q.x, ry = cy - q.y, rz = cz - q.z;
+            const R dd = add_rn(add_rn(mul_rn(rx, rx), mul_rn(ry, ry)), mul_rn(rz, rz));
+            const bool shell = rbl && dd >= t_rs_hi && dd <= t_rc;
+            const bool core = rbl ? (dd <= t_rs_lo && dd > R(0.0001)) : (dd <= t_rc && dd > R(0.0001));
+            const unsigned cm = __ballot_sync(FULL, core);
+            const unsigned sm = rbl ? __ballot_sync(FULL, shell) : 0u;
+            if (lane == ii) {
+              my_cm = cm;
+              my_sm = sm;
+            }
+          }
+          if (!owner || stray) my_cm = my_sm = 0u;
+          // picks among this atom's shells (every pice-th in traversal order, after `skip` more),
+          // by a predicated walk over the set bits: no data-dependent branches
+          unsigned pk = my_sm;
+          if (rbl && pice > 1) {
+            unsigned x = my_sm;
+            int c = skip;
+            pk = 0u;
+            const int steps = __reduce_max_sync(FULL, __popc(x));
+            for (int t = 0; t < steps; ++t) {
+              const unsigned low = x & (0u - x);
+              pk |= (c == 0) ? low : 0u;
+              c = (low == 0u) ? c : (c == 0 ? pice - 1 : c - 1);
+              x ^= low;
+            }
+            skip = c;
+          }
+          // the selected pairs, in traversal order, into the atom's queue
+          unsigned sel = my_cm | pk;
+          const int steps2 = __reduce_max_sync(FULL, __popc(sel));
+          for (int t = 0; t < steps2; ++t) {
+            const unsigned low = sel & (0u - sel);
+            sel ^= low;
+            if (low) {
+              const int b = 31 - __clz(low);
+              const bool sh = (pk & low) != 0u;
+              if (MODE == kLIST) {
+                const int id = __ldg(&s.smeta[s_hist[wid][nh][b] & kJsMask]).x;
+                if (!sh) {
+                  if (n_core < cap) out_core[(size_t)i * cap + n_core] = id;
+                  ++n_core;
+                } else {
+                  if (n_shell < cap) out_shell[(size_t)i * cap + n_shell] = id;
+                  ++n_shell;
+                }
+              } else {
+                s_q[wid][qc][lane] = (unsigned short)(((nh << 5) | b) | (sh ? 0x8000 : 0));
+                ++qc;
+              }
+            }
+          }
+          __syncwarp();  // the history and the queues are read before they are written again
+          ++nh;
+          if (QUEUE) {
+            if (__any_sync(FULL, qc > kTileQ - 32) || nh == kTileHist) flush();
+          } else if (nh == kTileHist) {
+            nh = 0;
+          }
+        }
+        __syncwarp();  // segment table reused by the next row group
       }
+
       if (MODE == kLIST) {
-        if (act) {
+        if (owner && !stray) {
           out_nc[i] = n_core;
           out_ns[i] = n_shell;
         }
         continue;
       }
       flush();
-      if (act) {
-        double r9[9];
-        r9[0] = a.f[0];
-        r9[1] = a.f[1];
-        r9[2] = a.f[2];
-        if (MODE == kCOUL_RBL) {
-          r9[0] = r9[0] + s.qqr2e * a.g[0];
-          r9[1] = r9[1] + s.qqr2e * a.g[1];
-          r9[2] = r9[2] + s.qqr2e * a.g[2];
-        }
-#pragma unroll
-        for (int k = 0; k < 6; ++k) r9[3 + k] = VIRIAL ? a.vir[k] : 0.0;
-        if (MODE == kEAM_RHO || MODE == kEAM_ENERGY) {
-          const double rho = a.rho;
-          double p = rho * (1.0 / s.eam_drho) + 1.0;
-          int m = (int)p;
-          m = max(1, min(m, s.eam_nrho - 1));
-          p -= m;
-          p = fmin(p, 1.0);
-          const double* c = s.frho_s + 7 * m;
-          if (MODE == kEAM_RHO) {
-            s.eam_fp[i] = (c[0] * p + c[1]) * p + c[2];
-          } else {
-            const double fpv = (c[0] * p + c[1]) * p + c[2];
-            double phi = ((c[3] * p + c[4]) * p + c[5]) * p + c[6];
-            if (rho > s.eam_rhomax) phi += fpv * (rho - s.eam_rhomax);
-            r9[0] = phi;
-            r9[1] = a.e1;
-          }
-        } else if (MODE == kENERGY) {
-          r9[0] = a.e0;
-          r9[1] = a.e1;
-        } else {
-          s.f[i] = make_double4(r9[0], r9[1], r9[2], 0.0);
-        }
-#pragma unroll
-        for (int k = 0; k < 9; ++k) red[k] += r9[k];
-      }
+      acc_combine<F32>(ff, acc, cmb, k, nat);
+      double r9[9];
+      acc_to_r9<MODE, F32, VIRIAL>(s, cmb, acc, r9);
+      if (owner && !stray) finish_atom<MODE>(s, i, r9);
+      add_red(r9, owner && !stray);
     }
   }
   if (MODE == kLIST || MODE == kEAM_RHO) return;
@@ -1148,11 +1563,6 @@ k_pair_cells(const SysDev* __restrict__ S, const int2* __restrict__ work, int ca
                          MODE == kEAM_ENERGY || VIRIAL ||
                          (MODE == kEAM_FORCE && s.neigh == RBMD_NEIGH_RBL));
   if (!need_red) return;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    const double w = warp_sum(red[k]);
-    if (lane == 0) s_red[wid][k] = w;
-  }
   __syncthreads();
   const int blk = wk.y / kCellWarps;
   if (threadIdx.x < 9) {
@@ -1180,8 +1590,8 @@ k_pair_cells(const SysDev* __restrict__ S, const int2* __restrict__ work, int ca
 template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
 static void go(const Batch& b, cudaStream_t st) {
   if (b.dense)
-    k_pair_cells<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kCellWarps * 32, 0, st>>>(b.sys, b.pair.d, 0, nullptr,
-                                                                                nullptr, nullptr, nullptr);
+    k_pair_tile<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kCellWarps * 32, 0, st>>>(b.sys, b.pair.d, 0, nullptr,
+                                                                               nullptr, nullptr, nullptr);
   else if (b.lean)
     k_pair2<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kPairWarps * 32, 0, st>>>(b.sys, b.pair.d);
   else
@@ -1243,7 +1653,7 @@ void launch_rbl_lists(const SysDev* sys, int slot, int n, int ncell, int dense, 
   for (int k = 0; k < nb; ++k) h[k] = make_int2(slot, k * per);
   cudaMemcpyAsync(d_work, h, sizeof(int2) * nb, cudaMemcpyHostToDevice, st);
   if (dense)
-    k_pair_cells<double, kLIST, false, false><<<nb, kCellWarps * 32, 0, st>>>(sys, d_work, cap, n_core, n_shell,
+    k_pair_tile<double, kLIST, false, false><<<nb, kCellWarps * 32, 0, st>>>(sys, d_work, cap, n_core, n_shell,
                                                                              ids, ids + (size_t)n * cap);
   else
     k_pair<double, kLIST, false, false><<<nb, kPairWarps * 32, 0, st>>>(sys, d_work, cap, n_core, n_shell,
@@ -1363,7 +1773,7 @@ int launch_rbl_lists_static(const SysDev* sys, int slot, int n, int ncell, int d
   b.cell.n = nc;
   launch_cells(b, st);
   if (dense)
-    k_pair_cells<double, kLIST, false, false><<<np, kCellWarps * 32, 0, st>>>(sys, w_pair, cap, out->n_core,
+    k_pair_tile<double, kLIST, false, false><<<np, kCellWarps * 32, 0, st>>>(sys, w_pair, cap, out->n_core,
                                                                              out->n_shell, out->rows, shell_rows);
   else
     k_pair<double, kLIST, false, false><<<np, kPairWarps * 32, 0, st>>>(sys, w_pair, cap, out->n_core,

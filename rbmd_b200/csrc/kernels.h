@@ -25,6 +25,7 @@ struct Batch {
   int dense = 0;             // pair kernel: 1 = warp per home cell, 0 = warp per atom
   int lean = 0;              // warp per atom with segment tables (dims >= 2 nc + 1 everywhere)
   int max_P = 0;             // largest P (or Ewald nk) in the batch
+  long long natoms = 0;      // atoms over all systems of the batch
 };
 
 enum FinalMode { kFinalForceOnly = 0, kFinalKick = 1, kFinalInit = 2 };
@@ -65,7 +66,8 @@ long long static_list_ints(int n, int ncell, int dense, int cap);
 int launch_rbl_lists_static(const SysDev* sys, int slot, int n, int ncell, int dense, int cap, int* scratch,
                             cudaStream_t s, StaticLists* out);
 
-constexpr int kCellWarpsHost = 4;  // home cells per block of the dense pair kernel
+constexpr int kCellWarpsHost = 4;  // home cells per block of the tile pair kernel
+constexpr double kTileMinPerCell = 3.0;  // mean atoms per cell from which the tile kernel is used
 
 double fma_peak_tflops(int fp64, cudaStream_t s);
 

@@ -40,9 +40,9 @@ def eam_small(oracle_mod, **kw):
 
 
 def pair(ctx_factory, oracle_mod, sd, layout="auto", **ctxkw):
-    """GPU context + system and the oracle twin.  `layout` selects the pair kernel: "auto" (lean
-    segment-table traversal when the box allows it), "atom" (general warp-per-atom traversal),
-    "cell" (warp per home cell)."""
+    """GPU context + system and the oracle twin.  `layout` selects the pair kernel: "auto" (the
+    library's choice), "atom" (general warp-per-atom traversal), "lean" (warp per atom with segment
+    tables), "cell" (tile: warp per home cell, candidates shared by the cell's atoms)."""
     import os
     ctx = ctx_factory(**ctxkw)
     old = os.environ.get("RBMD_PAIR_LAYOUT")
@@ -58,7 +58,7 @@ def pair(ctx_factory, oracle_mod, sd, layout="auto", **ctxkw):
     return ctx, sid, o
 
 
-LAYOUTS = ["auto", "atom", "cell"]
+LAYOUTS = ["auto", "atom", "lean", "cell"]
 
 
 CASES = {
@@ -83,7 +83,7 @@ def test_cells_bit_exact(ctx_factory, oracle_mod, case):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("layout", ["auto", "cell"])
+@pytest.mark.parametrize("layout", ["lean", "cell"])
 @pytest.mark.parametrize("case,mode", [("lj_rbl", A.RBL_STRIDE), ("nacl_rbe_rbl", A.RBL_STRIDE),
                                        ("water_cvff_rbe_rbl", A.RBL_STRIDE),
                                        ("water_cvff_rbe_rbl", A.RBL_PHILOX), ("eam_rbl", A.RBL_STRIDE)])
@@ -185,8 +185,8 @@ def _push_outside(sd):
     return sd
 
 
-@pytest.mark.parametrize("layout", ["auto", "atom"])
-@pytest.mark.parametrize("case", ["lj_rbl", "nacl_rbe_rbl", "eam_rbl", "lj_verlet"])
+@pytest.mark.parametrize("layout", ["atom", "lean", "cell"])
+@pytest.mark.parametrize("case", ["lj_rbl", "nacl_rbe_rbl", "eam_rbl", "lj_verlet", "water_cvff_rbe_rbl"])
 def test_forces_atoms_outside_box(ctx_factory, oracle_mod, case, layout):
     sd = _push_outside(CASES[case](oracle_mod))
     sd.params.precision = A.PREC_FP64
@@ -198,11 +198,17 @@ def test_forces_atoms_outside_box(ctx_factory, oracle_mod, case, layout):
     assert ctx.thermo(sid)["status"] == 0
 
 
-def test_cell_layout_reports_atoms_outside_box(ctx_factory, oracle_mod):
-    sd = _push_outside(lj_small())
-    ctx, sid, _ = pair(ctx_factory, oracle_mod, sd, layout="cell")
-    ctx.compute_forces(sid)
-    assert ctx.thermo(sid)["status"] & A.STATUS_CELL_RANGE
+@pytest.mark.parametrize("layout", ["lean", "cell"])
+def test_rbl_lists_atoms_outside_box(ctx_factory, oracle_mod, layout):
+    sd = _push_outside(CASES["water_cvff_rbe_rbl"](oracle_mod))
+    sd.params.rbl_mode = A.RBL_PHILOX
+    ctx, sid, o = pair(ctx_factory, oracle_mod, sd, layout=layout)
+    gn, gs, gi = ctx.rbl_lists(sid, cap=1024)
+    on, os_, oi = o.rbl_lists(cap=1024)
+    assert np.array_equal(gn, on) and np.array_equal(gs, os_)
+    for i in range(sd.n):
+        k = gn[i] + gs[i]
+        assert np.array_equal(gi[i, :k], oi[i, :k]), f"atom {i}"
 
 
 @pytest.mark.parametrize("case", ["nacl_rbe_rbl", "water_cvff_rbe_rbl"])
