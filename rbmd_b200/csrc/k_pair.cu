@@ -934,6 +934,57 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
   }
 }
 
+// Hardware approximations (flush-to-zero) for the FP32 tile evaluation; every argument there is
+// a normal number (d2 > 1e-4, exponents in [-alpha rc2 log2 e, 0]).
+__device__ inline float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ inline float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ inline float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// FP32 force of one RBL pair as a single vector factor: LJ (cutoff rs for core pairs of the
+// Coulomb modes, rc for LJ/CUT, shell pairs x pice) plus qqr2e times the real-space Coulomb term
+// (erfc by Abramowitz & Stegun 7.1.26, |error| <= 1.5e-7), the same windows as eval_pair_f32_pre.
+// alpha_l2 = alpha log2(e), so exp(-alpha d2) = 2^(-alpha_l2 d2).
+template <int MODE>
+__device__ inline float tile_pair_f32(bool core, float d2, float qi, float qj, int tp, float w, float pice,
+                                      float rc2, float rs2, float sa, float alpha_l2, float qq, const float* tab,
+                                      bool special) {
+  const float clj = tab[2 * tp], s6 = tab[2 * tp + 1];
+  const float inv_r = rsqrt_approx(d2);
+  const float inv_d2 = inv_r * inv_r;
+  const float sd6 = s6 * inv_d2 * inv_d2 * inv_d2;
+  const float ljf = clj * (2.0f * sd6 - 1.0f) * sd6 * inv_d2;
+  float fl;
+  if (MODE == kLJ_RBL) {
+    fl = core ? ((d2 < rc2 && d2 > 0.0001f) ? ljf : 0.0f) : ((d2 < rc2 && d2 > rs2) ? pice * ljf : 0.0f);
+    return fl;
+  }
+  fl = core ? ((d2 < rs2 && d2 > 0.0001f) ? w * ljf : 0.0f) : ((d2 < rc2 && d2 > rs2) ? w * (pice * ljf) : 0.0f);
+  const bool in = core ? (d2 < rc2 && d2 > 0.0001f) : (special ? (d2 < rc2 && d2 > rs2) : (d2 < rc2 && d2 > 0.0001f));
+  float fc = 0.0f;
+  if (in) {
+    const float x = sa * (d2 * inv_r);
+    const float e = ex2_approx(-alpha_l2 * d2);
+    const float t = rcp_approx(1.0f + 0.3275911f * x);
+    const float erfc = t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f)))) * e;
+    const float g = erfc * inv_d2 + 1.1283791671f * sa * e * inv_r;  // 2/sqrt(pi)
+    fc = -qi * qj * g * inv_r;
+    if (!core) fc *= pice;
+  }
+  return fl + qq * fc;
+}
+
 // ------------------------------------------------------------------------------------------------
 // Tile variant (dense systems: many atoms per cell).  One warp per home cell.  Every atom of a
 // home cell walks the same candidate sequence -- the (2 nc + 1)^2 traversal rows of the home cell,
@@ -955,8 +1006,8 @@ constexpr int kCellWarps = 4;    // home cells per block (kCellWarpsHost on the 
 constexpr int kTileQ = 48;       // queued pairs per atom between evaluations (a batch adds <= 32)
 constexpr int kJsBits = 25;      // queue entry: sorted index | shift code << 25 | shell << 31
 constexpr int kJsMask = (1 << kJsBits) - 1;
-constexpr int kTileSp = 4;       // special partners per atom cached in shared memory
-constexpr int kTileHist = 16;    // batches of candidates kept for the queued pairs (power of 2)
+constexpr int kTileSp = 2;       // special partners per atom cached in shared memory (water: 2)
+constexpr int kTileHist = 6;     // batches of candidates kept for the queued pairs
 
 template <typename R> __device__ inline R cls_thr(const SysDev& s, int k);
 template <> __device__ inline double cls_thr<double>(const SysDev& s, int k) { return s.cls_d[k]; }
@@ -1193,8 +1244,17 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
   // bit 15 set for a shell pair
   __shared__ unsigned short s_q[kCellWarps][kTileQ][32];
   __shared__ R4 s_pi[kCellWarps][32];          // chunk atom positions (far away for box-outside atoms)
+  // FP32 path: per chunk atom its type, molecule, special count and first special slot; the
+  // concatenated-queue offsets; and its force accumulator
+  __shared__ int4 s_ainfo[kCellWarps][32];
+  __shared__ int s_off[kCellWarps][33];
+  __shared__ float s_acc[kCellWarps][32][3];
   __shared__ int s_hist[kCellWarps][kTileHist][32];  // packed candidates of the batches since the
                                                      // last evaluation; queue entries index it
+  // FP32 path: the same candidates' shifted positions, charges and (atom id | type << 25), so
+  // that the evaluation reads shared memory only
+  __shared__ float4 s_hp[kCellWarps][kTileHist][32];
+  __shared__ int s_hid[kCellWarps][kTileHist][32];
   __shared__ int s_sa[kCellWarps][64];         // segment first sorted index
   __shared__ int s_sb[kCellWarps][64];         // segment begin in the flattened sequence
   __shared__ int s_se[kCellWarps][64];         // segment end in the flattened sequence
@@ -1231,9 +1291,9 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
   const R t_rc = cls_thr<R>(s, 0), t_rs_hi = cls_thr<R>(s, 1), t_rs_lo = cls_thr<R>(s, 2);
   const R far = R(1e30);
   const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
-  const float spice = (float)pice, fsa = (float)sqrt(s.alpha), falpha = (float)s.alpha;
-  const float fLx = (float)s.L[0], fLy = (float)s.L[1], fLz = (float)s.L[2];
+  const float spice = (float)pice, fsa = (float)sqrt(s.alpha);
   const float frc2 = (float)s.rc2, frs2 = (float)s.rs2;
+  const float falpha_l2 = (float)(s.alpha * 1.4426950408889634), fqq = (float)s.qqr2e;  // alpha log2(e)
   if (lane < 9) s_red[wid][lane] = 0.0;  // per-warp reduction values, added in a fixed order
   // lane 0 adds the warp total of v (owner lanes' values, in lane order) to s_red[wid][k]
   auto add_red = [&](const double (&v)[9], bool take) {
@@ -1286,6 +1346,10 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
         R4 q = p4;
         if (stray) q.x = q.y = q.z = far;
         s_pi[wid][lane] = q;
+        if constexpr (F32) {
+          s_ainfo[wid][lane] = make_int4(ti, moli, nsp, SPECIAL ? s.sp_off[i] : 0);
+          s_acc[wid][lane][0] = s_acc[wid][lane][1] = s_acc[wid][lane][2] = 0.0f;
+        }
         if (SPECIAL && nsp <= kTileSp)
           for (int t = 0; t < nsp; ++t) {
             s_spi[wid][t][lane] = spi[t];
@@ -1324,74 +1388,89 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
         const int qa = __shfl_sync(FULL, qc, a);
         const int maxq = __reduce_max_sync(FULL, member ? qa : 0);
         const int rounds = (maxq + k - 1) / k;
-        if (F32) {
-          // software pipelined: round t + 1's entry, position and metadata are loaded before
-          // round t is evaluated
-          int e_n = 0;
-          float4 pj_n = make_float4(0.f, 0.f, 0.f, 0.f);
-          int4 mj_n = make_int4(0, 0, 0, 0);
-          bool v_n = member && m < qa;
-          if (v_n) {
-            const int h = s_q[wid][m][a];
-            e_n = s_hist[wid][(h >> 5) & (kTileHist - 1)][h & 31] | (int)((unsigned)(h & 0x8000) << 16);
-            pj_n = __ldg(&s.sxf[e_n & kJsMask]);
-            mj_n = __ldg(&s.smeta[e_n & kJsMask]);
-          }
-          for (int t = 0; t < rounds; ++t) {
-            const int e = e_n;
-            const float4 pj = pj_n;
-            const int4 mj = mj_n;
-            const bool v = v_n;
-            const int q2 = (t + 1) * k + m;
-            v_n = member && q2 < qa;
-            if (v_n) {
-              const int h = s_q[wid][q2][a];
-              e_n = s_hist[wid][(h >> 5) & (kTileHist - 1)][h & 31] | (int)((unsigned)(h & 0x8000) << 16);
-              pj_n = __ldg(&s.sxf[e_n & kJsMask]);
-              mj_n = __ldg(&s.smeta[e_n & kJsMask]);
-            }
+        if constexpr (F32) {
+          // all queues concatenated (atom a's entries at [s_off[a], s_off[a + 1])) and evaluated 32
+          // at a time with every lane busy; each round's per-atom runs are summed by a segmented
+          // warp scan and added to the atoms' accumulators by the runs' last lanes, so every
+          // atom's sum is formed in a fixed order
+          const int incl = warp_incl_scan(owner ? qc : 0, lane);
+          if (lane < nat) s_off[wid][lane + 1] = incl;
+          if (lane == 0) s_off[wid][0] = 0;
+          const int total = __shfl_sync(FULL, incl, 31);
+          __syncwarp();
+          int ca = 0;  // this lane's atom cursor (monotone over the rounds)
+          for (int e0 = 0; e0 < total; e0 += 32) {
+            const int e = e0 + lane;
+            const bool v = e < total;
+            float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+            int key = 32 + lane;  // never equal to an atom index
             if (v) {
-              const float rx = (pj.x - (float)s_shift[0][(e >> kJsBits) & 3]) - (float)pix;
-              const float ry = (pj.y - (float)s_shift[1][(e >> (kJsBits + 2)) & 3]) - (float)piy;
-              const float rz = (pj.z - (float)s_shift[2][(e >> (kJsBits + 4)) & 3]) - (float)piz;
+              while (e >= s_off[wid][ca + 1]) ++ca;
+              key = ca;
+              const unsigned h = s_q[wid][e - s_off[wid][ca]][ca];
+              const float4 pj = s_hp[wid][(h >> 5) & 0x3ff][h & 31];
+              const int idt = s_hid[wid][(h >> 5) & 0x3ff][h & 31];
+              const float4 pa = s_pi[wid][ca];
+              const int4 ai = s_ainfo[wid][ca];
+              const float rx = pj.x - pa.x, ry = pj.y - pa.y, rz = pj.z - pa.z;
+              const int idj = idt & kJsMask, tj = idt >> kJsBits;
               float w = 1.0f;
               if (SPECIAL) {
-                if (nsp <= kTileSp) {
-                  for (int t2 = 0; t2 < nsp; ++t2)
-                    if (s_spi[wid][t2][a] == mj.x) w = s_spw[wid][t2][a];
+                if (ai.z <= kTileSp) {
+                  for (int t2 = 0; t2 < ai.z; ++t2)
+                    if (s_spi[wid][t2][ca] == idj) w = s_spw[wid][t2][ca];
                 } else {
-                  for (int t2 = 0; t2 < nsp; ++t2)
-                    if (spi[t2] == mj.x) w = (float)spw[t2];
+                  for (int t2 = 0; t2 < ai.z; ++t2)
+                    if (__ldg(&s.sp_ids[ai.w + t2]) == idj) w = (float)__ldg(&s.sp_w[ai.w + t2]);
                 }
               }
-              eval_pair_f32_pre<MODE, false>(moli, (float)qi, e >= 0, rx, ry, rz, ti, mj.y, mj.z, pj.w, w, spice, frc2,
-                                      frs2, fsa, falpha, s_tab, ntypes, fLx, fLy, fLz, ff[0], ff[1], ff[2], ff[3],
-                                      ff[4], ff[5], SPECIAL);
+              bool skip_pair = false;
+              if constexpr (MODE == kLJ_RBL) {
+                const int ej = s_hist[wid][(h >> 5) & 0x3ff][h & 31];
+                skip_pair = ai.y == __ldg(&s.smeta[ej & kJsMask]).z;  // same molecule
+              }
+              if (!skip_pair) {
+                const float d2 = rx * rx + ry * ry + rz * rz;
+                const float f = tile_pair_f32<MODE>((h & 0x8000u) == 0u, d2, pa.w, pj.w, ai.x * ntypes + tj, w, spice,
+                                                    frc2, frs2, fsa, falpha_l2, fqq, s_tab, SPECIAL);
+                fx = f * rx;
+                fy = f * ry;
+                fz = f * rz;
+              }
+            }
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+              const float tx = __shfl_up_sync(FULL, fx, d), ty = __shfl_up_sync(FULL, fy, d);
+              const float tz = __shfl_up_sync(FULL, fz, d);
+              const int tk = __shfl_up_sync(FULL, key, d);
+              if (lane >= d && tk == key) {
+                fx += tx;
+                fy += ty;
+                fz += tz;
+              }
+            }
+            const int nk = __shfl_down_sync(FULL, key, 1);
+            if (v && (lane == 31 || nk != key)) {
+              s_acc[wid][key][0] += fx;
+              s_acc[wid][key][1] += fy;
+              s_acc[wid][key][2] += fz;
             }
           }
-          qc = 0;
-          nh = 0;
-          __syncwarp();
-          return;
-        }
-        for (int t = 0; t < rounds; ++t) {
-          const int q = t * k + m;
-          if (member && q < qa) {
-            const int h = s_q[wid][q][a];
-            const int e = s_hist[wid][(h >> 5) & (kTileHist - 1)][h & 31] | (int)((unsigned)(h & 0x8000) << 16);
-            const int js = e & kJsMask;
-            const bool core = e >= 0;
-            const R4 pj = load_sorted<R>(s, js);
-            const R rx = (pj.x - s_shift[0][(e >> kJsBits) & 3]) - pix;
-            const R ry = (pj.y - s_shift[1][(e >> (kJsBits + 2)) & 3]) - piy;
-            const R rz = (pj.z - s_shift[2][(e >> (kJsBits + 4)) & 3]) - piz;
-            if (F32)
-              eval_pair_f32<MODE, SPECIAL>(s, moli, (float)qi, js, core, (float)rx, (float)ry, (float)rz, ti, spi,
-                                           spw, nsp, spice, frc2, frs2, fsa, falpha, s_tab, ntypes, fLx, fLy,
-                                           fLz, ff[0], ff[1], ff[2], ff[3], ff[4], ff[5]);
-            else
+        } else {
+          for (int t = 0; t < rounds; ++t) {
+            const int q = t * k + m;
+            if (member && q < qa) {
+              const int h = s_q[wid][q][a];
+              const int e = s_hist[wid][(h >> 5) & 0x3ff][h & 31] | (int)((unsigned)(h & 0x8000) << 16);
+              const int js = e & kJsMask;
+              const bool core = e >= 0;
+              const R4 pj = load_sorted<R>(s, js);
+              const R rx = (pj.x - s_shift[0][(e >> kJsBits) & 3]) - pix;
+              const R ry = (pj.y - s_shift[1][(e >> (kJsBits + 2)) & 3]) - piy;
+              const R rz = (pj.z - s_shift[2][(e >> (kJsBits + 4)) & 3]) - piz;
               eval_pair<R, MODE, SPECIAL, VIRIAL>(s, i, ti, moli, qi, fpi, js, core, rx, ry, rz, spi, spw, nsp,
                                                   (R)pice, acc);
+            }
           }
         }
         qc = 0;
@@ -1450,7 +1529,7 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
         __syncwarp();
         // candidate p of the flattened sequence: the load of batch b + 1 is issued before batch b
         // is classified
-        int seg = 0, ent_n = 0;
+        int seg = 0, ent_n = 0, idt_n = 0;
         bool val_n = false;
         R4 pj_n;
         pj_n.x = pj_n.y = pj_n.z = pj_n.w = R(0);
@@ -1461,12 +1540,16 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
             const int js = s_sa[wid][seg] + (p - s_sb[wid][seg]);
             ent_n = js | s_code[wid][seg];
             pj_n = load_sorted<R>(s, js);
+            if (F32) {
+              const int4 mj = __ldg(&s.smeta[js]);
+              idt_n = mj.x | (mj.y << kJsBits);
+            }
           }
         };
         fetch(lane);
         for (int base = 0; base < total; base += 32) {
           const R4 pj = pj_n;
-          const int ent = ent_n;
+          const int ent = ent_n, idt = idt_n;
           const bool val = val_n;
           if (base + 32 < total) fetch(base + 32 + lane);
           R cx = far, cy = far, cz = far;
@@ -1475,7 +1558,11 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
             cy = pj.y - s_shift[1][(ent >> (kJsBits + 2)) & 3];
             cz = pj.z - s_shift[2][(ent >> (kJsBits + 4)) & 3];
           }
-          s_hist[wid][nh][lane] = val ? ent : 0;
+          if constexpr (!F32 || MODE == kLJ_RBL) s_hist[wid][nh][lane] = val ? ent : 0;
+          if (F32) {
+            s_hp[wid][nh][lane] = make_float4((float)cx, (float)cy, (float)cz, (float)pj.w);
+            s_hid[wid][nh][lane] = idt;
+          }
           // every atom of the chunk against the batch: two ballots each, kept by the atom's lane
           unsigned my_cm = 0u, my_sm = 0u;
           for (int ii = 0; ii < nat; ++ii) {
@@ -1517,7 +1604,7 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
             if (low) {
               const int b = 31 - __clz(low);
               const bool sh = (pk & low) != 0u;
-              if (MODE == kLIST) {
+              if constexpr (MODE == kLIST) {
                 const int id = __ldg(&s.smeta[s_hist[wid][nh][b] & kJsMask]).x;
                 if (!sh) {
                   if (n_core < cap) out_core[(size_t)i * cap + n_core] = id;
@@ -1551,9 +1638,19 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
         continue;
       }
       flush();
-      acc_combine<F32>(ff, acc, cmb, k, nat);
       double r9[9];
-      acc_to_r9<MODE, F32, VIRIAL>(s, cmb, acc, r9);
+      if constexpr (F32) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) r9[q] = 0.0;
+        if (owner) {  // Coulomb already scaled by qqr2e inside the pair factor
+          r9[0] = (double)s_acc[wid][lane][0];
+          r9[1] = (double)s_acc[wid][lane][1];
+          r9[2] = (double)s_acc[wid][lane][2];
+        }
+      } else {
+        acc_combine<F32>(ff, acc, cmb, k, nat);
+        acc_to_r9<MODE, F32, VIRIAL>(s, cmb, acc, r9);
+      }
       if (owner && !stray) finish_atom<MODE>(s, i, r9);
       add_red(r9, owner && !stray);
     }
