@@ -317,7 +317,8 @@ typedef struct rbmd_eam_file {
   const double* zr;     /* [nr] */
   const double* rhor;   /* [nr] */
 } rbmd_eam_file;
-/* Number of rows the spline arrays need: (nrho+1) and (nr+1). */
+/* nrho and nr of the resampled tables; the spline arrays of rbmd_eam_build_splines then need
+ * (nrho + 1) * 7 and (nr + 1) * 7 doubles (row 0 unused). */
 int rbmd_eam_spline_sizes(const rbmd_eam_file* in, int32_t* nrho_out, int32_t* nr_out);
 /* file2array + array2spline (framework/run/ExecutionNVT.cpp:933-1079): fills the three Vec7
  * tables (caller allocates (nrho+1)*7, (nr+1)*7, (nr+1)*7 doubles) and rhomax. */

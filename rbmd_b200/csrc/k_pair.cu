@@ -1013,6 +1013,12 @@ template <typename R> __device__ inline R cls_thr(const SysDev& s, int k);
 template <> __device__ inline double cls_thr<double>(const SysDev& s, int k) { return s.cls_d[k]; }
 template <> __device__ inline float cls_thr<float>(const SysDev& s, int k) { return s.cls_f[k]; }
 
+// Squared distance of the tile kernel: FP64 with every product and sum rounded separately (the
+// oracle's order); FP32 as two fused multiply-adds, the same expression in classification and
+// evaluation so that both see the same value.
+__device__ inline double tile_d2(double x, double y, double z) { return add_rn(add_rn(mul_rn(x, x), mul_rn(y, y)), mul_rn(z, z)); }
+__device__ inline float tile_d2(float x, float y, float z) { return __fmaf_rn(z, z, __fmaf_rn(y, y, __fmul_rn(x, x))); }
+
 // Picked shells of one batch: the set bits of sm at ranks r, r + pice, ... where r is the number
 // of shells still to skip; r leaves as the skip count for the next batch.
 __device__ inline unsigned pick_shells(unsigned sm, int pice, int& r) {
@@ -1196,7 +1202,7 @@ __device__ void tile_stray(const SysDev& s, int si, int skip, int pice, bool rbl
             ry = (pj.y - oy) - p4.y;
             rz = (pj.z - oz) - p4.z;
           }
-          const R dd = add_rn(add_rn(mul_rn(rx, rx), mul_rn(ry, ry)), mul_rn(rz, rz));
+          const R dd = tile_d2(rx, ry, rz);
           const bool shell = rbl && dd >= t_rs_hi && dd <= t_rc;
           const bool core = rbl ? (dd <= t_rs_lo && dd > R(0.0001)) : (dd <= t_rc && dd > R(0.0001));
           const unsigned cm = __ballot_sync(FULL, core), sm = __ballot_sync(FULL, shell);
@@ -1430,7 +1436,7 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
                 skip_pair = ai.y == __ldg(&s.smeta[ej & kJsMask]).z;  // same molecule
               }
               if (!skip_pair) {
-                const float d2 = rx * rx + ry * ry + rz * rz;
+                const float d2 = tile_d2(rx, ry, rz);
                 const float f = tile_pair_f32<MODE>((h & 0x8000u) == 0u, d2, pa.w, pj.w, ai.x * ntypes + tj, w, spice,
                                                     frc2, frs2, fsa, falpha_l2, fqq, s_tab, SPECIAL);
                 fx = f * rx;
@@ -1568,7 +1574,7 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
           for (int ii = 0; ii < nat; ++ii) {
             const R4 q = s_pi[wid][ii];
             const R rx = cx - q.x, ry = cy - q.y, rz = cz - q.z;
-            const R dd = add_rn(add_rn(mul_rn(rx, rx), mul_rn(ry, ry)), mul_rn(rz, rz));
+            const R dd = tile_d2(rx, ry, rz);
             const bool shell = rbl && dd >= t_rs_hi && dd <= t_rc;
             const bool core = rbl ? (dd <= t_rs_lo && dd > R(0.0001)) : (dd <= t_rc && dd > R(0.0001));
             const unsigned cm = __ballot_sync(FULL, core);

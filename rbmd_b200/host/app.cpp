@@ -1,0 +1,573 @@
+// app.cpp -- the `rbmd` host (see app.hpp).
+#include "app.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <random>
+#include <stdexcept>
+
+namespace rbmd_host {
+
+namespace {
+
+const double kPi = 3.14159265358979323846;
+
+std::string dir_of(const std::string& path) {
+  const size_t k = path.find_last_of('/');
+  return k == std::string::npos ? std::string(".") : path.substr(0, k);
+}
+
+bool exists(const std::string& p) { return std::ifstream(p).good(); }
+
+// Gaussian velocities as the reference draws them (ModelFileInitCondition::Velocity, :605-655;
+// MeshFreeCondition::InitMassAndVelocity): three Box-Muller normals per atom scaled by sigma.
+// The stream is a seeded mt19937_64 where the reference takes std::random_device.
+void gauss_velocities(Para& p, const std::vector<double>& sigma_of_atom) {
+  std::mt19937_64 g(p.params.seed);
+  std::uniform_real_distribution<double> u(0.0, 1.0);
+  p.velocity.assign(3 * (size_t)p.n, 0.0);
+  for (int i = 0; i < p.n; ++i)
+    for (int k = 0; k < 3; ++k) {
+      double u1 = u(g);
+      while (u1 <= 0.0) u1 = u(g);
+      const double u2 = u(g);
+      p.velocity[3 * (size_t)i + k] = std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * kPi * u2) * sigma_of_atom[i];
+    }
+}
+
+int units_of(const std::string& u) {
+  if (u == "LJ") return RBMD_UNITS_LJ;
+  if (u == "REAL") return RBMD_UNITS_REAL;
+  if (u == "METAL") return RBMD_UNITS_METAL;
+  throw std::runtime_error("unit must be LJ, REAL or METAL, not \"" + u + "\"");
+}
+
+}  // namespace
+
+rbmd_system_desc Para::desc() const {
+  rbmd_system_desc d;
+  std::memset(&d, 0, sizeof(d));
+  d.n_atoms = n;
+  d.n_types = n_types;
+  for (int k = 0; k < 3; ++k) {
+    d.box_lo[k] = lo[k];
+    d.box_hi[k] = hi[k];
+  }
+  d.position = position.data();
+  d.velocity = velocity.empty() ? nullptr : velocity.data();
+  d.charge = charge.empty() ? nullptr : charge.data();
+  d.mass = mass.data();
+  d.type = type.data();
+  d.molecule = molecule.empty() ? nullptr : molecule.data();
+  d.epsilon = eps.data();
+  d.sigma = sigma.data();
+  d.n_bonds = (int32_t)bond_type.size();
+  d.n_bond_types = (int32_t)bond_k.size();
+  d.bond_atoms = bond_atoms.empty() ? nullptr : bond_atoms.data();
+  d.bond_type = bond_type.empty() ? nullptr : bond_type.data();
+  d.bond_k = bond_k.empty() ? nullptr : bond_k.data();
+  d.bond_r0 = bond_r0.empty() ? nullptr : bond_r0.data();
+  d.n_angles = (int32_t)angle_type.size();
+  d.n_angle_types = (int32_t)angle_k.size();
+  d.angle_atoms = angle_atoms.empty() ? nullptr : angle_atoms.data();
+  d.angle_type = angle_type.empty() ? nullptr : angle_type.data();
+  d.angle_k = angle_k.empty() ? nullptr : angle_k.data();
+  d.angle_theta0 = angle_theta0.empty() ? nullptr : angle_theta0.data();
+  if (!sp_off.empty()) {
+    d.special_offsets = sp_off.data();
+    d.special_ids = sp_ids.data();
+    d.special_weights = sp_w.data();
+  }
+  d.eam_nrho = eam_nrho;
+  d.eam_nr = eam_nr;
+  d.eam_drho = eam_drho;
+  d.eam_dr = eam_dr;
+  d.eam_rhomax = eam_rhomax;
+  d.eam_cut = eam_cut;
+  d.eam_frho_spline = frho_spline.empty() ? nullptr : frho_spline.data();
+  d.eam_rhor_spline = rhor_spline.empty() ? nullptr : rhor_spline.data();
+  d.eam_z2r_spline = z2r_spline.empty() ? nullptr : z2r_spline.data();
+  return d;
+}
+
+// ------------------------------------------------------------------------------------------ init
+ModelFileInitCondition::ModelFileInitCondition(const Json& cfg, const std::string& base_dir) {
+  _file = cfg.string("file", "");
+  if (_file.empty()) throw std::runtime_error("read_data needs \"file\"");
+  if (!exists(_file) && exists(base_dir + "/" + _file)) _file = base_dir + "/" + _file;
+  _atom_style = cfg.string("atom_style", "atomic");
+  _velocity_type = cfg.string("velocity_type", "GAUSS");
+}
+
+void ModelFileInitCondition::Execute(Para& p) {
+  const DataFile d = read_data_file(_file, _atom_style, p.unit);
+  p.init_way = "read_data";
+  p.n = d.n_atoms;
+  p.n_types = d.n_types;
+  for (int k = 0; k < 3; ++k) {
+    p.lo[k] = d.lo[k];
+    p.hi[k] = d.hi[k];
+  }
+  p.position = d.position;
+  p.charge = d.charge;
+  p.type = d.type;
+  p.molecule = d.molecule;
+  p.eps = d.type_eps;
+  p.sigma = d.type_sigma;
+  p.mass.resize(p.n);
+  for (int i = 0; i < p.n; ++i) p.mass[i] = d.type_mass[d.type[i]];
+  p.bond_atoms = d.bond_atoms;
+  p.bond_type = d.bond_type;
+  p.bond_k = d.bond_k;
+  p.bond_r0 = d.bond_r0;
+  p.angle_atoms = d.angle_atoms;
+  p.angle_type = d.angle_type;
+  p.angle_k = d.angle_k;
+  p.angle_theta0 = d.angle_theta0;
+  if (!d.velocity.empty()) {
+    p.velocity = d.velocity;
+  } else if (_velocity_type == "GAUSS") {
+    // REAL: sqrt(kB 298 / m); other units sqrt(1 / m) (ModelFileInitCondition.cpp:622-633)
+    std::vector<double> sg(p.n);
+    for (int i = 0; i < p.n; ++i)
+      sg[i] = std::sqrt((p.unit == "REAL" ? 1.9872067e-3 * 298.0 : 1.0) / p.mass[i]);
+    gauss_velocities(p, sg);
+  } else {
+    p.velocity.assign(3 * (size_t)p.n, 0.0);  // "ZERO", "TEST" and anything else (:641)
+  }
+}
+
+MeshFreeCondition::MeshFreeCondition(const Json& cfg) {
+  const std::vector<double> dims = cfg.numbers("dims");
+  if (dims.size() != 3) throw std::runtime_error("inbuild needs \"dims\": [nx, ny, nz]");
+  const char* keys[3] = {"x_range", "y_range", "z_range"};
+  for (int k = 0; k < 3; ++k) {
+    _dims[k] = (int)dims[k];
+    if (_dims[k] <= 0) throw std::runtime_error("inbuild dims must be positive");
+    const std::vector<double> r = cfg.numbers(keys[k]);
+    if (r.size() != 2 || !(r[1] > r[0])) throw std::runtime_error(std::string("inbuild needs \"") + keys[k] + "\": [lo, hi]");
+    _range[k][0] = r[0];
+    _range[k][1] = r[1];
+  }
+  _velocity_type = cfg.string("velocity_type", "GAUSS");
+}
+
+void MeshFreeCondition::Execute(Para& p) {
+  // one atom at the centre of every cell of the dims grid, x fastest (RunWorklet InitPosition)
+  p.init_way = "inbuild";
+  p.params.init_inbuild = 1;
+  p.n = _dims[0] * _dims[1] * _dims[2];
+  p.n_types = 1;
+  double sp[3];
+  for (int k = 0; k < 3; ++k) {
+    p.lo[k] = _range[k][0];
+    p.hi[k] = _range[k][1];
+    sp[k] = (_range[k][1] - _range[k][0]) / _dims[k];
+  }
+  p.position.resize(3 * (size_t)p.n);
+  int a = 0;
+  for (int kz = 0; kz < _dims[2]; ++kz)
+    for (int ky = 0; ky < _dims[1]; ++ky)
+      for (int kx = 0; kx < _dims[0]; ++kx, ++a) {
+        p.position[3 * (size_t)a] = p.lo[0] + (kx + 0.5) * sp[0];
+        p.position[3 * (size_t)a + 1] = p.lo[1] + (ky + 0.5) * sp[1];
+        p.position[3 * (size_t)a + 2] = p.lo[2] + (kz + 0.5) * sp[2];
+      }
+  p.mass.assign(p.n, 1.0);
+  p.type.assign(p.n, 0);
+  p.molecule.clear();
+  p.charge.assign(p.n, 0.0);
+  p.eps.assign(1, 1.0);
+  p.sigma.assign(1, 1.0);
+  if (_velocity_type == "GAUSS")
+    gauss_velocities(p, std::vector<double>(p.n, 1.0));  // unit variance (MeshFreeCondition.cpp:82-98)
+  else
+    p.velocity.assign(3 * (size_t)p.n, 0.0);
+}
+
+// ----------------------------------------------------------------------------------- execution
+ExecutionMD::ExecutionMD(Para& para, int device) : _para(para), _device(device) {}
+
+ExecutionMD::~ExecutionMD() {
+  if (_ctx) rbmd_ctx_destroy(_ctx);
+}
+
+void ExecutionMD::check(int rc, const char* what) {
+  if (rc == RBMD_OK) return;
+  const char* msg = _ctx ? rbmd_last_error(_ctx) : "";
+  throw std::runtime_error(std::string(what) + " failed (status " + std::to_string(rc) + "): " + (msg ? msg : ""));
+}
+
+void ExecutionMD::Init() {
+  rbmd_device_cfg cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.device = _device;
+  cfg.batched = 0;
+  cfg.use_graphs = 1;
+  check(rbmd_ctx_create(&cfg, &_ctx), "rbmd_ctx_create");
+  const rbmd_system_desc d = _para.desc();
+  check(rbmd_system_add(_ctx, &d, &_para.params, &_sys), "rbmd_system_add");
+  check(rbmd_init(_ctx, &_sys, 1), "rbmd_init");
+}
+
+rbmd_thermo ExecutionMD::Thermo() {
+  rbmd_thermo t;
+  check(rbmd_get_thermo(_ctx, _sys, &t), "rbmd_get_thermo");
+  return t;
+}
+
+void ExecutionMD::State(std::vector<double>& x, std::vector<double>& v, std::vector<int>& image) {
+  x.resize(3 * (size_t)_para.n);
+  v.resize(3 * (size_t)_para.n);
+  image.resize(3 * (size_t)_para.n);
+  check(rbmd_get_state(_ctx, _sys, x.data(), v.data(), image.data()), "rbmd_get_state");
+}
+
+void ExecutionNVT::Execute() { check(rbmd_step(_ctx, &_sys, 1, 1), "rbmd_step"); }
+
+// ------------------------------------------------------------------------------------- outputs
+ThermoOutput::ThermoOutput(int interval, const std::string& path, bool console)
+    : _interval(std::max(1, interval)), _console(console) {
+  _file = std::fopen(path.c_str(), "w");
+  if (!_file) throw std::runtime_error("cannot write " + path);
+}
+
+ThermoOutput::~ThermoOutput() {
+  if (_file) std::fclose(_file);
+}
+
+void ThermoOutput::Execute(Executioner& ex) {
+  const int64_t step = ex.CurrentStep();
+  if (step == 0)
+    std::fprintf(_file, "Step Time VanderWaalsEnergy NearCoulombicEnergy FarCoulombicEnergy KinticEnergy "
+                        "PotentialEnergy TotalEnergy BondEnergy AngleEnergy Temperature Pressure\n");
+  if (step % _interval != 0 && step != ex.NumStep()) return;
+  const rbmd_thermo t = ex.Run().Thermo();
+  const double vdw = t.e_lj + t.e_eam;
+  std::fprintf(_file, "%lld %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g\n", (long long)step,
+               ex.CurrentTime(), vdw, t.e_coul_near, t.e_coul_far, t.kinetic_energy, t.potential_energy,
+               t.total_energy, t.e_bond, t.e_angle, t.temperature, t.pressure);
+  std::fflush(_file);
+  if (_console)
+    std::printf("step %lld  T %.6g  E_pot %.10g  E_tot %.10g  P %.6g%s\n", (long long)step, t.temperature,
+                t.potential_energy, t.total_energy, t.pressure, t.status ? "  (device status set)" : "");
+  if (t.status) throw std::runtime_error("device status word " + std::to_string(t.status) + " at step " + std::to_string(step));
+}
+
+TrajectoryOutput::TrajectoryOutput(int interval, const std::string& path) : _interval(std::max(1, interval)) {
+  _file = std::fopen(path.c_str(), "w");
+  if (!_file) throw std::runtime_error("cannot write " + path);
+}
+
+TrajectoryOutput::~TrajectoryOutput() {
+  if (_file) std::fclose(_file);
+}
+
+void TrajectoryOutput::Execute(Executioner& ex) {
+  const int64_t step = ex.CurrentStep();
+  if (step % _interval != 0 && step != ex.NumStep()) return;
+  std::vector<double> x, v;
+  std::vector<int> img;
+  ex.Run().State(x, v, img);
+  const size_t n = x.size() / 3;
+  std::fprintf(_file, "step %lld atoms %zu\n", (long long)step, n);
+  for (size_t i = 0; i < n; ++i)
+    std::fprintf(_file, "%zu %.10g %.10g %.10g %d %d %d\n", i + 1, x[3 * i], x[3 * i + 1], x[3 * i + 2], img[3 * i],
+                 img[3 * i + 1], img[3 * i + 2]);
+  std::fflush(_file);
+}
+
+// --------------------------------------------------------------------------------- executioner
+Executioner::Executioner(ExecutionMD& run, int64_t num_steps, double dt) : _run(run), _num_steps(num_steps), _dt(dt) {}
+
+void Executioner::Init() { _run.Init(); }
+
+void Executioner::PreStep() {
+  for (auto& o : _outputs) o->Execute(*this);
+}
+
+void Executioner::TakeStep() {
+  ++_current_step;
+  _current_time += _dt;
+  _run.Execute();
+}
+
+void Executioner::Execute() {
+  // num_steps + 1 iterations with the outputs before each (Executioner.cpp:100-135)
+  while (KeepGoing()) {
+    PreStep();
+    TakeStep();
+  }
+}
+
+// --------------------------------------------------------------------------------- application
+Application::Application(int argc, char** argv) : _argv(argv, argv + argc) {}
+
+void Application::HelpMessages() const {
+  std::printf(
+      "usage: rbmd [cuda] -j <input>.json [--device N] [--dump-system <out>.json]\n"
+      "  Runs RBMD's per-step force-and-integrate path on a B200 (sm_100a).\n"
+      "  cuda        device word of the reference CLI (the only backend this build carries)\n"
+      "  -j FILE     input in RBMD's JSON schema (comments and trailing commas allowed)\n"
+      "  --device N  CUDA ordinal (default 0)\n"
+      "  --dump-system OUT  write the resolved system and parameters as JSON and stop (no GPU use)\n");
+}
+
+void Application::ParseCLI() {
+  for (size_t k = 1; k < _argv.size(); ++k) {
+    const std::string& a = _argv[k];
+    if (a == "-h" || a == "--help") {
+      _help = true;
+    } else if (a == "-j" && k + 1 < _argv.size()) {
+      _json_path = _argv[++k];
+    } else if (a == "--device" && k + 1 < _argv.size()) {
+      _device = std::atoi(_argv[++k].c_str());
+    } else if (a == "--dump-system" && k + 1 < _argv.size()) {
+      _dump_path = _argv[++k];
+    } else if (a == "cuda" || a == "mpi" || a == "dcu") {
+      _device_word = a;
+    } else {
+      throw std::runtime_error("unknown argument \"" + a + "\" (try --help)");
+    }
+  }
+  if (_help) return;
+  if (_json_path.size() < 5 || _json_path.compare(_json_path.size() - 5, 5, ".json") != 0)
+    throw std::runtime_error("-j needs a .json input file");  // JsonParser.h:73-77
+  if (_device_word == "mpi" || _device_word == "dcu")
+    throw std::runtime_error("device \"" + _device_word + "\" is not built here; this library runs the cuda (sm_100a) path");
+}
+
+int Application::Run() {
+  try {
+    ParseCLI();
+    if (_help) {
+      HelpMessages();
+      return 0;
+    }
+    CreateActions();
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "rbmd: %s\n", e.what());
+    return 1;
+  }
+  return 0;
+}
+
+void MDApplication::ReadHyperParameters(const Json& hp) {
+  rbmd_params& P = _para.params;
+  if (const Json* ff = hp.find("force_field")) {
+    _ff_type = ff->string("type", "LJ/CUT");
+    if (_ff_type == "LJ/CUT") P.force_field = RBMD_FF_LJ_CUT;
+    else if (_ff_type == "LJ/CUT/COUL/LONG") P.force_field = RBMD_FF_LJ_CUT_COUL_LONG;
+    else if (_ff_type == "CVFF") P.force_field = RBMD_FF_CVFF;
+    else if (_ff_type == "EAM") P.force_field = RBMD_FF_EAM;
+    else throw std::runtime_error("force_field type \"" + _ff_type + "\" is not supported");
+    _potential_file = ff->string("potential_file", "");
+  }
+  if (const Json* nb = hp.find("neighbor")) {
+    const std::string t = nb->string("type", "RBL");
+    if (t == "RBL") P.neighbor = RBMD_NEIGH_RBL;
+    else if (t == "VERLETLIST" || t == "VERLET-LIST") P.neighbor = RBMD_NEIGH_VERLET;
+    else throw std::runtime_error("neighbor type \"" + t + "\" is not supported");
+    P.cut_off = nb->number("cut_off", P.cut_off);
+    P.r_core = nb->number("r_core", P.r_core);
+    P.neighbor_sample_num = (int32_t)nb->number("neighbor_sample_num", P.neighbor_sample_num);
+  }
+  P.coulomb = RBMD_COUL_NONE;
+  if (const Json* cl = hp.find("coulomb")) {
+    const std::string t = cl->string("type", "RBE");
+    if (t == "RBE") P.coulomb = RBMD_COUL_RBE;
+    else if (t == "EWALD") P.coulomb = RBMD_COUL_EWALD;
+    else throw std::runtime_error("coulomb type \"" + t + "\" is not supported");
+    P.coulomb_sample_num = (int32_t)cl->number("coulomb_sample_num", P.coulomb_sample_num);
+    P.alpha = cl->number("alpha", P.alpha);
+    const std::vector<double> km = cl->numbers("kmax");
+    if (km.size() == 1) P.kmax[0] = P.kmax[1] = P.kmax[2] = (int32_t)km[0];
+    else if (km.size() == 3)
+      for (int k = 0; k < 3; ++k) P.kmax[k] = (int32_t)km[k];
+  }
+  P.fix_shake = RBMD_SHAKE_NULL;
+  if (const Json* ex = hp.find("extend")) {
+    if (ex->has("fix_shake")) P.fix_shake = ex->boolean("fix_shake", false) ? RBMD_SHAKE_TRUE : RBMD_SHAKE_FALSE;
+    const std::vector<double> sb = ex->numbers("special_bonds");
+    if (!sb.empty()) {  // MDApplication.cpp:158-163: a non-empty list switches the special lists on
+      _special_bonds = true;
+      for (int k = 0; k < 3 && k < (int)sb.size(); ++k) _special_w[k] = (double)(int)sb[k];  // read as ints
+      for (int k = 0; k < 3; ++k) P.special_bonds[k] = _special_w[k];
+    }
+  }
+}
+
+void MDApplication::ReadExecution(const Json& ex) {
+  rbmd_params& P = _para.params;
+  const std::string ens = ex.string("ensemble", "NVT");
+  if (ens == "NVT") P.ensemble = RBMD_ENS_NVT;
+  else if (ens == "NVE") P.ensemble = RBMD_ENS_NVE;
+  else if (ens == "NPT") throw std::runtime_error("ensemble NPT is not implemented by this library");
+  else throw std::runtime_error("ensemble \"" + ens + "\" is not supported");
+  const std::vector<double> t = ex.numbers("temperature");
+  for (int k = 0; k < 3 && k < (int)t.size(); ++k) P.temperature[k] = t[k];
+  const std::vector<double> pr = ex.numbers("pressure");
+  for (int k = 0; k < 3 && k < (int)pr.size(); ++k) P.pressure[k] = pr[k];
+  const std::string tc = ex.string("temp_ctrl_type", "NOSE_HOOVER");
+  if (P.ensemble == RBMD_ENS_NVE) P.temp_ctrl = RBMD_TC_NONE;
+  else if (tc == "NOSE_HOOVER") P.temp_ctrl = RBMD_TC_NOSE_HOOVER;
+  else if (tc == "BERENDSEN") P.temp_ctrl = RBMD_TC_BERENDSEN;
+  else if (tc == "TEMP_RESCALE") P.temp_ctrl = RBMD_TC_RESCALE;
+  else throw std::runtime_error("temp_ctrl_type \"" + tc + "\" is not supported");
+  P.timestep = ex.number("timestep", P.timestep);
+  P.num_steps = (int64_t)ex.number("num_steps", (double)P.num_steps);
+  // keys this library adds (absent from reference files): seed, precision, rbl_mode
+  P.seed = (uint64_t)ex.number("seed", (double)P.seed);
+  const std::string prec = ex.string("precision", "FP64");
+  if (prec == "FP64") P.precision = RBMD_PREC_FP64;
+  else if (prec == "MIXED") P.precision = RBMD_PREC_MIXED;
+  else throw std::runtime_error("precision must be FP64 or MIXED");
+  const std::string rm = ex.string("rbl_mode", "STRIDE");
+  if (rm == "STRIDE") P.rbl_mode = RBMD_RBL_STRIDE;
+  else if (rm == "PHILOX") P.rbl_mode = RBMD_RBL_PHILOX;
+  else throw std::runtime_error("rbl_mode must be STRIDE or PHILOX");
+}
+
+void MDApplication::CreateActions() {
+  _cfg = parse_json_file(_json_path);
+  _base_dir = dir_of(_json_path);
+  rbmd_params_default(&_para.params);
+  if (const Json* hp = _cfg.find("hyper_parameters")) ReadHyperParameters(*hp);
+  if (const Json* ex = _cfg.find("execution")) ReadExecution(*ex);
+  const Json* ic = _cfg.find("init_configuration");
+  if (!ic) throw std::runtime_error("input has no init_configuration");
+  std::unique_ptr<InitCondition> init;
+  if (const Json* rd = ic->find("read_data")) {
+    _para.unit = rd->string("unit", "LJ");
+    init.reset(new ModelFileInitCondition(*rd, _base_dir));
+  } else if (const Json* ib = ic->find("inbuild")) {
+    _para.unit = ib->string("unit", "LJ");
+    init.reset(new MeshFreeCondition(*ib));
+  } else {
+    throw std::runtime_error("init_configuration needs read_data or inbuild");
+  }
+  _para.params.units = units_of(_para.unit);
+  init->Execute(_para);
+  if (_para.init_way == "inbuild" && _para.params.coulomb != RBMD_COUL_NONE) {
+    // ExecutionMD::InitialCondition (ExecutionMD.cpp:157-168): -1 for the first half, +1 after
+    for (int i = 0; i < _para.n; ++i) _para.charge[i] = (i < _para.n / 2) ? -1.0 : 1.0;
+  }
+  if (_special_bonds) special_lists(_para.n, _para.bond_atoms, _special_w, _para.sp_off, _para.sp_ids, _para.sp_w);
+  if (_para.params.force_field == RBMD_FF_EAM) {
+    if (_potential_file.empty()) throw std::runtime_error("EAM needs force_field.potential_file");
+    std::string path = _potential_file;
+    if (!exists(path) && exists(_base_dir + "/" + path)) path = _base_dir + "/" + path;
+    rbmd_eam_file f;
+    std::memset(&f, 0, sizeof(f));
+    if (rbmd_eam_read_funcfl(path.c_str(), &f, nullptr, nullptr, nullptr) != RBMD_OK)
+      throw std::runtime_error("cannot read EAM potential " + path);
+    std::vector<double> frho(f.nrho), zr(f.nr), rhor(f.nr);
+    if (rbmd_eam_read_funcfl(path.c_str(), &f, frho.data(), zr.data(), rhor.data()) != RBMD_OK)
+      throw std::runtime_error("cannot read EAM potential " + path);
+    f.frho = frho.data();
+    f.zr = zr.data();
+    f.rhor = rhor.data();
+    int32_t nrho = 0, nr = 0;
+    if (rbmd_eam_spline_sizes(&f, &nrho, &nr) != RBMD_OK) throw std::runtime_error("bad EAM table sizes in " + path);
+    _para.frho_spline.assign(7 * ((size_t)nrho + 1), 0.0);  // rows 1..nrho (row 0 unused)
+    _para.rhor_spline.assign(7 * ((size_t)nr + 1), 0.0);
+    _para.z2r_spline.assign(7 * ((size_t)nr + 1), 0.0);
+    if (rbmd_eam_build_splines(&f, _para.frho_spline.data(), _para.rhor_spline.data(), _para.z2r_spline.data(),
+                               &_para.eam_nrho, &_para.eam_drho, &_para.eam_nr, &_para.eam_dr, &_para.eam_rhomax) != RBMD_OK)
+      throw std::runtime_error("cannot build EAM splines from " + path);
+    _para.eam_cut = f.cut_off;
+  }
+  if (const Json* outs = _cfg.find("outputs")) {
+    if (const Json* th = outs->find("thermo_out")) _thermo_interval = (int)th->number("interval", 1);
+    if (const Json* tr = outs->find("trajectory_out")) _traj_interval = (int)tr->number("interval", 100);
+  }
+}
+
+void MDApplication::DumpSystem(const std::string& path) const {
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) throw std::runtime_error("cannot write " + path);
+  auto darr = [&](const char* name, const std::vector<double>& v) {
+    std::fprintf(f, "\"%s\": [", name);
+    for (size_t k = 0; k < v.size(); ++k) std::fprintf(f, "%s%.17g", k ? "," : "", v[k]);
+    std::fprintf(f, "],\n");
+  };
+  auto iarr = [&](const char* name, const std::vector<int>& v) {
+    std::fprintf(f, "\"%s\": [", name);
+    for (size_t k = 0; k < v.size(); ++k) std::fprintf(f, "%s%d", k ? "," : "", v[k]);
+    std::fprintf(f, "],\n");
+  };
+  const rbmd_params& P = _para.params;
+  std::fprintf(f, "{\n\"n_atoms\": %d, \"n_types\": %d, \"init_way\": \"%s\",\n", _para.n, _para.n_types,
+               _para.init_way.c_str());
+  std::fprintf(f, "\"box_lo\": [%.17g,%.17g,%.17g], \"box_hi\": [%.17g,%.17g,%.17g],\n", _para.lo[0], _para.lo[1],
+               _para.lo[2], _para.hi[0], _para.hi[1], _para.hi[2]);
+  std::fprintf(f,
+               "\"params\": {\"force_field\": %d, \"neighbor\": %d, \"coulomb\": %d, \"ensemble\": %d, "
+               "\"temp_ctrl\": %d, \"units\": %d, \"precision\": %d, \"rbl_mode\": %d, \"fix_shake\": %d, "
+               "\"init_inbuild\": %d, \"neighbor_sample_num\": %d, \"cut_off\": %.17g, \"r_core\": %.17g, "
+               "\"coulomb_sample_num\": %d, \"kmax\": [%d,%d,%d], \"alpha\": %.17g, \"temperature\": [%.17g,%.17g,%.17g], "
+               "\"timestep\": %.17g, \"num_steps\": %lld, \"special_bonds\": [%.17g,%.17g,%.17g], \"seed\": %llu},\n",
+               P.force_field, P.neighbor, P.coulomb, P.ensemble, P.temp_ctrl, P.units, P.precision, P.rbl_mode,
+               P.fix_shake, P.init_inbuild, P.neighbor_sample_num, P.cut_off, P.r_core, P.coulomb_sample_num,
+               P.kmax[0], P.kmax[1], P.kmax[2], P.alpha, P.temperature[0], P.temperature[1], P.temperature[2],
+               P.timestep, (long long)P.num_steps, P.special_bonds[0], P.special_bonds[1], P.special_bonds[2],
+               (unsigned long long)P.seed);
+  darr("position", _para.position);
+  darr("velocity", _para.velocity);
+  darr("charge", _para.charge);
+  darr("mass", _para.mass);
+  darr("epsilon", _para.eps);
+  darr("sigma", _para.sigma);
+  iarr("type", _para.type);
+  iarr("molecule", _para.molecule);
+  iarr("bond_atoms", _para.bond_atoms);
+  iarr("bond_type", _para.bond_type);
+  darr("bond_k", _para.bond_k);
+  darr("bond_r0", _para.bond_r0);
+  iarr("angle_atoms", _para.angle_atoms);
+  iarr("angle_type", _para.angle_type);
+  darr("angle_k", _para.angle_k);
+  darr("angle_theta0", _para.angle_theta0);
+  iarr("special_offsets", _para.sp_off);
+  iarr("special_ids", _para.sp_ids);
+  darr("special_weights", _para.sp_w);
+  std::fprintf(f, "\"eam\": {\"nrho\": %d, \"nr\": %d, \"drho\": %.17g, \"dr\": %.17g, \"rhomax\": %.17g, \"cut\": %.17g},\n",
+               _para.eam_nrho, _para.eam_nr, _para.eam_drho, _para.eam_dr, _para.eam_rhomax, _para.eam_cut);
+  std::fprintf(f, "\"outputs\": {\"thermo_interval\": %d, \"trajectory_interval\": %d}\n}\n", _thermo_interval,
+               _traj_interval);
+  std::fclose(f);
+}
+
+int MDApplication::Run() {
+  try {
+    ParseCLI();
+    if (_help) {
+      HelpMessages();
+      return 0;
+    }
+    CreateActions();
+    if (!_dump_path.empty()) {
+      DumpSystem(_dump_path);
+      return 0;
+    }
+    ExecutionNVT run(_para, _device);
+    Executioner ex(run, _para.params.num_steps, _para.params.timestep);
+    if (_thermo_interval > 0) ex.AddOutput(std::unique_ptr<Output>(new ThermoOutput(_thermo_interval, "energy.rbmd", true)));
+    if (_traj_interval > 0) ex.AddOutput(std::unique_ptr<Output>(new TrajectoryOutput(_traj_interval, "trajectory.rbmd")));
+    const auto t0 = std::chrono::steady_clock::now();
+    ex.Init();
+    ex.Execute();
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::printf("rbmd: %lld steps of %d atoms in %.3f s (%.4g atom-steps/s)\n", (long long)ex.CurrentStep(), _para.n,
+                secs, (double)_para.n * (double)ex.CurrentStep() / secs);
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "rbmd: %s\n", e.what());
+    return 1;
+  }
+  return 0;
+}
+
+}  // namespace rbmd_host

@@ -1,0 +1,203 @@
+// app.hpp -- the `rbmd` host: RBMD's Application -> Executioner -> Execution(MD/NVT) shape driving
+// the sm_100a library through its C ABI (include/rbmd_gpu.h).
+//
+//   reference                                   here
+//   Application (application/Application.h:52)  Application: CLI, device set-up, actions, Run
+//   MDApplication (MDApplication.cpp)           MDApplication: JSON sections -> Para, outputs
+//   InitCondition + ModelFileInitCondition /    InitCondition, ModelFileInitCondition (read_data),
+//     MeshFreeCondition (InitCondition/)          MeshFreeCondition (inbuild)
+//   Executioner (executioner/Executioner.h:38)  Executioner: num_steps + 1 iterations, outputs
+//                                                 before each step
+//   Execution / ExecutionMD / ExecutionNVT      Execution, ExecutionMD, ExecutionNVT: rbmd_init
+//     (run/)                                      once, rbmd_step per step
+//   ThermoOutput, TrajectoryOutput (output/)    ThermoOutput (energy.rbmd), TrajectoryOutput
+#pragma once
+
+#include <cstdio>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "data_file.hpp"
+#include "json.hpp"
+#include "rbmd_gpu.h"
+
+namespace rbmd_host {
+
+// Everything the C ABI needs for one system: parameters and the arrays the descriptor points into.
+struct Para {
+  rbmd_params params{};
+  std::string init_way;  // "read_data" or "inbuild"
+  std::string unit = "LJ";
+  int n = 0, n_types = 0;
+  double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  std::vector<double> position, velocity, charge, mass, eps, sigma;
+  std::vector<int> type, molecule;
+  std::vector<int> bond_atoms, bond_type, angle_atoms, angle_type;
+  std::vector<double> bond_k, bond_r0, angle_k, angle_theta0;
+  std::vector<int> sp_off, sp_ids;
+  std::vector<double> sp_w;
+  // EAM
+  int eam_nrho = 0, eam_nr = 0;
+  double eam_drho = 0, eam_dr = 0, eam_rhomax = 0, eam_cut = 0;
+  std::vector<double> frho_spline, rhor_spline, z2r_spline;
+
+  rbmd_system_desc desc() const;  // pointers into this object
+};
+
+class InitCondition {
+ public:
+  virtual ~InitCondition() = default;
+  virtual void Execute(Para& para) = 0;
+};
+
+// read_data (InitCondition/ModelFileInitCondition.cpp)
+class ModelFileInitCondition : public InitCondition {
+ public:
+  ModelFileInitCondition(const Json& cfg, const std::string& base_dir);
+  void Execute(Para& para) override;
+
+ private:
+  std::string _file, _atom_style, _velocity_type;
+};
+
+// inbuild (InitCondition/MeshFreeCondition.cpp): one atom per lattice cell centre
+class MeshFreeCondition : public InitCondition {
+ public:
+  explicit MeshFreeCondition(const Json& cfg);
+  void Execute(Para& para) override;
+
+ private:
+  int _dims[3] = {1, 1, 1};
+  double _range[3][2] = {{0, 1}, {0, 1}, {0, 1}};
+  std::string _velocity_type;
+};
+
+class Execution {
+ public:
+  virtual ~Execution() = default;
+  virtual void Init() = 0;
+  virtual void Execute() = 0;
+  virtual void SetParameters() {}
+};
+
+// Owns the library context and the system (run/ExecutionMD.cpp).
+class ExecutionMD : public Execution {
+ public:
+  ExecutionMD(Para& para, int device);
+  ~ExecutionMD() override;
+  void Init() override;
+  rbmd_thermo Thermo();
+  void State(std::vector<double>& x, std::vector<double>& v, std::vector<int>& image);
+
+ protected:
+  void check(int rc, const char* what);
+  Para& _para;
+  int _device;
+  rbmd_ctx* _ctx = nullptr;
+  int32_t _sys = -1;
+};
+
+// NVT / NVE velocity Verlet with the configured thermostat (run/ExecutionNVT.cpp)
+class ExecutionNVT : public ExecutionMD {
+ public:
+  using ExecutionMD::ExecutionMD;
+  void Execute() override;
+};
+
+class Executioner;
+
+class Output {
+ public:
+  virtual ~Output() = default;
+  virtual void Execute(Executioner& ex) = 0;
+};
+
+// energy.rbmd columns of output/ThermoOutput.cpp:223-291 plus temperature and pressure
+class ThermoOutput : public Output {
+ public:
+  ThermoOutput(int interval, const std::string& path, bool console);
+  ~ThermoOutput() override;
+  void Execute(Executioner& ex) override;
+
+ private:
+  int _interval;
+  FILE* _file = nullptr;
+  bool _console;
+};
+
+// positions every `interval` steps, one "step N" block of "id type x y z ix iy iz" lines
+class TrajectoryOutput : public Output {
+ public:
+  TrajectoryOutput(int interval, const std::string& path);
+  ~TrajectoryOutput() override;
+  void Execute(Executioner& ex) override;
+
+ private:
+  int _interval;
+  FILE* _file = nullptr;
+};
+
+class Executioner {
+ public:
+  Executioner(ExecutionMD& run, int64_t num_steps, double dt);
+  void AddOutput(std::unique_ptr<Output> o) { _outputs.push_back(std::move(o)); }
+  void Init();
+  void Execute();
+  int64_t CurrentStep() const { return _current_step; }
+  int64_t NumStep() const { return _num_steps; }
+  double CurrentTime() const { return _current_time; }
+  ExecutionMD& Run() { return _run; }
+
+ private:
+  void PreStep();
+  void TakeStep();
+  bool KeepGoing() const { return _current_step <= _num_steps; }
+  ExecutionMD& _run;
+  std::vector<std::unique_ptr<Output>> _outputs;
+  int64_t _num_steps;
+  int64_t _current_step = 0;
+  double _dt, _current_time = 0.0;
+};
+
+class Application {
+ public:
+  Application(int argc, char** argv);
+  virtual ~Application() = default;
+  // returns the process exit status; errors are reported on stderr, never by exit()
+  virtual int Run();
+
+ protected:
+  virtual void ParseCLI();
+  virtual void CreateActions() = 0;
+  void HelpMessages() const;
+  std::vector<std::string> _argv;
+  std::string _device_word;  // cuda | mpi | dcu | "" (serial)
+  std::string _json_path;
+  std::string _dump_path;    // --dump-system: write the resolved system and stop (no device use)
+  int _device = 0;
+  bool _help = false;
+};
+
+// JSON-driven molecular dynamics (application/MDApplication.cpp)
+class MDApplication : public Application {
+ public:
+  using Application::Application;
+  int Run() override;
+
+ protected:
+  void CreateActions() override;
+
+ private:
+  void ReadHyperParameters(const Json& hp);
+  void ReadExecution(const Json& ex);
+  void DumpSystem(const std::string& path) const;
+  Json _cfg;
+  Para _para;
+  int _thermo_interval = 0, _traj_interval = 0;
+  bool _special_bonds = false;
+  double _special_w[3] = {0, 0, 0};
+  std::string _ff_type, _potential_file, _base_dir;
+};
+
+}  // namespace rbmd_host

@@ -439,3 +439,118 @@ def serving_stream(n_requests=512, n_min=1000, n_max=64000, rate=50.0, seed=7):
     gaps = rng.exponential(1.0 / rate, n_requests)
     arrivals = np.cumsum(gaps) - gaps[0]
     return sizes, arrivals
+
+
+def write_funcfl(body, path, z=29, mass=63.55, a0=3.615, lattice="fcc"):
+    """Writes a funcfl body (johnson_funcfl() or read_funcfl() dict) as a funcfl file: comment,
+    "Z mass a0 lattice", "nrho drho nr dr cut", then F(rho), Z(r) and rho(r), five per line."""
+    with open(path, "w") as f:
+        f.write("funcfl written by rbmd_b200.synth\n")
+        f.write(f"{z} {mass!r} {a0!r} {lattice}\n")
+        f.write(f"{int(body['nrho'])} {float(body['drho'])!r} {int(body['nr'])} {float(body['dr'])!r} "
+                f"{float(body['cut'])!r}\n")
+        for key in ("frho", "zr", "rhor"):
+            v = np.asarray(body[key], np.float64)
+            for k in range(0, len(v), 5):
+                f.write(" ".join(repr(float(x)) for x in v[k:k + 5]) + "\n")
+    return path
+
+
+def write_rbmd_input(sd, directory, atom_style=None, thermo_interval=1, name="rbmd", potential_file=None):
+    """Writes `sd` as the reference's inputs: a LAMMPS data file (every double at full precision,
+    velocities included) and an rbmd.json in the reference schema that runs it with sd.params
+    (plus the optional keys seed, precision and rbl_mode).  Returns the json path.  The data file
+    carries per-type masses, so sd's masses must be uniform within each type."""
+    import json as _json
+    import os as _os
+    p = sd.params
+    n, nt = sd.n, len(sd.eps)
+    if atom_style is None:
+        atom_style = "full" if sd.molecule is not None else ("charge" if sd.charge is not None else "atomic")
+    tmass = np.zeros(nt)
+    for t in range(nt):
+        m = sd.mass[sd.types == t]
+        if len(m) and not np.all(m == m[0]):
+            raise ValueError(f"type {t} has more than one mass")
+        tmass[t] = m[0] if len(m) else 1.0
+    units = {A.UNITS_LJ: "LJ", A.UNITS_REAL: "REAL", A.UNITS_METAL: "METAL"}[p.units]
+    _os.makedirs(directory, exist_ok=True)
+    data = _os.path.join(directory, f"{name}.data")
+    q = sd.charge if sd.charge is not None else np.zeros(n)
+    mol = sd.molecule if sd.molecule is not None else np.arange(n)
+    nb = 0 if sd.bond_atoms is None else len(sd.bond_type)
+    na = 0 if sd.angle_atoms is None or sd.angle_type is None else len(sd.angle_type)
+    with open(data, "w") as f:
+        f.write(f"LAMMPS data file written by rbmd_b200.synth ({sd.name})\n\n")
+        f.write(f"{n} atoms\n{nt} atom types\n")
+        if nb:
+            f.write(f"{nb} bonds\n{len(sd.bond_k)} bond types\n")
+        if na:
+            f.write(f"{na} angles\n{len(sd.angle_k)} angle types\n")
+        f.write("\n")
+        for k, ax in enumerate("xyz"):
+            f.write(f"{float(sd.box_lo[k])!r} {float(sd.box_hi[k])!r} {ax}lo {ax}hi\n")
+        f.write("\nMasses\n\n")
+        for t in range(nt):
+            f.write(f"{t + 1} {float(tmass[t])!r}\n")
+        f.write("\nPair Coeffs # lj/cut\n\n")
+        for t in range(nt):
+            f.write(f"{t + 1} {float(sd.eps[t])!r} {float(sd.sig[t])!r}\n")
+        if nb:
+            f.write("\nBond Coeffs # harmonic\n\n")
+            for t in range(len(sd.bond_k)):
+                f.write(f"{t + 1} {float(sd.bond_k[t])!r} {float(sd.bond_r0[t])!r}\n")
+        if na:
+            f.write("\nAngle Coeffs # harmonic\n\n")
+            for t in range(len(sd.angle_k)):
+                f.write(f"{t + 1} {float(sd.angle_k[t])!r} {float(sd.angle_theta0[t])!r}\n")
+        f.write(f"\nAtoms # {atom_style}\n\n")
+        for i in range(n):
+            x, y, z = (repr(float(c)) for c in sd.pos[i])
+            if atom_style == "full":
+                f.write(f"{i + 1} {int(mol[i]) + 1} {int(sd.types[i]) + 1} {float(q[i])!r} {x} {y} {z} 0 0 0\n")
+            elif atom_style == "charge":
+                f.write(f"{i + 1} {int(sd.types[i]) + 1} {float(q[i])!r} {x} {y} {z} 0 0 0\n")
+            else:
+                f.write(f"{i + 1} {int(sd.types[i]) + 1} {x} {y} {z} 0 0 0\n")
+        if sd.vel is not None:
+            f.write("\nVelocities\n\n")
+            for i in range(n):
+                f.write(f"{i + 1} " + " ".join(repr(float(c)) for c in sd.vel[i]) + "\n")
+        if nb:
+            f.write("\nBonds\n\n")
+            for b in range(nb):
+                f.write(f"{b + 1} {int(sd.bond_type[b]) + 1} {int(sd.bond_atoms[2 * b]) + 1} "
+                        f"{int(sd.bond_atoms[2 * b + 1]) + 1}\n")
+        if na:
+            f.write("\nAngles\n\n")
+            for a in range(na):
+                i3 = sd.angle_atoms[3 * a:3 * a + 3] + 1
+                f.write(f"{a + 1} {int(sd.angle_type[a]) + 1} {i3[0]} {i3[1]} {i3[2]}\n")
+    ff = {v: k for k, v in A.FORCE_FIELDS.items()}[p.force_field]
+    hp = {"force_field": {"type": ff} if potential_file is None else {"type": ff, "potential_file": potential_file},
+          "neighbor": {"type": "RBL" if p.neighbor == A.NEIGH_RBL else "VERLETLIST", "cut_off": p.cut_off,
+                       "r_core": p.r_core, "neighbor_sample_num": p.neighbor_sample_num},
+          "extend": {}}
+    if p.coulomb != A.COUL_NONE:
+        hp["coulomb"] = {"type": "RBE" if p.coulomb == A.COUL_RBE else "EWALD",
+                         "coulomb_sample_num": p.coulomb_sample_num, "alpha": p.alpha,
+                         "kmax": [int(k) for k in p.kmax]}
+    if p.fix_shake != A.SHAKE_NULL:
+        hp["extend"]["fix_shake"] = bool(p.fix_shake == A.SHAKE_TRUE)
+    if sd.special_offsets is not None:
+        hp["extend"]["special_bonds"] = [int(w) for w in p.special_bonds]
+    tc = {v: k for k, v in A.TEMP_CTRLS.items()}.get(p.temp_ctrl, "NOSE_HOOVER")
+    cfg = {"init_configuration": {"read_data": {"file": f"{name}.data", "unit": units, "atom_style": atom_style,
+                                                "velocity_type": "GAUSS"}},
+           "hyper_parameters": hp,
+           "execution": {"ensemble": "NVE" if p.temp_ctrl == A.TC_NONE else "NVT",
+                         "temperature": list(p.temperature), "temp_ctrl_type": tc, "timestep": p.timestep,
+                         "num_steps": int(p.num_steps), "seed": int(p.seed),
+                         "precision": "MIXED" if p.precision == A.PREC_MIXED else "FP64",
+                         "rbl_mode": "PHILOX" if p.rbl_mode == A.RBL_PHILOX else "STRIDE"},
+           "outputs": {"thermo_out": {"interval": int(thermo_interval)}}}
+    path = _os.path.join(directory, f"{name}.json")
+    with open(path, "w") as f:
+        _json.dump(cfg, f, indent=2)
+    return path

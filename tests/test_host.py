@@ -1,0 +1,169 @@
+"""The `rbmd -j` host on the CPU: JSON dialect, LAMMPS data reading, special lists, inbuild lattice,
+EAM potential files and error reporting, through `--dump-system` (which resolves the input and
+writes it out without touching a GPU)."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from rbmd_b200 import _abi as A
+from rbmd_b200 import synth
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+RBMD = os.path.join(ROOT, "rbmd_b200", "_lib", "rbmd")
+
+
+@pytest.fixture(scope="module")
+def rbmd_bin():
+    if not os.path.exists(RBMD):
+        pytest.fail(f"{RBMD} is not built (python -m rbmd_b200.build)")
+    return RBMD
+
+
+def dump(rbmd_bin, json_path, tmp_path):
+    out = tmp_path / "dump.json"
+    r = subprocess.run([rbmd_bin, "-j", str(json_path), "--dump-system", str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return json.load(open(out))
+
+
+def test_help_and_bad_arguments(rbmd_bin):
+    r = subprocess.run([rbmd_bin, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "-j" in r.stdout
+    r = subprocess.run([rbmd_bin, "-j", "input.txt"], capture_output=True, text=True)
+    assert r.returncode == 1 and ".json" in r.stderr  # JsonParser.h: -j must name a .json file
+    r = subprocess.run([rbmd_bin, "mpi", "-j", "x.json"], capture_output=True, text=True)
+    assert r.returncode == 1 and "not built" in r.stderr
+
+
+def test_json_dialect_and_inbuild(rbmd_bin, tmp_path):
+    """BOM, // and /* */ comments and trailing commas as in the reference's bundled inputs; the
+    inbuild lattice puts one atom at every cell centre, x fastest, charges -1 then +1."""
+    text = "﻿" + """{
+  // inbuild lattice
+  "init_configuration": {
+    "inbuild": { "dims": [ 4, 3, 2 ], "x_range": [ 0.0, 8.0 ], "y_range": [ 0.0, 6.0 ],
+                 "z_range": [ 0.0, 4.0 ], "velocity_type": "ZERO", "unit": "LJ", },
+  },
+  /* block comment */
+  "hyper_parameters": {
+    "force_field": { "type": "LJ/CUT/COUL/LONG" },
+    "neighbor": { "type": "RBL", "cut_off": 1.9, "r_core": 1.0, "neighbor_sample_num": 20, },
+    "coulomb": { "type": "RBE", "coulomb_sample_num": 50, "alpha": 0.7, "kmax": 2 },
+    "extend": { },
+  },
+  "execution": { "ensemble": "NVT", "temperature": [ 1.5, 1.5, 0.2 ], "temp_ctrl_type": "BERENDSEN",
+                 "timestep": 0.002, "num_steps": 7, "seed": 11, },
+  "outputs": { "thermo_out": { "interval": 2 } }
+}
+"""
+    p = tmp_path / "in.json"
+    p.write_text(text, encoding="utf-8")
+    j = dump(rbmd_bin, p, tmp_path)
+    assert j["n_atoms"] == 24 and j["init_way"] == "inbuild"
+    P = j["params"]
+    assert P["force_field"] == A.FF_LJ_CUT_COUL_LONG and P["coulomb"] == A.COUL_RBE
+    assert P["kmax"] == [2, 2, 2] and P["coulomb_sample_num"] == 50 and P["alpha"] == 0.7
+    assert P["temp_ctrl"] == A.TC_BERENDSEN and P["init_inbuild"] == 1 and P["num_steps"] == 7
+    assert P["seed"] == 11 and P["fix_shake"] == A.SHAKE_NULL
+    pos = np.array(j["position"]).reshape(-1, 3)
+    assert np.allclose(pos[0], [1.0, 1.0, 1.0]) and np.allclose(pos[1], [3.0, 1.0, 1.0])
+    assert np.allclose(pos[4], [1.0, 3.0, 1.0]) and np.allclose(pos[12], [1.0, 1.0, 3.0])
+    q = np.array(j["charge"])
+    assert (q[:12] == -1).all() and (q[12:] == 1).all()
+    assert np.array(j["velocity"]).max() == 0.0
+    assert j["outputs"]["thermo_interval"] == 2
+
+
+@pytest.mark.parametrize("special", [True, False])
+def test_read_data_water_full(rbmd_bin, tmp_path, special):
+    sd = synth.spce_water(n_mol=64)
+    if not special:
+        sd.special_offsets = sd.special_ids = sd.special_weights = None
+    path = synth.write_rbmd_input(sd, str(tmp_path))
+    j = dump(rbmd_bin, path, tmp_path)
+    assert j["n_atoms"] == sd.n and j["n_types"] == len(sd.eps)
+    assert np.array_equal(np.array(j["position"]).reshape(-1, 3), sd.pos)
+    assert np.array_equal(np.array(j["velocity"]).reshape(-1, 3), sd.vel)
+    assert np.array_equal(j["charge"], sd.charge) and np.array_equal(j["mass"], sd.mass)
+    assert np.array_equal(j["type"], sd.types) and np.array_equal(j["molecule"], sd.molecule)
+    assert np.array_equal(j["bond_atoms"], sd.bond_atoms) and np.array_equal(j["bond_type"], sd.bond_type)
+    assert np.array_equal(j["angle_atoms"], sd.angle_atoms) and np.array_equal(j["angle_type"], sd.angle_type)
+    assert np.array_equal(j["bond_k"], sd.bond_k) and np.array_equal(j["angle_theta0"], sd.angle_theta0)
+    assert np.array_equal(j["epsilon"], sd.eps) and np.array_equal(j["sigma"], sd.sig)
+    assert j["box_lo"] == list(sd.box_lo) and j["box_hi"] == list(sd.box_hi)
+    P = j["params"]
+    assert P["force_field"] == A.FF_CVFF and P["fix_shake"] == A.SHAKE_TRUE and P["units"] == A.UNITS_REAL
+    if special:  # the bond-graph lists, built in C++ from the Bonds section
+        assert np.array_equal(j["special_offsets"], sd.special_offsets)
+        assert np.array_equal(j["special_ids"], sd.special_ids)
+        assert np.array_equal(j["special_weights"], sd.special_weights)
+    else:
+        assert j["special_offsets"] == []
+
+
+def test_special_lists_match_reference_rule(rbmd_bin, tmp_path):
+    """A chain and a branched molecule: 1-2, 1-3 and 1-4 partners in the multimap order of the
+    bond list, an unbonded atom listing itself with weight 1 (SetSpecialBonds)."""
+    pos = np.array([[1.0 + k, 2.0, 2.0] for k in range(7)])
+    sd = synth.SystemData(pos, np.ones(7), np.zeros(7), [1.0], [1.0], [0, 0, 0], [12, 12, 12],
+                          vel=np.zeros((7, 3)), charge=np.zeros(7), molecule=np.array([0, 0, 0, 0, 1, 1, 2]))
+    sd.bond_atoms = np.array([0, 1, 1, 2, 2, 3, 4, 5], np.int32)
+    sd.bond_type = np.zeros(4, np.int32)
+    sd.bond_k, sd.bond_r0 = np.array([100.0]), np.array([1.0])
+    w = (1.0, 0.0, 0.5)
+    sd.special_offsets, sd.special_ids, sd.special_weights = synth.special_lists(
+        7, [(0, 1), (1, 2), (2, 3), (4, 5)], w)
+    sd.params.special_bonds[:] = [1, 0, 0]  # the reference reads the weights as integers
+    path = synth.write_rbmd_input(sd, str(tmp_path), atom_style="full")
+    j = dump(rbmd_bin, path, tmp_path)
+    ref_off, ref_ids, ref_w = synth.special_lists(7, [(0, 1), (1, 2), (2, 3), (4, 5)], (1.0, 0.0, 0.0))
+    assert np.array_equal(j["special_offsets"], ref_off)
+    assert np.array_equal(j["special_ids"], ref_ids)
+    assert np.array_equal(j["special_weights"], ref_w)
+    off = j["special_offsets"]
+    assert j["special_ids"][off[6]:off[7]] == [6] and j["special_weights"][off[6]] == 1.0
+
+
+def test_eam_potential_file(rbmd_bin, tmp_path, oracle_mod):
+    body = synth.johnson_funcfl(n=2000)
+    pot = synth.write_funcfl(body, str(tmp_path / "cu.eam"))
+    sd = synth.eam_cu(cells=3)
+    path = synth.write_rbmd_input(sd, str(tmp_path), atom_style="atomic", potential_file="cu.eam")
+    j = dump(rbmd_bin, path, tmp_path)
+    ref = oracle_mod.eam_splines(oracle_mod.read_funcfl(pot))
+    e = j["eam"]
+    assert (e["nrho"], e["nr"]) == (ref["nrho"], ref["nr"])
+    assert e["drho"] == ref["drho"] and e["dr"] == ref["dr"] and e["rhomax"] == ref["rhomax"]
+    assert e["cut"] == ref["cut"]
+    assert j["params"]["force_field"] == A.FF_EAM and j["params"]["units"] == A.UNITS_METAL
+
+
+@pytest.mark.parametrize("mutate,message", [
+    (lambda cfg: cfg["execution"].update(ensemble="NPT"), "NPT"),
+    (lambda cfg: cfg["init_configuration"]["read_data"].update(atom_style="molecular"), "atom_style"),
+    (lambda cfg: cfg["init_configuration"]["read_data"].update(file="missing.data"), "missing.data"),
+    (lambda cfg: cfg["hyper_parameters"]["force_field"].update(type="OPLS-AA"), "OPLS-AA"),
+])
+def test_errors_are_reported(rbmd_bin, tmp_path, mutate, message):
+    sd = synth.spce_water(n_mol=8)
+    path = synth.write_rbmd_input(sd, str(tmp_path))
+    cfg = json.load(open(path))
+    mutate(cfg)
+    json.dump(cfg, open(path, "w"))
+    r = subprocess.run([rbmd_bin, "-j", path, "--dump-system", str(tmp_path / "d.json")], capture_output=True,
+                       text=True)
+    assert r.returncode == 1 and message in r.stderr
+
+
+def test_truncated_data_file(rbmd_bin, tmp_path):
+    sd = synth.spce_water(n_mol=8)
+    path = synth.write_rbmd_input(sd, str(tmp_path))
+    data = tmp_path / "rbmd.data"
+    lines = data.read_text().splitlines()
+    data.write_text("\n".join(lines[:lines.index("Velocities") - 3]) + "\n")
+    r = subprocess.run([rbmd_bin, "-j", path, "--dump-system", str(tmp_path / "d.json")], capture_output=True,
+                       text=True)
+    assert r.returncode == 1 and "Atoms" in r.stderr
