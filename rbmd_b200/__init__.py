@@ -239,6 +239,16 @@ class Context:
         self._check(lib().rbmd_serve_stop(self.h))
 
 
+def system_bytes(sd, params=None):
+    """Device bytes a system takes (rbmd_system_bytes): the figure serving admission charges."""
+    desc = sd.desc()
+    out = C.c_int64()
+    rc = lib().rbmd_system_bytes(C.byref(desc), C.byref(params if params is not None else sd.params), C.byref(out))
+    if rc:
+        raise RbmdError(rc, "rbmd_system_bytes")
+    return out.value
+
+
 def eam_splines(file_dict):
     """rbmd_eam_build_splines on a funcfl body given as a dict of numpy arrays."""
     L = lib()
