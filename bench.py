@@ -111,17 +111,23 @@ class Clocks:
 
 
 class Dist:
-    def __init__(self):
+    """One process per GPU from torchrun's environment.  Systems are independent, so the only
+    collectives are the barriers around the timed region and the max / sum of the timing.  The
+    backend is NCCL (RBMD_DIST_BACKEND=gloo runs the same logic on host tensors, for CPU tests)."""
+
+    def __init__(self, backend=None, timeout_s=600):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend or os.environ.get("RBMD_DIST_BACKEND", "nccl")
         self.torch = None
         if self.world > 1:
             import datetime
             import torch
             import torch.distributed as td
-            torch.cuda.set_device(self.local)
-            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            if self.backend == "nccl":
+                torch.cuda.set_device(self.local)
+            td.init_process_group(self.backend, timeout=datetime.timedelta(seconds=timeout_s))
             self.torch = torch
             self.td = td
 
@@ -132,7 +138,8 @@ class Dist:
     def reduce(self, x, op="max"):
         if self.world == 1:
             return x
-        t = self.torch.tensor([float(x)], device=f"cuda:{self.local}", dtype=self.torch.float64)
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = self.torch.tensor([float(x)], device=dev, dtype=self.torch.float64)
         self.td.all_reduce(t, op=self.td.ReduceOp.MAX if op == "max" else self.td.ReduceOp.SUM)
         return float(t.item())
 
@@ -188,7 +195,8 @@ def kernel_profile(ctx, ids, systems):
     ctx.step(ids, 2)
     ctx.sync()
     out = {}
-    for name in ("nhc", "kick_drift", "cells", "shake", "rbe_sample", "rho", "bonded", "pair", "final", "rattle"):
+    for name in ("nhc", "kick_drift", "cells", "shake", "rbe_sample", "rho", "bonded", "pair_tile", "pair_lean",
+                 "pair_atom", "final", "rattle"):
         ms, n, units = ctx.profile_get(name)
         if n:
             out[name] = dict(avg_ms=ms, launches=n, units_per_launch=units)
@@ -306,21 +314,43 @@ def cpu_port_rate(seconds, threads=None):
                 sample=f"one {sd.n}-atom saline system of the stream's parameters, {steps} NVT steps in {dt:.1f} s")
 
 
+PAIR_KERNELS = {"pair_tile": "k_pair_tile (warp per home cell: shared candidate batches, RBL picks, LJ + erfc)",
+                "pair_lean": "k_pair2 (warp per atom with segment tables)", "pair_atom": "k_pair (general warp per atom)"}
+
+
+def profiled_traffic(name):
+    """DRAM bytes (read + write) per atom of a pair kernel, from its committed ncu summary
+    profiles/k_<name>_saline_small.md (line "traffic_bytes_per_atom: X"); None without one."""
+    path = os.path.join(ROOT, "profiles", f"k_{name}_saline_small.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("traffic_bytes_per_atom:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
 def roofline(prof, pairs_per_atom, peaks, fp32_peak):
-    p = prof.get("pair")
-    if not p:
+    """Roofline of the dominant pair kernel (largest device time over the profiled steps)."""
+    recs = {k: v for k, v in prof.items() if k in PAIR_KERNELS}
+    if not recs:
         return None, None
+    name = max(recs, key=lambda k: recs[k]["avg_ms"] * recs[k]["launches"])
+    p = recs[name]
     atoms = p["units_per_launch"]
     secs = p["avg_ms"] * 1e-3
-    # algorithmic HBM bytes per atom of the pair kernel: its own position+charge (16 B FP32 copy),
-    # metadata (16 B), the force written (32 B); neighbour reuse is cache traffic, not counted
+    # algorithmic HBM bytes per atom: its sorted FP32 position + charge (16 B), sorted metadata
+    # (16 B) and the FP64 force written (32 B); neighbour reuse is cache traffic, not counted
     bytes_alg = 64.0 * atoms
     flops = (26 + 14) * pairs_per_atom * atoms  # LJ + Coulomb pair convention (flops per pair)
     hbm = peaks.get("hbm_gbs", 6650.0)
     achieved_gbs = bytes_alg / secs / 1e9
+    tpa = profiled_traffic(name)
     r_hbm = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s", "frac": achieved_gbs / hbm,
-             "traffic": None, "kernel": "k_pair (fused RBL traversal + LJ/erfc pair forces)",
-             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+             "traffic": None if tpa is None else tpa * atoms, "kernel": PAIR_KERNELS[name],
+             "launch_ms": p["avg_ms"], "atoms_per_launch": atoms, "bytes_alg_per_atom": 64.0,
+             "traffic_source": None if tpa is None else f"profiles/k_{name}_saline_small.md, scaled by atoms",
+             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
     tf = flops / secs / 1e12
     r_fp32 = {"bound": "fp32", "achieved": tf, "peak": fp32_peak, "unit": "TFLOP/s",
               "frac": tf / fp32_peak if fp32_peak else None,

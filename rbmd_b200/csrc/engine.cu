@@ -91,6 +91,9 @@ static void derive(const rbmd_system_desc& d, const rbmd_params& p, rbmd_derived
 
 // ------------------------------------------------------------------------------ context
 namespace {
+// Profiler record of a batch's pair launch, by traversal layout.
+const char* pair_name(const Batch& b) { return b.dense ? "pair_tile" : (b.lean ? "pair_lean" : "pair_atom"); }
+
 // Exact thresholds for the reference's window tests.  fl(c - x) is non-increasing in x, so
 // {x : fl(c - x) > e} is a down-set of the floats and thr_below returns its largest element;
 // likewise {x : fl(x - c) > e} is an up-set and thr_above returns its smallest element.
@@ -766,13 +769,11 @@ void Context::timed(const char* name, double units, F&& fn) {
 }
 
 void Context::enqueue_forces(const Batch& b, FinalMode mode, int virial) {
-  double natoms = 0;
-  (void)natoms;
   timed("cells", 0, [&] { launch_cells(b, stream); });
   if (b.coul == RBMD_COUL_RBE) timed("rbe_sample", 0, [&] { launch_rbe_sample(b, stream); });
   if (b.coul != RBMD_COUL_NONE) timed("rho", 0, [&] { launch_rho(b, stream, b.coul == RBMD_COUL_EWALD); });
   if (b.has_bonded) timed("bonded", 0, [&] { launch_bonded(b, stream, virial); });
-  timed("pair", (double)b.natoms, [&] { launch_pair(b, stream, virial); });
+  timed(pair_name(b), (double)b.natoms, [&] { launch_pair(b, stream, virial); });
   timed("final", (double)b.natoms, [&] { launch_final(b, stream, mode, virial); });
 }
 
@@ -784,7 +785,7 @@ void Context::enqueue_step(const Batch& b) {
   if (b.coul == RBMD_COUL_RBE) timed("rbe_sample", 0, [&] { launch_rbe_sample(b, stream); });
   if (b.coul != RBMD_COUL_NONE) timed("rho", 0, [&] { launch_rho(b, stream, b.coul == RBMD_COUL_EWALD); });
   if (b.has_bonded) timed("bonded", 0, [&] { launch_bonded(b, stream, 0); });
-  timed("pair", (double)b.natoms, [&] { launch_pair(b, stream, 0); });
+  timed(pair_name(b), (double)b.natoms, [&] { launch_pair(b, stream, 0); });
   timed("final", (double)b.natoms, [&] { launch_final(b, stream, kFinalKick, 0); });
   if (b.has_shake) {
     timed("rattle", 0, [&] { launch_rattle(b, stream); });
