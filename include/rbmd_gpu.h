@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBMD_ABI_VERSION 1
+#define RBMD_ABI_VERSION 2
 
 /* ---------------------------------------------------------------- status codes */
 enum rbmd_status {
@@ -117,13 +117,15 @@ typedef struct rbmd_params {
   int32_t kmax[3];              /* Ewald k range (energy in RBE mode, force in EWALD mode) */
   double alpha;                 /* Ewald splitting, reference convention: erfc(sqrt(alpha) r) */
   double temperature[3];        /* T_start, T_stop, T_damp */
-  double pressure[3];           /* P_start, P_stop, P_damp (NPT) */
+  double pressure[3];           /* P_start, P_stop, P_damp (NPT; ensemble NPT needs temp_ctrl
+                                   BERENDSEN and press_ctrl BERENDSEN, ExecutionNPT.cpp:90-141) */
   int32_t press_ctrl;           /* enum rbmd_press_ctrl */
   int32_t pad0;
   double timestep;
   int64_t num_steps;            /* length of the run, used for temperature ramps */
   double special_bonds[3];      /* 1-2, 1-3, 1-4 LJ weights */
   uint64_t seed;                /* Philox key */
+  double bulk_modulus;          /* NPT Berendsen: pressure[3] of the reference's 4-entry "pressure" */
 } rbmd_params;
 
 /* Fill *p with the reference defaults (LJ units, RBL, NH, FP64, stride picks, seed 1). */
@@ -211,7 +213,9 @@ enum rbmd_status_bit {
   RBMD_STATUS_SHAKE_NO_CONVERGE = 4, /* SHAKE iteration hit its 5000-step limit */
   RBMD_STATUS_RATTLE_SINGULAR = 8,   /* RATTLE 3x3 system with |det| < 1e-4 */
   RBMD_STATUS_NON_FINITE = 16,       /* a force component was Inf or NaN */
-  RBMD_STATUS_RBE_SLOTS = 32         /* Metropolis chain ran out of proposal slots */
+  RBMD_STATUS_RBE_SLOTS = 32,        /* Metropolis chain ran out of proposal slots */
+  RBMD_STATUS_BOX_RANGE = 64         /* NPT: the box left the range its cell tables were sized for
+                                        (0.8 to 1.25 of the initial edge); the box stays put */
 };
 
 typedef struct rbmd_device_cfg {

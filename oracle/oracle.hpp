@@ -62,6 +62,10 @@ inline void par_for(long n, Fn&& fn) {
 }
 
 constexpr double kPi = 3.14159265358979323846;          // vtkm::Pi()
+// NPT box limits of this implementation (the reference has none): a remap whose edge would leave
+// [kBoxShrink, kBoxGrow] x the initial edge, or give fewer cells than num_cycles, is refused with
+// RBMD_STATUS_BOX_RANGE and the box stays put.  The CUDA path sizes its cell tables by kBoxGrow.
+constexpr double kBoxGrow = 1.25, kBoxShrink = 0.8;
 constexpr double kPif = 3.1415927410125732421875;        // (double)vtkm::Pif(), the float pi
 
 struct Units {  // ExecutionMD::InitParameters, framework/run/ExecutionMD.cpp:329-360
@@ -129,6 +133,10 @@ class System {
   Units u;
   Derived dv;
   double lo[3], hi[3], L[3];
+  double L0[3];                  // box edges at set-up (barostat range limits)
+  int ncell_cap = 0;             // NPT: cells of the largest accepted box
+  double baro_pressure = 0.0;    // NPT: pressure and virial the barostat last used (PARA_PRESSURE)
+  double baro_virial[6] = {0, 0, 0, 0, 0, 0};
   int64_t step = 0;  // Executioner::_current_step
   Thermostat th;
   Cells cells;
@@ -163,6 +171,9 @@ class System {
 
   // helpers
   void min_image(double r[3]) const;
+  void set_box(const double nlo[3], const double nhi[3]);
+  void pressure_scalar(double vir[6], double& press) const;
+  void barostat_berendsen();
   void compute_tempe();
   void compute_temp_target();
   void nhc_integrate();

@@ -127,19 +127,20 @@ System::System(const rbmd_system_desc& d, const rbmd_params& prm) : p(prm) {
   }
 
   // ---- derived parameters
-  dv.volume = L[0] * L[1] * L[2];
-  dv.rho = N / dv.volume;  // PARA_RHO, ModelFileInitCondition.cpp:207
   double rc = p.cut_off;
   double rs = (p.neighbor == RBMD_NEIGH_RBL) ? p.r_core : p.cut_off;  // Neighbor.cpp:39-47
-  // ContPointLocator::SetRange/SetCutOff/SetRs, locator/ContPointLocator.h:44-73
   dv.num_cycles = (int)std::ceil(rc / rs);
-  dv.ncell = 1;
-  for (int k = 0; k < 3; ++k) {
-    dv.dims[k] = (int)(L[k] / (rc / dv.num_cycles));
-    if (dv.dims[k] < 1) dv.dims[k] = 1;
-    dv.d[k] = L[k] / dv.dims[k];
-    dv.ncell *= dv.dims[k];
+  {
+    const double lo0[3] = {lo[0], lo[1], lo[2]}, hi0[3] = {hi[0], hi[1], hi[2]};
+    set_box(lo0, hi0);
   }
+  for (int k = 0; k < 3; ++k) L0[k] = L[k];
+  if (p.ensemble == RBMD_ENS_NPT) {
+    // cell capacity of the largest box the barostat accepts (kBoxGrow x the initial edge)
+    ncell_cap = 1;
+    for (int k = 0; k < 3; ++k) ncell_cap *= std::max(1, (int)((kBoxGrow * L0[k]) / (rc / dv.num_cycles)));
+  }
+  dv.rho = N / dv.volume;  // PARA_RHO, ModelFileInitCondition.cpp:207
   // RBL capacity arithmetic: ExecutionMD.cpp:582-592 (near), 772-783 (LJ), 1033-1040 (EAM)
   if (p.neighbor == RBMD_NEIGH_RBL) {
     double coeff = 1.0;
@@ -158,7 +159,30 @@ System::System(const rbmd_system_desc& d, const rbmd_params& prm) : p(prm) {
     dv.rs_num = dv.rc_num = 0;
     dv.pice_num = 1;
   }
-  // S = H_x H_y H_z - 1, ExecForceFunction.h:771-797 (also RBEPSample.h:40-63)
+  f_near.assign(3 * N, 0.0);
+  f_far.assign(3 * N, 0.0);
+  f_bonded.assign(3 * N, 0.0);
+}
+
+void System::set_box(const double nlo[3], const double nhi[3]) {
+  // Everything that follows from the box: PARA_RANGE / PARA_BOX / volume, the locator's dims
+  // (ContPointLocator::SetRange, locator/ContPointLocator.h:44-73) and the RBE normalisation
+  // S = H_x H_y H_z - 1 (ExecForceFunction.h:771-797, RBEPSample.h:40-63).  Called at set-up and
+  // by the barostat after each accepted remap.
+  const double rc = p.cut_off;
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = nlo[k];
+    hi[k] = nhi[k];
+    L[k] = hi[k] - lo[k];
+  }
+  dv.volume = L[0] * L[1] * L[2];
+  dv.ncell = 1;
+  for (int k = 0; k < 3; ++k) {
+    dv.dims[k] = (int)(L[k] / (rc / dv.num_cycles));
+    if (dv.dims[k] < 1) dv.dims[k] = 1;
+    dv.d[k] = L[k] / dv.dims[k];
+    dv.ncell *= dv.dims[k];
+  }
   if (p.coulomb != RBMD_COUL_NONE) {
     double H[3];
     for (int k = 0; k < 3; ++k) {
@@ -169,13 +193,10 @@ System::System(const rbmd_system_desc& d, const rbmd_params& prm) : p(prm) {
     }
     dv.S = H[0] * H[1] * H[2] - 1;
   }
-  cells.dims[0] = dv.dims[0];
-  cells.dims[1] = dv.dims[1];
-  cells.dims[2] = dv.dims[2];
-  for (int k = 0; k < 3; ++k) cells.d[k] = dv.d[k];
-  f_near.assign(3 * N, 0.0);
-  f_far.assign(3 * N, 0.0);
-  f_bonded.assign(3 * N, 0.0);
+  for (int k = 0; k < 3; ++k) {
+    cells.dims[k] = dv.dims[k];
+    cells.d[k] = dv.d[k];
+  }
 }
 
 void System::min_image(double r[3]) const {

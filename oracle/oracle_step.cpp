@@ -793,7 +793,75 @@ void System::step_once() {
       double coeff = std::sqrt(1.0 + dtt * (p.temperature[0] / th.temperature - 1.0));
       for (auto& vv : v) vv = coeff * vv;
     }
+    // ExecutionNPT::Solve (ExecutionNPT.cpp:90-122): the same sequence, then the barostat
+    if (p.ensemble == RBMD_ENS_NPT) barostat_berendsen();
   }
+}
+
+// ------------------------------------------------------------------ NPT Berendsen barostat
+void System::pressure_scalar(double vir[6], double& press) const {
+  // ExecutionMD::ComputeVirial (ExecutionMD.cpp:1263-1370) and Compute_Pressure_Scalar
+  // (ExecutionNPT.cpp:1429-1447, ExecutionNVT.cpp:1258-1276).  The temperature is PARA_TEMPT as
+  // ComputeTempe left it, before the end-of-step velocity rescale.
+  for (int k = 0; k < 6; ++k) vir[k] = virial[k];
+  if (p.fix_shake == RBMD_SHAKE_TRUE)
+    for (size_t a = 0; a < shake_virial_atom.size() / 6; ++a)
+      for (int k = 0; k < 6; ++k) vir[k] += shake_virial_atom[6 * a + k];
+  if (p.force_field == RBMD_FF_EAM)
+    for (int k = 0; k < 6; ++k) vir[k] = 0;
+  press = (th.tdof * u.boltz * th.temperature + vir[0] + vir[1] + vir[2]) / 3.0 * (1.0 / dv.volume) * u.nktv2p;
+}
+
+void System::barostat_berendsen() {
+  // ExecutionNPT::fix_press_berendsen (ExecutionNPT.cpp:1334-1368): isotropic dilation
+  // mu = (1 - dt / P_damp (P_target - P) / B)^(1/3), P_target ramped from P_start to P_stop over the
+  // run; remap (:1506-1538) scales the range about its centre and carries every atom along in
+  // reduced coordinates (X2Lamda / Lamda2X worklets, RunWorklet.cpp:2638-2703); ApplyPbc
+  // (ExecutionMD.cpp:1239-1249) wraps with the new range; the locator is rebuilt.
+  double vir[6], press;
+  pressure_scalar(vir, press);
+  baro_pressure = press;
+  for (int k = 0; k < 6; ++k) baro_virial[k] = vir[k];
+  double delta = (double)step;  // currentstep - beginstep, beginstep = 0
+  if (delta != 0.0) delta = delta / (double)p.num_steps;
+  const double dt_over_period = p.timestep / p.pressure[2];
+  const double bulkmodulus_inv = 1.0 / p.bulk_modulus;
+  const double p_target = p.pressure[0] + delta * (p.pressure[1] - p.pressure[0]);
+  const double dilation = std::pow(1.0 - dt_over_period * (p_target - press) * bulkmodulus_inv, 1.0 / 3.0);
+  double nlo[3], nhi[3];
+  bool ok = std::isfinite(dilation) && dilation > 0.0;
+  const double rc = p.cut_off;
+  int ncell = 1;
+  for (int k = 0; k < 3 && ok; ++k) {
+    const double ctr = 0.5 * (lo[k] + hi[k]);
+    nlo[k] = (lo[k] - ctr) * dilation + ctr;
+    nhi[k] = (hi[k] - ctr) * dilation + ctr;
+    const double nL = nhi[k] - nlo[k];
+    const int dims = std::max(1, (int)(nL / (rc / dv.num_cycles)));
+    ncell *= dims;
+    if (!(nL >= kBoxShrink * L0[k] && nL <= kBoxGrow * L0[k]) || dims < dv.num_cycles) ok = false;
+  }
+  if (!ok || ncell > ncell_cap) {
+    status |= RBMD_STATUS_BOX_RANGE;
+    return;
+  }
+  const double olo[3] = {lo[0], lo[1], lo[2]};
+  const double hinv[3] = {1.0 / L[0], 1.0 / L[1], 1.0 / L[2]};  // set_global_box h_inv of the old box
+  set_box(nlo, nhi);
+  for (int i = 0; i < N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      double& xx = x[3 * i + k];
+      const double lamda = hinv[k] * (xx - olo[k]);
+      xx = L[k] * lamda + lo[k];
+      if (xx < lo[k]) {
+        xx += L[k];
+        image[3 * i + k] -= 1;
+      } else if (xx >= hi[k]) {
+        xx -= L[k];
+        image[3 * i + k] += 1;
+      }
+    }
+  build_cells();
 }
 
 // ------------------------------------------------------------------ a6 / a8 / a13 / a15 energies
@@ -906,17 +974,17 @@ void System::thermo(rbmd_thermo* out) {
     out->potential_energy = e_lj + out->e_coul_far + e_coul + e_bond_avg + e_angle_avg;
   else out->potential_energy = e_eam;
   out->total_energy = out->potential_energy + out->kinetic_energy;
-  double vir[6];
-  for (int k = 0; k < 6; ++k) vir[k] = virial[k];
-  if (p.fix_shake == RBMD_SHAKE_TRUE)
-    for (size_t a = 0; a < shake_virial_atom.size() / 6; ++a)
-      for (int k = 0; k < 6; ++k) vir[k] += shake_virial_atom[6 * a + k];
-  if (p.force_field == RBMD_FF_EAM)
-    for (int k = 0; k < 6; ++k) vir[k] = 0;
+  double vir[6], press;
+  pressure_scalar(vir, press);
+  if (p.ensemble == RBMD_ENS_NPT && step > 0) {
+    // NPT: the pressure of the step is the one the barostat used (PARA_PRESSURE,
+    // ExecutionNPT.cpp:1446), taken before the remap
+    press = baro_pressure;
+    for (int k = 0; k < 6; ++k) vir[k] = baro_virial[k];
+  }
   for (int k = 0; k < 6; ++k) out->virial[k] = vir[k];
   out->volume = dv.volume;
-  out->pressure = (th.tdof * u.boltz * th.temperature + vir[0] + vir[1] + vir[2]) / 3.0 *
-                  (1.0 / dv.volume) * u.nktv2p;
+  out->pressure = press;
   for (int k = 0; k < 3; ++k) {
     out->nhc_eta[k] = th.eta[k];
     out->box_lo[k] = lo[k];

@@ -5,7 +5,7 @@ a probe with the host compiler.
 """
 import ctypes as C
 
-RBMD_ABI_VERSION = 1
+RBMD_ABI_VERSION = 2
 
 # status
 OK, ERR_ARG, ERR_OOM, ERR_NUMERIC, ERR_TIMEOUT, ERR_CUDA, ERR_STATE, ERR_BUDGET, ERR_UNSUPPORTED, ERR_IO = range(10)
@@ -14,7 +14,7 @@ STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_OOM", 3: "ERR_NUMERIC", 4: "ERR_T
 
 # bits of the device status word (rbmd_thermo.status), enum rbmd_status_bit
 (STATUS_SHAKE_OVERFLOW, STATUS_SHAKE_SINGULAR, STATUS_SHAKE_NO_CONVERGE, STATUS_RATTLE_SINGULAR,
- STATUS_NON_FINITE, STATUS_RBE_SLOTS) = (1, 2, 4, 8, 16, 32)
+ STATUS_NON_FINITE, STATUS_RBE_SLOTS, STATUS_BOX_RANGE) = (1, 2, 4, 8, 16, 32, 64)
 
 FF_LJ_CUT, FF_LJ_CUT_COUL_LONG, FF_CVFF, FF_EAM = 0, 1, 2, 3
 NEIGH_RBL, NEIGH_VERLET = 0, 1
@@ -26,6 +26,7 @@ RBL_STRIDE, RBL_PHILOX = 0, 1
 RANDOM_PHILOX, RANDOM_TEST = 0, 1
 SHAKE_NULL, SHAKE_FALSE, SHAKE_TRUE = -1, 0, 1
 ENS_NVT, ENS_NVE, ENS_NPT = 0, 1, 2
+PC_BERENDSEN = 0
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 FORCE_FIELDS = {"LJ/CUT": FF_LJ_CUT, "LJ/CUT/COUL/LONG": FF_LJ_CUT_COUL_LONG, "CVFF": FF_CVFF, "EAM": FF_EAM}
@@ -49,7 +50,7 @@ class Params(C.Structure):
         ("alpha", C.c_double), ("temperature", C.c_double * 3), ("pressure", C.c_double * 3),
         ("press_ctrl", C.c_int32), ("pad0", C.c_int32),
         ("timestep", C.c_double), ("num_steps", C.c_int64),
-        ("special_bonds", C.c_double * 3), ("seed", C.c_uint64),
+        ("special_bonds", C.c_double * 3), ("seed", C.c_uint64), ("bulk_modulus", C.c_double),
     ]
 
 
@@ -145,6 +146,7 @@ def default_params(**kw):
     p.alpha = 0.1
     p.temperature[:] = (1.0, 1.0, 0.5)
     p.pressure[:] = (1.0, 1.0, 1000.0)
+    p.bulk_modulus = 10.0
     p.press_ctrl = 0
     p.timestep = 0.005
     p.num_steps = 1000

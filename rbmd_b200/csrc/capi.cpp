@@ -52,6 +52,7 @@ void rbmd_params_default(rbmd_params* p) {
   p->timestep = 0.005;
   p->num_steps = 1000;
   p->seed = 1;
+  p->bulk_modulus = 10.0;
 }
 
 int rbmd_ctx_create(const rbmd_device_cfg* cfg, rbmd_ctx** out) {

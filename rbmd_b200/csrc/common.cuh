@@ -24,8 +24,11 @@ constexpr int kMaxF32Types = 16;       // atom types of the FP32 (mixed) pair ta
 // device error word bits (rbmd_thermo.status)
 enum : int {
   kErrShakeOverflow = 1, kErrShakeSingular = 2, kErrShakeNoConverge = 4, kErrRattleSingular = 8,
-  kErrNonFinite = 16, kErrRbeSlots = 32
+  kErrNonFinite = 16, kErrRbeSlots = 32, kErrBoxRange = 64
 };
+
+// NPT box limits (edges relative to the initial box); cell tables are sized for kBoxGrow.
+constexpr double kBoxGrow = 1.25, kBoxShrink = 0.8;
 
 // Random stream tags (third Philox counter word); must match the oracle's.
 enum : uint32_t {
@@ -46,6 +49,12 @@ struct SysState {
   double virial[6];        // last virial sum (when requested)
   double shake_virial[6];  // sum of the last SHAKE virials
   double energy[8];        // energy scratch: lj, coul, eam_embed, eam_pair, bond, angle, ewald, self
+  double baro_pressure;    // NPT: pressure the barostat used this step (PARA_PRESSURE)
+  double baro_virial[6];   // NPT: virial behind it
+  double baro_lo_old[3];   // NPT: range minimum before this step's remap
+  double baro_hinv_old[3]; // NPT: 1 / edge before this step's remap
+  int baro_apply;          // NPT: this step's remap was accepted
+  int baro_pad;
   int64_t step;            // Executioner current step
   int status;              // error word
   int pad;
@@ -61,6 +70,11 @@ struct SysDev {
   int lean;   // segment-table traversal usable (every dimension holds >= 2 nc + 1 cells)
   int dense;  // pair kernel layout: tile (warp per home cell, dense systems) or warp per atom
   int blocks_pair, blocks_atom, blocks_rho, blocks_tri, rbe_mmax, rbe_slots, has_triples, n_triples;
+  // NPT Berendsen barostat: the box changes on the device every step.  Cell arrays and the cell
+  // work table hold ncell_cap cells (the box at kBoxGrow x L0); kmax indexes the Ewald k lists.
+  int npt, ncell_cap, kmax[3], npt_pad;
+  double L0[3];
+  double p_start, p_stop, p_damp, bulk;
   // geometry and physics
   double lo[3], hi[3], L[3], d[3];
   double rc, rs, rc2, rs2, alpha, volume, S;

@@ -187,13 +187,30 @@ int Context::upload_record(System* s) {
   return RBMD_OK;
 }
 
+// NPT systems change their box on the device every step: bring the host mirror of the record, and
+// the derived quantities the getters report, up to date.
+int Context::refresh(System* s) {
+  if (!s->dev.npt) return RBMD_OK;
+  cudaMemcpyAsync(&s->dev, d_sys_ + s->slot, sizeof(SysDev), cudaMemcpyDeviceToHost, stream);
+  const int rc = sync();
+  if (rc) return rc;
+  for (int k = 0; k < 3; ++k) {
+    s->dv.dims[k] = s->dev.dims[k];
+    s->dv.cell_width[k] = s->dev.d[k];
+  }
+  s->dv.n_cells = s->dev.ncell;
+  s->dv.volume = s->dev.volume;
+  s->dv.S_rbe = s->dev.S;
+  return RBMD_OK;
+}
+
 int64_t Context::estimate_bytes(const rbmd_system_desc& d, const rbmd_params& p) {
   rbmd_derived dv;
   derive(d, p, dv);
   const int64_t n = d.n_atoms;
   int64_t b = n * (32 * 3 + 16 + 12 + 4 * 2 + 32 + 16 + 16 + 8);  // x v f meta image cells sorted sx sxf smeta fp
   if (p.fix_shake == RBMD_SHAKE_TRUE && d.n_angles > 0) b += n * 32 * 3;
-  b += (int64_t)dv.n_cells * 16;
+  b += (int64_t)dv.n_cells * 16 * (p.ensemble == RBMD_ENS_NPT ? 2 : 1);  // NPT: room for kBoxGrow^3
   const int P = p.coulomb == RBMD_COUL_RBE ? p.coulomb_sample_num : 0;
   int64_t nk = P;
   if (p.coulomb == RBMD_COUL_EWALD)
@@ -221,6 +238,15 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   if (!(p.cut_off > 0) || (p.neighbor == RBMD_NEIGH_RBL && !(p.r_core > 0 && p.r_core <= p.cut_off)))
     return fail(RBMD_ERR_ARG, "cut_off must be > 0 and 0 < r_core <= cut_off");
   if (!(p.timestep > 0)) return fail(RBMD_ERR_ARG, "timestep must be > 0");
+  if (p.ensemble < 0 || p.ensemble > 2) return fail(RBMD_ERR_ARG, "unknown ensemble");
+  if (p.ensemble == RBMD_ENS_NPT) {
+    // ExecutionNPT::Solve implements the barostat only in its BERENDSEN temperature branch
+    // (ExecutionNPT.cpp:90-141; the NOSE_HOOVER branch integrates without any pressure control)
+    if (p.temp_ctrl != RBMD_TC_BERENDSEN || p.press_ctrl != RBMD_PC_BERENDSEN)
+      return fail(RBMD_ERR_UNSUPPORTED, "ensemble NPT needs temp_ctrl BERENDSEN and press_ctrl BERENDSEN");
+    if (!(p.pressure[2] > 0) || !(p.bulk_modulus > 0))
+      return fail(RBMD_ERR_ARG, "NPT needs a pressure damping time (pressure[2]) and bulk_modulus > 0");
+  }
   if (p.precision == RBMD_PREC_MIXED && d.n_types > kMaxF32Types)
     return fail(RBMD_ERR_UNSUPPORTED, "mixed precision supports at most " + std::to_string(kMaxF32Types) +
                                           " atom types");
@@ -333,6 +359,25 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
       D.dense = (stencil_ok && n < (1 << 25)) ? 1 : 0;
     }
   }
+  if (p.ensemble == RBMD_ENS_NPT) {
+    // The box changes every step: the general traversal (any dims), cell tables for the largest
+    // box the barostat accepts.
+    D.npt = 1;
+    D.lean = 0;
+    D.dense = 0;
+    D.ncell_cap = 1;
+    for (int k = 0; k < 3; ++k) {
+      D.L0[k] = D.L[k];
+      D.kmax[k] = p.kmax[k];
+      D.ncell_cap *= std::max(1, (int)((kBoxGrow * D.L0[k]) / (D.rc / D.nc)));
+    }
+    D.p_start = p.pressure[0];
+    D.p_stop = p.pressure[1];
+    D.p_damp = p.pressure[2];
+    D.bulk = p.bulk_modulus;
+  } else {
+    D.ncell_cap = D.ncell;
+  }
   D.blocks_pair = D.dense ? (D.ncell + kCellWarpsHost - 1) / kCellWarpsHost : (n + kPairWarps - 1) / kPairWarps;
   D.blocks_atom = (n + kAtomBlock - 1) / kAtomBlock;
   D.blocks_rho = (n + kRhoChunk - 1) / kRhoChunk;
@@ -365,7 +410,7 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
     double smax = 0;
     for (int k = 0; k < 3; ++k) {
       D.rbe_sigma[k] = std::sqrt(p.alpha / 2.0) * D.L[k] / kPi;
-      smax = std::max(smax, D.rbe_sigma[k]);
+      smax = std::max(smax, D.rbe_sigma[k] * (D.npt ? kBoxGrow : 1.0));  // NPT: table for the largest box
     }
     D.rbe_mmax = std::min(4096, (int)std::ceil(12.0 * smax) + 4);
     D.rbe_slots = std::min(1024, D.P + kRbeSlack);
@@ -476,9 +521,9 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   D.meta = (int4*)dal(sizeof(int4) * n);
   D.image = (int*)dal(sizeof(int) * 3 * n);
   D.cell_of_atom = (int*)dal(sizeof(int) * n);
-  D.cell_count = (int*)dal(sizeof(int) * D.ncell);
-  D.cell_start = (int*)dal(sizeof(int) * (D.ncell + 1));
-  D.cell_fill = (int*)dal(sizeof(int) * D.ncell);
+  D.cell_count = (int*)dal(sizeof(int) * D.ncell_cap);
+  D.cell_start = (int*)dal(sizeof(int) * (D.ncell_cap + 1));
+  D.cell_fill = (int*)dal(sizeof(int) * D.ncell_cap);
   D.sorted = (int*)dal(sizeof(int) * n);
   D.rank = (int*)dal(sizeof(int) * n);
   D.sx = (double4*)dal(sizeof(double4) * n);
@@ -640,7 +685,7 @@ static bool same_group(const System* a, const System* b) {
   return x.ff == y.ff && x.neigh == y.neigh && x.coul == y.coul && x.prec == y.prec &&
          x.temp_ctrl == y.temp_ctrl && x.special == y.special && x.has_triples == y.has_triples &&
          ((x.n_bonds + x.n_angles) > 0) == ((y.n_bonds + y.n_angles) > 0) && x.dense == y.dense &&
-         x.lean == y.lean;
+         x.lean == y.lean && x.npt == y.npt;
 }
 
 Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& rc) {
@@ -659,6 +704,7 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
   b.has_bonded = (g.n_bonds + g.n_angles) > 0;
   b.dense = g.dense;
   b.lean = g.lean;
+  b.npt = g.npt;
   std::vector<int> slots;
   std::vector<int2> wa, wp, wc, wr, wt, wm;
   for (System* s : group) {
@@ -672,7 +718,7 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
       for (int k = 0; k < D.ncell; k += kCellWarpsHost) wp.push_back(make_int2(s->slot, k));
     else
       for (int k = 0; k < D.n; k += kPairWarps) wp.push_back(make_int2(s->slot, k));
-    for (int k = 0; k < D.ncell; k += kCellBlock) wc.push_back(make_int2(s->slot, k));
+    for (int k = 0; k < D.ncell_cap; k += kCellBlock) wc.push_back(make_int2(s->slot, k));
     for (int k = 0; k < D.n; k += kRhoChunk) wr.push_back(make_int2(s->slot, k));
     for (int k = 0; k < D.n_triples; k += 128) wt.push_back(make_int2(s->slot, k));
     for (int k = 0; k < D.n_bonds + D.n_angles; k += 128) wm.push_back(make_int2(s->slot, k));
@@ -784,13 +830,16 @@ void Context::enqueue_step(const Batch& b) {
   if (b.has_shake) timed("shake", 0, [&] { launch_shake(b, stream); });
   if (b.coul == RBMD_COUL_RBE) timed("rbe_sample", 0, [&] { launch_rbe_sample(b, stream); });
   if (b.coul != RBMD_COUL_NONE) timed("rho", 0, [&] { launch_rho(b, stream, b.coul == RBMD_COUL_EWALD); });
-  if (b.has_bonded) timed("bonded", 0, [&] { launch_bonded(b, stream, 0); });
-  timed(pair_name(b), (double)b.natoms, [&] { launch_pair(b, stream, 0); });
-  timed("final", (double)b.natoms, [&] { launch_final(b, stream, kFinalKick, 0); });
+  // NPT: the barostat needs the virial of this evaluation
+  const int vir = b.npt;
+  if (b.has_bonded) timed("bonded", 0, [&] { launch_bonded(b, stream, vir); });
+  timed(pair_name(b), (double)b.natoms, [&] { launch_pair(b, stream, vir); });
+  timed("final", (double)b.natoms, [&] { launch_final(b, stream, kFinalKick, vir); });
   if (b.has_shake) {
     timed("rattle", 0, [&] { launch_rattle(b, stream); });
     if (b.temp_ctrl != RBMD_TC_NOSE_HOOVER) timed("ke", 0, [&] { launch_ke_thermostat(b, stream); });
   }
+  if (b.npt) timed("barostat", 0, [&] { launch_barostat(b, stream); });
 }
 
 int Context::init(const int32_t* ids, int n) {
@@ -961,9 +1010,10 @@ int Context::get_thermo(int id, rbmd_thermo* out) {
   System* s = find(id);
   if (!s) return fail(RBMD_ERR_STATE, "unknown system id");
   if (!out) return fail(RBMD_ERR_ARG, "null output");
+  int rc = refresh(s);
+  if (rc) return rc;
   const SysDev& D = s->dev;
   int32_t one = id;
-  int rc;
   auto bs = [&] {
     rbmd_device_cfg saved = cfg;
     cfg.batched = 0;
@@ -977,6 +1027,11 @@ int Context::get_thermo(int id, rbmd_thermo* out) {
   void* fsave = nullptr;
   if (cudaMalloc(&fsave, sizeof(double4) * D.n) != cudaSuccess) return fail(RBMD_ERR_OOM, "thermo scratch");
   cudaMemcpyAsync(fsave, D.f, sizeof(double4) * D.n, cudaMemcpyDeviceToDevice, stream);
+  // NPT: bond and angle energies are those of the step's force evaluation, before the remap
+  // (PARA_BOND_ENERGY / PARA_ANGLE_ENERGY are set there and read by ThermoOutput::Execute)
+  std::vector<double> te_step(D.npt ? s->n_terms : 0);
+  if (!te_step.empty())
+    cudaMemcpyAsync(te_step.data(), D.term_energy, sizeof(double) * te_step.size(), cudaMemcpyDeviceToHost, stream);
   cudaMemsetAsync(&D.st->virial[0], 0, sizeof(double) * 6, stream);
   launch_cells(b, stream);
   if (b.coul == RBMD_COUL_RBE) launch_rbe_sample(b, stream);
@@ -994,6 +1049,7 @@ int Context::get_thermo(int id, rbmd_thermo* out) {
   rc = sync();
   cudaFree(fsave);
   if (rc) return rc;
+  if (!te_step.empty() && st.step > 0) te.swap(te_step);
   std::memset(out, 0, sizeof(*out));
   const int n = D.n;
   out->step = st.step;
@@ -1025,9 +1081,15 @@ int Context::get_thermo(int id, rbmd_thermo* out) {
     for (int k = 0; k < 6; ++k) vir[k] += st.shake_virial[k];
   if (D.ff == RBMD_FF_EAM)
     for (int k = 0; k < 6; ++k) vir[k] = 0;
+  out->pressure = (st.tdof * D.boltz * st.temperature + vir[0] + vir[1] + vir[2]) / 3.0 * (1.0 / D.volume) * D.nktv2p;
+  if (D.npt && st.step > 0) {
+    // NPT: the pressure of the step is the one the barostat used (PARA_PRESSURE,
+    // ExecutionNPT.cpp:1446), taken before the remap
+    out->pressure = st.baro_pressure;
+    for (int k = 0; k < 6; ++k) vir[k] = st.baro_virial[k];
+  }
   for (int k = 0; k < 6; ++k) out->virial[k] = vir[k];
   out->volume = D.volume;
-  out->pressure = (st.tdof * D.boltz * st.temperature + vir[0] + vir[1] + vir[2]) / 3.0 * (1.0 / D.volume) * D.nktv2p;
   for (int k = 0; k < 3; ++k) {
     out->nhc_eta[k] = st.eta[k];
     out->box_lo[k] = D.lo[k];
@@ -1050,6 +1112,8 @@ int Context::get_cells(int id, int32_t* dims, int32_t* coa, int32_t* sorted, int
   cfg = saved;
   if (rc) return rc;
   launch_cells(bs[0]->b, stream);
+  rc = refresh(s);
+  if (rc) return rc;
   const SysDev& D = s->dev;
   if (dims)
     for (int k = 0; k < 3; ++k) dims[k] = D.dims[k];
@@ -1096,6 +1160,8 @@ int Context::get_rbl_lists(int id, int cap, int32_t* nc, int32_t* ns, int32_t* i
   cfg = saved;
   if (rc) return rc;
   launch_cells(bs[0]->b, stream);
+  rc = refresh(s);
+  if (rc) return rc;
   const int n = s->dev.n;
   int *d_nc = nullptr, *d_ns = nullptr, *d_ids = nullptr;
   if (cudaMalloc(&d_nc, sizeof(int) * n) != cudaSuccess || cudaMalloc(&d_ns, sizeof(int) * n) != cudaSuccess ||
@@ -1137,6 +1203,8 @@ int Context::get_rbl_lists_static(int id, int cap, int32_t* nc, int32_t* ns, int
   if (!s) return fail(RBMD_ERR_STATE, "unknown system id");
   if (cap <= 0 || !nc || !ns || !ids) return fail(RBMD_ERR_ARG, "bad list buffers");
   if (s->dev.neigh != RBMD_NEIGH_RBL) return fail(RBMD_ERR_STATE, "system does not use RBL");
+  const int rr = refresh(s);
+  if (rr) return rr;
   const SysDev& D = s->dev;
   const long long need = static_list_ints(D.n, D.ncell, D.dense, cap);
   if (need > kStaticListInts)
@@ -1172,8 +1240,11 @@ int Context::get_kspace(int id, int32_t* m, double* rhok) {
 }
 
 int Context::get_derived(int id, rbmd_derived* out) {
+  std::lock_guard<std::recursive_mutex> lk(mu);
   System* s = find(id);
   if (!s) return fail(RBMD_ERR_STATE, "unknown system id");
+  const int rc = refresh(s);
+  if (rc) return rc;
   *out = s->dv;
   return RBMD_OK;
 }

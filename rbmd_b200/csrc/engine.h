@@ -87,6 +87,7 @@ class Context {
   };
   int ensure_slots(int need);
   int upload_record(System* s);
+  int refresh(System* s);
   std::vector<BatchRec*> batches_for(const int32_t* ids, int n, int& rc);
   BatchRec* build_batch(const std::vector<System*>& group, int& rc);
   void drop_batches_with(int id);

@@ -93,6 +93,10 @@ __global__ void k_nhc_a(const SysDev* __restrict__ S, const int* __restrict__ sl
   const SysDev& s = S[slots[k]];
   SysState* st = s.st;
   st->step += 1;
+  // NPT: the step's force evaluation accumulates the virial the barostat reads (the RBL pair
+  // kernels add nothing to it, so it starts from zero here)
+  if (s.npt)
+    for (int c = 0; c < 6; ++c) st->virial[c] = 0.0;
   if (s.temp_ctrl == RBMD_TC_NOSE_HOOVER) {
     compute_temp_target(s, st);
     st->vscale_a = nhc_half(s, st);

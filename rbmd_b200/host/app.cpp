@@ -405,18 +405,30 @@ void MDApplication::ReadExecution(const Json& ex) {
   const std::string ens = ex.string("ensemble", "NVT");
   if (ens == "NVT") P.ensemble = RBMD_ENS_NVT;
   else if (ens == "NVE") P.ensemble = RBMD_ENS_NVE;
-  else if (ens == "NPT") throw std::runtime_error("ensemble NPT is not implemented by this library");
+  else if (ens == "NPT") P.ensemble = RBMD_ENS_NPT;
   else throw std::runtime_error("ensemble \"" + ens + "\" is not supported");
   const std::vector<double> t = ex.numbers("temperature");
   for (int k = 0; k < 3 && k < (int)t.size(); ++k) P.temperature[k] = t[k];
+  // "pressure": [P_start, P_stop, P_damp, bulk modulus] (ExecutionMD.cpp:152, ExecutionNPT.cpp:953);
+  // the reference reads the fourth entry unconditionally, here it is optional (default 10)
   const std::vector<double> pr = ex.numbers("pressure");
   for (int k = 0; k < 3 && k < (int)pr.size(); ++k) P.pressure[k] = pr[k];
+  if (pr.size() >= 4) P.bulk_modulus = pr[3];
   const std::string tc = ex.string("temp_ctrl_type", "NOSE_HOOVER");
   if (P.ensemble == RBMD_ENS_NVE) P.temp_ctrl = RBMD_TC_NONE;
   else if (tc == "NOSE_HOOVER") P.temp_ctrl = RBMD_TC_NOSE_HOOVER;
   else if (tc == "BERENDSEN") P.temp_ctrl = RBMD_TC_BERENDSEN;
   else if (tc == "TEMP_RESCALE") P.temp_ctrl = RBMD_TC_RESCALE;
   else throw std::runtime_error("temp_ctrl_type \"" + tc + "\" is not supported");
+  if (P.ensemble == RBMD_ENS_NPT) {
+    // ExecutionNPT::Solve (ExecutionNPT.cpp:90-141) controls the pressure only in its BERENDSEN
+    // temperature branch, with press_ctrl_type BERENDSEN
+    const std::string pc = ex.string("press_ctrl_type", "BERENDSEN");
+    if (pc != "BERENDSEN") throw std::runtime_error("press_ctrl_type \"" + pc + "\" is not supported (BERENDSEN)");
+    if (P.temp_ctrl != RBMD_TC_BERENDSEN)
+      throw std::runtime_error("ensemble NPT needs temp_ctrl_type BERENDSEN (the reference's only NPT path)");
+    P.press_ctrl = RBMD_PC_BERENDSEN;
+  }
   P.timestep = ex.number("timestep", P.timestep);
   P.num_steps = (int64_t)ex.number("num_steps", (double)P.num_steps);
   // keys this library adds (absent from reference files): seed, precision, rbl_mode
@@ -509,12 +521,14 @@ void MDApplication::DumpSystem(const std::string& path) const {
                "\"temp_ctrl\": %d, \"units\": %d, \"precision\": %d, \"rbl_mode\": %d, \"fix_shake\": %d, "
                "\"init_inbuild\": %d, \"neighbor_sample_num\": %d, \"cut_off\": %.17g, \"r_core\": %.17g, "
                "\"coulomb_sample_num\": %d, \"kmax\": [%d,%d,%d], \"alpha\": %.17g, \"temperature\": [%.17g,%.17g,%.17g], "
-               "\"timestep\": %.17g, \"num_steps\": %lld, \"special_bonds\": [%.17g,%.17g,%.17g], \"seed\": %llu},\n",
+               "\"timestep\": %.17g, \"num_steps\": %lld, \"special_bonds\": [%.17g,%.17g,%.17g], \"seed\": %llu, "
+               "\"pressure\": [%.17g,%.17g,%.17g], \"bulk_modulus\": %.17g, \"press_ctrl\": %d},\n",
                P.force_field, P.neighbor, P.coulomb, P.ensemble, P.temp_ctrl, P.units, P.precision, P.rbl_mode,
                P.fix_shake, P.init_inbuild, P.neighbor_sample_num, P.cut_off, P.r_core, P.coulomb_sample_num,
                P.kmax[0], P.kmax[1], P.kmax[2], P.alpha, P.temperature[0], P.temperature[1], P.temperature[2],
                P.timestep, (long long)P.num_steps, P.special_bonds[0], P.special_bonds[1], P.special_bonds[2],
-               (unsigned long long)P.seed);
+               (unsigned long long)P.seed, P.pressure[0], P.pressure[1], P.pressure[2], P.bulk_modulus,
+               P.press_ctrl);
   darr("position", _para.position);
   darr("velocity", _para.velocity);
   darr("charge", _para.charge);

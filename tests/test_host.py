@@ -142,7 +142,8 @@ def test_eam_potential_file(rbmd_bin, tmp_path, oracle_mod):
 
 
 @pytest.mark.parametrize("mutate,message", [
-    (lambda cfg: cfg["execution"].update(ensemble="NPT"), "NPT"),
+    (lambda cfg: cfg["execution"].update(ensemble="NPT", temp_ctrl_type="NOSE_HOOVER"), "BERENDSEN"),
+    (lambda cfg: cfg["execution"].update(ensemble="NPT", temp_ctrl_type="BERENDSEN", press_ctrl_type="MTK"), "MTK"),
     (lambda cfg: cfg["init_configuration"]["read_data"].update(atom_style="molecular"), "atom_style"),
     (lambda cfg: cfg["init_configuration"]["read_data"].update(file="missing.data"), "missing.data"),
     (lambda cfg: cfg["hyper_parameters"]["force_field"].update(type="OPLS-AA"), "OPLS-AA"),
@@ -156,6 +157,21 @@ def test_errors_are_reported(rbmd_bin, tmp_path, mutate, message):
     r = subprocess.run([rbmd_bin, "-j", path, "--dump-system", str(tmp_path / "d.json")], capture_output=True,
                        text=True)
     assert r.returncode == 1 and message in r.stderr
+
+
+@pytest.mark.parametrize("pressure,bulk", [([1.0, 2.0, 100.0], 10.0), ([1.0, 2.0, 100.0, 25000.0], 25000.0)])
+def test_npt_berendsen_input(rbmd_bin, tmp_path, pressure, bulk):
+    """ensemble NPT with BERENDSEN temperature and pressure control; the optional fourth pressure
+    entry is the bulk modulus (ExecutionNPT.cpp:953)."""
+    sd = synth.spce_water(n_mol=8)
+    path = synth.write_rbmd_input(sd, str(tmp_path))
+    cfg = json.load(open(path))
+    cfg["execution"].update(ensemble="NPT", temp_ctrl_type="BERENDSEN", press_ctrl_type="BERENDSEN",
+                            pressure=pressure)
+    json.dump(cfg, open(path, "w"))
+    P = dump(rbmd_bin, path, tmp_path)["params"]
+    assert P["ensemble"] == A.ENS_NPT and P["temp_ctrl"] == A.TC_BERENDSEN and P["press_ctrl"] == A.PC_BERENDSEN
+    assert P["pressure"] == pressure[:3] and P["bulk_modulus"] == bulk
 
 
 def test_truncated_data_file(rbmd_bin, tmp_path):

@@ -228,3 +228,74 @@ def test_nose_hoover_moves_toward_target(oracle_mod):
     o.step(200)
     t1 = o.thermo()["temperature"]
     assert abs(t1 - 1.5) < abs(t0 - 1.5)
+
+
+def _npt(sd, p_start=0.5, p_stop=0.5, p_damp=0.5, bulk=10.0, num_steps=100):
+    p = sd.params
+    p.ensemble, p.temp_ctrl, p.press_ctrl = A.ENS_NPT, A.TC_BERENDSEN, A.PC_BERENDSEN
+    p.pressure[:] = (p_start, p_stop, p_damp)
+    p.bulk_modulus = bulk
+    p.num_steps = num_steps
+    return sd
+
+
+def test_berendsen_barostat_one_step_closed_form(oracle_mod):
+    """One NPT step = the Berendsen NVT step followed by the dilation
+    mu = (1 - dt/P_damp (P_target - P) / B)^(1/3) about the box centre, atoms carried along in
+    reduced coordinates (ExecutionNPT.cpp:1334-1368, 1506-1538)."""
+    base = synth.lj_fcc(cells=5)
+    base.params.temp_ctrl = A.TC_BERENDSEN
+    nvt = oracle_mod.Oracle(base.copy())
+    nvt.init()
+    nvt.step(1)
+    x_nvt, v_nvt, img_nvt = nvt.state()
+    sd = _npt(base.copy(), p_start=0.2, p_stop=1.2, num_steps=50)
+    o = oracle_mod.Oracle(sd)
+    o.init()
+    o.step(1)
+    t = o.thermo()
+    P = t["pressure"]
+    assert P == pytest.approx(nvt.thermo()["pressure"], rel=1e-12)  # the NVT step's own pressure
+    target = 0.2 + (1 / 50) * (1.2 - 0.2)
+    mu = (1 - sd.params.timestep / 0.5 * (target - P) / 10.0) ** (1 / 3)
+    lo0, hi0 = base.box_lo, base.box_hi
+    ctr = 0.5 * (lo0 + hi0)
+    lo1, hi1 = (lo0 - ctr) * mu + ctr, (hi0 - ctr) * mu + ctr
+    assert np.allclose(t["box_lo"], lo1, rtol=0, atol=1e-13) and np.allclose(t["box_hi"], hi1, rtol=0, atol=1e-13)
+    assert t["volume"] == pytest.approx(np.prod(hi1 - lo1), rel=1e-13)
+    lam = (x_nvt - lo0) / (hi0 - lo0)
+    x1 = lam * (hi1 - lo1) + lo1
+    x, v, img = o.state()
+    wrap = np.floor((x1 - lo1) / (hi1 - lo1))
+    assert np.allclose(x, x1 - wrap * (hi1 - lo1), rtol=0, atol=1e-12)
+    assert np.array_equal(img, img_nvt + wrap.astype(np.int32))
+    assert np.array_equal(v, v_nvt)  # the barostat leaves velocities alone
+    assert t["status"] == 0
+
+
+def test_berendsen_barostat_moves_volume_toward_target(oracle_mod):
+    """While the pressure stays above the target the box grows every step; below it, it shrinks
+    (the fcc start melts within these steps, so the pressure itself is not monotone)."""
+    for target, grows in ((0.2, True), (3.0, False)):
+        o = oracle_mod.Oracle(_npt(synth.lj_fcc(cells=5), p_start=target, p_stop=target, p_damp=0.2))
+        o.init()
+        vols = [o.thermo()["volume"]]
+        for _ in range(30):
+            o.step(1)
+            t = o.thermo()
+            assert (t["pressure"] > target) == grows
+            vols.append(t["volume"])
+        d = np.diff(vols)
+        assert (d > 0).all() if grows else (d < 0).all()
+
+
+def test_barostat_refuses_boxes_outside_the_cell_range(oracle_mod):
+    """A dilation past 1.25x (or below 0.8x) the initial edge leaves the box alone and sets
+    RBMD_STATUS_BOX_RANGE."""
+    sd = _npt(synth.lj_fcc(cells=5), p_start=-1e6, p_stop=-1e6, p_damp=0.01, bulk=1.0)
+    o = oracle_mod.Oracle(sd)
+    o.init()
+    o.step(1)
+    t = o.thermo()
+    assert t["status"] & A.STATUS_BOX_RANGE
+    assert list(t["box_lo"]) == list(sd.box_lo) and list(t["box_hi"]) == list(sd.box_hi)
