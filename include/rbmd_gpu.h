@@ -92,7 +92,11 @@ enum rbmd_ensemble {
   RBMD_ENS_NVT = 0, RBMD_ENS_NVE = 1, RBMD_ENS_NPT = 2
 };
 enum rbmd_press_ctrl {
-  RBMD_PC_BERENDSEN = 0      /* "Berendsen" isotropic volume rescale */
+  RBMD_PC_BERENDSEN = 0,     /* "BERENDSEN": isotropic volume rescale at the end of the step
+                                (ExecutionNPT::fix_press_berendsen); needs temp_ctrl BERENDSEN */
+  RBMD_PC_NOSE_HOOVER = 1    /* "NOSE_HOOVER": isotropic MTK barostat with its own chain
+                                (ExecutionNPT::InitialIntegrate / FinalIntegrate); needs temp_ctrl
+                                NOSE_HOOVER */
 };
 
 /* ---------------------------------------------------------------- run parameters */
@@ -117,8 +121,9 @@ typedef struct rbmd_params {
   int32_t kmax[3];              /* Ewald k range (energy in RBE mode, force in EWALD mode) */
   double alpha;                 /* Ewald splitting, reference convention: erfc(sqrt(alpha) r) */
   double temperature[3];        /* T_start, T_stop, T_damp */
-  double pressure[3];           /* P_start, P_stop, P_damp (NPT; ensemble NPT needs temp_ctrl
-                                   BERENDSEN and press_ctrl BERENDSEN, ExecutionNPT.cpp:90-141) */
+  double pressure[3];           /* P_start, P_stop, P_damp (NPT; ExecutionNPT.cpp:90-141 controls the
+                                   pressure for temp_ctrl / press_ctrl BERENDSEN / BERENDSEN and
+                                   NOSE_HOOVER / NOSE_HOOVER, the two pairs accepted here) */
   int32_t press_ctrl;           /* enum rbmd_press_ctrl */
   int32_t pad0;
   double timestep;

@@ -109,6 +109,12 @@ struct Thermostat {  // ExecutionNVT::InitialCondition / SetUp, ExecutionNVT.cpp
   double tdof = 0;
 };
 
+struct Barostat {  // ExecutionNPT MTK state, ExecutionNPT.cpp:145-232, 1545-1603 (iso, pdim 3)
+  double omega_dot[3] = {0, 0, 0}, omega_mass[3] = {0, 0, 0};
+  double etap[3] = {0, 0, 0}, etap_dot[4] = {0, 0, 0, 0}, etap_dotdot[3] = {0, 0, 0}, etap_mass[3] = {0, 0, 0};
+  double p_hydro = 0, p_current = 0, mtk_term1 = 0, mtk_term2 = 0;
+};
+
 class System {
  public:
   System(const rbmd_system_desc& desc, const rbmd_params& params);
@@ -139,6 +145,7 @@ class System {
   double baro_virial[6] = {0, 0, 0, 0, 0, 0};
   int64_t step = 0;  // Executioner::_current_step
   Thermostat th;
+  Barostat bs;
   Cells cells;
 
   // last force evaluation by-products
@@ -174,6 +181,14 @@ class System {
   void set_box(const double nlo[3], const double nhi[3]);
   void pressure_scalar(double vir[6], double& press) const;
   void barostat_berendsen();
+  bool mtk() const { return p.ensemble == RBMD_ENS_NPT && p.press_ctrl == RBMD_PC_NOSE_HOOVER; }
+  void mtk_setup();
+  void nhc_press_integrate();
+  void compute_press_target();
+  void nh_omega_dot();
+  void nh_v_press();
+  void mtk_remap();
+  void step_mtk();
   void compute_tempe();
   void compute_temp_target();
   void nhc_integrate();

@@ -756,12 +756,17 @@ void System::init() {
   for (int ich = 1; ich < 3; ich++)
     th.eta_dotdot[ich] = (th.eta_mass[ich - 1] * th.eta_dot[ich - 1] * th.eta_dot[ich - 1] -
                           u.boltz * th.t_target) / th.eta_mass[ich];
+  if (mtk()) mtk_setup();
   compute_force();
 }
 
 void System::step_once() {
   // Executioner::TakeStep (framework/executioner/Executioner.cpp:112-117) -> ExecutionNVT
   // PreSolve/Solve (framework/run/ExecutionNVT.cpp:76-135)
+  if (mtk()) {
+    step_mtk();
+    return;
+  }
   step += 1;
   if (p.coulomb == RBMD_COUL_RBE) sample_k();
   const bool shk = (p.fix_shake == RBMD_SHAKE_TRUE) && !angle_atoms.empty();
@@ -862,6 +867,180 @@ void System::barostat_berendsen() {
       }
     }
   build_cells();
+}
+
+// ------------------------------------------------------------------ NPT MTK barostat
+// ExecutionNPT with temp_ctrl_type and press_ctrl_type NOSE_HOOVER: an isotropic
+// Martyna-Tobias-Klein barostat (p_flag 1 1 1, pdim 3) with a 3-link chain on the barostat
+// velocity, integrated around velocity Verlet (ExecutionNPT.cpp:145-232, 1545-2066).
+void System::mtk_setup() {
+  // SetUp, barostat part (ExecutionNPT.cpp:1573-1602); t_target of step 0
+  const double p_freq = 1 / p.pressure[2], p_freq_max = p_freq;
+  const double kt = u.boltz * th.t_target;
+  const double nkt = (N + 1) * kt;
+  for (int i = 0; i < 3; ++i) bs.omega_mass[i] = nkt / (p_freq * p_freq);
+  bs.etap_mass[0] = u.boltz * th.t_target / (p_freq_max * p_freq_max);
+  for (int ich = 1; ich < 3; ich++) bs.etap_mass[ich] = u.boltz * th.t_target / (p_freq_max * p_freq_max);
+  for (int ich = 1; ich < 3; ich++)
+    bs.etap_dotdot[ich] = (bs.etap_mass[ich - 1] * bs.etap_dot[ich - 1] * bs.etap_dot[ich - 1] -
+                           u.boltz * th.t_target) / bs.etap_mass[ich];
+}
+
+void System::nhc_press_integrate() {
+  // NHCPressIntegrate, ExecutionNPT.cpp:1831-1915 (mpchain 3, nc_pchain 1, no drag)
+  const int mpchain = 3;
+  const double dt = p.timestep, dthalf = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt;
+  const double kt = u.boltz * th.t_target;
+  const double pdrag_factor = 1.0;
+  double kecurrent = 0.0;
+  for (int i = 0; i < 3; ++i) kecurrent += bs.omega_mass[i] * bs.omega_dot[i] * bs.omega_dot[i];
+  const double lkt_press = kt;
+  bs.etap_dotdot[0] = (kecurrent - lkt_press) / bs.etap_mass[0];
+  const double ncfac = 1.0;
+  double expfac;
+  for (int ich = mpchain - 1; ich > 0; ich--) {
+    expfac = std::exp(-ncfac * dt8 * bs.etap_dot[ich + 1]);
+    bs.etap_dot[ich] *= expfac;
+    bs.etap_dot[ich] += bs.etap_dotdot[ich] * ncfac * dt4;
+    bs.etap_dot[ich] *= pdrag_factor;
+    bs.etap_dot[ich] *= expfac;
+  }
+  expfac = std::exp(-ncfac * dt8 * bs.etap_dot[1]);
+  bs.etap_dot[0] *= expfac;
+  bs.etap_dot[0] += bs.etap_dotdot[0] * ncfac * dt4;
+  bs.etap_dot[0] *= pdrag_factor;
+  bs.etap_dot[0] *= expfac;
+  for (int ich = 0; ich < mpchain; ich++) bs.etap[ich] += ncfac * dthalf * bs.etap_dot[ich];
+  const double factor_etap = std::exp(-ncfac * dthalf * bs.etap_dot[0]);
+  for (int i = 0; i < 3; ++i) bs.omega_dot[i] *= factor_etap;
+  kecurrent = 0.0;
+  for (int i = 0; i < 3; ++i) kecurrent += bs.omega_mass[i] * bs.omega_dot[i] * bs.omega_dot[i];
+  bs.etap_dotdot[0] = (kecurrent - lkt_press) / bs.etap_mass[0];
+  bs.etap_dot[0] *= expfac;
+  bs.etap_dot[0] += bs.etap_dotdot[0] * ncfac * dt4;
+  bs.etap_dot[0] *= expfac;
+  for (int ich = 1; ich < mpchain; ich++) {
+    expfac = std::exp(-ncfac * dt8 * bs.etap_dot[ich + 1]);
+    bs.etap_dot[ich] *= expfac;
+    bs.etap_dotdot[ich] = (bs.etap_mass[ich - 1] * bs.etap_dot[ich - 1] * bs.etap_dot[ich - 1] -
+                           u.boltz * th.t_target) / bs.etap_mass[ich];
+    bs.etap_dot[ich] += bs.etap_dotdot[ich] * ncfac * dt4;
+    bs.etap_dot[ich] *= expfac;
+  }
+}
+
+void System::compute_press_target() {
+  // ComputePressTarget, ExecutionNPT.cpp:1631-1669.  The division by pdim sits inside the loop
+  // there, so p_hydro = ((P/3 + P)/3 + P)/3 for an isotropic target P; kept as written.
+  bs.p_hydro = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    double pt;
+    if (p.pressure[1] == p.pressure[0]) {
+      pt = p.pressure[0];
+    } else {
+      double delta = (double)step;
+      if (delta != 0.0) delta = delta / (double)p.num_steps;
+      pt = p.pressure[0] + delta * (p.pressure[1] - p.pressure[0]);
+    }
+    bs.p_hydro += pt;
+    bs.p_hydro /= 3;
+  }
+}
+
+void System::nh_omega_dot() {
+  // NHOmegaDot, ExecutionNPT.cpp:1942-1986 (mtk_flag 1, no drag); volume from PARA_BOX
+  const double dthalf = 0.5 * p.timestep;
+  const double volume = L[0] * L[1] * L[2];
+  bs.mtk_term1 = th.tdof * u.boltz * th.temperature;
+  bs.mtk_term1 /= 3 * N;
+  for (int i = 0; i < 3; ++i) {
+    const double f_omega = (bs.p_current - bs.p_hydro) * volume / (bs.omega_mass[i] * u.nktv2p) +
+                           bs.mtk_term1 / bs.omega_mass[i];
+    bs.omega_dot[i] += f_omega * dthalf;
+  }
+  bs.mtk_term2 = 0.0;
+  for (int i = 0; i < 3; ++i) bs.mtk_term2 += bs.omega_dot[i];
+  bs.mtk_term2 /= 3 * N;
+}
+
+void System::nh_v_press() {
+  // NH_V_Press, ExecutionNPT.cpp:1988-1997: the per-dimension factor is applied twice
+  const double dt4 = 0.25 * p.timestep;
+  double fac[3];
+  for (int k = 0; k < 3; ++k) fac[k] = std::exp(-dt4 * (bs.omega_dot[k] + bs.mtk_term2));
+  for (int rep = 0; rep < 2; ++rep)
+    for (int i = 0; i < N; ++i)
+      for (int k = 0; k < 3; ++k) v[3 * i + k] = fac[k] * v[3 * i + k];
+}
+
+void System::mtk_remap() {
+  // ReMap, ExecutionNPT.cpp:1999-2066: the range scaled by exp(dto omega_dot) about the fixed point
+  // (the range centre set_global_box stored), atoms carried along in reduced coordinates, no wrap.
+  const double dto = 0.5 * p.timestep;
+  const double rc = p.cut_off;
+  double nlo[3], nhi[3];
+  bool ok = true;
+  int ncell = 1;
+  for (int k = 0; k < 3; ++k) {
+    const double fixedpoint = 0.5 * (lo[k] + hi[k]);
+    const double expfac = std::exp(dto * bs.omega_dot[k]);
+    nlo[k] = (lo[k] - fixedpoint) * expfac + fixedpoint;
+    nhi[k] = (hi[k] - fixedpoint) * expfac + fixedpoint;
+    const double nL = nhi[k] - nlo[k];
+    const int dims = (std::isfinite(nL) && nL > 0) ? std::max(1, (int)(nL / (rc / dv.num_cycles))) : 0;
+    ncell *= std::max(dims, 1);
+    if (!(nL >= kBoxShrink * L0[k] && nL <= kBoxGrow * L0[k]) || dims < dv.num_cycles) ok = false;
+  }
+  if (!ok || ncell > ncell_cap) {
+    status |= RBMD_STATUS_BOX_RANGE;
+    return;
+  }
+  const double olo[3] = {lo[0], lo[1], lo[2]};
+  const double hinv[3] = {1.0 / L[0], 1.0 / L[1], 1.0 / L[2]};
+  set_box(nlo, nhi);
+  for (int i = 0; i < N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      double& xx = x[3 * i + k];
+      const double lamda = hinv[k] * (xx - olo[k]);
+      xx = L[k] * lamda + lo[k];
+    }
+  build_cells();
+}
+
+void System::step_mtk() {
+  // ExecutionNPT::Solve, NOSE_HOOVER branch (ExecutionNPT.cpp:123-141): InitialIntegrate
+  // (:1671-1711), ConstraintA, ComputeForce, FinalIntegrate (:1713-1741), ConstraintB.  RBE
+  // samples are drawn after the two half-step remaps, for the box the force is evaluated in.
+  step += 1;
+  const bool shk = (p.fix_shake == RBMD_SHAKE_TRUE) && !angle_atoms.empty();
+  std::vector<double> old_x, old_v, old_v2;
+  double vir[6], press;
+  nhc_press_integrate();
+  compute_temp_target();
+  nhc_integrate();
+  pressure_scalar(vir, press);
+  bs.p_current = press;
+  compute_press_target();
+  nh_omega_dot();
+  nh_v_press();
+  update_velocity(&old_v);
+  mtk_remap();
+  update_position(&old_x);
+  mtk_remap();
+  if (shk) shake(old_x, old_v);
+  if (p.coulomb == RBMD_COUL_RBE) sample_k();
+  compute_force();
+  update_velocity(&old_v2);
+  nh_v_press();
+  compute_tempe();
+  pressure_scalar(vir, press);
+  bs.p_current = press;
+  baro_pressure = press;
+  for (int k = 0; k < 6; ++k) baro_virial[k] = vir[k];
+  nh_omega_dot();
+  nhc_integrate();
+  nhc_press_integrate();
+  if (shk) rattle(old_v2);
 }
 
 // ------------------------------------------------------------------ a6 / a8 / a13 / a15 energies

@@ -26,7 +26,8 @@ RBL_STRIDE, RBL_PHILOX = 0, 1
 RANDOM_PHILOX, RANDOM_TEST = 0, 1
 SHAKE_NULL, SHAKE_FALSE, SHAKE_TRUE = -1, 0, 1
 ENS_NVT, ENS_NVE, ENS_NPT = 0, 1, 2
-PC_BERENDSEN = 0
+PC_BERENDSEN, PC_NOSE_HOOVER = 0, 1
+PRESS_CTRLS = {"BERENDSEN": PC_BERENDSEN, "NOSE_HOOVER": PC_NOSE_HOOVER}
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 FORCE_FIELDS = {"LJ/CUT": FF_LJ_CUT, "LJ/CUT/COUL/LONG": FF_LJ_CUT_COUL_LONG, "CVFF": FF_CVFF, "EAM": FF_EAM}

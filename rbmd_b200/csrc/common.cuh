@@ -54,7 +54,15 @@ struct SysState {
   double baro_lo_old[3];   // NPT: range minimum before this step's remap
   double baro_hinv_old[3]; // NPT: 1 / edge before this step's remap
   int baro_apply;          // NPT: this step's remap was accepted
+  int mtk_ok[2];           // MTK: which of the two half-step remaps were accepted
   int baro_pad;
+  // MTK barostat (isotropic): barostat velocity and mass, its chain, targets, NH_V_Press factors
+  double omega_dot[3], omega_mass[3];
+  double etap[3], etap_dot[4], etap_dotdot[3], etap_mass[3];
+  double p_hydro, p_current, mtk_term1, mtk_term2;
+  double f_press[3];
+  // MTK half-step remaps: range minimum and 1 / edge of the box before each, and the box between
+  double mtk_lo0[3], mtk_hinv0[3], mtk_lo1[3], mtk_hi1[3], mtk_L1[3], mtk_hinv1[3];
   int64_t step;            // Executioner current step
   int status;              // error word
   int pad;
@@ -70,8 +78,9 @@ struct SysDev {
   int lean;   // segment-table traversal usable (every dimension holds >= 2 nc + 1 cells)
   int dense;  // pair kernel layout: tile (warp per home cell, dense systems) or warp per atom
   int blocks_pair, blocks_atom, blocks_rho, blocks_tri, rbe_mmax, rbe_slots, has_triples, n_triples;
-  // NPT Berendsen barostat: the box changes on the device every step.  Cell arrays and the cell
-  // work table hold ncell_cap cells (the box at kBoxGrow x L0); kmax indexes the Ewald k lists.
+  // NPT barostats (npt 1: Berendsen at the end of the step, 2: MTK around the integrator): the
+  // box changes on the device every step.  Cell arrays and the cell work table hold ncell_cap cells
+  // (the box at kBoxGrow x L0); kmax indexes the Ewald k lists.
   int npt, ncell_cap, kmax[3], npt_pad;
   double L0[3];
   double p_start, p_stop, p_damp, bulk;

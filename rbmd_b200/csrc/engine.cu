@@ -240,12 +240,16 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   if (!(p.timestep > 0)) return fail(RBMD_ERR_ARG, "timestep must be > 0");
   if (p.ensemble < 0 || p.ensemble > 2) return fail(RBMD_ERR_ARG, "unknown ensemble");
   if (p.ensemble == RBMD_ENS_NPT) {
-    // ExecutionNPT::Solve implements the barostat only in its BERENDSEN temperature branch
-    // (ExecutionNPT.cpp:90-141; the NOSE_HOOVER branch integrates without any pressure control)
-    if (p.temp_ctrl != RBMD_TC_BERENDSEN || p.press_ctrl != RBMD_PC_BERENDSEN)
-      return fail(RBMD_ERR_UNSUPPORTED, "ensemble NPT needs temp_ctrl BERENDSEN and press_ctrl BERENDSEN");
-    if (!(p.pressure[2] > 0) || !(p.bulk_modulus > 0))
-      return fail(RBMD_ERR_ARG, "NPT needs a pressure damping time (pressure[2]) and bulk_modulus > 0");
+    // ExecutionNPT::Solve (ExecutionNPT.cpp:90-141) controls the pressure for BERENDSEN /
+    // BERENDSEN (fix_press_berendsen) and NOSE_HOOVER / NOSE_HOOVER (MTK); its other pairings
+    // integrate without any pressure control, or not at all (TEMP_RESCALE)
+    const bool ber = p.temp_ctrl == RBMD_TC_BERENDSEN && p.press_ctrl == RBMD_PC_BERENDSEN;
+    const bool mtk = p.temp_ctrl == RBMD_TC_NOSE_HOOVER && p.press_ctrl == RBMD_PC_NOSE_HOOVER;
+    if (!ber && !mtk)
+      return fail(RBMD_ERR_UNSUPPORTED,
+                  "ensemble NPT needs temp_ctrl / press_ctrl BERENDSEN / BERENDSEN or NOSE_HOOVER / NOSE_HOOVER");
+    if (!(p.pressure[2] > 0)) return fail(RBMD_ERR_ARG, "NPT needs a pressure damping time pressure[2] > 0");
+    if (ber && !(p.bulk_modulus > 0)) return fail(RBMD_ERR_ARG, "NPT Berendsen needs bulk_modulus > 0");
   }
   if (p.precision == RBMD_PREC_MIXED && d.n_types > kMaxF32Types)
     return fail(RBMD_ERR_UNSUPPORTED, "mixed precision supports at most " + std::to_string(kMaxF32Types) +
@@ -362,7 +366,7 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   if (p.ensemble == RBMD_ENS_NPT) {
     // The box changes every step: the general traversal (any dims), cell tables for the largest
     // box the barostat accepts.
-    D.npt = 1;
+    D.npt = p.press_ctrl == RBMD_PC_NOSE_HOOVER ? 2 : 1;
     D.lean = 0;
     D.dense = 0;
     D.ncell_cap = 1;
@@ -824,7 +828,8 @@ void Context::enqueue_forces(const Batch& b, FinalMode mode, int virial) {
 }
 
 void Context::enqueue_step(const Batch& b) {
-  timed("nhc", 0, [&] { launch_nhc_a(b, stream); });
+  if (b.npt == 2) timed("mtk", 0, [&] { launch_mtk_begin(b, stream); });
+  else timed("nhc", 0, [&] { launch_nhc_a(b, stream); });
   timed("kick_drift", 0, [&] { launch_kick_drift(b, stream); });
   timed("cells", 0, [&] { launch_cells(b, stream); });
   if (b.has_shake) timed("shake", 0, [&] { launch_shake(b, stream); });
@@ -839,7 +844,7 @@ void Context::enqueue_step(const Batch& b) {
     timed("rattle", 0, [&] { launch_rattle(b, stream); });
     if (b.temp_ctrl != RBMD_TC_NOSE_HOOVER) timed("ke", 0, [&] { launch_ke_thermostat(b, stream); });
   }
-  if (b.npt) timed("barostat", 0, [&] { launch_barostat(b, stream); });
+  if (b.npt == 1) timed("barostat", 0, [&] { launch_barostat(b, stream); });
 }
 
 int Context::init(const int32_t* ids, int n) {
@@ -856,9 +861,17 @@ int Context::init(const int32_t* ids, int n) {
     for (int c = 0; c < 3; ++c) st0.eta[c] = st0.eta_dot[c] = st0.eta_dotdot[c] = 0.0;
     st0.eta_dot[3] = 0;
     st0.vscale_pending = st0.vscale_pending_c = st0.vscale_a = 1.0;
+    // barostat state (ExecutionNPT::InitialCondition, ExecutionNPT.cpp:196-225); MTK reads the
+    // virial of the init force evaluation at its first step
+    for (int c = 0; c < 6; ++c) st0.virial[c] = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      st0.omega_dot[c] = st0.omega_mass[c] = 0.0;
+      st0.etap[c] = st0.etap_dot[c] = st0.etap_dotdot[c] = st0.etap_mass[c] = 0.0;
+    }
+    st0.etap_dot[3] = 0.0;
     cudaMemcpyAsync(s->dev.st, &st0, sizeof(SysState), cudaMemcpyHostToDevice, stream);
   }
-  for (BatchRec* br : bs) enqueue_forces(br->b, kFinalInit, 0);
+  for (BatchRec* br : bs) enqueue_forces(br->b, kFinalInit, br->b.npt == 2 ? 1 : 0);
   return check_cuda("init");
 }
 

@@ -14,77 +14,9 @@
 // The scalar thermostat work runs on the device in the last block of each system (last-block
 // reduction of the kinetic-energy partials), so a whole step is a fixed kernel sequence with no
 // host round trip and can be captured in a CUDA graph.
-#include "kernels.h"
+#include "chain.cuh"
 
 namespace rbmd {
-
-// ------------------------------------------------------------------ scalar thermostat pieces
-__device__ inline void compute_tempe(const SysDev& s, SysState* st, double sum) {
-  // ExecutionNVT::ComputeTempe, ExecutionNVT.cpp:736-773
-  st->tempT_sum = sum;
-  const double n = s.n, kB = s.kB;
-  if (s.inbuild) st->temperature = 0.5 * sum / (3 * n / 2.0);
-  else if (s.fix_shake == RBMD_SHAKE_NULL) st->temperature = 0.5 * sum / ((3 * n - 3) * kB / 2.0);
-  else if (s.fix_shake == RBMD_SHAKE_TRUE) st->temperature = 0.5 * sum / ((3 * n - n - 3) * kB / 2.0);
-  else st->temperature = 0.5 * sum / ((3 * n) * kB / 2.0);
-}
-
-__device__ inline void compute_temp_target(const SysDev& s, SysState* st) {
-  // ExecutionNVT::ComputeTempTarget, ExecutionNVT.cpp:1124-1147
-  if (s.t_stop == s.t_start) {
-    st->t_target = s.t_start;
-  } else {
-    double delta = (double)st->step;
-    if (delta != 0.0) delta = delta / (double)s.num_steps;
-    st->t_target = s.t_start + delta * (s.t_stop - s.t_start);
-  }
-  st->ke_target = st->tdof * s.boltz * st->t_target;
-}
-
-// One half of ExecutionNVT::NHCTempIntegrate (ExecutionNVT.cpp:1172-1256); returns the velocity
-// factor and rescales the stored temperature as the reference does.
-__device__ inline double nhc_half(const SysDev& s, SysState* st) {
-  const int mtchain = 3;
-  const double dt = s.dt, dthalf = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt;
-  const double boltz = s.boltz, tf = st->t_freq;
-  double kecurrent = st->tdof * boltz * st->temperature;
-  st->eta_mass[0] = st->tdof * boltz * st->t_target / (tf * tf);
-  for (int ich = 1; ich < mtchain; ich++) st->eta_mass[ich] = boltz * st->t_target / (tf * tf);
-  if (st->eta_mass[0] > 0.0) st->eta_dotdot[0] = (kecurrent - st->ke_target) / st->eta_mass[0];
-  else st->eta_dotdot[0] = 0.0;
-  const double ncfac = 1.0;
-  double expfac;
-  for (int ich = mtchain - 1; ich > 0; ich--) {
-    expfac = exp(-ncfac * dt8 * st->eta_dot[ich + 1]);
-    st->eta_dot[ich] *= expfac;
-    st->eta_dot[ich] += st->eta_dotdot[ich] * ncfac * dt4;
-    st->eta_dot[ich] *= st->tdrag;
-    st->eta_dot[ich] *= expfac;
-  }
-  expfac = exp(-ncfac * dt8 * st->eta_dot[1]);
-  st->eta_dot[0] *= expfac;
-  st->eta_dot[0] += st->eta_dotdot[0] * ncfac * dt4;
-  st->eta_dot[0] *= st->tdrag;
-  st->eta_dot[0] *= expfac;
-  const double factor = exp(-ncfac * dthalf * st->eta_dot[0]);
-  st->temperature = st->temperature * factor * factor;
-  kecurrent = st->tdof * boltz * st->temperature;
-  if (st->eta_mass[0] > 0.0) st->eta_dotdot[0] = (kecurrent - st->ke_target) / st->eta_mass[0];
-  else st->eta_dotdot[0] = 0.0;
-  for (int ich = 0; ich < mtchain; ich++) st->eta[ich] += ncfac * dthalf * st->eta_dot[ich];
-  st->eta_dot[0] *= expfac;
-  st->eta_dot[0] += st->eta_dotdot[0] * ncfac * dt4;
-  st->eta_dot[0] *= expfac;
-  for (int ich = 1; ich < mtchain; ich++) {
-    expfac = exp(-ncfac * dt8 * st->eta_dot[ich + 1]);
-    st->eta_dot[ich] *= expfac;
-    st->eta_dotdot[ich] = (st->eta_mass[ich - 1] * st->eta_dot[ich - 1] * st->eta_dot[ich - 1] -
-                           boltz * st->t_target) / st->eta_mass[ich];
-    st->eta_dot[ich] += st->eta_dotdot[ich] * ncfac * dt4;
-    st->eta_dot[ich] *= expfac;
-  }
-  return factor;
-}
 
 // Step start: Executioner::TakeStep increments the step; InitialIntegrate runs the first chain half.
 __global__ void k_nhc_a(const SysDev* __restrict__ S, const int* __restrict__ slots, int n) {
@@ -93,8 +25,8 @@ __global__ void k_nhc_a(const SysDev* __restrict__ S, const int* __restrict__ sl
   const SysDev& s = S[slots[k]];
   SysState* st = s.st;
   st->step += 1;
-  // NPT: the step's force evaluation accumulates the virial the barostat reads (the RBL pair
-  // kernels add nothing to it, so it starts from zero here)
+  // NPT Berendsen: the step's force evaluation accumulates the virial the barostat reads (the RBL
+  // pair kernels add nothing to it, so it starts from zero here)
   if (s.npt)
     for (int c = 0; c < 6; ++c) st->virial[c] = 0.0;
   if (s.temp_ctrl == RBMD_TC_NOSE_HOOVER) {
@@ -105,7 +37,10 @@ __global__ void k_nhc_a(const SysDev* __restrict__ S, const int* __restrict__ sl
   }
 }
 
-// v = v * pending * a; v += F/m dt/2; x += v dt; periodic wrap with image flags.
+// v = v * pending * a; v += F/m dt/2; x += v dt; periodic wrap with image flags.  MTK systems
+// (npt 2) also take the NH_V_Press factors twice before the kick and are remapped to the first
+// half-step box before the drift and to the second after it (InitialIntegrate,
+// ExecutionNPT.cpp:1671-1711); the wrap uses the first box and the second remap does not wrap.
 __global__ void k_kick_drift(const SysDev* __restrict__ S, const int2* __restrict__ work) {
   const int2 wk = work[blockIdx.x];
   const SysDev& s = S[wk.x];
@@ -121,6 +56,13 @@ __global__ void k_kick_drift(const SysDev* __restrict__ S, const int2* __restric
   vx = fa * vx;
   vy = fa * vy;
   vz = fa * vz;
+  const bool mtk = s.npt == 2;
+  if (mtk)
+    for (int r = 0; r < 2; ++r) {
+      vx = st->f_press[0] * vx;
+      vy = st->f_press[1] * vy;
+      vz = st->f_press[2] * vz;
+    }
   if (s.has_triples) s.vold[i] = make_double4(vx, vy, vz, v.w);
   const double m = v.w, dt = s.dt, c = s.fmt2v;
   vx += 0.5 * F.x / m * dt * c;
@@ -128,17 +70,30 @@ __global__ void k_kick_drift(const SysDev* __restrict__ S, const int2* __restric
   vz += 0.5 * F.z / m * dt * c;
   s.v[i] = make_double4(vx, vy, vz, m);
   double4 x = s.x[i];
+  if (mtk && st->mtk_ok[0]) {
+    x.x = __dadd_rn(__dmul_rn(st->mtk_L1[0], __dmul_rn(st->mtk_hinv0[0], __dsub_rn(x.x, st->mtk_lo0[0]))), st->mtk_lo1[0]);
+    x.y = __dadd_rn(__dmul_rn(st->mtk_L1[1], __dmul_rn(st->mtk_hinv0[1], __dsub_rn(x.y, st->mtk_lo0[1]))), st->mtk_lo1[1]);
+    x.z = __dadd_rn(__dmul_rn(st->mtk_L1[2], __dmul_rn(st->mtk_hinv0[2], __dsub_rn(x.z, st->mtk_lo0[2]))), st->mtk_lo1[2]);
+  }
   if (s.has_triples) s.xold[i] = x;
   double p[3] = {x.x + vx * dt, x.y + vy * dt, x.z + vz * dt};
+  const double* blo = mtk ? st->mtk_lo1 : s.lo;
+  const double* bhi = mtk ? st->mtk_hi1 : s.hi;
+  const double* bL = mtk ? st->mtk_L1 : s.L;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    if (p[k] < s.lo[k]) {
-      p[k] += s.L[k];
+    if (p[k] < blo[k]) {
+      p[k] += bL[k];
       s.image[3 * i + k] -= 1;
-    } else if (p[k] >= s.hi[k]) {
-      p[k] -= s.L[k];
+    } else if (p[k] >= bhi[k]) {
+      p[k] -= bL[k];
       s.image[3 * i + k] += 1;
     }
+  }
+  if (mtk && st->mtk_ok[1]) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      p[k] = __dadd_rn(__dmul_rn(s.L[k], __dmul_rn(st->mtk_hinv1[k], __dsub_rn(p[k], st->mtk_lo1[k]))), s.lo[k]);
   }
   s.x[i] = make_double4(p[0], p[1], p[2], x.w);
 }
@@ -383,6 +338,12 @@ k_final(const SysDev* __restrict__ S, const int2* __restrict__ work, int mode) {
       v.x += 0.5 * F[0] / m * dt * c;
       v.y += 0.5 * F[1] / m * dt * c;
       v.z += 0.5 * F[2] / m * dt * c;
+      if (s.npt == 2)  // FinalIntegrate: NH_V_Press after the kick (ExecutionNPT.cpp:1713-1720)
+        for (int r = 0; r < 2; ++r) {
+          v.x = st->f_press[0] * v.x;
+          v.y = st->f_press[1] * v.y;
+          v.z = st->f_press[2] * v.z;
+        }
       s.v[i] = v;
     }
     ke = (v.w * (v.x * v.x + v.y * v.y + v.z * v.z)) * s.mvv2e;
@@ -429,12 +390,22 @@ k_final(const SysDev* __restrict__ S, const int2* __restrict__ work, int mode) {
         for (int ich = 1; ich < 3; ich++)
           st->eta_dotdot[ich] = (st->eta_mass[ich - 1] * st->eta_dot[ich - 1] * st->eta_dot[ich - 1] -
                                  s.boltz * st->t_target) / st->eta_mass[ich];
+        if (s.npt == 2) mtk_setup(s, st);
       } else if (mode == kFinalKick) {
         const bool shk_thermo = s.has_triples && s.temp_ctrl != RBMD_TC_NOSE_HOOVER;
         if (!shk_thermo) {
           compute_tempe(s, st, s_tot[0]);
           if (s.temp_ctrl == RBMD_TC_NOSE_HOOVER) {
+            if (s.npt == 2) {
+              // FinalIntegrate: pressure of this step's forces, barostat velocity half step
+              double vir[6];
+              st->p_current = pressure_scalar(s, st, vir);
+              st->baro_pressure = st->p_current;
+              for (int k = 0; k < 6; ++k) st->baro_virial[k] = vir[k];
+              omega_dot_half(s, st);
+            }
             const double fb = nhc_half(s, st);
+            if (s.npt == 2) nhc_press_half(s, st);
             st->vscale_pending = fb;
             st->vscale_pending_c = s.has_triples ? 1.0 : fb;  // RATTLE rebuilds triples from pre-kick v
           } else if (s.temp_ctrl == RBMD_TC_RESCALE) {

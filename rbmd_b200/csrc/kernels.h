@@ -24,7 +24,7 @@ struct Batch {
   int has_shake = 0, has_bonded = 0;
   int dense = 0;             // pair kernel: 1 = warp per home cell, 0 = warp per atom
   int lean = 0;              // warp per atom with segment tables (dims >= 2 nc + 1 everywhere)
-  int npt = 0;               // NPT systems: virial every step, barostat at the end of the step
+  int npt = 0;               // NPT barostat: 0 none, 1 Berendsen (end of step), 2 MTK (around the integrator)
   int max_P = 0;             // largest P (or Ewald nk) in the batch
   long long natoms = 0;      // atoms over all systems of the batch
 };
@@ -47,6 +47,9 @@ void launch_energy(const Batch& b, cudaStream_t s);
 void launch_ewald_energy(const Batch& b, cudaStream_t s);
 // NPT Berendsen barostat of every system of an NPT batch: new box and tables, then the remap.
 void launch_barostat(const Batch& b, cudaStream_t s);
+// MTK barostat systems: step start (both chains' first halves, barostat velocity, the two
+// half-step boxes); replaces launch_nhc_a for such batches.
+void launch_mtk_begin(const Batch& b, cudaStream_t s);
 
 // RBL list materialisation for parity checks (not on the step path).
 void launch_rbl_lists(const SysDev* sys, int slot, int n, int ncell, int dense, int cap, int* n_core,

@@ -421,13 +421,17 @@ void MDApplication::ReadExecution(const Json& ex) {
   else if (tc == "TEMP_RESCALE") P.temp_ctrl = RBMD_TC_RESCALE;
   else throw std::runtime_error("temp_ctrl_type \"" + tc + "\" is not supported");
   if (P.ensemble == RBMD_ENS_NPT) {
-    // ExecutionNPT::Solve (ExecutionNPT.cpp:90-141) controls the pressure only in its BERENDSEN
-    // temperature branch, with press_ctrl_type BERENDSEN
-    const std::string pc = ex.string("press_ctrl_type", "BERENDSEN");
-    if (pc != "BERENDSEN") throw std::runtime_error("press_ctrl_type \"" + pc + "\" is not supported (BERENDSEN)");
-    if (P.temp_ctrl != RBMD_TC_BERENDSEN)
-      throw std::runtime_error("ensemble NPT needs temp_ctrl_type BERENDSEN (the reference's only NPT path)");
-    P.press_ctrl = RBMD_PC_BERENDSEN;
+    // ExecutionNPT::Solve (ExecutionNPT.cpp:90-141) controls the pressure for temp_ctrl_type /
+    // press_ctrl_type BERENDSEN / BERENDSEN and NOSE_HOOVER / NOSE_HOOVER only
+    const std::string pc = ex.string("press_ctrl_type", tc);
+    if (pc == "BERENDSEN") P.press_ctrl = RBMD_PC_BERENDSEN;
+    else if (pc == "NOSE_HOOVER") P.press_ctrl = RBMD_PC_NOSE_HOOVER;
+    else throw std::runtime_error("press_ctrl_type \"" + pc + "\" is not supported (BERENDSEN, NOSE_HOOVER)");
+    const bool ok = (P.press_ctrl == RBMD_PC_BERENDSEN && P.temp_ctrl == RBMD_TC_BERENDSEN) ||
+                    (P.press_ctrl == RBMD_PC_NOSE_HOOVER && P.temp_ctrl == RBMD_TC_NOSE_HOOVER);
+    if (!ok)
+      throw std::runtime_error("ensemble NPT needs temp_ctrl_type and press_ctrl_type both BERENDSEN or both "
+                               "NOSE_HOOVER (the reference controls the pressure in no other pairing)");
   }
   P.timestep = ex.number("timestep", P.timestep);
   P.num_steps = (int64_t)ex.number("num_steps", (double)P.num_steps);

@@ -1,5 +1,5 @@
-"""NPT Berendsen barostat on the sm_100a path against the FP64 oracle (ExecutionNPT.cpp:90-141,
-1334-1368, 1429-1447, 1506-1538).
+"""NPT barostats on the sm_100a path against the FP64 oracle: Berendsen (ExecutionNPT.cpp:90-122,
+1334-1368, 1429-1447, 1506-1538) and the isotropic MTK barostat (:123-141, 1545-2066).
 
 The box, its cell dims, the volume-dependent k-space tables and the remapped atoms are rebuilt on
 the device every step; after a few steps they must agree with the oracle: box edges and volume to
@@ -17,9 +17,10 @@ from test_gpu_parity import eam_small, lj_small, pair, water_small
 pytestmark = pytest.mark.gpu
 
 
-def npt(sd, p_start, p_stop, p_damp, bulk, num_steps=200):
+def npt(sd, p_start, p_stop, p_damp, bulk, num_steps=200, mtk=False):
     p = sd.params
-    p.ensemble, p.temp_ctrl, p.press_ctrl = A.ENS_NPT, A.TC_BERENDSEN, A.PC_BERENDSEN
+    p.ensemble = A.ENS_NPT
+    p.temp_ctrl, p.press_ctrl = (A.TC_NOSE_HOOVER, A.PC_NOSE_HOOVER) if mtk else (A.TC_BERENDSEN, A.PC_BERENDSEN)
     p.pressure[:] = (p_start, p_stop, p_damp)
     p.bulk_modulus = bulk
     p.num_steps = num_steps
@@ -35,6 +36,16 @@ CASES = {
                                                         kmax=(5, 5, 5)), 0.0, 0.0, 0.5, 5.0),
     "water_cvff_rbe_rbl": lambda om: npt(water_small(), 1.0, 1.0, 1000.0, 2.0e4),
     "eam_rbl": lambda om: npt(eam_small(om), 0.0, 0.0, 1.0, 1.0e6),
+}
+
+# MTK: (system, P_start, P_stop, P_damp); P_damp about 100-1000 time steps
+MTK_CASES = {
+    "lj_rbl": lambda om: npt(lj_small(), 0.2, 0.6, 0.5, 0, mtk=True),
+    "nacl_rbe_rbl": lambda om: npt(synth.nacl_melt(n_side=10), 0.0, 0.0, 0.5, 0, mtk=True),
+    "nacl_ewald_verlet": lambda om: npt(synth.nacl_melt(n_side=10, coulomb=A.COUL_EWALD, neighbor=A.NEIGH_VERLET,
+                                                        kmax=(5, 5, 5)), 0.0, 0.0, 0.5, 0, mtk=True),
+    "water_cvff_rbe_rbl": lambda om: npt(water_small(), 1.0, 1.0, 200.0, 0, mtk=True),
+    "eam_rbl": lambda om: npt(eam_small(om), 0.0, 0.0, 1.0, 0, mtk=True),
 }
 
 
@@ -72,6 +83,23 @@ def test_npt_steps_track_oracle(ctx_factory, oracle_mod, case, graphs):
     o.step(4)
     tg, _ = compare(ctx, sid, o)
     assert tg["volume"] != v0  # the box moved
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+@pytest.mark.parametrize("case", list(MTK_CASES))
+def test_mtk_steps_track_oracle(ctx_factory, oracle_mod, case, graphs):
+    sd = MTK_CASES[case](oracle_mod)
+    ctx, sid, o = pair(ctx_factory, oracle_mod, sd, graphs=graphs)
+    ctx.init(sid)
+    o.init()
+    v0 = o.thermo()["volume"]
+    ctx.step(sid, 3)
+    o.step(3)
+    ctx.step(sid, 5)
+    o.step(5)
+    tg, _ = compare(ctx, sid, o)
+    assert tg["volume"] != v0
+    assert tg["nhc_eta"][0] == pytest.approx(o.thermo()["nhc_eta"][0], rel=1e-8, abs=1e-14)
 
 
 def test_npt_cell_dims_change_and_cells_match(ctx_factory, oracle_mod):
@@ -138,8 +166,10 @@ def test_npt_mixed_precision(ctx_factory, oracle_mod):
 
 
 def test_npt_batched_equals_alone(ctx_factory, oracle_mod):
-    """NPT systems batch with each other (not with NVT ones) and give the same bits as alone."""
-    systems = [npt(lj_small(seed=s), 0.2, 0.2, 0.5, 10.0) for s in (1, 2)] + [lj_small(seed=3)]
+    """NPT systems batch with each other (not with NVT ones or the other barostat) and give the same
+    bits as alone."""
+    systems = [npt(lj_small(seed=s), 0.2, 0.2, 0.5, 10.0) for s in (1, 2)] + [lj_small(seed=3)] + \
+              [npt(lj_small(seed=s), 0.2, 0.2, 0.5, 0, mtk=True) for s in (4, 5)]
     for k, sd in enumerate(systems):
         sd.params.seed = 70 + k
     results = {}
@@ -163,7 +193,10 @@ def test_npt_validation(ctx_factory):
     ctx = ctx_factory()
     sd = npt(lj_small(), 0.2, 0.2, 0.5, 10.0)
     sd.params.temp_ctrl = A.TC_NOSE_HOOVER
-    with pytest.raises(Exception, match="BERENDSEN"):
+    with pytest.raises(Exception, match="NOSE_HOOVER"):
+        ctx.add_system(sd)
+    sd = npt(lj_small(), 0.2, 0.2, 0.0, 0, mtk=True)
+    with pytest.raises(Exception, match="damping"):
         ctx.add_system(sd)
     sd = npt(lj_small(), 0.2, 0.2, 0.5, 0.0)
     with pytest.raises(Exception, match="bulk_modulus"):

@@ -142,7 +142,9 @@ def test_eam_potential_file(rbmd_bin, tmp_path, oracle_mod):
 
 
 @pytest.mark.parametrize("mutate,message", [
-    (lambda cfg: cfg["execution"].update(ensemble="NPT", temp_ctrl_type="NOSE_HOOVER"), "BERENDSEN"),
+    (lambda cfg: cfg["execution"].update(ensemble="NPT", temp_ctrl_type="NOSE_HOOVER", press_ctrl_type="BERENDSEN"),
+     "both"),
+    (lambda cfg: cfg["execution"].update(ensemble="NPT", temp_ctrl_type="TEMP_RESCALE"), "TEMP_RESCALE"),
     (lambda cfg: cfg["execution"].update(ensemble="NPT", temp_ctrl_type="BERENDSEN", press_ctrl_type="MTK"), "MTK"),
     (lambda cfg: cfg["init_configuration"]["read_data"].update(atom_style="molecular"), "atom_style"),
     (lambda cfg: cfg["init_configuration"]["read_data"].update(file="missing.data"), "missing.data"),
@@ -159,18 +161,20 @@ def test_errors_are_reported(rbmd_bin, tmp_path, mutate, message):
     assert r.returncode == 1 and message in r.stderr
 
 
-@pytest.mark.parametrize("pressure,bulk", [([1.0, 2.0, 100.0], 10.0), ([1.0, 2.0, 100.0, 25000.0], 25000.0)])
-def test_npt_berendsen_input(rbmd_bin, tmp_path, pressure, bulk):
-    """ensemble NPT with BERENDSEN temperature and pressure control; the optional fourth pressure
-    entry is the bulk modulus (ExecutionNPT.cpp:953)."""
+@pytest.mark.parametrize("ctrl,pressure,bulk", [("BERENDSEN", [1.0, 2.0, 100.0], 10.0),
+                                                ("BERENDSEN", [1.0, 2.0, 100.0, 25000.0], 25000.0),
+                                                ("NOSE_HOOVER", [1.0, 1.0, 1000.0], 10.0)])
+def test_npt_input(rbmd_bin, tmp_path, ctrl, pressure, bulk):
+    """ensemble NPT with BERENDSEN or NOSE_HOOVER temperature and pressure control; the optional
+    fourth pressure entry is the Berendsen bulk modulus (ExecutionNPT.cpp:953)."""
     sd = synth.spce_water(n_mol=8)
     path = synth.write_rbmd_input(sd, str(tmp_path))
     cfg = json.load(open(path))
-    cfg["execution"].update(ensemble="NPT", temp_ctrl_type="BERENDSEN", press_ctrl_type="BERENDSEN",
-                            pressure=pressure)
+    cfg["execution"].update(ensemble="NPT", temp_ctrl_type=ctrl, press_ctrl_type=ctrl, pressure=pressure)
     json.dump(cfg, open(path, "w"))
     P = dump(rbmd_bin, path, tmp_path)["params"]
-    assert P["ensemble"] == A.ENS_NPT and P["temp_ctrl"] == A.TC_BERENDSEN and P["press_ctrl"] == A.PC_BERENDSEN
+    assert P["ensemble"] == A.ENS_NPT
+    assert P["temp_ctrl"] == A.TEMP_CTRLS[ctrl] and P["press_ctrl"] == A.PRESS_CTRLS[ctrl]
     assert P["pressure"] == pressure[:3] and P["bulk_modulus"] == bulk
 
 

@@ -299,3 +299,39 @@ def test_barostat_refuses_boxes_outside_the_cell_range(oracle_mod):
     t = o.thermo()
     assert t["status"] & A.STATUS_BOX_RANGE
     assert list(t["box_lo"]) == list(sd.box_lo) and list(t["box_hi"]) == list(sd.box_hi)
+
+
+def _mtk(sd, p_target, p_damp, num_steps=100):
+    p = sd.params
+    p.ensemble, p.temp_ctrl, p.press_ctrl = A.ENS_NPT, A.TC_NOSE_HOOVER, A.PC_NOSE_HOOVER
+    p.pressure[:] = (p_target, p_target, p_damp)
+    p.num_steps = num_steps
+    return sd
+
+
+def test_mtk_with_a_heavy_barostat_is_the_nose_hoover_step(oracle_mod):
+    """With P_damp huge the barostat mass (N+1) kT P_damp^2 freezes omega_dot at ~0: the MTK step
+    (ExecutionNPT.cpp:1671-1741) must then reduce to the NVT Nose-Hoover step."""
+    base = synth.nacl_melt(n_side=8)
+    base.params.temp_ctrl = A.TC_NOSE_HOOVER
+    nvt = oracle_mod.Oracle(base.copy())
+    o = oracle_mod.Oracle(_mtk(base.copy(), 0.0, 1e9))
+    for s in (nvt, o):
+        s.init()
+        s.step(10)
+    x0, v0, _ = nvt.state()
+    x1, v1, _ = o.state()
+    assert np.abs(x1 - x0).max() < 1e-9 and np.abs(v1 - v0).max() < 1e-9
+    assert o.thermo()["volume"] == pytest.approx(nvt.thermo()["volume"], rel=1e-12)
+
+
+def test_mtk_volume_follows_the_pressure(oracle_mod):
+    """The barostat velocity integrates (P - p_hydro) V / W: a box under a pressure above the
+    (reference-weighted) target grows, below it shrinks."""
+    for target, grows in ((0.0, True), (6.0, False)):
+        o = oracle_mod.Oracle(_mtk(synth.lj_fcc(cells=5), target, 0.5))
+        o.init()
+        v0 = o.thermo()["volume"]
+        o.step(20)
+        t = o.thermo()
+        assert (t["volume"] > v0) == grows and t["status"] == 0
