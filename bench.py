@@ -258,6 +258,33 @@ def measure_accuracy(device):
                 mixed_vs_ewald=rr(f["mixed"], f["ewald"]), atoms=sd.n)
 
 
+def measure_drift(device, steps=1000, every=100):
+    """Energy conservation of the LJ fluid (4000 atoms, RBL rs 1.2 with 100 shell samples, NVE,
+    dt 0.005): total energy per atom every `every` steps in FP64 and in mixed precision.  Reports
+    the relative drift (E_end - E_0) / |E_0|, the largest excursion and the mixed-vs-FP64 energy
+    difference along the run."""
+    import rbmd_b200
+    from rbmd_b200 import _abi as A, synth
+    out = {}
+    traj = {}
+    for tag, prec in (("fp64", A.PREC_FP64), ("mixed", A.PREC_MIXED)):
+        sd = synth.lj_fcc(precision=prec)
+        ctx = rbmd_b200.Context(device=device)
+        sid = ctx.add_system(sd)
+        ctx.init(sid)
+        e = [ctx.thermo(sid)["total_energy"]]
+        for _ in range(steps // every):
+            ctx.step(sid, every)
+            e.append(ctx.thermo(sid)["total_energy"])
+        ctx.close()
+        e = np.array(e)
+        traj[tag] = e
+        out[tag] = dict(drift=float((e[-1] - e[0]) / abs(e[0])), max_excursion=float(np.abs(e - e[0]).max() / abs(e[0])))
+    out["energy_mixed_vs_fp64"] = float(np.abs(traj["mixed"] - traj["fp64"]).max() / abs(traj["fp64"][0]))
+    out.update(atoms=4000, steps=steps, ensemble="NVE", e0_per_atom=float(traj["fp64"][0]))
+    return out
+
+
 def measure_e2e(systems, arrivals, args, device):
     """The stream through rbmd_serve_*: submissions at the Poisson times, results back to host."""
     import rbmd_b200
@@ -406,6 +433,7 @@ def main():
     if dist.rank == 0:
         if not args.skip_accuracy:
             extra["accuracy"] = measure_accuracy(device)
+            extra["drift"] = measure_drift(device)
         if not args.skip_plain:
             extra["plain_fp64"] = measure_plain(systems, args, device)
     e2e = None
@@ -438,6 +466,7 @@ def main():
             line["speedup_vs_plain_fp64"] = res["value"] / dist.world / plain["value"]
         if "accuracy" in extra:
             line["force_rel_rms"] = extra["accuracy"]
+            line["energy_drift"] = extra["drift"]
         if e2e is not None:
             line["e2e"] = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"],
                            "d2h_bytes_per_step": e2e["d2h"], "wall_s": e2e["wall_s"], "p50_latency_s": e2e["p50_s"],

@@ -279,3 +279,13 @@ def test_errors_are_status_codes(ctx_factory):
     with pytest.raises(rbmd_b200.RbmdError) as e:
         ctx.add_system(sd)
     assert e.value.code == A.ERR_NUMERIC
+
+
+def test_energy_drift_mixed_matches_fp64():
+    """The LJ fluid (4000 atoms, RBL, NVE, dt 0.005) over 1000 steps: mixed precision conserves
+    energy as well as FP64 (drifts within 2e-4 of each other, both below 5e-3 of |E_0|)."""
+    import bench
+    d = bench.measure_drift(0)
+    assert abs(d["fp64"]["drift"]) < 5e-3 and abs(d["mixed"]["drift"]) < 5e-3
+    assert abs(d["mixed"]["drift"] - d["fp64"]["drift"]) < 2e-4
+    assert d["energy_mixed_vs_fp64"] < 2e-3
