@@ -258,6 +258,46 @@ def measure_accuracy(device):
                 mixed_vs_ewald=rr(f["mixed"], f["ewald"]), atoms=sd.n)
 
 
+def measure_traj_accuracy(device, sizes=(1000, 4000, 16000, 64000), checkpoints=2, every=5):
+    """Mixed-vs-FP64 force error along trajectories: saline systems of the stream's sizes run in
+    mixed precision; at each checkpoint the FP64 path evaluates the same state at the same step
+    (same RBE draws and RBL stride), so the difference is the mixed path's error alone.  Reports
+    the relative RMS per system and over all checkpoints of all systems."""
+    import rbmd_b200
+    from rbmd_b200 import _abi as A, synth
+    num = den = 0.0
+    per = []
+    ctx = rbmd_b200.Context(device=device)
+    for k, n in enumerate(sizes):
+        sd = synth.saline(n, seed=60 + k)
+        sd.params.seed = 700 + k
+        sid = ctx.add_system(sd)
+        s64 = sd.copy()
+        s64.params.precision = A.PREC_FP64
+        ref = ctx.add_system(s64)
+        ctx.init(sid)
+        worst = 0.0
+        for _ in range(checkpoints):
+            ctx.step(sid, every)
+            x, v, img = ctx.state(sid)
+            step = ctx.thermo(sid)["step"]
+            ctx.compute_forces(sid)
+            fm = ctx.forces(sid)
+            ctx.set_state(ref, x, v, img)
+            ctx.set_step(ref, step)
+            ctx.compute_forces(ref)
+            f64 = ctx.forces(ref)
+            a, b = float(((fm - f64) ** 2).sum()), float((f64 ** 2).sum())
+            num += a
+            den += b
+            worst = max(worst, (a / b) ** 0.5)
+        per.append({"atoms": sd.n, "max_rel_rms": worst})
+        ctx.remove_system(sid)
+        ctx.remove_system(ref)
+    ctx.close()
+    return {"aggregate_rel_rms": (num / den) ** 0.5, "systems": per, "steps_between": every}
+
+
 def measure_drift(device, steps=1000, every=100):
     """Energy conservation of the LJ fluid (4000 atoms, RBL rs 1.2 with 100 shell samples, NVE,
     dt 0.005): total energy per atom every `every` steps in FP64 and in mixed precision.  Reports
@@ -433,6 +473,7 @@ def main():
     if dist.rank == 0:
         if not args.skip_accuracy:
             extra["accuracy"] = measure_accuracy(device)
+            extra["accuracy"]["trajectory_mixed_vs_fp64"] = measure_traj_accuracy(device)
             extra["drift"] = measure_drift(device)
         if not args.skip_plain:
             extra["plain_fp64"] = measure_plain(systems, args, device)

@@ -228,7 +228,8 @@ typedef struct rbmd_device_cfg {
   int32_t batched;              /* 1: one segment-indexed launch per kernel over all systems of a
                                    rbmd_step call; 0: one launch per system (the plain path) */
   int32_t use_graphs;           /* 1: capture the step of a fixed system set as a CUDA graph */
-  int32_t pad0;
+  int32_t autotune;             /* 1: rbmd_init / rbmd_step run rbmd_autotune on systems that have not
+                                   been tuned yet (before their first force evaluation or graph) */
   int64_t hbm_budget_bytes;     /* admission budget for the serving loop (0 = free memory) */
 } rbmd_device_cfg;
 
@@ -268,6 +269,10 @@ int rbmd_get_state(rbmd_ctx* ctx, int32_t sys_id, double* position, double* velo
                    int32_t* image);
 int rbmd_set_state(rbmd_ctx* ctx, int32_t sys_id, const double* position, const double* velocity,
                    const int32_t* image);
+/* Sets the step counter (Executioner::_current_step) that keys the system's random draws and
+ * temperature / pressure ramps: a restart from a checkpoint written at that step, or a second
+ * system evaluated at the same draws (no reference counterpart). */
+int rbmd_set_step(rbmd_ctx* ctx, int32_t sys_id, int64_t step);
 /* Thermo quantities; energies are evaluated at the current positions on request (the reference
  * recomputes them every step for ThermoOutput, framework/output/ThermoOutput.cpp:144-186). */
 int rbmd_get_thermo(rbmd_ctx* ctx, int32_t sys_id, rbmd_thermo* out);
@@ -382,6 +387,33 @@ int rbmd_profile_get(rbmd_ctx* ctx, const char* kernel, double* avg_ms, int64_t*
 /* rbmd_step bracketed by CUDA events recorded on the context stream; *ms is the device time of
  * the nsteps steps (the call synchronises). */
 int rbmd_step_timed(rbmd_ctx* ctx, const int32_t* sys_ids, int32_t n, int32_t nsteps, double* ms);
+
+/* ---------------------------------------------------------------- autotuner (no reference counterpart) */
+/* Pair traversal layouts of the force kernels. */
+enum rbmd_pair_layout {
+  RBMD_LAYOUT_TILE = 0,     /* warp per home cell, candidate batches shared by the cell's atoms */
+  RBMD_LAYOUT_LEAN = 1,     /* warp per atom over per-row segment tables (dims >= 2 nc + 1) */
+  RBMD_LAYOUT_GENERAL = 2   /* warp per atom, any box */
+};
+typedef struct rbmd_tune_result {
+  int32_t n_systems;        /* systems of the group (grouped as rbmd_step batches them) */
+  int32_t layout;           /* chosen enum rbmd_pair_layout */
+  int64_t atoms;            /* atoms of the group */
+  double ms[3];             /* measured pair-kernel time per layout (index = layout); -1: unusable or
+                               not timed */
+  int32_t from_cache;       /* 1: taken from an earlier decision for the same signature */
+  int32_t pad0;
+} rbmd_tune_result;
+/* Times every pair layout the systems can use, one group at a time (cell list built once, one
+ * warm-up, best of three launches on the library stream), and keeps the fastest for the group.  A
+ * decision is cached per signature (force field, neighbour, Coulomb, precision, special bonds,
+ * bonded terms, SHAKE, barostat, atoms per cell and group size, both binned by factors of 2), so
+ * later groups with the same signature take it without timing.  Positions, velocities and forces
+ * are left as they were.  NPT systems always use RBMD_LAYOUT_GENERAL (their cell dims change).
+ * Up to cap results are written; *n_groups gets the number of groups.  Layouts differ only in
+ * summation order, so results after tuning agree with untuned ones to rounding, not bit for bit. */
+int rbmd_autotune(rbmd_ctx* ctx, const int32_t* sys_ids, int32_t n, rbmd_tune_result* results, int32_t cap,
+                  int32_t* n_groups);
 /* Non-tensor pipe peak of the device from a dependent FMA chain microbenchmark (fp64 = 0: FFMA,
  * 1: DFMA); *tflops counts an FMA as 2 flops. */
 int rbmd_fma_peak(rbmd_ctx* ctx, int32_t fp64, double* tflops);

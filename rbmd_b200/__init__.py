@@ -46,9 +46,9 @@ def _ip(a):
 class Context:
     """One CUDA device context: systems, batched steps, serving loop."""
 
-    def __init__(self, device=0, batched=True, graphs=True, hbm_budget_bytes=0):
+    def __init__(self, device=0, batched=True, graphs=True, hbm_budget_bytes=0, autotune=False):
         L = lib()
-        cfg = A.DeviceCfg(device=device, batched=int(batched), use_graphs=int(graphs),
+        cfg = A.DeviceCfg(device=device, batched=int(batched), use_graphs=int(graphs), autotune=int(autotune),
                           hbm_budget_bytes=int(hbm_budget_bytes))
         h = C.c_void_p()
         rc = L.rbmd_ctx_create(C.byref(cfg), C.byref(h))
@@ -125,6 +125,9 @@ class Context:
         self._check(lib().rbmd_get_state(self.h, sid, _dp(x), _dp(v), _ip(img)))
         return x, v, img
 
+    def set_step(self, sid, step):
+        self._check(lib().rbmd_set_step(self.h, sid, int(step)))
+
     def set_state(self, sid, x=None, v=None, image=None):
         x = None if x is None else np.ascontiguousarray(x, np.float64)
         v = None if v is None else np.ascontiguousarray(v, np.float64)
@@ -188,6 +191,15 @@ class Context:
         ms = C.c_double()
         self._check(lib().rbmd_step_timed(self.h, _ip(a), n, nsteps, C.byref(ms)))
         return ms.value
+
+    def autotune(self, ids, cap=256):
+        """Time the pair layouts of these systems (grouped as rbmd_step groups them) and keep the
+        fastest per group; returns one dict per group (layout chosen, ms per layout, from_cache)."""
+        a, n = self._ids(ids)
+        res = (A.TuneResult * cap)()
+        ng = C.c_int32()
+        self._check(lib().rbmd_autotune(self.h, _ip(a), n, res, cap, C.byref(ng)))
+        return [res[k].as_dict() for k in range(min(ng.value, cap))]
 
     def fma_peak(self, fp64=False):
         v = C.c_double()

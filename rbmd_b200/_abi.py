@@ -107,7 +107,20 @@ class Derived(C.Structure):
 
 class DeviceCfg(C.Structure):
     _fields_ = [("device", C.c_int32), ("batched", C.c_int32), ("use_graphs", C.c_int32),
-                ("pad0", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
+                ("autotune", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
+
+
+LAYOUT_TILE, LAYOUT_LEAN, LAYOUT_GENERAL = 0, 1, 2
+LAYOUT_NAMES = {LAYOUT_TILE: "tile", LAYOUT_LEAN: "lean", LAYOUT_GENERAL: "general"}
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("n_systems", C.c_int32), ("layout", C.c_int32), ("atoms", C.c_int64), ("ms", C.c_double * 3),
+                ("from_cache", C.c_int32), ("pad0", C.c_int32)]
+
+    def as_dict(self):
+        return dict(n_systems=self.n_systems, layout=LAYOUT_NAMES[self.layout], atoms=self.atoms,
+                    ms={LAYOUT_NAMES[k]: self.ms[k] for k in range(3)}, from_cache=bool(self.from_cache))
 
 
 class ServeCfg(C.Structure):
@@ -182,6 +195,7 @@ def declare(lib, prefix="rbmd"):
         "get_forces": ([ctx, C.c_int32, dptr], C.c_int),
         "get_state": ([ctx, C.c_int32, dptr, dptr, iptr], C.c_int),
         "set_state": ([ctx, C.c_int32, dptr, dptr, iptr], C.c_int),
+        "set_step": ([ctx, C.c_int32, C.c_int64], C.c_int),
         "get_thermo": ([ctx, C.c_int32, P(Thermo)], C.c_int),
         "get_cells": ([ctx, C.c_int32, iptr, iptr, iptr, iptr, iptr], C.c_int),
         "get_rbl_lists": ([ctx, C.c_int32, C.c_int32, iptr, iptr, iptr], C.c_int),
@@ -202,6 +216,7 @@ def declare(lib, prefix="rbmd"):
         "profile_get": ([ctx, C.c_char_p, dptr, P(C.c_int64), dptr], C.c_int),
         "step_timed": ([ctx, iptr, C.c_int32, C.c_int32, dptr], C.c_int),
         "fma_peak": ([ctx, C.c_int32, dptr], C.c_int),
+        "autotune": ([ctx, iptr, C.c_int32, P(TuneResult), C.c_int32, iptr], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, f"{prefix}_{name}")
@@ -214,10 +229,10 @@ HEADER_FUNCTIONS = [
     "rbmd_abi_version", "rbmd_params_default", "rbmd_ctx_create", "rbmd_ctx_destroy",
     "rbmd_last_error", "rbmd_system_bytes", "rbmd_system_add", "rbmd_system_remove", "rbmd_init",
     "rbmd_step", "rbmd_sync", "rbmd_compute_forces", "rbmd_get_forces", "rbmd_get_state",
-    "rbmd_set_state", "rbmd_get_thermo", "rbmd_get_cells", "rbmd_get_rbl_lists", "rbmd_get_rbl_lists_static",
+    "rbmd_set_state", "rbmd_set_step", "rbmd_get_thermo", "rbmd_get_cells", "rbmd_get_rbl_lists", "rbmd_get_rbl_lists_static",
     "rbmd_get_kspace",
     "rbmd_get_derived", "rbmd_eam_spline_sizes", "rbmd_eam_build_splines", "rbmd_eam_read_funcfl",
     "rbmd_serve_start", "rbmd_serve_submit", "rbmd_serve_poll", "rbmd_serve_wait",
     "rbmd_serve_result", "rbmd_serve_stop", "rbmd_launch_count", "rbmd_profile_enable",
-    "rbmd_profile_get", "rbmd_step_timed", "rbmd_fma_peak",
+    "rbmd_profile_get", "rbmd_step_timed", "rbmd_fma_peak", "rbmd_autotune",
 ]

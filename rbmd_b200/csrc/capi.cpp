@@ -146,6 +146,11 @@ int rbmd_set_state(rbmd_ctx* ctx, int32_t id, const double* x, const double* v, 
   return ctx->c->set_state(id, x, v, image);
 }
 
+int rbmd_set_step(rbmd_ctx* ctx, int32_t id, int64_t step) {
+  CTX_CHECK(ctx);
+  return ctx->c->set_step(id, step);
+}
+
 int rbmd_get_thermo(rbmd_ctx* ctx, int32_t id, rbmd_thermo* out) {
   CTX_CHECK(ctx);
   return ctx->c->get_thermo(id, out);
@@ -384,6 +389,17 @@ int rbmd_profile_get(rbmd_ctx* ctx, const char* kernel, double* avg_ms, int64_t*
   if (launches) *launches = r.n;
   if (units_per_launch) *units_per_launch = r.n ? r.units_sum / r.n : 0.0;
   return RBMD_OK;
+}
+
+int rbmd_autotune(rbmd_ctx* ctx, const int32_t* ids, int32_t n, rbmd_tune_result* results, int32_t cap,
+                  int32_t* n_groups) {
+  CTX_CHECK(ctx);
+  if (!ids || n <= 0 || cap < 0 || (cap > 0 && !results)) return ctx->c->fail(RBMD_ERR_ARG, "bad autotune arguments");
+  int ng = 0;
+  rbmd_tune_result dummy;
+  const int rc = ctx->c->autotune(ids, n, cap > 0 ? results : &dummy, cap, &ng, true);
+  if (n_groups) *n_groups = ng;
+  return rc;
 }
 
 int rbmd_step_timed(rbmd_ctx* ctx, const int32_t* ids, int32_t n, int32_t nsteps, double* ms) {

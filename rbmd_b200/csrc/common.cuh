@@ -98,6 +98,11 @@ struct SysDev {
   double cls_d[3];
   float cls_f[3];
   int cls_pad;
+  // Mixed precision: bands [band[0], band[1]] around the rs thresholds and [band[2], band[3]]
+  // around the rc threshold of FP32 squared distance (a bound on the FP32 rounding error) inside
+  // which a pair is classified again in FP64; below band[0] a pair is surely core, between
+  // band[1] and band[2] surely shell, above band[3] surely out
+  float band[4];
   uint32_t seed_lo, seed_hi;
   // atom arrays (original order)
   double4* x;          // x, y, z, charge

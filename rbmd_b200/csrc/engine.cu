@@ -319,6 +319,36 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   D.cls_f[0] = thr_below<float>((float)D.rc2, 0.0001f);
   D.cls_f[1] = thr_above<float>((float)D.rs2, 0.0001f);
   D.cls_f[2] = thr_below<float>((float)D.rs2, 0.0001f);
+  {
+    // Error band of FP32 squared distances (mixed precision).  Each FP32 displacement component
+    // inherits the rounding of the candidate position, the image shift, their difference, the home
+    // position and the result: |e| <= u (3 Xmax + 6 Lmax + rc) with u = 2^-24, positions within
+    // Xmax of the origin and shifts up to 3 Lmax; then |d2_32 - d2_64| <= 2 sqrt(3) r e + 3 e^2 +
+    // 4 u r^2 near r^2 = t, doubled for safety.  NPT boxes are bounded by their largest box.
+    const double u = std::ldexp(1.0, -24), grow = p.ensemble == RBMD_ENS_NPT ? kBoxGrow : 1.0;
+    double xmax = 0.0, lmax = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      xmax = std::max(xmax, std::fabs(0.5 * (D.lo[k] + D.hi[k])) + 1.25 * grow * D.L[k]);
+      lmax = std::max(lmax, grow * D.L[k]);
+    }
+    const double e = u * (3 * xmax + 6 * lmax + D.rc);
+    auto band = [&](double t) { return 2.0 * (2.0 * std::sqrt(3.0) * std::sqrt(t) * e + 3 * e * e + 4 * u * t); };
+    auto ulpf = [](double t) { const float f = (float)t; return (double)(std::nextafter(f, 2 * f + 1) - f); };
+    // band edges rounded outwards to float
+    auto down = [](double v) { float f = (float)v; return (double)f > v ? std::nextafter(f, -INFINITY) : f; };
+    auto up = [](double v) { float f = (float)v; return (double)f < v ? std::nextafter(f, INFINITY) : f; };
+    const double w_rc = band(D.rc2) + 2 * ulpf(D.rc2) + std::fabs((double)D.cls_f[0] - D.cls_d[0]);
+    D.band[2] = down(D.cls_d[0] - w_rc);
+    D.band[3] = up(D.cls_d[0] + w_rc);
+    if (p.neighbor == RBMD_NEIGH_RBL) {
+      const double w_rs = band(D.rs2) + 2 * ulpf(D.rs2) +
+                          std::max(std::fabs((double)D.cls_f[1] - D.cls_d[1]), std::fabs((double)D.cls_f[2] - D.cls_d[2]));
+      D.band[0] = down(D.cls_d[2] - w_rs);
+      D.band[1] = up(D.cls_d[1] + w_rs);
+    } else {
+      D.band[0] = D.band[1] = -1.0f;  // one threshold only: nothing is banded below rc
+    }
+  }
   D.alpha = p.alpha;
   D.volume = s->dv.volume;
   D.S = s->dv.S_rbe;
@@ -353,7 +383,9 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   D.lean = stencil_ok ? 1 : 0;
   D.dense = (stencil_ok && p.precision == RBMD_PREC_MIXED && n < (1 << 25) &&
              (double)n >= kTileMinPerCell * (double)D.ncell) ? 1 : 0;
-  if (const char* lay = std::getenv("RBMD_PAIR_LAYOUT")) {
+  const char* lay = std::getenv("RBMD_PAIR_LAYOUT");
+  s->tuned = lay != nullptr && lay[0] != '\0' && std::strcmp(lay, "auto") != 0;  // a forced layout is not retuned
+  if (lay) {
     if (std::strcmp(lay, "atom") == 0) {
       D.lean = 0;
       D.dense = 0;
@@ -367,6 +399,7 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
     // The box changes every step: the general traversal (any dims), cell tables for the largest
     // box the barostat accepts.
     D.npt = p.press_ctrl == RBMD_PC_NOSE_HOOVER ? 2 : 1;
+    s->tuned = true;  // one layout only
     D.lean = 0;
     D.dense = 0;
     D.ncell_cap = 1;
@@ -608,7 +641,9 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
     up(D.z2r_s, d.eam_z2r_spline, sizeof(double) * 7 * (d.eam_nr + 1));
   }
   D.atom_part = (double*)dal(sizeof(double) * 8 * D.blocks_atom);
-  D.vir_part = (double*)dal(sizeof(double) * 9 * D.blocks_pair);
+  // pair-kernel partials: enough blocks for any layout the autotuner may switch to
+  D.vir_part = (double*)dal(sizeof(double) * 9 *
+                            std::max((D.ncell_cap + kCellWarpsHost - 1) / kCellWarpsHost, (n + kPairWarps - 1) / kPairWarps));
   D.tri_part = (double*)dal(sizeof(double) * 6 * std::max(1, D.blocks_tri));
   D.st = (SysState*)dal(sizeof(SysState));
   if (oom) {
@@ -684,12 +719,13 @@ int Context::remove_system(int id) {
 }
 
 // ------------------------------------------------------------------------------ batches
-static bool same_group(const System* a, const System* b) {
+bool same_group(const System* a, const System* b, bool layout) {
   const SysDev &x = a->dev, &y = b->dev;
   return x.ff == y.ff && x.neigh == y.neigh && x.coul == y.coul && x.prec == y.prec &&
          x.temp_ctrl == y.temp_ctrl && x.special == y.special && x.has_triples == y.has_triples &&
-         ((x.n_bonds + x.n_angles) > 0) == ((y.n_bonds + y.n_angles) > 0) && x.dense == y.dense &&
-         x.lean == y.lean && x.npt == y.npt;
+         ((x.n_bonds + x.n_angles) > 0) == ((y.n_bonds + y.n_angles) > 0) && x.npt == y.npt && x.rc2 == y.rc2 &&
+         x.rs2 == y.rs2 &&
+         (!layout || (x.dense == y.dense && x.lean == y.lean));
 }
 
 Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& rc) {
@@ -711,8 +747,13 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
   b.npt = g.npt;
   std::vector<int> slots;
   std::vector<int2> wa, wp, wc, wr, wt, wm;
+  for (int k = 0; k < 4; ++k) b.band[k] = g.band[k];
   for (System* s : group) {
     const SysDev& D = s->dev;
+    b.band[0] = std::min(b.band[0], D.band[0]);
+    b.band[1] = std::max(b.band[1], D.band[1]);
+    b.band[2] = std::min(b.band[2], D.band[2]);
+    b.band[3] = std::max(b.band[3], D.band[3]);
     slots.push_back(s->slot);
     br->ids.push_back(s->id);
     b.max_P = std::max(b.max_P, std::max(D.P, D.nk_ewald));
@@ -773,7 +814,7 @@ std::vector<Context::BatchRec*> Context::batches_for(const int32_t* ids, int n, 
     bool placed = false;
     if (cfg.batched)
       for (auto& g : groups)
-        if (same_group(g[0], s)) {
+        if (same_group(g[0], s, true)) {
           g.push_back(s);
           placed = true;
           break;
@@ -850,6 +891,10 @@ void Context::enqueue_step(const Batch& b) {
 int Context::init(const int32_t* ids, int n) {
   std::lock_guard<std::recursive_mutex> lk(mu);
   int rc;
+  if (cfg.autotune) {  // before the first force evaluation: nothing to keep
+    rc = autotune(ids, n, nullptr, 0, nullptr, false);
+    if (rc) return rc;
+  }
   auto bs = batches_for(ids, n, rc);
   if (rc) return rc;
   for (int k = 0; k < n; ++k) {
@@ -879,6 +924,10 @@ int Context::step(const int32_t* ids, int n, int nsteps) {
   std::lock_guard<std::recursive_mutex> lk(mu);
   if (nsteps <= 0) return RBMD_OK;
   int rc;
+  if (cfg.autotune) {
+    rc = autotune(ids, n, nullptr, 0, nullptr, true);
+    if (rc) return rc;
+  }
   auto bs = batches_for(ids, n, rc);
   if (rc) return rc;
   const bool graphs = cfg.use_graphs && !prof.on;
@@ -1016,6 +1065,16 @@ int Context::set_state(int id, const double* x, const double* v, const int32_t* 
     sync();
   }
   return check_cuda("set_state");
+}
+
+int Context::set_step(int id, int64_t step) {
+  std::lock_guard<std::recursive_mutex> lk(mu);
+  System* s = find(id);
+  if (!s) return fail(RBMD_ERR_STATE, "unknown system id");
+  if (step < 0) return fail(RBMD_ERR_ARG, "negative step");
+  cudaMemcpyAsync(&s->dev.st->step, &step, sizeof(int64_t), cudaMemcpyHostToDevice, stream);
+  const int rc = sync();
+  return rc ? rc : check_cuda("set_step");
 }
 
 int Context::get_thermo(int id, rbmd_thermo* out) {

@@ -31,6 +31,7 @@ struct System {
   int n_terms = 0;
   int P = 0;
   std::vector<double> charge;   // host copy (energies)
+  bool tuned = false;           // pair layout chosen by the autotuner (or fixed: NPT, environment)
 };
 
 struct Profiler {
@@ -44,6 +45,10 @@ struct Profiler {
   };
   std::map<std::string, Rec> recs;
 };
+
+// Systems that one launch can cover: same kernel configuration (and, with layout, the same pair
+// traversal layout).
+bool same_group(const System* a, const System* b, bool layout);
 
 class Context {
  public:
@@ -59,6 +64,7 @@ class Context {
   int get_forces(int id, double* f);
   int get_state(int id, double* x, double* v, int32_t* image);
   int set_state(int id, const double* x, const double* v, const int32_t* image);
+  int set_step(int id, int64_t step);
   int get_thermo(int id, rbmd_thermo* out);
   int get_cells(int id, int32_t* dims, int32_t* coa, int32_t* sorted, int32_t* lo, int32_t* up);
   int get_rbl_lists(int id, int cap, int32_t* nc, int32_t* ns, int32_t* ids);
@@ -66,6 +72,7 @@ class Context {
   int get_kspace(int id, int32_t* m, double* rhok);
   int get_derived(int id, rbmd_derived* out);
   int device_status(int id, int* status);
+  int autotune(const int32_t* ids, int n, rbmd_tune_result* out, int cap, int* n_groups, bool keep_forces = true);
 
   int fail(int code, const std::string& msg);
   std::string last_error;
@@ -88,6 +95,8 @@ class Context {
   int ensure_slots(int need);
   int upload_record(System* s);
   int refresh(System* s);
+  void set_layout(System* s, int layout);
+  std::vector<int> usable_layouts(const System* s) const;
   std::vector<BatchRec*> batches_for(const int32_t* ids, int n, int& rc);
   BatchRec* build_batch(const std::vector<System*>& group, int& rc);
   void drop_batches_with(int id);
@@ -102,6 +111,7 @@ class Context {
   int slot_cap_ = 0;
   int next_id_ = 0;
   std::map<std::vector<int>, BatchRec*> batch_cache_;
+  std::map<std::vector<int64_t>, int> tune_cache_;  // autotuner decisions by group signature
 };
 
 }  // namespace rbmd

@@ -52,6 +52,26 @@ __device__ inline double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ inline float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ inline float add_rn(float a, float b) { return __fadd_rn(a, b); }
 
+// Mixed precision: an FP32 squared distance carries the rounding of the FP32 positions and image
+// shifts.  A pair whose FP32 value lies within that error band of a classification threshold
+// (centres amb_c, half-widths amb_w, set on the host from a bound on the error) is classified
+// again from the FP64 positions with the FP64 kernels' arithmetic and thresholds, so that core /
+// shell membership, and with it the RBL picks, are exactly those of the FP64 path.  m is the
+// candidate's image offset in cells (wrapped - unwrapped cell index) per dimension.
+__device__ __forceinline__ bool f32_banded(const SysDev& s, float dd) {
+  return (dd >= s.band[0] && dd <= s.band[1]) || (dd >= s.band[2] && dd <= s.band[3]);
+}
+__device__ __forceinline__ void classify_fp64(const SysDev& s, double pix, double piy, double piz, int js, int mx, int my,
+                                           int mz, bool rbl, bool& core, bool& shell) {
+  const double4 pj = ldg4(&s.sx[js]);
+  const double rx = (pj.x - s.d[0] * (double)mx) - pix;
+  const double ry = (pj.y - s.d[1] * (double)my) - piy;
+  const double rz = (pj.z - s.d[2] * (double)mz) - piz;
+  const double dd = add_rn(add_rn(mul_rn(rx, rx), mul_rn(ry, ry)), mul_rn(rz, rz));
+  shell = rbl && dd >= s.cls_d[1] && dd <= s.cls_d[0];
+  core = rbl ? (dd <= s.cls_d[2] && dd > 0.0001) : (dd <= s.cls_d[0] && dd > 0.0001);
+}
+
 __device__ inline double r_sqrt(double x) { return sqrt(x); }
 __device__ inline float r_sqrt(float x) { return sqrtf(x); }
 __device__ inline double r_exp(double x) { return exp(x); }
@@ -379,6 +399,12 @@ k_pair(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int
             core = !shell && (rs2 - d2 > R(0.0001) && d2 > R(0.0001));
           } else {
             core = (rc2 - d2 > R(0.0001) && d2 > R(0.0001));
+          }
+          if constexpr (sizeof(R) == 4) {
+            if (f32_banded(s, (float)d2))
+              classify_fp64(s, xi.x, xi.y, xi.z, js, (int)rintf((float)(s_coff[wid][0][lo] / s.d[0])),
+                            (int)rintf((float)(s_coff[wid][1][lo] / s.d[1])),
+                            (int)rintf((float)(s_coff[wid][2][lo] / s.d[2])), rbl, core, shell);
           }
         }
         bool sel = core;
@@ -814,6 +840,12 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
           } else {
             core = (rc2 - dd > R(0.0001) && dd > R(0.0001));
           }
+          if constexpr (sizeof(R) == 4) {
+            if (f32_banded(s, (float)dd))
+              classify_fp64(s, xi.x, xi.y, xi.z, js, (int)rintf((float)(s_so[wid][0][seg] / d0)),
+                            (int)rintf((float)(s_so[wid][1][seg] / d1)), (int)rintf((float)(s_so[wid][2][seg] / d2c)),
+                            rbl, core, shell);
+          }
         }
         bool sel = core;
         if (rbl) {
@@ -957,31 +989,25 @@ __device__ inline float rcp_approx(float x) {
 // (erfc by Abramowitz & Stegun 7.1.26, |error| <= 1.5e-7), the same windows as eval_pair_f32_pre.
 // alpha_l2 = alpha log2(e), so exp(-alpha d2) = 2^(-alpha_l2 d2).
 template <int MODE>
-__device__ inline float tile_pair_f32(bool core, float d2, float qi, float qj, int tp, float w, float pice,
-                                      float rc2, float rs2, float sa, float alpha_l2, float qq, const float* tab,
-                                      bool special) {
+// The pair's class is exact (the FP64 decision, with the reference's 1e-4 margins around rs^2
+// and rc^2), and it implies every cutoff test of the reference's force functions (core: d2 < rs^2
+// and > 1e-4; shell: rs^2 < d2 < rc^2), so none is repeated here on the FP32 d2.
+__device__ inline float tile_pair_f32(bool core, float d2, float qi, float qj, int tp, float w, float pice, float sa,
+                                      float alpha_l2, float qq, const float* tab) {
   const float clj = tab[2 * tp], s6 = tab[2 * tp + 1];
   const float inv_r = rsqrt_approx(d2);
   const float inv_d2 = inv_r * inv_r;
   const float sd6 = s6 * inv_d2 * inv_d2 * inv_d2;
   const float ljf = clj * (2.0f * sd6 - 1.0f) * sd6 * inv_d2;
-  float fl;
-  if (MODE == kLJ_RBL) {
-    fl = core ? ((d2 < rc2 && d2 > 0.0001f) ? ljf : 0.0f) : ((d2 < rc2 && d2 > rs2) ? pice * ljf : 0.0f);
-    return fl;
-  }
-  fl = core ? ((d2 < rs2 && d2 > 0.0001f) ? w * ljf : 0.0f) : ((d2 < rc2 && d2 > rs2) ? w * (pice * ljf) : 0.0f);
-  const bool in = core ? (d2 < rc2 && d2 > 0.0001f) : (special ? (d2 < rc2 && d2 > rs2) : (d2 < rc2 && d2 > 0.0001f));
-  float fc = 0.0f;
-  if (in) {
-    const float x = sa * (d2 * inv_r);
-    const float e = ex2_approx(-alpha_l2 * d2);
-    const float t = rcp_approx(1.0f + 0.3275911f * x);
-    const float erfc = t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f)))) * e;
-    const float g = erfc * inv_d2 + 1.1283791671f * sa * e * inv_r;  // 2/sqrt(pi)
-    fc = -qi * qj * g * inv_r;
-    if (!core) fc *= pice;
-  }
+  if (MODE == kLJ_RBL) return core ? ljf : pice * ljf;
+  const float fl = core ? w * ljf : w * (pice * ljf);
+  const float x = sa * (d2 * inv_r);
+  const float e = ex2_approx(-alpha_l2 * d2);
+  const float t = rcp_approx(1.0f + 0.3275911f * x);
+  const float erfc = t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f)))) * e;
+  const float g = erfc * inv_d2 + 1.1283791671f * sa * e * inv_r;  // 2/sqrt(pi)
+  float fc = -qi * qj * g * inv_r;
+  if (!core) fc *= pice;
   return fl + qq * fc;
 }
 
@@ -991,7 +1017,10 @@ __device__ inline float tile_pair_f32(bool core, float d2, float qi, float qj, i
 // each one or two contiguous ranges of the cell-ordered arrays -- so the warp streams that
 // sequence once, 32 candidates per batch (one per lane), and classifies each batch against every
 // atom of the cell in turn: two ballots (core, shell) per (atom, batch), the window tests done as
-// single compares against exact thresholds.  The lane that owns an atom then turns its masks into
+// single compares against exact thresholds.  In FP32 the compares are against the edges of the
+// FP32 rounding bands around rs^2 and rc^2; the few pairs inside a band are classified again from
+// the FP64 positions, so the classes -- and the RBL picks that count them -- are exactly the FP64
+// path's.  The lane that owns an atom then turns its masks into
 // picks -- every pice-th shell atom in traversal order, located with __fns from a running skip
 // count -- and queues the selected pairs as packed ints.  When any queue is nearly full the warp
 // evaluates all queues in lock step; with 16 or fewer atoms in the cell each queue is shared by
@@ -1018,6 +1047,50 @@ template <> __device__ inline float cls_thr<float>(const SysDev& s, int k) { ret
 // evaluation so that both see the same value.
 __device__ inline double tile_d2(double x, double y, double z) { return add_rn(add_rn(mul_rn(x, x), mul_rn(y, y)), mul_rn(z, z)); }
 __device__ inline float tile_d2(float x, float y, float z) { return __fmaf_rn(z, z, __fmaf_rn(y, y, __fmul_rn(x, x))); }
+
+// FP32 RBL classification against the band edges (SysDev::band), as two flags whose ballots
+// carry three outcomes out of the hot loop: x alone = core, y alone = shell, both = banded (to be
+// classified in FP64), neither = out (or the pair of an atom with itself).  Outside the bands the
+// outcome equals the FP64 classification.  Each flag is one chain of compares (one predicate).
+__device__ __forceinline__ void band_classify(float dd, float b0, float b1, float b2, float b3, bool& x, bool& y) {
+  x = ((dd <= b1) | (dd >= b2)) & (dd <= b3) & (dd > 0.0001f);
+  y = (dd >= b0) & (dd <= b3);
+}
+
+// Tile layout, FP32 RBL: the banded pairs of this lane's home atom (bits of amb, candidate lanes
+// of the batch) classified from the FP64 positions; returns the corrected (core, shell) words.
+// The candidates are identified from the batch's history row: queue entries (hist: sorted index |
+// shift code) where the kernel keeps them, else atom ids with the shifted FP32 positions (hid, hp),
+// from which the sorted index (rank) and the image of each dimension follow.  Runs for about one
+// batch in fifty.
+__device__ __forceinline__ uint2 tile_fix_banded(const SysDev& s, const int* hist, const int* hid, const float4* hp4,
+                                              int si, unsigned amb, unsigned my_cm, unsigned my_sm) {
+  if (amb) {
+    const double4 hp = ldg4(&s.sx[si]);
+    while (amb) {
+      const int b = __ffs(amb) - 1;
+      amb &= amb - 1;
+      int js, m[3];
+      if (hist) {
+        const int ent = hist[b];
+        js = ent & kJsMask;
+        for (int k = 0; k < 3; ++k) m[k] = (((ent >> (kJsBits + 2 * k)) & 3) - 1) * s.dims[k];
+      } else {
+        js = __ldg(&s.rank[hid[b] & kJsMask]);
+        const double4 pj = ldg4(&s.sx[js]);
+        const float4 c = hp4[b];  // pj - shift, rounded to FP32
+        const double sh[3] = {pj.x - (double)c.x, pj.y - (double)c.y, pj.z - (double)c.z};
+        for (int k = 0; k < 3; ++k) m[k] = (int)rint(sh[k] / (s.d[k] * (double)s.dims[k])) * s.dims[k];
+      }
+      bool core, shell;
+      classify_fp64(s, hp.x, hp.y, hp.z, js, m[0], m[1], m[2], true, core, shell);
+      const unsigned bit = 1u << b;
+      my_cm = core ? (my_cm | bit) : (my_cm & ~bit);
+      my_sm = shell ? (my_sm | bit) : (my_sm & ~bit);
+    }
+  }
+  return make_uint2(my_cm, my_sm);
+}
 
 // Picked shells of one batch: the set bits of sm at ranks r, r + pice, ... where r is the number
 // of shells still to skip; r leaves as the skip count for the next batch.
@@ -1203,8 +1276,12 @@ __device__ void tile_stray(const SysDev& s, int si, int skip, int pice, bool rbl
             rz = (pj.z - oz) - p4.z;
           }
           const R dd = tile_d2(rx, ry, rz);
-          const bool shell = rbl && dd >= t_rs_hi && dd <= t_rc;
-          const bool core = rbl ? (dd <= t_rs_lo && dd > R(0.0001)) : (dd <= t_rc && dd > R(0.0001));
+          bool shell = rbl && dd >= t_rs_hi && dd <= t_rc;
+          bool core = rbl ? (dd <= t_rs_lo && dd > R(0.0001)) : (dd <= t_rc && dd > R(0.0001));
+          if constexpr (sizeof(R) == 4) {
+            if (kk < ce && f32_banded(s, (float)dd))
+              classify_fp64(s, xd.x, xd.y, xd.z, kk, w0 - n0, w1 - n1, w2 - n2, rbl, core, shell);
+          }
           const unsigned cm = __ballot_sync(FULL, core), sm = __ballot_sync(FULL, shell);
           const unsigned pk = rbl ? pick_shells(sm, pice, skip) : 0u;
           const bool sel = ((cm | pk) >> lane) & 1u;
@@ -1242,7 +1319,7 @@ __device__ void tile_stray(const SysDev& s, int si, int skip, int pice, bool rbl
 template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
 __global__ void __launch_bounds__(kCellWarps * 32, RBMD_TILE_MIN_BLOCKS)
 k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int* out_nc, int* out_ns,
-            int* out_core, int* out_shell) {
+            int* out_core, int* out_shell, float4 band) {
   using R4 = typename Vec4<R>::T;
   constexpr bool F32 = sizeof(R) == 4 && (MODE == kLJ_RBL || MODE == kCOUL_RBL);
   constexpr bool QUEUE = MODE != kLIST;
@@ -1295,11 +1372,13 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
                     ((MODE == kEAM_RHO || MODE == kEAM_FORCE) && s.neigh == RBMD_NEIGH_RBL));
   const int pice = rbl ? s.pice : 1;
   const R t_rc = cls_thr<R>(s, 0), t_rs_hi = cls_thr<R>(s, 1), t_rs_lo = cls_thr<R>(s, 2);
+  // FP32 band edges: one set for the whole launch, the union of its systems' bands (a batch's
+  // systems share rc and rs)
+  const float b0 = band.x, b1 = band.y, b2 = band.z, b3 = band.w;
+  const float spice = (float)pice, fsa = (float)sqrt(s.alpha);
+  const float falpha_l2 = (float)(s.alpha * 1.4426950408889634), fqq = (float)s.qqr2e;  // alpha log2(e)
   const R far = R(1e30);
   const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
-  const float spice = (float)pice, fsa = (float)sqrt(s.alpha);
-  const float frc2 = (float)s.rc2, frs2 = (float)s.rs2;
-  const float falpha_l2 = (float)(s.alpha * 1.4426950408889634), fqq = (float)s.qqr2e;  // alpha log2(e)
   if (lane < 9) s_red[wid][lane] = 0.0;  // per-warp reduction values, added in a fixed order
   // lane 0 adds the warp total of v (owner lanes' values, in lane order) to s_red[wid][k]
   auto add_red = [&](const double (&v)[9], bool take) {
@@ -1438,7 +1517,7 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
               if (!skip_pair) {
                 const float d2 = tile_d2(rx, ry, rz);
                 const float f = tile_pair_f32<MODE>((h & 0x8000u) == 0u, d2, pa.w, pj.w, ai.x * ntypes + tj, w, spice,
-                                                    frc2, frs2, fsa, falpha_l2, fqq, s_tab, SPECIAL);
+                                                    fsa, falpha_l2, fqq, s_tab);
                 fx = f * rx;
                 fy = f * ry;
                 fz = f * rz;
@@ -1557,7 +1636,9 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
           const R4 pj = pj_n;
           const int ent = ent_n, idt = idt_n;
           const bool val = val_n;
-          if (base + 32 < total) fetch(base + 32 + lane);
+          // FP32: the next batch is fetched after the classification loop, which then runs with
+          // fewer live registers; FP64 fetches it here
+          if (!F32 && base + 32 < total) fetch(base + 32 + lane);
           R cx = far, cy = far, cz = far;
           if (val) {
             cx = pj.x - s_shift[0][(ent >> kJsBits) & 3];
@@ -1571,19 +1652,51 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
           }
           // every atom of the chunk against the batch: two ballots each, kept by the atom's lane
           unsigned my_cm = 0u, my_sm = 0u;
-          for (int ii = 0; ii < nat; ++ii) {
-            const R4 q = s_pi[wid][ii];
-            const R rx = cx - q.x, ry = cy - q.y, rz = cz - q.z;
-            const R dd = tile_d2(rx, ry, rz);
-            const bool shell = rbl && dd >= t_rs_hi && dd <= t_rc;
-            const bool core = rbl ? (dd <= t_rs_lo && dd > R(0.0001)) : (dd <= t_rc && dd > R(0.0001));
-            const unsigned cm = __ballot_sync(FULL, core);
-            const unsigned sm = rbl ? __ballot_sync(FULL, shell) : 0u;
-            if (lane == ii) {
-              my_cm = cm;
-              my_sm = sm;
+          // FP32 RBL (the LJ / Coulomb modes, where rbl is known at compile time, and EAM over RBL):
+          // the band edges are the thresholds; banded pairs come out with both bits set and are
+          // classified again from the FP64 positions (rare)
+          constexpr bool kBandOnly = F32;  // no other classification compiled in
+          if (kBandOnly || (sizeof(R) == 4 && rbl)) {
+            for (int ii = 0; ii < nat; ++ii) {
+              const R4 q = s_pi[wid][ii];
+              const float dd = tile_d2((float)cx - (float)q.x, (float)cy - (float)q.y, (float)cz - (float)q.z);
+              bool core, shell;
+              band_classify(dd, b0, b1, b2, b3, core, shell);
+              const unsigned cm = __ballot_sync(FULL, core);
+              const unsigned sm = __ballot_sync(FULL, shell);
+              if (lane == ii) {
+                my_cm = cm;
+                my_sm = sm;
+              }
+            }
+            const unsigned amb = my_cm & my_sm;  // banded candidates of this lane's home atom
+            my_cm &= ~amb;
+            my_sm &= ~amb;
+            if (__any_sync(FULL, amb != 0u)) {
+              const uint2 r = (F32 && MODE != kLJ_RBL)
+                                  ? tile_fix_banded(s, nullptr, &s_hid[wid][nh][0], &s_hp[wid][nh][0], g0 + lane, amb,
+                                                    my_cm, my_sm)
+                                  : tile_fix_banded(s, &s_hist[wid][nh][0], nullptr, nullptr, g0 + lane, amb, my_cm, my_sm);
+              my_cm = r.x;
+              my_sm = r.y;
             }
           }
+          if constexpr (!kBandOnly) if (!(sizeof(R) == 4 && rbl)) {
+            for (int ii = 0; ii < nat; ++ii) {
+              const R4 q = s_pi[wid][ii];
+              const R rx = cx - q.x, ry = cy - q.y, rz = cz - q.z;
+              const R dd = tile_d2(rx, ry, rz);
+              const bool shell = rbl && dd >= t_rs_hi && dd <= t_rc;
+              const bool core = rbl ? (dd <= t_rs_lo && dd > R(0.0001)) : (dd <= t_rc && dd > R(0.0001));
+              const unsigned cm = __ballot_sync(FULL, core);
+              const unsigned sm = rbl ? __ballot_sync(FULL, shell) : 0u;
+              if (lane == ii) {
+                my_cm = cm;
+                my_sm = sm;
+              }
+            }
+          }
+          if (F32 && base + 32 < total) fetch(base + 32 + lane);
           if (!owner || stray) my_cm = my_sm = 0u;
           // picks among this atom's shells (every pice-th in traversal order, after `skip` more),
           // by a predicated walk over the set bits: no data-dependent branches
@@ -1693,8 +1806,8 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
 template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
 static void go(const Batch& b, cudaStream_t st) {
   if (b.dense)
-    k_pair_tile<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kCellWarps * 32, 0, st>>>(b.sys, b.pair.d, 0, nullptr,
-                                                                               nullptr, nullptr, nullptr);
+    k_pair_tile<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kCellWarps * 32, 0, st>>>(
+        b.sys, b.pair.d, 0, nullptr, nullptr, nullptr, nullptr, make_float4(b.band[0], b.band[1], b.band[2], b.band[3]));
   else if (b.lean)
     k_pair2<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kPairWarps * 32, 0, st>>>(b.sys, b.pair.d);
   else
@@ -1757,7 +1870,7 @@ void launch_rbl_lists(const SysDev* sys, int slot, int n, int ncell, int dense, 
   cudaMemcpyAsync(d_work, h, sizeof(int2) * nb, cudaMemcpyHostToDevice, st);
   if (dense)
     k_pair_tile<double, kLIST, false, false><<<nb, kCellWarps * 32, 0, st>>>(sys, d_work, cap, n_core, n_shell,
-                                                                             ids, ids + (size_t)n * cap);
+                                                                             ids, ids + (size_t)n * cap, float4{});
   else
     k_pair<double, kLIST, false, false><<<nb, kPairWarps * 32, 0, st>>>(sys, d_work, cap, n_core, n_shell,
                                                                        ids, ids + (size_t)n * cap);
@@ -1877,7 +1990,8 @@ int launch_rbl_lists_static(const SysDev* sys, int slot, int n, int ncell, int d
   launch_cells(b, st);
   if (dense)
     k_pair_tile<double, kLIST, false, false><<<np, kCellWarps * 32, 0, st>>>(sys, w_pair, cap, out->n_core,
-                                                                             out->n_shell, out->rows, shell_rows);
+                                                                             out->n_shell, out->rows, shell_rows,
+                                                                             float4{});
   else
     k_pair<double, kLIST, false, false><<<np, kPairWarps * 32, 0, st>>>(sys, w_pair, cap, out->n_core,
                                                                        out->n_shell, out->rows, shell_rows);

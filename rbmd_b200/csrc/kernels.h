@@ -26,6 +26,7 @@ struct Batch {
   int lean = 0;              // warp per atom with segment tables (dims >= 2 nc + 1 everywhere)
   int npt = 0;               // NPT barostat: 0 none, 1 Berendsen (end of step), 2 MTK (around the integrator)
   int max_P = 0;             // largest P (or Ewald nk) in the batch
+  float band[4] = {0, 0, 0, 0};  // FP32 classification bands: union over the batch (same rc, rs)
   long long natoms = 0;      // atoms over all systems of the batch
 };
 

@@ -207,6 +207,7 @@ void ExecutionMD::Init() {
   cfg.device = _device;
   cfg.batched = 0;
   cfg.use_graphs = 1;
+  cfg.autotune = _para.autotune ? 1 : 0;
   check(rbmd_ctx_create(&cfg, &_ctx), "rbmd_ctx_create");
   const rbmd_system_desc d = _para.desc();
   check(rbmd_system_add(_ctx, &d, &_para.params, &_sys), "rbmd_system_add");
@@ -435,8 +436,9 @@ void MDApplication::ReadExecution(const Json& ex) {
   }
   P.timestep = ex.number("timestep", P.timestep);
   P.num_steps = (int64_t)ex.number("num_steps", (double)P.num_steps);
-  // keys this library adds (absent from reference files): seed, precision, rbl_mode
+  // keys this library adds (absent from reference files): seed, precision, rbl_mode, autotune
   P.seed = (uint64_t)ex.number("seed", (double)P.seed);
+  _para.autotune = ex.boolean("autotune", false);
   const std::string prec = ex.string("precision", "FP64");
   if (prec == "FP64") P.precision = RBMD_PREC_FP64;
   else if (prec == "MIXED") P.precision = RBMD_PREC_MIXED;

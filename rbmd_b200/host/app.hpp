@@ -29,6 +29,7 @@ struct Para {
   rbmd_params params{};
   std::string init_way;  // "read_data" or "inbuild"
   std::string unit = "LJ";
+  bool autotune = false;  // execution.autotune: time the pair layouts before the first step
   int n = 0, n_types = 0;
   double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
   std::vector<double> position, velocity, charge, mass, eps, sigma;

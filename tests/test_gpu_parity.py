@@ -289,3 +289,26 @@ def test_energy_drift_mixed_matches_fp64():
     assert abs(d["fp64"]["drift"]) < 5e-3 and abs(d["mixed"]["drift"]) < 5e-3
     assert abs(d["mixed"]["drift"] - d["fp64"]["drift"]) < 2e-4
     assert d["energy_mixed_vs_fp64"] < 2e-3
+
+
+def test_mixed_precision_classification_is_exact_along_trajectories(oracle_mod):
+    """FP32 squared distances near rs^2 or rc^2 are classified again in FP64, so the mixed path
+    picks the same RBL pairs as the FP64 oracle along a trajectory: its force error stays at the
+    FP32 arithmetic level (a different pick would add ~1e-3 or more)."""
+    import rbmd_b200
+    for k, n in enumerate((1000, 4000, 12000)):
+        sd = synth.saline(n, seed=40 + k)
+        sd.params.seed = 900 + k
+        ctx = rbmd_b200.Context()
+        sid = ctx.add_system(sd)
+        ctx.init(sid)
+        for _ in range(3):
+            ctx.step(sid, 5)
+            x, v, img = ctx.state(sid)
+            ctx.compute_forces(sid)
+            o = oracle_mod.Oracle(sd)
+            o.set_state(x, v, img)
+            o.set_step(ctx.thermo(sid)["step"])
+            o.compute_forces()
+            assert rel_rms(ctx.forces(sid), o.forces()) < 1e-4
+        ctx.close()
