@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBMD_ABI_VERSION 2
+#define RBMD_ABI_VERSION 3
 
 /* ---------------------------------------------------------------- status codes */
 enum rbmd_status {
@@ -184,6 +184,17 @@ typedef struct rbmd_system_desc {
   const double* eam_frho_spline; /* [(eam_nrho+1)*7] */
   const double* eam_rhor_spline; /* [(eam_nr+1)*7] */
   const double* eam_z2r_spline;  /* [(eam_nr+1)*7] */
+  /* harmonic dihedrals (CVFF, ComputeDihedralHarmonicWorklet, MolecularWorklet.h:669-973):
+   * E = K [1 + d cos(n phi)]; the reference evaluates them when special_bonds are given, the data
+   * file has a Dihedrals section and force_field.dihedral_type is "Harmonic" (ExecutionNVT.cpp:
+   * 223-228, 585-658); leave n_dihedrals 0 otherwise */
+  int32_t n_dihedrals;
+  int32_t n_dihedral_types;
+  const int32_t* dihedral_atoms;        /* [4*n_dihedrals] i j k l */
+  const int32_t* dihedral_type;         /* [n_dihedrals] 0-based */
+  const double* dihedral_k;             /* [n_dihedral_types] K */
+  const int32_t* dihedral_sign;         /* [n_dihedral_types] d: 1 (cos shift +1), else -1 */
+  const int32_t* dihedral_multiplicity; /* [n_dihedral_types] n >= 0 */
 } rbmd_system_desc;
 
 /* ---------------------------------------------------------------- results */
@@ -209,6 +220,7 @@ typedef struct rbmd_thermo {
   double box_hi[3];
   int32_t status;               /* device-side error word of the system (0 = ok), bits below */
   int32_t pad0;
+  double e_dihedral;            /* per-dihedral average (PARA_DIHEDRAL_ENERGY), in potential_energy */
 } rbmd_thermo;
 
 /* Bits of rbmd_thermo.status, sticky until the system is removed. */

@@ -128,6 +128,8 @@ class System {
   std::vector<double> eps, sig;
   std::vector<int> bond_atoms, bond_type, angle_atoms, angle_type;
   std::vector<double> bond_k, bond_r0, angle_k, angle_theta0;
+  std::vector<int> dihedral_atoms, dihedral_type, dihedral_sign, dihedral_mult;
+  std::vector<double> dihedral_k;
   std::vector<int> special_offsets, special_ids;
   std::vector<double> special_weights;
   std::vector<int> mol_offsets, mol_atoms;  // molecule member CSR (ContTopology source/offsets)
@@ -153,7 +155,7 @@ class System {
   std::vector<double> rhok;       // [2P]
   std::vector<double> f_near, f_far, f_bonded;  // [3N]
   double virial[6] = {0, 0, 0, 0, 0, 0};
-  double e_bond_avg = 0, e_angle_avg = 0;
+  double e_bond_avg = 0, e_angle_avg = 0, e_dihedral_avg = 0;
   std::vector<double> shake_virial_atom;  // [6 * n_angles]
   int status = 0;
 

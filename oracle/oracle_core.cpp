@@ -96,6 +96,13 @@ System::System(const rbmd_system_desc& d, const rbmd_params& prm) : p(prm) {
       angle_theta0.assign(d.angle_theta0, d.angle_theta0 + d.n_angle_types);
     }
   }
+  if (d.n_dihedrals > 0 && p.force_field == RBMD_FF_CVFF) {
+    dihedral_atoms.assign(d.dihedral_atoms, d.dihedral_atoms + 4 * d.n_dihedrals);
+    dihedral_type.assign(d.dihedral_type, d.dihedral_type + d.n_dihedrals);
+    dihedral_k.assign(d.dihedral_k, d.dihedral_k + d.n_dihedral_types);
+    dihedral_sign.assign(d.dihedral_sign, d.dihedral_sign + d.n_dihedral_types);
+    dihedral_mult.assign(d.dihedral_multiplicity, d.dihedral_multiplicity + d.n_dihedral_types);
+  }
   if (d.special_offsets) {
     special_offsets.assign(d.special_offsets, d.special_offsets + N + 1);
     int ns = special_offsets[N];

@@ -404,6 +404,91 @@ void System::bonded_force(std::vector<double>& F) {
     vir[5] += rij[1] * fi[2] + rkj[1] * fk[2];
   }
   e_angle_avg = na > 0 ? e_angle / na : 0.0;
+  // ComputeDihedralHarmonicWorklet, MolecularWorklet.h:669-973: E = K [1 + d cos(n phi)], forces
+  // reduced per atom id, energy averaged over dihedrals (ExecutionNVT.cpp:585-658)
+  double e_dih = 0;
+  const int nd = (int)dihedral_type.size();
+  for (int t = 0; t < nd; ++t) {
+    const int i1 = dihedral_atoms[4 * t], i2 = dihedral_atoms[4 * t + 1], i3 = dihedral_atoms[4 * t + 2],
+              i4 = dihedral_atoms[4 * t + 3];
+    const int ty = dihedral_type[t];
+    const double K = dihedral_k[ty];
+    const int m = dihedral_mult[ty];
+    const double cos_shift = dihedral_sign[ty] == 1 ? 1.0 : -1.0, sin_shift = 0.0;
+    double vb1[3], vb2[3], vb2m[3], vb3[3];
+    for (int k = 0; k < 3; ++k) {
+      vb1[k] = x[3 * i1 + k] - x[3 * i2 + k];
+      vb2[k] = x[3 * i3 + k] - x[3 * i2 + k];
+      vb3[k] = x[3 * i4 + k] - x[3 * i3 + k];
+    }
+    min_image(vb1);
+    min_image(vb2);
+    min_image(vb3);
+    for (int k = 0; k < 3; ++k) vb2m[k] = -vb2[k];
+    const double ax = vb1[1] * vb2m[2] - vb1[2] * vb2m[1];
+    const double ay = vb1[2] * vb2m[0] - vb1[0] * vb2m[2];
+    const double az = vb1[0] * vb2m[1] - vb1[1] * vb2m[0];
+    const double bx = vb3[1] * vb2m[2] - vb3[2] * vb2m[1];
+    const double by = vb3[2] * vb2m[0] - vb3[0] * vb2m[2];
+    const double bz = vb3[0] * vb2m[1] - vb3[1] * vb2m[0];
+    const double rasq = ax * ax + ay * ay + az * az;
+    const double rbsq = bx * bx + by * by + bz * bz;
+    const double rgsq = vb2m[0] * vb2m[0] + vb2m[1] * vb2m[1] + vb2m[2] * vb2m[2];
+    const double rg = std::sqrt(rgsq);
+    double rginv = 0.0, ra2inv = 0.0, rb2inv = 0.0;
+    if (rg > 0) rginv = 1.0 / rg;
+    if (rasq > 0) ra2inv = 1.0 / rasq;
+    if (rbsq > 0) rb2inv = 1.0 / rbsq;
+    const double rabinv = std::sqrt(ra2inv * rb2inv);
+    double c = (ax * bx + ay * by + az * bz) * rabinv;
+    const double s = rg * rabinv * (ax * vb3[0] + ay * vb3[1] + az * vb3[2]);
+    if (c > 1.0) c = 1.0;
+    if (c < -1.0) c = -1.0;
+    double pp = 1.0, ddf1 = 0.0, df1 = 0.0;
+    for (int q = 0; q < m; q++) {
+      ddf1 = pp * c - df1 * s;
+      df1 = pp * s + df1 * c;
+      pp = ddf1;
+    }
+    pp = pp * cos_shift + df1 * sin_shift;
+    df1 = df1 * cos_shift - ddf1 * sin_shift;
+    df1 *= -m;
+    pp += 1.0;
+    if (m == 0) {
+      pp = 1.0 + cos_shift;
+      df1 = 0.0;
+    }
+    e_dih += K * pp;
+    const double fg = vb1[0] * vb2m[0] + vb1[1] * vb2m[1] + vb1[2] * vb2m[2];
+    const double hg = vb3[0] * vb2m[0] + vb3[1] * vb2m[1] + vb3[2] * vb2m[2];
+    const double fga = fg * ra2inv * rginv;
+    const double hgb = hg * rb2inv * rginv;
+    const double gaa = -ra2inv * rg;
+    const double gbb = rb2inv * rg;
+    const double dtf[3] = {gaa * ax, gaa * ay, gaa * az};
+    const double dtg[3] = {fga * ax - hgb * bx, fga * ay - hgb * by, fga * az - hgb * bz};
+    const double dth[3] = {gbb * bx, gbb * by, gbb * bz};
+    const double df = -K * df1;
+    double f1[3], f2[3], f3[3], f4[3];
+    for (int k = 0; k < 3; ++k) {
+      const double s2 = df * dtg[k];
+      f1[k] = df * dtf[k];
+      f2[k] = s2 - f1[k];
+      f4[k] = df * dth[k];
+      f3[k] = -s2 - f4[k];
+      F[3 * i1 + k] += f1[k];
+      F[3 * i2 + k] += f2[k];
+      F[3 * i3 + k] += f3[k];
+      F[3 * i4 + k] += f4[k];
+    }
+    vir[0] += vb1[0] * f1[0] + vb2[0] * f3[0] + (vb3[0] + vb2[0]) * f4[0];
+    vir[1] += vb1[1] * f1[1] + vb2[1] * f3[1] + (vb3[1] + vb2[1]) * f4[1];
+    vir[2] += vb1[2] * f1[2] + vb2[2] * f3[2] + (vb3[2] + vb2[2]) * f4[2];
+    vir[3] += vb1[0] * f1[1] + vb2[0] * f3[1] + (vb3[0] + vb2[0]) * f4[1];
+    vir[4] += vb1[0] * f1[2] + vb2[0] * f3[2] + (vb3[0] + vb2[0]) * f4[2];
+    vir[5] += vb1[1] * f1[2] + vb2[1] * f3[2] + (vb3[1] + vb2[1]) * f4[2];
+  }
+  e_dihedral_avg = nd > 0 ? e_dih / nd : 0.0;
   for (int k = 0; k < 6; ++k) virial[k] += vir[k];
 }
 
@@ -1140,6 +1225,7 @@ void System::thermo(rbmd_thermo* out) {
   out->e_eam = e_eam;
   out->e_bond = e_bond_avg;
   out->e_angle = e_angle_avg;
+  out->e_dihedral = e_dihedral_avg;
   if (p.coulomb != RBMD_COUL_NONE && p.force_field != RBMD_FF_LJ_CUT && p.force_field != RBMD_FF_EAM) {
     double sq = 0;
     for (int i = 0; i < N; ++i) sq += q[i] * q[i];
@@ -1150,7 +1236,7 @@ void System::thermo(rbmd_thermo* out) {
   if (p.force_field == RBMD_FF_LJ_CUT) out->potential_energy = e_lj;
   else if (p.force_field == RBMD_FF_LJ_CUT_COUL_LONG) out->potential_energy = e_lj + out->e_coul_far + e_coul;
   else if (p.force_field == RBMD_FF_CVFF)
-    out->potential_energy = e_lj + out->e_coul_far + e_coul + e_bond_avg + e_angle_avg;
+    out->potential_energy = e_lj + out->e_coul_far + e_coul + e_bond_avg + e_angle_avg + e_dihedral_avg;
   else out->potential_energy = e_eam;
   out->total_energy = out->potential_energy + out->kinetic_energy;
   double vir[6], press;

@@ -5,7 +5,7 @@ a probe with the host compiler.
 """
 import ctypes as C
 
-RBMD_ABI_VERSION = 2
+RBMD_ABI_VERSION = 3
 
 # status
 OK, ERR_ARG, ERR_OOM, ERR_NUMERIC, ERR_TIMEOUT, ERR_CUDA, ERR_STATE, ERR_BUDGET, ERR_UNSUPPORTED, ERR_IO = range(10)
@@ -71,6 +71,9 @@ class SystemDesc(C.Structure):
         ("eam_drho", C.c_double), ("eam_dr", C.c_double), ("eam_rhomax", C.c_double),
         ("eam_cut", C.c_double),
         ("eam_frho_spline", dptr), ("eam_rhor_spline", dptr), ("eam_z2r_spline", dptr),
+        ("n_dihedrals", C.c_int32), ("n_dihedral_types", C.c_int32),
+        ("dihedral_atoms", iptr), ("dihedral_type", iptr), ("dihedral_k", dptr), ("dihedral_sign", iptr),
+        ("dihedral_multiplicity", iptr),
     ]
 
 
@@ -82,7 +85,7 @@ class Thermo(C.Structure):
         ("e_eam", C.c_double), ("potential_energy", C.c_double), ("total_energy", C.c_double),
         ("pressure", C.c_double), ("virial", C.c_double * 6), ("nhc_eta", C.c_double * 3),
         ("nhc_eta_dot", C.c_double * 4), ("volume", C.c_double), ("box_lo", C.c_double * 3),
-        ("box_hi", C.c_double * 3), ("status", C.c_int32), ("pad0", C.c_int32),
+        ("box_hi", C.c_double * 3), ("status", C.c_int32), ("pad0", C.c_int32), ("e_dihedral", C.c_double),
     ]
 
     def as_dict(self):

@@ -141,11 +141,18 @@ struct SysDev {
   int* angle_type;
   double* angle_k;
   double* angle_t0;
-  double4* term_force; // [2 n_bonds + 3 n_angles] per-term forces
+  int n_dihedrals;      // harmonic dihedrals (CVFF with special bonds and a Dihedrals section)
+  int dih_pad;
+  int* dih_atoms;       // [4 n_dihedrals]
+  int* dih_type;        // [n_dihedrals]
+  double* dih_k;        // per type: K
+  int* dih_sign;        // per type: d (1 or other: -1)
+  int* dih_mult;        // per type: n
+  double4* term_force; // [2 n_bonds + 3 n_angles + 4 n_dihedrals] per-term forces
   int* aterm_off;      // [n + 1] atom -> term-force slots (CSR)
   int* aterm;          // slots
-  double* term_energy; // [n_bonds + n_angles]
-  double* term_vir;    // [6 (n_bonds + n_angles)] per-term virials (pressure requests)
+  double* term_energy; // [n_bonds + n_angles + n_dihedrals]
+  double* term_vir;    // [6 (n_bonds + n_angles + n_dihedrals)] per-term virials (pressure requests)
   // k space
   int* km;             // [3P] sampled m vectors
   double4* kv;         // [P or nk] k vector + coefficient -4 pi / (V k^2) (Ewald: x exp(-k^2/4a))

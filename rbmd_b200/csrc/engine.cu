@@ -220,7 +220,8 @@ int64_t Context::estimate_bytes(const rbmd_system_desc& d, const rbmd_params& p)
                           : 0;
   const int64_t brho = (n + kRhoChunk - 1) / kRhoChunk;
   b += nk * 48 + nke * 48 + brho * 16 * std::max(nk, nke);
-  b += (int64_t)(d.n_bonds * 2 + d.n_angles * 3) * 48 + (d.n_bonds + d.n_angles) * 56;
+  b += (int64_t)(d.n_bonds * 2 + d.n_angles * 3 + d.n_dihedrals * 4) * 48 +
+       (int64_t)(d.n_bonds + d.n_angles + d.n_dihedrals) * 76;
   if (d.special_offsets) b += (int64_t)d.special_offsets[n] * 12 + 4 * (n + 1);
   if (p.force_field == RBMD_FF_EAM) b += (int64_t)(d.eam_nrho + 2 * d.eam_nr + 3) * 56;
   b += ((n + kPairWarps - 1) / kPairWarps) * 72 + ((n + kAtomBlock - 1) / kAtomBlock) * 64 + 4096;
@@ -274,6 +275,19 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   if (d.n_bonds > 0 && (!d.bond_atoms || !d.bond_type || !d.bond_k || !d.bond_r0))
     return fail(RBMD_ERR_ARG, "bond arrays missing");
   if (d.n_angles > 0 && !d.angle_atoms) return fail(RBMD_ERR_ARG, "angle atoms missing");
+  if (d.n_dihedrals < 0 || (d.n_dihedrals > 0 && (!d.dihedral_atoms || !d.dihedral_type || !d.dihedral_k ||
+                                                   !d.dihedral_sign || !d.dihedral_multiplicity)))
+    return fail(RBMD_ERR_ARG, "dihedral arrays missing");
+  for (int q = 0; q < d.n_dihedrals; ++q) {
+    if (d.dihedral_type[q] < 0 || d.dihedral_type[q] >= d.n_dihedral_types)
+      return fail(RBMD_ERR_ARG, "dihedral type out of range");
+    for (int t = 0; t < 4; ++t)
+      if (d.dihedral_atoms[4 * q + t] < 0 || d.dihedral_atoms[4 * q + t] >= d.n_atoms)
+        return fail(RBMD_ERR_ARG, "dihedral atom out of range");
+  }
+  for (int t = 0; t < d.n_dihedrals && t < 1; ++t)
+    for (int y = 0; y < d.n_dihedral_types; ++y)
+      if (d.dihedral_multiplicity[y] < 0) return fail(RBMD_ERR_ARG, "dihedral multiplicity must be >= 0");
   if (p.force_field == RBMD_FF_CVFF && d.n_angles > 0 && (!d.angle_type || !d.angle_k || !d.angle_theta0))
     return fail(RBMD_ERR_ARG, "angle coefficients missing");
 
@@ -506,7 +520,8 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
     for (int i = 0; i < n; ++i) mol_atoms[fill[hmeta[i].y]++] = i;
   }
   // bonded term slots per atom
-  const int nterms = D.n_bonds + D.n_angles;
+  D.n_dihedrals = (p.force_field == RBMD_FF_CVFF) ? d.n_dihedrals : 0;
+  const int nterms = D.n_bonds + D.n_angles + D.n_dihedrals;
   s->n_terms = nterms;
   std::vector<int> aterm_off(n + 1, 0), aterm;
   if (nterms > 0) {
@@ -517,6 +532,9 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
     }
     for (int a = 0; a < D.n_angles; ++a)
       for (int t = 0; t < 3; ++t) per[d.angle_atoms[3 * a + t]].push_back(2 * D.n_bonds + 3 * a + t);
+    for (int q = 0; q < D.n_dihedrals; ++q)
+      for (int t = 0; t < 4; ++t)
+        per[d.dihedral_atoms[4 * q + t]].push_back(2 * D.n_bonds + 3 * D.n_angles + 4 * q + t);
     for (int i = 0; i < n; ++i) {
       aterm_off[i + 1] = aterm_off[i] + (int)per[i].size();
       aterm.insert(aterm.end(), per[i].begin(), per[i].end());
@@ -591,7 +609,19 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
       up(D.bond_k, d.bond_k, sizeof(double) * d.n_bond_types);
       up(D.bond_r0, d.bond_r0, sizeof(double) * d.n_bond_types);
     }
-    D.term_force = (double4*)dal(sizeof(double4) * (2 * D.n_bonds + 3 * D.n_angles));
+    if (D.n_dihedrals > 0) {
+      D.dih_atoms = (int*)dal(sizeof(int) * 4 * D.n_dihedrals);
+      D.dih_type = (int*)dal(sizeof(int) * D.n_dihedrals);
+      D.dih_k = (double*)dal(sizeof(double) * d.n_dihedral_types);
+      D.dih_sign = (int*)dal(sizeof(int) * d.n_dihedral_types);
+      D.dih_mult = (int*)dal(sizeof(int) * d.n_dihedral_types);
+      up(D.dih_atoms, d.dihedral_atoms, sizeof(int) * 4 * D.n_dihedrals);
+      up(D.dih_type, d.dihedral_type, sizeof(int) * D.n_dihedrals);
+      up(D.dih_k, d.dihedral_k, sizeof(double) * d.n_dihedral_types);
+      up(D.dih_sign, d.dihedral_sign, sizeof(int) * d.n_dihedral_types);
+      up(D.dih_mult, d.dihedral_multiplicity, sizeof(int) * d.n_dihedral_types);
+    }
+    D.term_force = (double4*)dal(sizeof(double4) * (2 * D.n_bonds + 3 * D.n_angles + 4 * D.n_dihedrals));
     D.term_energy = (double*)dal(sizeof(double) * nterms);
     D.term_vir = (double*)dal(sizeof(double) * 6 * nterms);
     D.aterm_off = (int*)dal(sizeof(int) * (n + 1));
@@ -723,7 +753,8 @@ bool same_group(const System* a, const System* b, bool layout) {
   const SysDev &x = a->dev, &y = b->dev;
   return x.ff == y.ff && x.neigh == y.neigh && x.coul == y.coul && x.prec == y.prec &&
          x.temp_ctrl == y.temp_ctrl && x.special == y.special && x.has_triples == y.has_triples &&
-         ((x.n_bonds + x.n_angles) > 0) == ((y.n_bonds + y.n_angles) > 0) && x.npt == y.npt && x.rc2 == y.rc2 &&
+         ((x.n_bonds + x.n_angles + x.n_dihedrals) > 0) == ((y.n_bonds + y.n_angles + y.n_dihedrals) > 0) &&
+         x.npt == y.npt && x.rc2 == y.rc2 &&
          x.rs2 == y.rs2 &&
          (!layout || (x.dense == y.dense && x.lean == y.lean));
 }
@@ -741,7 +772,7 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
   b.temp_ctrl = g.temp_ctrl;
   b.special = g.special;
   b.has_shake = g.has_triples;
-  b.has_bonded = (g.n_bonds + g.n_angles) > 0;
+  b.has_bonded = (g.n_bonds + g.n_angles + g.n_dihedrals) > 0;
   b.dense = g.dense;
   b.lean = g.lean;
   b.npt = g.npt;
@@ -766,7 +797,7 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
     for (int k = 0; k < D.ncell_cap; k += kCellBlock) wc.push_back(make_int2(s->slot, k));
     for (int k = 0; k < D.n; k += kRhoChunk) wr.push_back(make_int2(s->slot, k));
     for (int k = 0; k < D.n_triples; k += 128) wt.push_back(make_int2(s->slot, k));
-    for (int k = 0; k < D.n_bonds + D.n_angles; k += 128) wm.push_back(make_int2(s->slot, k));
+    for (int k = 0; k < D.n_bonds + D.n_angles + D.n_dihedrals; k += 128) wm.push_back(make_int2(s->slot, k));
   }
   auto mk = [&](const std::vector<int2>& h, Work& w) {
     w.n = (int)h.size();
@@ -1131,6 +1162,9 @@ int Context::get_thermo(int id, rbmd_thermo* out) {
   double eb = 0, ea = 0;
   for (int t = 0; t < D.n_bonds; ++t) eb += te[t];
   for (int t = 0; t < D.n_angles; ++t) ea += te[D.n_bonds + t];
+  double ed = 0;
+  for (int t = 0; t < D.n_dihedrals; ++t) ed += te[D.n_bonds + D.n_angles + t];
+  out->e_dihedral = D.n_dihedrals ? ed / D.n_dihedrals : 0.0;
   out->e_bond = D.n_bonds ? eb / D.n_bonds : 0.0;
   out->e_angle = D.n_angles ? ea / D.n_angles : 0.0;
   if (D.ff == RBMD_FF_EAM) {
@@ -1144,7 +1178,8 @@ int Context::get_thermo(int id, rbmd_thermo* out) {
   if (D.ff == RBMD_FF_LJ_CUT) out->potential_energy = out->e_lj;
   else if (D.ff == RBMD_FF_LJ_CUT_COUL_LONG) out->potential_energy = out->e_lj + out->e_coul_far + out->e_coul_near;
   else if (D.ff == RBMD_FF_CVFF)
-    out->potential_energy = out->e_lj + out->e_coul_far + out->e_coul_near + out->e_bond + out->e_angle;
+    out->potential_energy =
+        out->e_lj + out->e_coul_far + out->e_coul_near + out->e_bond + out->e_angle + out->e_dihedral;
   else out->potential_energy = out->e_eam;
   out->total_energy = out->potential_energy + out->kinetic_energy;
   double vir[6];

@@ -127,7 +127,85 @@ __global__ void k_bonded(const SysDev* __restrict__ S, const int2* __restrict__ 
   const int2 wk = work[blockIdx.x];
   const SysDev& s = S[wk.x];
   const int t = wk.y + threadIdx.x;
-  if (t >= s.n_bonds + s.n_angles) return;
+  if (t >= s.n_bonds + s.n_angles + s.n_dihedrals) return;
+  if (t >= s.n_bonds + s.n_angles) {
+    // ComputeDihedralHarmonicWorklet, MolecularWorklet.h:669-973: E = K [1 + d cos(n phi)]
+    const int q = t - s.n_bonds - s.n_angles;
+    const int i1 = s.dih_atoms[4 * q], i2 = s.dih_atoms[4 * q + 1], i3 = s.dih_atoms[4 * q + 2],
+              i4 = s.dih_atoms[4 * q + 3];
+    const int ty = s.dih_type[q];
+    const double K = s.dih_k[ty];
+    const int m = s.dih_mult[ty];
+    const double cos_shift = s.dih_sign[ty] == 1 ? 1.0 : -1.0, sin_shift = 0.0;
+    const double4 p1 = s.x[i1], p2 = s.x[i2], p3 = s.x[i3], p4 = s.x[i4];
+    double vb1[3] = {p1.x - p2.x, p1.y - p2.y, p1.z - p2.z};
+    double vb2[3] = {p3.x - p2.x, p3.y - p2.y, p3.z - p2.z};
+    double vb3[3] = {p4.x - p3.x, p4.y - p3.y, p4.z - p3.z};
+    min_image(vb1[0], vb1[1], vb1[2], s.L[0], s.L[1], s.L[2]);
+    min_image(vb2[0], vb2[1], vb2[2], s.L[0], s.L[1], s.L[2]);
+    min_image(vb3[0], vb3[1], vb3[2], s.L[0], s.L[1], s.L[2]);
+    const double vb2m[3] = {-vb2[0], -vb2[1], -vb2[2]};
+    const double ax = vb1[1] * vb2m[2] - vb1[2] * vb2m[1];
+    const double ay = vb1[2] * vb2m[0] - vb1[0] * vb2m[2];
+    const double az = vb1[0] * vb2m[1] - vb1[1] * vb2m[0];
+    const double bx = vb3[1] * vb2m[2] - vb3[2] * vb2m[1];
+    const double by = vb3[2] * vb2m[0] - vb3[0] * vb2m[2];
+    const double bz = vb3[0] * vb2m[1] - vb3[1] * vb2m[0];
+    const double rasq = ax * ax + ay * ay + az * az;
+    const double rbsq = bx * bx + by * by + bz * bz;
+    const double rg = sqrt(vb2m[0] * vb2m[0] + vb2m[1] * vb2m[1] + vb2m[2] * vb2m[2]);
+    const double rginv = rg > 0 ? 1.0 / rg : 0.0, ra2inv = rasq > 0 ? 1.0 / rasq : 0.0;
+    const double rb2inv = rbsq > 0 ? 1.0 / rbsq : 0.0;
+    const double rabinv = sqrt(ra2inv * rb2inv);
+    double c = (ax * bx + ay * by + az * bz) * rabinv;
+    const double sn = rg * rabinv * (ax * vb3[0] + ay * vb3[1] + az * vb3[2]);
+    c = fmin(fmax(c, -1.0), 1.0);
+    double pp = 1.0, ddf1 = 0.0, df1 = 0.0;
+    for (int r = 0; r < m; r++) {  // cos(n phi), sin(n phi) by the angle-addition recurrence
+      ddf1 = pp * c - df1 * sn;
+      df1 = pp * sn + df1 * c;
+      pp = ddf1;
+    }
+    pp = pp * cos_shift + df1 * sin_shift;
+    df1 = df1 * cos_shift - ddf1 * sin_shift;
+    df1 *= -m;
+    pp += 1.0;
+    if (m == 0) {
+      pp = 1.0 + cos_shift;
+      df1 = 0.0;
+    }
+    s.term_energy[t] = K * pp;
+    const double fg = vb1[0] * vb2m[0] + vb1[1] * vb2m[1] + vb1[2] * vb2m[2];
+    const double hg = vb3[0] * vb2m[0] + vb3[1] * vb2m[1] + vb3[2] * vb2m[2];
+    const double fga = fg * ra2inv * rginv, hgb = hg * rb2inv * rginv;
+    const double gaa = -ra2inv * rg, gbb = rb2inv * rg;
+    const double df = -K * df1;
+    const double a3[3] = {ax, ay, az}, b3[3] = {bx, by, bz};
+    double f1[3], f3[3], f4[3], f2[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double s2 = df * (fga * a3[k] - hgb * b3[k]);
+      f1[k] = df * (gaa * a3[k]);
+      f2[k] = s2 - f1[k];
+      f4[k] = df * (gbb * b3[k]);
+      f3[k] = -s2 - f4[k];
+    }
+    const int base = 2 * s.n_bonds + 3 * s.n_angles + 4 * q;
+    s.term_force[base] = make_double4(f1[0], f1[1], f1[2], 0.0);
+    s.term_force[base + 1] = make_double4(f2[0], f2[1], f2[2], 0.0);
+    s.term_force[base + 2] = make_double4(f3[0], f3[1], f3[2], 0.0);
+    s.term_force[base + 3] = make_double4(f4[0], f4[1], f4[2], 0.0);
+    if (virial) {
+      double* v = s.term_vir + 6 * (size_t)t;
+      v[0] = vb1[0] * f1[0] + vb2[0] * f3[0] + (vb3[0] + vb2[0]) * f4[0];
+      v[1] = vb1[1] * f1[1] + vb2[1] * f3[1] + (vb3[1] + vb2[1]) * f4[1];
+      v[2] = vb1[2] * f1[2] + vb2[2] * f3[2] + (vb3[2] + vb2[2]) * f4[2];
+      v[3] = vb1[0] * f1[1] + vb2[0] * f3[1] + (vb3[0] + vb2[0]) * f4[1];
+      v[4] = vb1[0] * f1[2] + vb2[0] * f3[2] + (vb3[0] + vb2[0]) * f4[2];
+      v[5] = vb1[1] * f1[2] + vb2[1] * f3[2] + (vb3[1] + vb2[1]) * f4[2];
+    }
+    return;
+  }
   if (t < s.n_bonds) {
     // ComputeBondHarmonicWorklet, MolecularWorklet.h:58-199
     const int i = s.bond_atoms[2 * t], j = s.bond_atoms[2 * t + 1];
@@ -317,7 +395,7 @@ k_final(const SysDev* __restrict__ S, const int2* __restrict__ work, int mode) {
       }
     }
     // ---- bonded terms (per-term forces gathered per atom)
-    if (s.n_bonds + s.n_angles > 0) {
+    if (s.n_bonds + s.n_angles + s.n_dihedrals > 0) {
       for (int k = s.aterm_off[i]; k < s.aterm_off[i + 1]; ++k) {
         const double4 tf = s.term_force[s.aterm[k]];
         F[0] += tf.x;
@@ -376,7 +454,7 @@ k_final(const SysDev* __restrict__ S, const int2* __restrict__ work, int mode) {
       if (VIRIAL) {
         double tv[6] = {0, 0, 0, 0, 0, 0};
         if (s.term_vir)
-          for (int t = 0; t < s.n_bonds + s.n_angles; ++t)
+          for (int t = 0; t < s.n_bonds + s.n_angles + s.n_dihedrals; ++t)
             for (int k = 0; k < 6; ++k) tv[k] += s.term_vir[6 * (size_t)t + k];
         for (int k = 0; k < 6; ++k) st->virial[k] = st->virial[k] + s_tot[1 + k] + tv[k];
       }

@@ -88,7 +88,7 @@ int Context::autotune(const int32_t* ids, int n, rbmd_tune_result* out, int cap,
                 use.end());
     }
     const SysDev& D0 = g[0]->dev;
-    const std::vector<int64_t> sig = {D0.ff, D0.neigh, D0.coul, D0.prec, D0.special, (D0.n_bonds + D0.n_angles) > 0,
+    const std::vector<int64_t> sig = {D0.ff, D0.neigh, D0.coul, D0.prec, D0.special, (D0.n_bonds + D0.n_angles + D0.n_dihedrals) > 0,
                                       D0.has_triples, D0.npt, log2_bin((double)r.atoms / cells), log2_bin((double)r.atoms)};
     int best = use.size() == 1 ? use[0] : -1;
     auto hit = tune_cache_.find(sig);

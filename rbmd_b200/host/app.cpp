@@ -90,6 +90,15 @@ rbmd_system_desc Para::desc() const {
   d.eam_frho_spline = frho_spline.empty() ? nullptr : frho_spline.data();
   d.eam_rhor_spline = rhor_spline.empty() ? nullptr : rhor_spline.data();
   d.eam_z2r_spline = z2r_spline.empty() ? nullptr : z2r_spline.data();
+  if (!dihedral_type.empty()) {
+    d.n_dihedrals = (int32_t)dihedral_type.size();
+    d.n_dihedral_types = (int32_t)dihedral_k.size();
+    d.dihedral_atoms = dihedral_atoms.data();
+    d.dihedral_type = dihedral_type.data();
+    d.dihedral_k = dihedral_k.data();
+    d.dihedral_sign = dihedral_sign.data();
+    d.dihedral_multiplicity = dihedral_multiplicity.data();
+  }
   return d;
 }
 
@@ -127,6 +136,12 @@ void ModelFileInitCondition::Execute(Para& p) {
   p.angle_type = d.angle_type;
   p.angle_k = d.angle_k;
   p.angle_theta0 = d.angle_theta0;
+  p.file_dihedrals = d.has_dihedrals;
+  p.dihedral_atoms = d.dihedral_atoms;
+  p.dihedral_type = d.dihedral_type;
+  p.dihedral_k = d.dihedral_k;
+  p.dihedral_sign = d.dihedral_sign;
+  p.dihedral_multiplicity = d.dihedral_multiplicity;
   if (!d.velocity.empty()) {
     p.velocity = d.velocity;
   } else if (_velocity_type == "GAUSS") {
@@ -244,13 +259,13 @@ void ThermoOutput::Execute(Executioner& ex) {
   const int64_t step = ex.CurrentStep();
   if (step == 0)
     std::fprintf(_file, "Step Time VanderWaalsEnergy NearCoulombicEnergy FarCoulombicEnergy KinticEnergy "
-                        "PotentialEnergy TotalEnergy BondEnergy AngleEnergy Temperature Pressure\n");
+                        "PotentialEnergy TotalEnergy BondEnergy AngleEnergy DihedralEnergy Temperature Pressure\n");
   if (step % _interval != 0 && step != ex.NumStep()) return;
   const rbmd_thermo t = ex.Run().Thermo();
   const double vdw = t.e_lj + t.e_eam;
-  std::fprintf(_file, "%lld %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g\n", (long long)step,
-               ex.CurrentTime(), vdw, t.e_coul_near, t.e_coul_far, t.kinetic_energy, t.potential_energy,
-               t.total_energy, t.e_bond, t.e_angle, t.temperature, t.pressure);
+  std::fprintf(_file, "%lld %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g\n",
+               (long long)step, ex.CurrentTime(), vdw, t.e_coul_near, t.e_coul_far, t.kinetic_energy,
+               t.potential_energy, t.total_energy, t.e_bond, t.e_angle, t.e_dihedral, t.temperature, t.pressure);
   std::fflush(_file);
   if (_console)
     std::printf("step %lld  T %.6g  E_pot %.10g  E_tot %.10g  P %.6g%s\n", (long long)step, t.temperature,
@@ -366,6 +381,7 @@ void MDApplication::ReadHyperParameters(const Json& hp) {
     else if (_ff_type == "EAM") P.force_field = RBMD_FF_EAM;
     else throw std::runtime_error("force_field type \"" + _ff_type + "\" is not supported");
     _potential_file = ff->string("potential_file", "");
+    _dihedral_type = ff->string("dihedral_type", "");  // ForceField.cpp:49
   }
   if (const Json* nb = hp.find("neighbor")) {
     const std::string t = nb->string("type", "RBL");
@@ -474,6 +490,20 @@ void MDApplication::CreateActions() {
     for (int i = 0; i < _para.n; ++i) _para.charge[i] = (i < _para.n / 2) ? -1.0 : 1.0;
   }
   if (_special_bonds) special_lists(_para.n, _para.bond_atoms, _special_w, _para.sp_off, _para.sp_ids, _para.sp_w);
+  // dihedral forces: CVFF with special_bonds (PARA_DIHEDRALS_FORCE) and a Dihedrals section
+  // (PARA_FILE_DIHEDRALS), style "Harmonic" (ExecutionNVT.cpp:223-228, 585-588); the reference has
+  // no other style (its DihedralsForce returns nothing otherwise)
+  const bool dihedrals = _para.params.force_field == RBMD_FF_CVFF && _special_bonds && _para.file_dihedrals;
+  if (dihedrals && _dihedral_type != "Harmonic")
+    throw std::runtime_error("the data file has Dihedrals: force_field.dihedral_type must be \"Harmonic\" (got \"" +
+                             _dihedral_type + "\")");
+  if (!dihedrals) {
+    _para.dihedral_atoms.clear();
+    _para.dihedral_type.clear();
+    _para.dihedral_k.clear();
+    _para.dihedral_sign.clear();
+    _para.dihedral_multiplicity.clear();
+  }
   if (_para.params.force_field == RBMD_FF_EAM) {
     if (_potential_file.empty()) throw std::runtime_error("EAM needs force_field.potential_file");
     std::string path = _potential_file;
@@ -551,6 +581,11 @@ void MDApplication::DumpSystem(const std::string& path) const {
   iarr("angle_type", _para.angle_type);
   darr("angle_k", _para.angle_k);
   darr("angle_theta0", _para.angle_theta0);
+  iarr("dihedral_atoms", _para.dihedral_atoms);
+  iarr("dihedral_type", _para.dihedral_type);
+  darr("dihedral_k", _para.dihedral_k);
+  iarr("dihedral_sign", _para.dihedral_sign);
+  iarr("dihedral_multiplicity", _para.dihedral_multiplicity);
   iarr("special_offsets", _para.sp_off);
   iarr("special_ids", _para.sp_ids);
   darr("special_weights", _para.sp_w);

@@ -38,6 +38,11 @@ struct Para {
   std::vector<double> bond_k, bond_r0, angle_k, angle_theta0;
   std::vector<int> sp_off, sp_ids;
   std::vector<double> sp_w;
+  // harmonic dihedrals (evaluated when special_bonds, a Dihedrals section and dihedral_type
+  // "Harmonic" are all given)
+  std::vector<int> dihedral_atoms, dihedral_type, dihedral_sign, dihedral_multiplicity;
+  std::vector<double> dihedral_k;
+  bool file_dihedrals = false;
   // EAM
   int eam_nrho = 0, eam_nr = 0;
   double eam_drho = 0, eam_dr = 0, eam_rhomax = 0, eam_cut = 0;
@@ -198,7 +203,7 @@ class MDApplication : public Application {
   int _thermo_interval = 0, _traj_interval = 0;
   bool _special_bonds = false;
   double _special_w[3] = {0, 0, 0};
-  std::string _ff_type, _potential_file, _base_dir;
+  std::string _ff_type, _potential_file, _base_dir, _dihedral_type;
 };
 
 }  // namespace rbmd_host

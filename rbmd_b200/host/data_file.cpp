@@ -63,6 +63,10 @@ DataFile read_data_file(const std::string& path, const std::string& atom_style, 
       iss >> d.n_bond_types;
     } else if (line.find("angle types") != std::string::npos) {
       iss >> d.n_angle_types;
+    } else if (line.find("dihedral types") != std::string::npos) {
+      iss >> d.n_dihedral_types;
+    } else if (line.find("dihedrals") != std::string::npos) {
+      iss >> d.n_dihedrals;
     } else if (line.find("atoms") != std::string::npos) {
       iss >> d.n_atoms;
     } else if (line.find("bonds") != std::string::npos) {
@@ -134,6 +138,21 @@ DataFile read_data_file(const std::string& path, const std::string& atom_style, 
         d.angle_theta0[a] = t0;
         return true;
       });
+    } else if (line.find("Dihedral Coeffs") != std::string::npos) {
+      d.dihedral_k.assign(d.n_dihedral_types, 0.0);
+      d.dihedral_sign.assign(d.n_dihedral_types, 1);
+      d.dihedral_multiplicity.assign(d.n_dihedral_types, 0);
+      section(f, d.n_dihedral_types, path, "Dihedral Coeffs", [&](std::istringstream& s) {
+        long t;
+        double k;
+        int sign, mult;
+        if (!(s >> t >> k >> sign >> mult)) return false;
+        const int a = checked_id(t, d.n_dihedral_types, path, "dihedral type");
+        d.dihedral_k[a] = k;
+        d.dihedral_sign[a] = sign;
+        d.dihedral_multiplicity[a] = mult;
+        return true;
+      });
     } else if (line.find("Atoms") != std::string::npos) {
       section(f, n, path, "Atoms", [&](std::istringstream& s) {
         long id, mol = 0, t;
@@ -180,6 +199,17 @@ DataFile read_data_file(const std::string& path, const std::string& atom_style, 
         d.bond_type.push_back(checked_id(t, d.n_bond_types, path, "bond type"));
         d.bond_atoms.push_back(checked_id(a, n, path, "atom"));
         d.bond_atoms.push_back(checked_id(b, n, path, "atom"));
+        return true;
+      });
+    } else if (line.find("Dihedrals") != std::string::npos) {
+      d.dihedral_atoms.clear();
+      d.dihedral_type.clear();
+      d.has_dihedrals = true;
+      section(f, d.n_dihedrals, path, "Dihedrals", [&](std::istringstream& s) {
+        long id, t, a, b, c, e;
+        if (!(s >> id >> t >> a >> b >> c >> e)) return false;
+        d.dihedral_type.push_back(checked_id(t, d.n_dihedral_types, path, "dihedral type"));
+        for (long x : {a, b, c, e}) d.dihedral_atoms.push_back(checked_id(x, n, path, "atom"));
         return true;
       });
     } else if (line.find("Angles") != std::string::npos) {

@@ -10,7 +10,7 @@ namespace rbmd_host {
 // indexed by atom id - 1 and type id - 1.
 struct DataFile {
   int n_atoms = 0, n_types = 0;
-  int n_bonds = 0, n_bond_types = 0, n_angles = 0, n_angle_types = 0;
+  int n_bonds = 0, n_bond_types = 0, n_angles = 0, n_angle_types = 0, n_dihedrals = 0, n_dihedral_types = 0;
   double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
   std::vector<double> type_mass;             // Masses (LJ units: all 1, Masses():296-299)
   std::vector<double> type_eps, type_sigma;  // Pair Coeffs: id eps sigma
@@ -23,6 +23,11 @@ struct DataFile {
   std::vector<int> molecule;                 // [n] 0-based (full); atom i is molecule i otherwise
   std::vector<int> bond_atoms, bond_type;    // [2 nb], [nb] 0-based
   std::vector<int> angle_atoms, angle_type;  // [3 na], [na] 0-based
+  // Dihedral Coeffs: id K d n (DihedralsCoeffs(), :359-376); Dihedrals: id type i j k l (:551-585)
+  std::vector<double> dihedral_k;
+  std::vector<int> dihedral_sign, dihedral_multiplicity;
+  std::vector<int> dihedral_atoms, dihedral_type;  // [4 nd], [nd] 0-based
+  bool has_dihedrals = false;                      // a Dihedrals section was read (PARA_FILE_DIHEDRALS)
 };
 
 // Reads `path` with atom_style "atomic", "charge" or "full" (Atoms(), :406-479); the unit decides

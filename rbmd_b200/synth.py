@@ -51,6 +51,8 @@ class SystemData:
         self.bond_atoms = self.bond_type = self.bond_k = self.bond_r0 = None
         self.angle_atoms = self.angle_type = self.angle_k = self.angle_theta0 = None
         self.special_offsets = self.special_ids = self.special_weights = None
+        self.dihedral_atoms = self.dihedral_type = self.dihedral_k = None
+        self.dihedral_sign = self.dihedral_multiplicity = None
         self.eam = None
         self.params = params if params is not None else A.default_params()
         self._desc = None
@@ -119,6 +121,14 @@ class SystemData:
             d.eam_frho_spline = dp(e["frho_spline"])
             d.eam_rhor_spline = dp(e["rhor_spline"])
             d.eam_z2r_spline = dp(e["z2r_spline"])
+        if self.dihedral_atoms is not None:
+            d.n_dihedrals = len(self.dihedral_type)
+            d.n_dihedral_types = len(self.dihedral_k)
+            d.dihedral_atoms = ip(self.dihedral_atoms)
+            d.dihedral_type = ip(self.dihedral_type)
+            d.dihedral_k = dp(self.dihedral_k)
+            d.dihedral_sign = ip(self.dihedral_sign)
+            d.dihedral_multiplicity = ip(self.dihedral_multiplicity)
         self._desc = d
         return d
 
@@ -334,6 +344,63 @@ def spce_water(n_mol=3000, density=1.0, T=300.0, seed=1, P=100, beta=0.3, **kw):
     return sd
 
 
+# united-atom CH2 chains (TraPPE-like LJ, CVFF harmonic bonds and angles, harmonic dihedrals
+# K [1 + d cos(n phi)] with n = 3) for the bonded terms that water lacks
+CH2 = dict(mass=14.027, sigma=3.95, eps=0.0914, r0=1.54, k_bond=260.0, theta=114.0, k_angle=62.1,
+           k_dih=1.4, sign=1, mult=3, q=0.1)
+
+
+def alkane_chains(n_side=5, length=6, spacing=11.0, T=300.0, seed=1, P=100, beta=0.3, jiggle=0.03, **kw):
+    """n_side^3 all-trans CH2 chains of `length` sites at randomly rotated simple-cubic sites
+    `spacing` A apart, positions jiggled by `jiggle` A so that the dihedrals carry forces, charges
+    +-q alternating along each chain; bonds, angles, dihedrals and 1-2/1-3/1-4 special lists
+    (weights 0, 0, 0: the reference reads special_bonds as integers) from the chain graph."""
+    rng = np.random.default_rng(seed)
+    half = np.deg2rad(CH2["theta"]) / 2
+    step_x, step_y = CH2["r0"] * np.sin(half), CH2["r0"] * np.cos(half)
+    base = np.array([[k * step_x, (k % 2) * step_y, 0.0] for k in range(length)])
+    base -= base.mean(0)
+    rot = _rotations(rng, n_side ** 3)
+    g = np.arange(n_side)
+    sites = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3) * spacing + spacing / 2
+    pos = (sites[:, None, :] + np.einsum("mij,kj->mki", rot, base)).reshape(-1, 3)
+    pos += rng.normal(scale=jiggle, size=pos.shape)
+    L = n_side * spacing
+    pos %= L
+    nmol = n_side ** 3
+    n = nmol * length
+    mass = np.full(n, CH2["mass"])
+    charge = np.tile(np.where(np.arange(length) % 2 == 0, CH2["q"], -CH2["q"]), nmol)
+    mol = np.repeat(np.arange(nmol), length).astype(np.int32)
+    vel = maxwell(mass, T, KB_REAL, MVV2E_REAL, rng)
+    params = A.default_params(force_field=A.FF_CVFF, neighbor=A.NEIGH_RBL, cut_off=10.0, r_core=5.0,
+                              neighbor_sample_num=100, coulomb=A.COUL_RBE, coulomb_sample_num=P,
+                              alpha=beta * beta, kmax=(3, 3, 3), units=A.UNITS_REAL, timestep=1.0,
+                              temp_ctrl=A.TC_NOSE_HOOVER, temperature=(T, T, 100.0), num_steps=1000, seed=seed,
+                              special_bonds=(0.0, 0.0, 0.0))
+    for k, v in kw.items():
+        _set(params, k, v)
+    sd = SystemData(pos, mass, np.zeros(n, np.int32), [CH2["eps"]], [CH2["sigma"]], [0, 0, 0], [L, L, L], vel=vel,
+                    charge=charge, molecule=mol, params=params, name=f"alkane_{n}")
+    first = (np.arange(nmol) * length)[:, None, None]
+    sd.bond_atoms = (first + np.stack([np.arange(length - 1), np.arange(1, length)], -1)[None]).reshape(-1).astype(np.int32)
+    sd.bond_type = np.zeros(nmol * (length - 1), np.int32)
+    sd.bond_k, sd.bond_r0 = np.array([CH2["k_bond"]]), np.array([CH2["r0"]])
+    tri = np.stack([np.arange(length - 2), np.arange(1, length - 1), np.arange(2, length)], -1)
+    sd.angle_atoms = (first + tri[None]).reshape(-1).astype(np.int32)
+    sd.angle_type = np.zeros(nmol * (length - 2), np.int32)
+    sd.angle_k, sd.angle_theta0 = np.array([CH2["k_angle"]]), np.array([CH2["theta"]])
+    quad = np.stack([np.arange(length - 3), np.arange(1, length - 2), np.arange(2, length - 1), np.arange(3, length)], -1)
+    sd.dihedral_atoms = (first + quad[None]).reshape(-1).astype(np.int32)
+    sd.dihedral_type = np.zeros(nmol * (length - 3), np.int32)
+    sd.dihedral_k = np.array([CH2["k_dih"]])
+    sd.dihedral_sign = np.array([CH2["sign"]], np.int32)
+    sd.dihedral_multiplicity = np.array([CH2["mult"]], np.int32)
+    sp = tuple(params.special_bonds)
+    sd.special_offsets, sd.special_ids, sd.special_weights = special_lists(n, sd.bond_atoms.reshape(-1, 2), sp)
+    return sd
+
+
 def saline(n_atoms_target, T=300.0, seed=1, P=100, beta=0.3, molar=0.15, precision=A.PREC_MIXED, **kw):
     """SPC/E water with `molar` NaCl at random lattice sites, close to n_atoms_target atoms."""
     waters_per_pair = 55.5 / molar
@@ -480,6 +547,7 @@ def write_rbmd_input(sd, directory, atom_style=None, thermo_interval=1, name="rb
     mol = sd.molecule if sd.molecule is not None else np.arange(n)
     nb = 0 if sd.bond_atoms is None else len(sd.bond_type)
     na = 0 if sd.angle_atoms is None or sd.angle_type is None else len(sd.angle_type)
+    nd = 0 if sd.dihedral_atoms is None else len(sd.dihedral_type)
     with open(data, "w") as f:
         f.write(f"LAMMPS data file written by rbmd_b200.synth ({sd.name})\n\n")
         f.write(f"{n} atoms\n{nt} atom types\n")
@@ -487,6 +555,8 @@ def write_rbmd_input(sd, directory, atom_style=None, thermo_interval=1, name="rb
             f.write(f"{nb} bonds\n{len(sd.bond_k)} bond types\n")
         if na:
             f.write(f"{na} angles\n{len(sd.angle_k)} angle types\n")
+        if nd:
+            f.write(f"{nd} dihedrals\n{len(sd.dihedral_k)} dihedral types\n")
         f.write("\n")
         for k, ax in enumerate("xyz"):
             f.write(f"{float(sd.box_lo[k])!r} {float(sd.box_hi[k])!r} {ax}lo {ax}hi\n")
@@ -504,6 +574,11 @@ def write_rbmd_input(sd, directory, atom_style=None, thermo_interval=1, name="rb
             f.write("\nAngle Coeffs # harmonic\n\n")
             for t in range(len(sd.angle_k)):
                 f.write(f"{t + 1} {float(sd.angle_k[t])!r} {float(sd.angle_theta0[t])!r}\n")
+        if nd:
+            f.write("\nDihedral Coeffs # harmonic\n\n")
+            for t in range(len(sd.dihedral_k)):
+                f.write(f"{t + 1} {float(sd.dihedral_k[t])!r} {int(sd.dihedral_sign[t])} "
+                        f"{int(sd.dihedral_multiplicity[t])}\n")
         f.write(f"\nAtoms # {atom_style}\n\n")
         for i in range(n):
             x, y, z = (repr(float(c)) for c in sd.pos[i])
@@ -527,11 +602,18 @@ def write_rbmd_input(sd, directory, atom_style=None, thermo_interval=1, name="rb
             for a in range(na):
                 i3 = sd.angle_atoms[3 * a:3 * a + 3] + 1
                 f.write(f"{a + 1} {int(sd.angle_type[a]) + 1} {i3[0]} {i3[1]} {i3[2]}\n")
+        if nd:
+            f.write("\nDihedrals\n\n")
+            for q in range(nd):
+                i4 = sd.dihedral_atoms[4 * q:4 * q + 4] + 1
+                f.write(f"{q + 1} {int(sd.dihedral_type[q]) + 1} {i4[0]} {i4[1]} {i4[2]} {i4[3]}\n")
     ff = {v: k for k, v in A.FORCE_FIELDS.items()}[p.force_field]
     hp = {"force_field": {"type": ff} if potential_file is None else {"type": ff, "potential_file": potential_file},
           "neighbor": {"type": "RBL" if p.neighbor == A.NEIGH_RBL else "VERLETLIST", "cut_off": p.cut_off,
                        "r_core": p.r_core, "neighbor_sample_num": p.neighbor_sample_num},
           "extend": {}}
+    if nd:
+        hp["force_field"]["dihedral_type"] = "Harmonic"
     if p.coulomb != A.COUL_NONE:
         hp["coulomb"] = {"type": "RBE" if p.coulomb == A.COUL_RBE else "EWALD",
                          "coulomb_sample_num": p.coulomb_sample_num, "alpha": p.alpha,

@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 RBMD = os.path.join(ROOT, "rbmd_b200", "_lib", "rbmd")
 COLS = ["Step", "Time", "VanderWaalsEnergy", "NearCoulombicEnergy", "FarCoulombicEnergy", "KinticEnergy",
-        "PotentialEnergy", "TotalEnergy", "BondEnergy", "AngleEnergy", "Temperature", "Pressure"]
+        "PotentialEnergy", "TotalEnergy", "BondEnergy", "AngleEnergy", "DihedralEnergy", "Temperature", "Pressure"]
 
 
 def _run_host(json_path, cwd):

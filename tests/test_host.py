@@ -187,3 +187,25 @@ def test_truncated_data_file(rbmd_bin, tmp_path):
     r = subprocess.run([rbmd_bin, "-j", path, "--dump-system", str(tmp_path / "d.json")], capture_output=True,
                        text=True)
     assert r.returncode == 1 and "Atoms" in r.stderr
+
+
+def test_dihedrals_read_when_the_reference_uses_them(rbmd_bin, tmp_path):
+    """Dihedral Coeffs / Dihedrals sections (ModelFileInitCondition.cpp:359-376, 551-585) reach the
+    library only with special_bonds and dihedral_type "Harmonic" (ExecutionNVT.cpp:223-228)."""
+    sd = synth.alkane_chains(n_side=2, length=6)
+    path = synth.write_rbmd_input(sd, str(tmp_path), atom_style="full")
+    j = dump(rbmd_bin, path, tmp_path)
+    assert np.array_equal(j["dihedral_atoms"], sd.dihedral_atoms)
+    assert np.array_equal(j["dihedral_type"], sd.dihedral_type)
+    assert j["dihedral_k"] == list(sd.dihedral_k) and j["dihedral_multiplicity"] == list(sd.dihedral_multiplicity)
+    assert j["dihedral_sign"] == list(sd.dihedral_sign)
+    cfg = json.load(open(path))
+    del cfg["hyper_parameters"]["extend"]["special_bonds"]  # no special bonds: no dihedral forces
+    json.dump(cfg, open(path, "w"))
+    assert dump(rbmd_bin, path, tmp_path)["dihedral_atoms"] == []
+    cfg["hyper_parameters"]["extend"]["special_bonds"] = [0, 0, 0]
+    cfg["hyper_parameters"]["force_field"]["dihedral_type"] = "Charmm"
+    json.dump(cfg, open(path, "w"))
+    r = subprocess.run([rbmd_bin, "-j", path, "--dump-system", str(tmp_path / "d.json")], capture_output=True,
+                       text=True)
+    assert r.returncode == 1 and "Harmonic" in r.stderr

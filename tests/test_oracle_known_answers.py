@@ -335,3 +335,52 @@ def test_mtk_volume_follows_the_pressure(oracle_mod):
         o.step(20)
         t = o.thermo()
         assert (t["volume"] > v0) == grows and t["status"] == 0
+
+
+def _one_dihedral(pos, K=1.7, sign=1, mult=3):
+    """Four CVFF atoms with every term but one harmonic dihedral switched off."""
+    sd = synth.alkane_chains(n_side=1, length=4, jiggle=0.0, coulomb=A.COUL_EWALD, neighbor=A.NEIGH_VERLET,
+                             cut_off=8.0, r_core=8.0, kmax=(2, 2, 2))
+    sd.box_hi = np.array([30.0, 30.0, 30.0])
+    sd.pos = np.ascontiguousarray(pos, np.float64)
+    sd.charge = np.zeros(4)
+    sd.eps = np.array([0.0])
+    sd.bond_k = np.array([0.0])
+    sd.angle_k = np.array([0.0])
+    sd.dihedral_k = np.array([K])
+    sd.dihedral_sign = np.array([sign], np.int32)
+    sd.dihedral_multiplicity = np.array([mult], np.int32)
+    return sd
+
+
+@pytest.mark.parametrize("sign,mult", [(1, 3), (-1, 1), (1, 2), (-1, 0)])
+def test_harmonic_dihedral_closed_form(oracle_mod, sign, mult):
+    """E = K [1 + d cos(n phi)] with phi the IUPAC torsion, and F = -dE/dx by central differences
+    (ComputeDihedralHarmonicWorklet, MolecularWorklet.h:669-973)."""
+    rng = np.random.default_rng(3 + mult)
+    pos = np.array([[10.0, 10.0, 10.0], [11.5, 10.2, 10.1], [12.1, 11.6, 10.0], [13.4, 11.9, 11.1]])
+    pos += rng.normal(scale=0.2, size=pos.shape)
+    K = 1.7
+    sd = _one_dihedral(pos, K, sign, mult)
+    o = oracle_mod.Oracle(sd)
+    o.compute_forces()
+    b1, b2, b3 = pos[1] - pos[0], pos[2] - pos[1], pos[3] - pos[2]
+    n1, n2 = np.cross(b1, b2), np.cross(b2, b3)
+    phi = np.arctan2(np.dot(np.cross(n1, n2), b2 / np.linalg.norm(b2)), np.dot(n1, n2))
+    e = o.thermo()["e_dihedral"]
+    expect = K * (1 + (1.0 if sign == 1 else -1.0) * np.cos(mult * phi)) if mult > 0 else K * (1 + (1.0 if sign == 1 else -1.0))
+    assert e == pytest.approx(expect, rel=1e-12, abs=1e-12)
+    f = o.forces()
+    h = 1e-6
+    for a in range(4):
+        for k in range(3):
+            ep, em = pos.copy(), pos.copy()
+            ep[a, k] += h
+            em[a, k] -= h
+            energies = []
+            for q in (ep, em):
+                oq = oracle_mod.Oracle(_one_dihedral(q, K, sign, mult))
+                oq.compute_forces()
+                energies.append(oq.thermo()["e_dihedral"])
+            assert f[a, k] == pytest.approx(-(energies[0] - energies[1]) / (2 * h), rel=1e-5, abs=1e-7)
+    assert np.abs(f.sum(0)).max() < 1e-12  # no net force
