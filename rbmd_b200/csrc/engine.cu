@@ -118,21 +118,52 @@ T thr_above(T c, T e) {
 Context::Context(const rbmd_device_cfg& c) : cfg(c) {
   cudaSetDevice(cfg.device);
   cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+  cudaMemPoolProps props;
+  std::memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = cfg.device;
+  if (cudaMemPoolCreate(&pool_, &props) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;  // never hand freed memory back at synchronisation points
+    cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep);
+  } else {
+    pool_ = nullptr;
+    cudaGetLastError();
+  }
+}
+
+void* Context::dmalloc(size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  void* p = nullptr;
+  const cudaError_t e = pool_ ? cudaMallocFromPoolAsync(&p, bytes, pool_, stream) : cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void Context::dfree(void* p) {
+  if (!p) return;
+  if (pool_) cudaFreeAsync(p, stream);
+  else cudaFree(p);
 }
 
 Context::~Context() {
   cudaStreamSynchronize(stream);
   for (auto& kv : batch_cache_) {
     if (kv.second->graph) cudaGraphExecDestroy(kv.second->graph);
-    for (void* p : kv.second->allocs) cudaFree(p);
+    for (void* p : kv.second->allocs) dfree(p);
     delete kv.second;
   }
   for (System* s : systems_) {
     if (!s) continue;
-    for (void* p : s->allocs) cudaFree(p);
+    for (void* p : s->allocs) dfree(p);
     delete s;
   }
   if (d_sys_) cudaFree(d_sys_);
+  cudaStreamSynchronize(stream);
+  if (pool_) cudaMemPoolDestroy(pool_);
   for (auto& r : prof.recs)
     for (auto& e : r.second.ev) {
       cudaEventDestroy(e.first);
@@ -525,20 +556,20 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   s->n_terms = nterms;
   std::vector<int> aterm_off(n + 1, 0), aterm;
   if (nterms > 0) {
-    std::vector<std::vector<int>> per(n);
-    for (int b = 0; b < D.n_bonds; ++b) {
-      per[d.bond_atoms[2 * b]].push_back(2 * b);
-      per[d.bond_atoms[2 * b + 1]].push_back(2 * b + 1);
-    }
-    for (int a = 0; a < D.n_angles; ++a)
-      for (int t = 0; t < 3; ++t) per[d.angle_atoms[3 * a + t]].push_back(2 * D.n_bonds + 3 * a + t);
-    for (int q = 0; q < D.n_dihedrals; ++q)
-      for (int t = 0; t < 4; ++t)
-        per[d.dihedral_atoms[4 * q + t]].push_back(2 * D.n_bonds + 3 * D.n_angles + 4 * q + t);
-    for (int i = 0; i < n; ++i) {
-      aterm_off[i + 1] = aterm_off[i] + (int)per[i].size();
-      aterm.insert(aterm.end(), per[i].begin(), per[i].end());
-    }
+    // slot s of the per-term forces belongs to atom owner(s); a counting sort over the slots in
+    // increasing order gives every atom its slots in that order
+    const int nslots = 2 * D.n_bonds + 3 * D.n_angles + 4 * D.n_dihedrals;
+    auto owner = [&](int sl) {
+      if (sl < 2 * D.n_bonds) return d.bond_atoms[sl];
+      sl -= 2 * D.n_bonds;
+      if (sl < 3 * D.n_angles) return d.angle_atoms[sl];
+      return d.dihedral_atoms[sl - 3 * D.n_angles];
+    };
+    for (int sl = 0; sl < nslots; ++sl) aterm_off[owner(sl) + 1]++;
+    for (int i = 0; i < n; ++i) aterm_off[i + 1] += aterm_off[i];
+    aterm.assign(nslots, 0);
+    std::vector<int> fill(aterm_off.begin(), aterm_off.end() - 1);
+    for (int sl = 0; sl < nslots; ++sl) aterm[fill[owner(sl)]++] = sl;
   }
   // self energy per atom (ExecutionMD::ComputeSelfEnergy, ExecutionMD.cpp:544-558)
   if (D.coul != RBMD_COUL_NONE) {
@@ -552,10 +583,9 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   bool oom = false;
   auto dal = [&](size_t bytes) -> void* {
     if (bytes == 0) bytes = 16;
-    void* ptr = nullptr;
-    if (cudaMalloc(&ptr, bytes) != cudaSuccess) {
+    void* ptr = dmalloc(bytes);
+    if (!ptr) {
       oom = true;
-      cudaGetLastError();
       return nullptr;
     }
     s->allocs.push_back(ptr);
@@ -677,7 +707,7 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   D.tri_part = (double*)dal(sizeof(double) * 6 * std::max(1, D.blocks_tri));
   D.st = (SysState*)dal(sizeof(SysState));
   if (oom) {
-    for (void* ptr : s->allocs) cudaFree(ptr);
+    for (void* ptr : s->allocs) dfree(ptr);
     return fail(RBMD_ERR_OOM, "device allocation failed for a system of " + std::to_string(n) + " atoms");
   }
   up(D.x, hx.data(), sizeof(double4) * n);
@@ -726,7 +756,7 @@ void Context::drop_batches_with(int id) {
     if (std::find(br->ids.begin(), br->ids.end(), id) != br->ids.end()) {
       cudaStreamSynchronize(stream);
       if (br->graph) cudaGraphExecDestroy(br->graph);
-      for (void* p : br->allocs) cudaFree(p);
+      for (void* p : br->allocs) dfree(p);
       delete br;
       it = batch_cache_.erase(it);
     } else {
@@ -739,9 +769,8 @@ int Context::remove_system(int id) {
   std::lock_guard<std::recursive_mutex> lk(mu);
   System* s = find(id);
   if (!s) return fail(RBMD_ERR_STATE, "unknown system id " + std::to_string(id));
-  cudaStreamSynchronize(stream);
   drop_batches_with(id);
-  for (void* p : s->allocs) cudaFree(p);
+  for (void* p : s->allocs) dfree(p);  // stream-ordered: after every launch that used them
   systems_[s->slot] = nullptr;
   free_slots_.push_back(s->slot);
   delete s;
@@ -802,8 +831,8 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
   auto mk = [&](const std::vector<int2>& h, Work& w) {
     w.n = (int)h.size();
     if (h.empty()) return;
-    void* ptr = nullptr;
-    if (cudaMalloc(&ptr, sizeof(int2) * h.size()) != cudaSuccess) {
+    void* ptr = dmalloc(sizeof(int2) * h.size());
+    if (!ptr) {
       rc = RBMD_ERR_OOM;
       return;
     }
@@ -817,8 +846,8 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
   mk(wr, b.rho);
   mk(wt, b.tri);
   mk(wm, b.term);
-  void* ps = nullptr;
-  if (cudaMalloc(&ps, sizeof(int) * slots.size()) != cudaSuccess) rc = RBMD_ERR_OOM;
+  void* ps = dmalloc(sizeof(int) * slots.size());
+  if (!ps) rc = RBMD_ERR_OOM;
   else {
     br->allocs.push_back(ps);
     cudaMemcpyAsync(ps, slots.data(), sizeof(int) * slots.size(), cudaMemcpyHostToDevice, stream);
@@ -1127,8 +1156,8 @@ int Context::get_thermo(int id, rbmd_thermo* out) {
   if (rc) return rc;
   const Batch& b = bs[0]->b;
   // keep the step's forces: the pressure evaluation below recomputes them in FP64
-  void* fsave = nullptr;
-  if (cudaMalloc(&fsave, sizeof(double4) * D.n) != cudaSuccess) return fail(RBMD_ERR_OOM, "thermo scratch");
+  void* fsave = dmalloc(sizeof(double4) * D.n);
+  if (!fsave) return fail(RBMD_ERR_OOM, "thermo scratch");
   cudaMemcpyAsync(fsave, D.f, sizeof(double4) * D.n, cudaMemcpyDeviceToDevice, stream);
   // NPT: bond and angle energies are those of the step's force evaluation, before the remap
   // (PARA_BOND_ENERGY / PARA_ANGLE_ENERGY are set there and read by ThermoOutput::Execute)
@@ -1149,8 +1178,8 @@ int Context::get_thermo(int id, rbmd_thermo* out) {
   cudaMemcpyAsync(&st, D.st, sizeof(SysState), cudaMemcpyDeviceToHost, stream);
   std::vector<double> te(s->n_terms);
   if (s->n_terms) cudaMemcpyAsync(te.data(), D.term_energy, sizeof(double) * s->n_terms, cudaMemcpyDeviceToHost, stream);
+  dfree(fsave);
   rc = sync();
-  cudaFree(fsave);
   if (rc) return rc;
   if (!te_step.empty() && st.step > 0) te.swap(te_step);
   std::memset(out, 0, sizeof(*out));

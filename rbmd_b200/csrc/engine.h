@@ -83,6 +83,11 @@ class Context {
 
   System* find(int id);
   static int64_t estimate_bytes(const rbmd_system_desc& d, const rbmd_params& p);
+  // Stream-ordered device memory from the context's own pool (which keeps freed memory for reuse):
+  // admitting and retiring systems then costs no device-wide synchronisation.  dmalloc returns
+  // nullptr (and clears the error) when the pool cannot grow.
+  void* dmalloc(size_t bytes);
+  void dfree(void* p);
 
  private:
   struct BatchRec {
@@ -108,6 +113,7 @@ class Context {
   std::vector<System*> systems_;
   std::vector<int> free_slots_;
   SysDev* d_sys_ = nullptr;
+  cudaMemPool_t pool_ = nullptr;
   int slot_cap_ = 0;
   int next_id_ = 0;
   std::map<std::vector<int>, BatchRec*> batch_cache_;

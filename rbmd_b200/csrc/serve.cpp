@@ -11,6 +11,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace rbmd {
@@ -110,6 +112,13 @@ int Server::stop() {
   if (th_.joinable()) th_.join();
   std::lock_guard<std::mutex> lk(mu_);
   running_ = false;
+  if (const char* tr = std::getenv("RBMD_SERVE_TRACE"))
+    if (tr[0] == '1')
+      std::fprintf(stderr,
+                   "serve phases (s): idle %.3f add %.3f init %.3f step %.3f state %.3f thermo %.3f remove %.3f; "
+                   "rounds %lld steps %lld\n",
+                   phase_[0], phase_[1], phase_[2], phase_[3], phase_[4], phase_[5], phase_[6], (long long)rounds_,
+                   (long long)round_steps_);
   // fail whatever is still queued or active
   for (Request* r : queue_) {
     r->state = RBMD_REQ_FAILED;
@@ -208,6 +217,12 @@ void Server::admit_locked(std::vector<Request*>& admitted) {
 }
 
 void Server::loop() {
+  double t_mark = monotonic_seconds();
+  auto lap = [&](int phase) {
+    const double t = monotonic_seconds();
+    phase_[phase] += t - t_mark;
+    t_mark = t;
+  };
   while (!stop_) {
     std::vector<Request*> admitted;
     {
@@ -215,9 +230,11 @@ void Server::loop() {
       admit_locked(admitted);
       if (admitted.empty() && active_.empty()) {
         cv_.wait_for(lk, std::chrono::milliseconds(2), [&] { return stop_ || !queue_.empty(); });
+        lap(0);
         continue;
       }
     }
+    lap(0);
     // upload + Init of the admitted systems (outside the queue lock)
     std::vector<int32_t> new_ids;
     for (Request* r : admitted) {
@@ -235,8 +252,11 @@ void Server::loop() {
       r->t_admit = monotonic_seconds();
       new_ids.push_back(sid);
     }
+    lap(1);
     if (!new_ids.empty()) {
       int rc = ctx_->init(new_ids.data(), (int)new_ids.size());
+      if (!rc) rc = ctx_->sync();
+      lap(2);
       if (rc) {
         std::lock_guard<std::mutex> lk(mu_);
         for (Request* r : admitted)
@@ -270,7 +290,10 @@ void Server::loop() {
       rc = ctx_->step(ids.data(), (int)ids.size(), k);
       if (!rc) rc = ctx_->sync();
       for (Request* r : stepping) r->remaining -= k;
+      ++rounds_;
+      round_steps_ += k;
     }
+    lap(3);
     // retire finished systems
     std::vector<Request*> keep;
     for (Request* r : active_) {
@@ -283,9 +306,12 @@ void Server::loop() {
       r->v.assign(3 * (size_t)n, 0.0);
       int st = rc;
       if (!st) st = ctx_->get_state(r->sys, r->x.data(), r->v.data(), nullptr);
+      lap(4);
       if (!st) st = ctx_->get_thermo(r->sys, &r->thermo);
       if (!st && r->thermo.status != 0) st = RBMD_ERR_NUMERIC;
+      lap(5);
       ctx_->remove_system(r->sys);
+      lap(6);
       std::lock_guard<std::mutex> lk(mu_);
       used_ -= r->bytes;
       finish(r, st);

@@ -65,6 +65,10 @@ class Server {
   std::vector<Request*> active_;
   std::map<int64_t, std::unique_ptr<Request>> all_;
   int64_t next_id_ = 1;
+  // seconds spent by the loop per phase (RBMD_SERVE_TRACE=1 prints them at stop): idle, add,
+  // init, step, retire-state, retire-thermo, retire-remove; rounds, steps
+  double phase_[7] = {0, 0, 0, 0, 0, 0, 0};
+  int64_t rounds_ = 0, round_steps_ = 0;
 };
 
 double monotonic_seconds();

@@ -106,10 +106,8 @@ int Context::autotune(const int32_t* ids, int n, rbmd_tune_result* out, int cap,
           off.push_back(tot);
           tot += sizeof(double4) * (size_t)s->dev.n;
         }
-        if (cudaMalloc(&fsave, tot) != cudaSuccess) {
-          cudaGetLastError();
-          return fail(RBMD_ERR_OOM, "autotune: force scratch");
-        }
+        fsave = dmalloc(tot);
+        if (!fsave) return fail(RBMD_ERR_OOM, "autotune: force scratch");
         for (size_t k = 0; k < g.size(); ++k)
           cudaMemcpyAsync((char*)fsave + off[k], g[k]->dev.f, sizeof(double4) * g[k]->dev.n,
                           cudaMemcpyDeviceToDevice, stream);
@@ -123,7 +121,7 @@ int Context::autotune(const int32_t* ids, int n, rbmd_tune_result* out, int cap,
         for (System* s : g) set_layout(s, l);
         BatchRec* br = build_batch(g, rc);
         if (rc) {
-          for (void* p : br->allocs) cudaFree(p);
+          for (void* p : br->allocs) dfree(p);
           delete br;
           break;
         }
@@ -140,7 +138,7 @@ int Context::autotune(const int32_t* ids, int n, rbmd_tune_result* out, int cap,
           if (rep == 0 || t < t_min) t_min = t;
         }
         cudaStreamSynchronize(stream);
-        for (void* p : br->allocs) cudaFree(p);
+        for (void* p : br->allocs) dfree(p);
         delete br;
         r.ms[l] = t_min;
         if (best < 0 || t_min < best_ms) {
@@ -154,8 +152,8 @@ int Context::autotune(const int32_t* ids, int n, rbmd_tune_result* out, int cap,
         for (size_t k = 0; k < g.size(); ++k)
           cudaMemcpyAsync(g[k]->dev.f, (char*)fsave + off[k], sizeof(double4) * g[k]->dev.n,
                           cudaMemcpyDeviceToDevice, stream);
+        dfree(fsave);
         cudaStreamSynchronize(stream);
-        cudaFree(fsave);
       }
       if (rc) return fail(rc, "autotune: work-table allocation failed");
       rc = check_cuda("autotune");
