@@ -333,6 +333,37 @@ typedef struct rbmd_derived {
 } rbmd_derived;
 int rbmd_get_derived(rbmd_ctx* ctx, int32_t sys_id, rbmd_derived* out);
 
+/* ---------------------------------------------------------------- trajectory observables */
+enum rbmd_observable { RBMD_OBS_MSD = 1, RBMD_OBS_VACF = 2 };
+/* Take the current positions and image counters (which & RBMD_OBS_MSD) and / or velocities
+ * (which & RBMD_OBS_VACF) as the reference configuration of rbmd_observe (MSDOutput::Execute at
+ * start_step, framework/output/MSDOutput.cpp:58-66; VACFOutput::Execute,
+ * framework/output/VACFOutput.cpp:54-57).  The reference zeroes the image counters at that point;
+ * here they are left alone and their values at the reset subtracted. */
+int rbmd_observe_reset(rbmd_ctx* ctx, int32_t sys_id, int32_t which);
+/* Atom averages against the reference configuration (MSDOutput::ExecuteMSD,
+ * framework/output/MSDOutput.cpp:116-134; VACFOutput::ExecuteMSD,
+ * framework/output/VACFOutput.cpp:108-118): msd[4] = (dx^2, dy^2, dz^2, |d|^2) of the unwrapped
+ * displacement x + (image - image0) L - x0 (L the current box), vacf[4] = (v0x vx, v0y vy, v0z vz,
+ * v0.v).  Either pointer may be NULL; RBMD_ERR_STATE when a requested average has no reference
+ * configuration yet. */
+int rbmd_observe(rbmd_ctx* ctx, int32_t sys_id, double* msd, double* vacf);
+/* RDF radii (RDFOutput::RDFOutput, framework/output/RDFOutput.cpp:42-53): n = (int)(radius / dr)
+ * bins at dr, 2 dr, ... accumulated by repeated addition.  radii may be NULL (count only); at most
+ * cap values are written.  RBMD_ERR_ARG unless radius > 0, dr > 0 and radius / dr >= 1. */
+int rbmd_rdf_bins(double radius, double dr, double* radii, int32_t cap, int32_t* n_bins);
+/* RDF pair counts of the current configuration (RDFOutput::ComputeRDF,
+ * framework/output/RDFOutput.cpp:181-262; ComputeRDFWorklet,
+ * framework/output/worklet/OutPutWorklet.cpp:230-310 and :578-640): counts[b] (n_bins of
+ * rbmd_rdf_bins) = number of (center, target, periodic image) triples with
+ * r_b < distance < r_b + 0.01 r_b, skipping pairs of one molecule when exclude_same_molecule.
+ * centers / targets are atom ids.  *volume (may be NULL) receives the box volume the counts were
+ * taken in; the reference's RDF value of one snapshot is
+ * counts[b] / (n_centers * (n_targets / volume) * 4/3 pi ((1.01 r_b)^3 - r_b^3)). */
+int rbmd_rdf_counts(rbmd_ctx* ctx, int32_t sys_id, const int32_t* centers, int32_t n_centers,
+                    const int32_t* targets, int32_t n_targets, double radius, double dr,
+                    int32_t exclude_same_molecule, int64_t* counts, double* volume);
+
 /* ---------------------------------------------------------------- EAM input helpers (host only) */
 /* funcfl file contents after the header lines (ExecutionNVT::ReadPotentialFile,
  * framework/run/ExecutionNVT.cpp:899-931). */

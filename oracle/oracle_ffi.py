@@ -233,3 +233,52 @@ def read_funcfl(path):
                                  _dp(frho), _dp(zr), _dp(rhor))
     return dict(nrho=int(nrho[0]), nr=int(nr[0]), drho=float(drho[0]), dr=float(dr[0]),
                 cut=float(cut[0]), frho=frho, zr=zr, rhor=rhor)
+
+
+# ---------------------------------------------------------------- trajectory observables
+def _observe_sigs():
+    L = lib()
+    i32, d, P = C.c_int32, C.c_double, C.POINTER
+    dp, ip, lp = P(C.c_double), P(C.c_int32), P(C.c_int64)
+    L.oracle_rdf_bins.argtypes = [d, d, dp, C.c_int]
+    L.oracle_msd_vacf.argtypes = [C.c_int, dp, ip, dp, dp, ip, dp, dp, dp, dp]
+    L.oracle_rdf_counts.argtypes = [dp, ip, dp, ip, C.c_int, ip, C.c_int, d, d, C.c_int, lp]
+    for f in (L.oracle_rdf_bins, L.oracle_msd_vacf, L.oracle_rdf_counts):
+        f.restype = C.c_int
+    return L
+
+
+def rdf_bins(radius, dr):
+    """RDF radii (RDFOutput.cpp:42-53): (int)(radius / dr) values, dr accumulated."""
+    L = _observe_sigs()
+    nb = L.oracle_rdf_bins(float(radius), float(dr), None, 0)
+    if nb < 0:
+        raise ValueError("bad radius / dr")
+    r = np.zeros(nb)
+    L.oracle_rdf_bins(float(radius), float(dr), _dp(r), nb)
+    return r
+
+
+def msd_vacf(x0, img0, v0, x, img, v, box_len):
+    """(msd[4], vacf[4]) atom averages of the unwrapped displacement and v0 . v."""
+    L = _observe_sigs()
+    a = [np.ascontiguousarray(t, np.float64) for t in (x0, v0, x, v, box_len)]
+    ii = [np.ascontiguousarray(t, np.int32) for t in (img0, img)]
+    msd, vacf = np.zeros(4), np.zeros(4)
+    L.oracle_msd_vacf(a[0].shape[0], _dp(a[0]), _ip(ii[0]), _dp(a[1]), _dp(a[2]), _ip(ii[1]), _dp(a[3]),
+                      _dp(a[4]), _dp(msd), _dp(vacf))
+    return msd, vacf
+
+
+def rdf_counts(x, molecule, box_len, centers, targets, radius, dr, exclude_same_molecule=True):
+    """Pair counts per RDF bin of one configuration (every periodic image inside the last edge)."""
+    L = _observe_sigs()
+    x = np.ascontiguousarray(x, np.float64)
+    mol = np.ascontiguousarray(molecule, np.int32)
+    bl = np.ascontiguousarray(box_len, np.float64)
+    c = np.ascontiguousarray(centers, np.int32)
+    t = np.ascontiguousarray(targets, np.int32)
+    counts = np.zeros(rdf_bins(radius, dr).size, np.int64)
+    L.oracle_rdf_counts(_dp(x), _ip(mol), _dp(bl), _ip(c), c.size, _ip(t), t.size, float(radius), float(dr),
+                        int(bool(exclude_same_molecule)), counts.ctypes.data_as(C.POINTER(C.c_int64)))
+    return counts

@@ -179,6 +179,33 @@ class Context:
         self._check(lib().rbmd_get_kspace(self.h, sid, _ip(m), _dp(rk)))
         return m, rk
 
+    # ---- trajectory observables (output/MSDOutput.cpp, VACFOutput.cpp, RDFOutput.cpp)
+    def observe_reset(self, sid, msd=True, vacf=True):
+        """Take the current positions and image counters (msd) and / or velocities (vacf) as the
+        reference configuration of observe()."""
+        which = (A.OBS_MSD if msd else 0) | (A.OBS_VACF if vacf else 0)
+        self._check(lib().rbmd_observe_reset(self.h, sid, which))
+
+    def observe(self, sid, msd=True, vacf=True):
+        """(msd, vacf): atom averages (x, y, z, total) against the reference configuration; None
+        for an average not asked for."""
+        m = np.zeros(4) if msd else None
+        v = np.zeros(4) if vacf else None
+        self._check(lib().rbmd_observe(self.h, sid, None if m is None else _dp(m), None if v is None else _dp(v)))
+        return m, v
+
+    def rdf_counts(self, sid, centers, targets, radius, dr, exclude_same_molecule=True):
+        """Pair counts per RDF bin (rdf_bins(radius, dr)) of the current configuration, and the
+        box volume they were taken in."""
+        c = np.ascontiguousarray(centers, np.int32)
+        t = np.ascontiguousarray(targets, np.int32)
+        counts = np.zeros(rdf_bins(radius, dr).size, np.int64)
+        vol = C.c_double()
+        self._check(lib().rbmd_rdf_counts(self.h, sid, _ip(c), c.size, _ip(t), t.size, float(radius), float(dr),
+                                          int(bool(exclude_same_molecule)), counts.ctypes.data_as(A.lptr),
+                                          C.byref(vol)))
+        return counts, vol.value
+
     # ---- diagnostics
     def launch_count(self):
         v = C.c_int64()
@@ -249,6 +276,33 @@ class Context:
 
     def serve_stop(self):
         self._check(lib().rbmd_serve_stop(self.h))
+
+
+def rdf_bins(radius, dr):
+    """RDF radii: (int)(radius / dr) bins at dr, 2 dr, ... accumulated (RDFOutput.cpp:42-53)."""
+    n = C.c_int32()
+    rc = lib().rbmd_rdf_bins(float(radius), float(dr), None, 0, C.byref(n))
+    if rc:
+        raise RbmdError(rc, "rdf_bins: radius and dr must be positive with radius / dr >= 1")
+    r = np.zeros(n.value)
+    lib().rbmd_rdf_bins(float(radius), float(dr), _dp(r), n.value, C.byref(n))
+    return r
+
+
+# single-precision pi of the reference's normalisation (vtkm::Pif, OutPutWorklet.cpp:303-306)
+PI_F32 = float(np.float32(np.pi))
+
+
+def rdf_snapshot(counts, radii, n_centers, n_targets, volume):
+    """One snapshot's RDF from its pair counts (ComputeRDFWorklet, OutPutWorklet.cpp:303-306):
+    counts / (n_centers * rho * (4/3 pi (1.01 r)^3 - 4/3 pi r^3)), rho = n_targets / volume.
+    NaN where the denominator is zero (no centers or targets), as in the reference."""
+    r = np.asarray(radii, np.float64)
+    rho = n_targets / volume
+    shell = (4 / 3.0) * PI_F32 * (r + r * 0.01) ** 3 - ((4 / 3.0) * PI_F32 * r ** 3)
+    den = n_centers * rho * shell
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.asarray(counts, np.float64) / den
 
 
 def system_bytes(sd, params=None):

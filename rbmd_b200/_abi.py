@@ -27,6 +27,7 @@ RANDOM_PHILOX, RANDOM_TEST = 0, 1
 SHAKE_NULL, SHAKE_FALSE, SHAKE_TRUE = -1, 0, 1
 ENS_NVT, ENS_NVE, ENS_NPT = 0, 1, 2
 PC_BERENDSEN, PC_NOSE_HOOVER = 0, 1
+OBS_MSD, OBS_VACF = 1, 2
 PRESS_CTRLS = {"BERENDSEN": PC_BERENDSEN, "NOSE_HOOVER": PC_NOSE_HOOVER}
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
@@ -38,6 +39,7 @@ UNITS = {"LJ": UNITS_LJ, "REAL": UNITS_REAL, "METAL": UNITS_METAL}
 
 dptr = C.POINTER(C.c_double)
 iptr = C.POINTER(C.c_int32)
+lptr = C.POINTER(C.c_int64)
 
 
 class Params(C.Structure):
@@ -220,6 +222,11 @@ def declare(lib, prefix="rbmd"):
         "step_timed": ([ctx, iptr, C.c_int32, C.c_int32, dptr], C.c_int),
         "fma_peak": ([ctx, C.c_int32, dptr], C.c_int),
         "autotune": ([ctx, iptr, C.c_int32, P(TuneResult), C.c_int32, iptr], C.c_int),
+        "observe_reset": ([ctx, C.c_int32, C.c_int32], C.c_int),
+        "observe": ([ctx, C.c_int32, dptr, dptr], C.c_int),
+        "rdf_bins": ([C.c_double, C.c_double, dptr, C.c_int32, iptr], C.c_int),
+        "rdf_counts": ([ctx, C.c_int32, iptr, C.c_int32, iptr, C.c_int32, C.c_double, C.c_double, C.c_int32,
+                        lptr, dptr], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, f"{prefix}_{name}")
@@ -238,4 +245,5 @@ HEADER_FUNCTIONS = [
     "rbmd_serve_start", "rbmd_serve_submit", "rbmd_serve_poll", "rbmd_serve_wait",
     "rbmd_serve_result", "rbmd_serve_stop", "rbmd_launch_count", "rbmd_profile_enable",
     "rbmd_profile_get", "rbmd_step_timed", "rbmd_fma_peak", "rbmd_autotune",
+    "rbmd_observe_reset", "rbmd_observe", "rbmd_rdf_bins", "rbmd_rdf_counts",
 ]

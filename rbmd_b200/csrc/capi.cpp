@@ -184,6 +184,32 @@ int rbmd_get_derived(rbmd_ctx* ctx, int32_t id, rbmd_derived* out) {
   return ctx->c->get_derived(id, out);
 }
 
+int rbmd_observe_reset(rbmd_ctx* ctx, int32_t id, int32_t which) {
+  CTX_CHECK(ctx);
+  return ctx->c->observe_reset(id, which);
+}
+
+int rbmd_observe(rbmd_ctx* ctx, int32_t id, double* msd, double* vacf) {
+  CTX_CHECK(ctx);
+  return ctx->c->observe(id, msd, vacf);
+}
+
+int rbmd_rdf_bins(double radius, double dr, double* radii, int32_t cap, int32_t* n_bins) {
+  std::vector<double> r;
+  const int nb = rbmd::rdf_bins(radius, dr, radii ? &r : nullptr);
+  if (nb < 0) return RBMD_ERR_ARG;
+  if (n_bins) *n_bins = nb;
+  if (radii)
+    for (int b = 0; b < nb && b < cap; ++b) radii[b] = r[b];
+  return RBMD_OK;
+}
+
+int rbmd_rdf_counts(rbmd_ctx* ctx, int32_t id, const int32_t* centers, int32_t nc, const int32_t* targets, int32_t nt,
+                    double radius, double dr, int32_t exclude_same_molecule, int64_t* counts, double* volume) {
+  CTX_CHECK(ctx);
+  return ctx->c->rdf_counts(id, centers, nc, targets, nt, radius, dr, exclude_same_molecule, counts, volume);
+}
+
 // ------------------------------------------------------------------ EAM input (host)
 int rbmd_eam_read_funcfl(const char* path, rbmd_eam_file* out, double* frho, double* zr, double* rhor) {
   // ExecutionNVT::ReadPotentialFile, framework/run/ExecutionNVT.cpp:899-931: two comment lines,

@@ -32,7 +32,16 @@ struct System {
   int P = 0;
   std::vector<double> charge;   // host copy (energies)
   bool tuned = false;           // pair layout chosen by the autotuner (or fixed: NPT, environment)
+  // MSD / VACF reference configuration (allocated by the first observe_reset)
+  double4* obs_x0 = nullptr;
+  double4* obs_v0 = nullptr;
+  int4* obs_img0 = nullptr;
+  int obs_have = 0;             // RBMD_OBS_* bits taken
 };
+
+// RDF bins of radius / dr (RDFOutput.cpp:42-53): (int)(radius / dr) radii, dr accumulated by
+// repeated addition.  Returns the bin count, or -1 for a bad (radius, dr).
+int rdf_bins(double radius, double dr, std::vector<double>* radii);
 
 struct Profiler {
   bool on = false;
@@ -73,6 +82,10 @@ class Context {
   int get_derived(int id, rbmd_derived* out);
   int device_status(int id, int* status);
   int autotune(const int32_t* ids, int n, rbmd_tune_result* out, int cap, int* n_groups, bool keep_forces = true);
+  int observe_reset(int id, int which);
+  int observe(int id, double* msd, double* vacf);
+  int rdf_counts(int id, const int32_t* centers, int nc, const int32_t* targets, int nt, double radius, double dr,
+                 int exclude_same_molecule, int64_t* counts, double* volume);
 
   int fail(int code, const std::string& msg);
   std::string last_error;

@@ -73,6 +73,25 @@ long long static_list_ints(int n, int ncell, int dense, int cap);
 int launch_rbl_lists_static(const SysDev* sys, int slot, int n, int ncell, int dense, int cap, int* scratch,
                             cudaStream_t s, StaticLists* out);
 
+// Trajectory observables (between steps, not on the step path).
+constexpr int kObsThreads = 256;
+constexpr int kObsMaxBlocks = 4 * 148;        // partial sums of the MSD / VACF reduction
+constexpr int kRdfTargetsPerBlock = 2048;     // targets one RDF block walks (grid.y splits the rest)
+constexpr int kRdfSharedBins = 8192;          // bins counted in shared memory (32 KB); above, in global
+int obs_blocks(int n);
+// which: bit 0 positions and image counters, bit 1 velocities
+void launch_obs_snapshot(const SysDev* sys, int slot, int n, int which, double4* x0, double4* v0, int4* img0,
+                         cudaStream_t s);
+// out[8] = (msd x, y, z, total, vacf x, y, z, total), averaged over atoms; part holds
+// obs_blocks(n) x 8 doubles.
+void launch_obs_msd_vacf(const SysDev* sys, int slot, int n, const double4* x0, const double4* v0, const int4* img0,
+                         double* part, double* out, cudaStream_t s);
+// Adds the RDF pair counts of one snapshot to counts[nb] (radii[b] = (b + 1) dr accumulated,
+// upper[b] = radii[b] + 0.01 radii[b]).
+void launch_rdf_count(const SysDev* sys, int slot, const int* centers, int nc, const int* targets, int nt,
+                      const double* radii, const double* upper, int nb, double dr, int exclude_mol,
+                      unsigned long long* counts, cudaStream_t s);
+
 constexpr int kCellWarpsHost = 4;  // home cells per block of the tile pair kernel
 constexpr double kTileMinPerCell = 3.0;  // mean atoms per cell from which the tile kernel is used
 

@@ -244,6 +244,22 @@ void ExecutionMD::State(std::vector<double>& x, std::vector<double>& v, std::vec
 
 void ExecutionNVT::Execute() { check(rbmd_step(_ctx, &_sys, 1, 1), "rbmd_step"); }
 
+void ExecutionMD::ObserveReset(int which) { check(rbmd_observe_reset(_ctx, _sys, which), "rbmd_observe_reset"); }
+
+void ExecutionMD::Observe(double* msd, double* vacf) { check(rbmd_observe(_ctx, _sys, msd, vacf), "rbmd_observe"); }
+
+double ExecutionMD::RdfCounts(const std::vector<int>& centers, const std::vector<int>& targets, double radius,
+                              double dr, bool exclude_same_molecule, std::vector<int64_t>& counts) {
+  int32_t nb = 0;
+  check(rbmd_rdf_bins(radius, dr, nullptr, 0, &nb), "rbmd_rdf_bins");
+  counts.assign(nb, 0);
+  double volume = 0.0;
+  check(rbmd_rdf_counts(_ctx, _sys, centers.data(), (int32_t)centers.size(), targets.data(), (int32_t)targets.size(),
+                        radius, dr, exclude_same_molecule ? 1 : 0, counts.data(), &volume),
+        "rbmd_rdf_counts");
+  return volume;
+}
+
 // ------------------------------------------------------------------------------------- outputs
 ThermoOutput::ThermoOutput(int interval, const std::string& path, bool console)
     : _interval(std::max(1, interval)), _console(console) {
@@ -294,6 +310,113 @@ void TrajectoryOutput::Execute(Executioner& ex) {
     std::fprintf(_file, "%zu %.10g %.10g %.10g %d %d %d\n", i + 1, x[3 * i], x[3 * i + 1], x[3 * i + 2], img[3 * i],
                  img[3 * i + 1], img[3 * i + 2]);
   std::fflush(_file);
+}
+
+CorrelationOutput::CorrelationOutput(bool vacf, int interval, int64_t start_step, int64_t end_step,
+                                     const std::string& path)
+    : _vacf(vacf), _interval(std::max(1, interval)), _start(start_step), _end(end_step) {
+  _file = std::fopen(path.c_str(), "w");
+  if (!_file) throw std::runtime_error("cannot write " + path);
+}
+
+CorrelationOutput::~CorrelationOutput() {
+  if (_file) std::fclose(_file);
+}
+
+void CorrelationOutput::Execute(Executioner& ex) {
+  // MSDOutput::Execute (MSDOutput.cpp:56-105), VACFOutput::Execute (VACFOutput.cpp:52-96)
+  const int64_t step = ex.CurrentStep();
+  if (step == _start) {
+    ex.Run().ObserveReset(_vacf ? RBMD_OBS_VACF : RBMD_OBS_MSD);
+    for (double& a : _ave) a = 0.0;
+  }
+  if (step >= _start && step <= _end) {
+    if (_vacf) ex.Run().Observe(nullptr, _ave);
+    else ex.Run().Observe(_ave, nullptr);
+  }
+  if (step == 0) std::fprintf(_file, _vacf ? "Step Time VACFx VACFy VACFz VACF_total\n"
+                                           : "Step Time MSD_x MSD_y MSD_z MSD_total sqrt(MSD_total) \n");
+  if (step < 1 || step % _interval != 0) return;
+  std::fprintf(_file, "%lld %g %g %g %g %g", (long long)step, ex.CurrentTime(), _ave[0], _ave[1], _ave[2], _ave[3]);
+  if (!_vacf) std::fprintf(_file, " %g", std::sqrt(_ave[3]));
+  std::fprintf(_file, "\n");
+  std::fflush(_file);
+}
+
+RDFOutput::RDFOutput(const Para& para, double radius, double dr, int64_t statistics_steps,
+                     const std::vector<std::pair<int, int>>& pairs, const std::string& path)
+    : _path(path), _radius(radius), _dr(dr), _stat(statistics_steps), _inbuild(para.init_way == "inbuild"),
+      _pairs(pairs) {
+  int32_t nb = 0;
+  if (rbmd_rdf_bins(radius, dr, nullptr, 0, &nb) != RBMD_OK)
+    throw std::runtime_error("rdf_out: radius and dr must be positive with radius / dr >= 1");
+  _radii.resize(nb);
+  rbmd_rdf_bins(radius, dr, _radii.data(), nb, &nb);
+  if (_inbuild) {
+    // ExecutionNVT::SetCenterTargetPositions (ExecutionNVT.cpp:293-322): first half against second
+    const int h = para.n / 2;
+    _centers.emplace_back();
+    _targets.emplace_back();
+    for (int i = 0; i < h; ++i) {
+      _centers[0].push_back(i);
+      _targets[0].push_back(h + i);
+    }
+  } else {
+    if (pairs.empty()) throw std::runtime_error("rdf_out needs \"atoms_pair\": [[type, type], ...]");
+    // atom ids of each type in id order (ModelFileInitCondition.cpp:786-806)
+    for (const auto& pr : pairs) {
+      for (int t : {pr.first, pr.second})
+        if (t < 0 || t >= para.n_types)
+          throw std::runtime_error("rdf_out: atoms_pair type " + std::to_string(t) + " out of range (types are 0-based)");
+      _centers.emplace_back();
+      _targets.emplace_back();
+      for (int i = 0; i < para.n; ++i) {
+        if (para.type[i] == pr.first) _centers.back().push_back(i);
+        if (para.type[i] == pr.second) _targets.back().push_back(i);
+      }
+    }
+  }
+  _rdf.assign(_centers.size(), std::vector<double>(nb, 0.0));
+}
+
+void RDFOutput::Execute(Executioner& ex) {
+  // RDFOutput::Execute / ComputeRDF (RDFOutput.cpp:107-262)
+  const int64_t step = ex.CurrentStep();
+  const int64_t lower = ex.NumStep() - _stat, upper = ex.NumStep() + 1;
+  if (step >= lower && step < upper) {
+    const float pif = 3.14159265358979323846f;  // vtkm::Pif() of the normalisation
+    for (size_t p = 0; p < _centers.size(); ++p) {
+      std::vector<int64_t> counts;
+      const double volume = ex.Run().RdfCounts(_centers[p], _targets[p], _radius, _dr, !_inbuild, counts);
+      const double nc = (double)_centers[p].size(), rho = (double)_targets[p].size() / volume;
+      for (size_t b = 0; b < _radii.size(); ++b) {
+        const double r = _radii[b];
+        const double dr3 = std::pow(r + r * 0.01, 3), r3 = std::pow(r, 3);
+        _rdf[p][b] += (double)counts[b] / (nc * rho * ((4 / 3.0) * pif * dr3 - ((4 / 3.0) * pif * r3)));
+      }
+    }
+  }
+  if (step != ex.NumStep() - 1) return;
+  FILE* f = std::fopen(_path.c_str(), "w");
+  if (!f) throw std::runtime_error("cannot write " + _path);
+  std::fprintf(f, "Radius ");
+  if (_inbuild) {
+    std::fprintf(f, "RDF\n");
+  } else {
+    for (const auto& pr : _pairs) std::fprintf(f, "RDF:%d-%d ", pr.first, pr.second);
+    std::fprintf(f, "\n");
+  }
+  const double div = (double)(upper - lower - 1);
+  for (size_t b = 0; b < _radii.size(); ++b) {
+    std::fprintf(f, "%g", _radii[b]);
+    for (size_t p = 0; p < _rdf.size(); ++p) {
+      const double v = _rdf[p][b] / div;
+      if (std::isnan(v)) std::fprintf(f, " ");
+      else std::fprintf(f, " %g", v);
+    }
+    std::fprintf(f, "\n");
+  }
+  std::fclose(f);
 }
 
 // --------------------------------------------------------------------------------- executioner
@@ -531,6 +654,46 @@ void MDApplication::CreateActions() {
   if (const Json* outs = _cfg.find("outputs")) {
     if (const Json* th = outs->find("thermo_out")) _thermo_interval = (int)th->number("interval", 1);
     if (const Json* tr = outs->find("trajectory_out")) _traj_interval = (int)tr->number("interval", 100);
+    // msd_out / vacf_out: interval (default 1), start_step and end_step (required);
+    // rdf_out: radius, dr, statistics_rdf_steps, atoms_pair (read_data) (MDApplication.cpp:221-235)
+    auto need = [](const Json* o, const char* out, const char* key) {
+      if (!o->find(key) || !o->find(key)->is_number())
+        throw std::runtime_error(std::string(out) + " needs a number \"" + key + "\"");
+      return o->find(key)->num;
+    };
+    for (const char* name : {"msd_out", "vacf_out"}) {
+      const Json* o = outs->find(name);
+      if (!o) continue;
+      Correlation& c = name[0] == 'm' ? _msd : _vacf;
+      c.on = true;
+      c.interval = (int)o->number("interval", 1);
+      c.start = (int64_t)need(o, name, "start_step");
+      c.end = (int64_t)need(o, name, "end_step");
+    }
+    if (const Json* o = outs->find("rdf_out")) {
+      _rdf.on = true;
+      _rdf.radius = need(o, "rdf_out", "radius");
+      _rdf.dr = need(o, "rdf_out", "dr");
+      _rdf.statistics_steps = (int64_t)need(o, "rdf_out", "statistics_rdf_steps");
+      if (const Json* ap = o->find("atoms_pair")) {
+        if (!ap->is_array()) throw std::runtime_error("rdf_out: atoms_pair must be an array of [type, type]");
+        for (const Json& e : ap->arr) {
+          if (!e.is_array() || e.arr.size() != 2 || !e.arr[0].is_number() || !e.arr[1].is_number())
+            throw std::runtime_error("rdf_out: atoms_pair must be an array of [type, type]");
+          _rdf.pairs.emplace_back((int)e.arr[0].num, (int)e.arr[1].num);
+        }
+      }
+      if (_para.init_way != "inbuild") {
+        if (_rdf.pairs.empty()) throw std::runtime_error("rdf_out needs \"atoms_pair\": [[type, type], ...]");
+        for (const auto& pr : _rdf.pairs)
+          for (int t : {pr.first, pr.second})
+            if (t < 0 || t >= _para.n_types)
+              throw std::runtime_error("rdf_out: atoms_pair type " + std::to_string(t) +
+                                       " out of range (types are 0-based)");
+      }
+      if (rbmd_rdf_bins(_rdf.radius, _rdf.dr, nullptr, 0, nullptr) != RBMD_OK)
+        throw std::runtime_error("rdf_out: radius and dr must be positive with radius / dr >= 1");
+    }
   }
 }
 
@@ -591,8 +754,20 @@ void MDApplication::DumpSystem(const std::string& path) const {
   darr("special_weights", _para.sp_w);
   std::fprintf(f, "\"eam\": {\"nrho\": %d, \"nr\": %d, \"drho\": %.17g, \"dr\": %.17g, \"rhomax\": %.17g, \"cut\": %.17g},\n",
                _para.eam_nrho, _para.eam_nr, _para.eam_drho, _para.eam_dr, _para.eam_rhomax, _para.eam_cut);
-  std::fprintf(f, "\"outputs\": {\"thermo_interval\": %d, \"trajectory_interval\": %d}\n}\n", _thermo_interval,
+  std::fprintf(f, "\"outputs\": {\"thermo_interval\": %d, \"trajectory_interval\": %d", _thermo_interval,
                _traj_interval);
+  for (const Correlation* c : {&_msd, &_vacf})
+    if (c->on)
+      std::fprintf(f, ", \"%s\": {\"interval\": %d, \"start_step\": %lld, \"end_step\": %lld}",
+                   c == &_msd ? "msd" : "vacf", c->interval, (long long)c->start, (long long)c->end);
+  if (_rdf.on) {
+    std::fprintf(f, ", \"rdf\": {\"radius\": %.17g, \"dr\": %.17g, \"statistics_rdf_steps\": %lld, \"atoms_pair\": [",
+                 _rdf.radius, _rdf.dr, (long long)_rdf.statistics_steps);
+    for (size_t k = 0; k < _rdf.pairs.size(); ++k)
+      std::fprintf(f, "%s[%d,%d]", k ? "," : "", _rdf.pairs[k].first, _rdf.pairs[k].second);
+    std::fprintf(f, "]}");
+  }
+  std::fprintf(f, "}\n}\n");
   std::fclose(f);
 }
 
@@ -612,6 +787,14 @@ int MDApplication::Run() {
     Executioner ex(run, _para.params.num_steps, _para.params.timestep);
     if (_thermo_interval > 0) ex.AddOutput(std::unique_ptr<Output>(new ThermoOutput(_thermo_interval, "energy.rbmd", true)));
     if (_traj_interval > 0) ex.AddOutput(std::unique_ptr<Output>(new TrajectoryOutput(_traj_interval, "trajectory.rbmd")));
+    if (_rdf.on)
+      ex.AddOutput(std::unique_ptr<Output>(
+          new RDFOutput(_para, _rdf.radius, _rdf.dr, _rdf.statistics_steps, _rdf.pairs, "rdf.rbmd")));
+    if (_msd.on)
+      ex.AddOutput(std::unique_ptr<Output>(new CorrelationOutput(false, _msd.interval, _msd.start, _msd.end, "msd.rbmd")));
+    if (_vacf.on)
+      ex.AddOutput(
+          std::unique_ptr<Output>(new CorrelationOutput(true, _vacf.interval, _vacf.start, _vacf.end, "vacf.rbmd")));
     const auto t0 = std::chrono::steady_clock::now();
     ex.Init();
     ex.Execute();

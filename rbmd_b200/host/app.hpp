@@ -95,6 +95,11 @@ class ExecutionMD : public Execution {
   void Init() override;
   rbmd_thermo Thermo();
   void State(std::vector<double>& x, std::vector<double>& v, std::vector<int>& image);
+  // trajectory observables (rbmd_observe_reset / rbmd_observe / rbmd_rdf_counts)
+  void ObserveReset(int which);
+  void Observe(double* msd, double* vacf);
+  double RdfCounts(const std::vector<int>& centers, const std::vector<int>& targets, double radius, double dr,
+                   bool exclude_same_molecule, std::vector<int64_t>& counts);  // returns the box volume
 
  protected:
   void check(int rc, const char* what);
@@ -142,6 +147,45 @@ class TrajectoryOutput : public Output {
  private:
   int _interval;
   FILE* _file = nullptr;
+};
+
+// msd.rbmd / vacf.rbmd (output/MSDOutput.cpp, output/VACFOutput.cpp): the reference configuration
+// is taken at start_step, the atom average recomputed every step of [start_step, end_step], and a
+// line "Step Time x y z total" (MSD: and sqrt(total)) written every `interval` steps from step 1,
+// holding the last average computed.
+class CorrelationOutput : public Output {
+ public:
+  CorrelationOutput(bool vacf, int interval, int64_t start_step, int64_t end_step, const std::string& path);
+  ~CorrelationOutput() override;
+  void Execute(Executioner& ex) override;
+
+ private:
+  bool _vacf;
+  int _interval;
+  int64_t _start, _end;
+  double _ave[4] = {0, 0, 0, 0};
+  FILE* _file = nullptr;
+};
+
+// rdf.rbmd (output/RDFOutput.cpp): pair counts of the last statistics_rdf_steps steps, normalised
+// per snapshot and averaged, written once at step num_steps - 1.  Pairs of atom types (0-based)
+// with same-molecule pairs skipped (read_data), or the first half of the atoms against the second
+// (inbuild).
+class RDFOutput : public Output {
+ public:
+  RDFOutput(const Para& para, double radius, double dr, int64_t statistics_steps,
+            const std::vector<std::pair<int, int>>& pairs, const std::string& path);
+  void Execute(Executioner& ex) override;
+
+ private:
+  std::string _path;
+  double _radius, _dr;
+  int64_t _stat;
+  bool _inbuild;
+  std::vector<std::pair<int, int>> _pairs;
+  std::vector<std::vector<int>> _centers, _targets;
+  std::vector<double> _radii;
+  std::vector<std::vector<double>> _rdf;
 };
 
 class Executioner {
@@ -201,6 +245,17 @@ class MDApplication : public Application {
   Json _cfg;
   Para _para;
   int _thermo_interval = 0, _traj_interval = 0;
+  struct Correlation {
+    bool on = false;
+    int interval = 1;
+    int64_t start = 0, end = 0;
+  } _msd, _vacf;
+  struct Rdf {
+    bool on = false;
+    double radius = 0, dr = 0;
+    int64_t statistics_steps = 0;
+    std::vector<std::pair<int, int>> pairs;
+  } _rdf;
   bool _special_bonds = false;
   double _special_w[3] = {0, 0, 0};
   std::string _ff_type, _potential_file, _base_dir, _dihedral_type;

@@ -209,3 +209,37 @@ def test_dihedrals_read_when_the_reference_uses_them(rbmd_bin, tmp_path):
     r = subprocess.run([rbmd_bin, "-j", path, "--dump-system", str(tmp_path / "d.json")], capture_output=True,
                        text=True)
     assert r.returncode == 1 and "Harmonic" in r.stderr
+
+
+def test_observable_outputs_input(rbmd_bin, tmp_path):
+    """msd_out / vacf_out / rdf_out keys of the reference's bundled inputs (MDApplication.cpp:221-235)."""
+    sd = synth.spce_water(n_mol=8)
+    path = synth.write_rbmd_input(sd, str(tmp_path))
+    cfg = json.load(open(path))
+    cfg["outputs"].update(
+        msd_out={"interval": 10, "start_step": 0, "end_step": 10000},
+        vacf_out={"start_step": 5, "end_step": 50},
+        rdf_out={"interval": 10, "radius": 10, "dr": 0.1, "statistics_rdf_steps": 1000, "atoms_pair": [[0, 0], [0, 1]]})
+    json.dump(cfg, open(path, "w"))
+    o = dump(rbmd_bin, path, tmp_path)["outputs"]
+    assert o["msd"] == {"interval": 10, "start_step": 0, "end_step": 10000}
+    assert o["vacf"] == {"interval": 1, "start_step": 5, "end_step": 50}
+    assert o["rdf"] == {"radius": 10, "dr": 0.1, "statistics_rdf_steps": 1000, "atoms_pair": [[0, 0], [0, 1]]}
+
+
+@pytest.mark.parametrize("outputs,message", [
+    ({"msd_out": {"interval": 10, "end_step": 100}}, "start_step"),
+    ({"rdf_out": {"radius": 10, "dr": 0.1, "statistics_rdf_steps": 10}}, "atoms_pair"),
+    ({"rdf_out": {"radius": 10, "dr": 0.1, "statistics_rdf_steps": 10, "atoms_pair": [[0, 2]]}}, "out of range"),
+    ({"rdf_out": {"radius": 10, "dr": 0.1, "statistics_rdf_steps": 10, "atoms_pair": [0, 1]}}, "atoms_pair"),
+    ({"rdf_out": {"radius": 0.05, "dr": 0.1, "statistics_rdf_steps": 10, "atoms_pair": [[0, 1]]}}, "radius"),
+])
+def test_observable_output_errors(rbmd_bin, tmp_path, outputs, message):
+    sd = synth.spce_water(n_mol=8)
+    path = synth.write_rbmd_input(sd, str(tmp_path))
+    cfg = json.load(open(path))
+    cfg["outputs"].update(outputs)
+    json.dump(cfg, open(path, "w"))
+    r = subprocess.run([rbmd_bin, "-j", path, "--dump-system", str(tmp_path / "d.json")], capture_output=True,
+                       text=True)
+    assert r.returncode == 1 and message in r.stderr, r.stderr

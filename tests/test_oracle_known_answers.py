@@ -384,3 +384,103 @@ def test_harmonic_dihedral_closed_form(oracle_mod, sign, mult):
                 energies.append(oq.thermo()["e_dihedral"])
             assert f[a, k] == pytest.approx(-(energies[0] - energies[1]) / (2 * h), rel=1e-5, abs=1e-7)
     assert np.abs(f.sum(0)).max() < 1e-12  # no net force
+
+
+# ------------------------------------------------------------------ trajectory observables
+def _radii(radius, dr):
+    """RDFOutput.cpp:42-53: (int)(radius / dr) values, dr added once per bin."""
+    out, r = [], 0.0
+    for _ in range(int(radius / dr)):
+        r += dr
+        out.append(r)
+    return np.array(out)
+
+
+@pytest.mark.parametrize("radius,dr", [(10.0, 0.1), (2.5, 0.01), (1.0, 0.3), (3.0, 3.0)])
+def test_rdf_bins_accumulate(oracle_mod, radius, dr):
+    r = oracle_mod.rdf_bins(radius, dr)
+    assert np.array_equal(r, _radii(radius, dr))
+    with pytest.raises(ValueError):
+        oracle_mod.rdf_bins(0.05, 0.1)
+
+
+def test_rdf_counts_simple_cubic_shells(oracle_mod):
+    """Known answer: a simple cubic lattice of spacing a in a periodic box of 4 a has, around every
+    atom, 6 / 12 / 8 / 6 / 24 / 24 images at a sqrt(1..6); a bin counts a shell when
+    r_b < a sqrt(m) < 1.01 r_b.  a = 1.003 keeps every shell away from the bin edges."""
+    a, m = 1.003, 4
+    g = np.arange(m) * a + 0.5 * a
+    x = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    n = x.shape[0]
+    radius, dr = 2.5, 0.01
+    r = _radii(radius, dr)
+    counts = oracle_mod.rdf_counts(x, np.arange(n), [m * a] * 3, np.arange(n), np.arange(n), radius, dr)
+    expect = np.zeros(r.size, np.int64)
+    for mm, z in ((1, 6), (2, 12), (3, 8), (4, 6), (5, 24), (6, 24)):
+        d = a * math.sqrt(mm)
+        expect[(r < d) & (d < r + r * 0.01)] += n * z
+    assert counts.sum() > 0 and np.array_equal(counts, expect)
+
+
+def _rdf_numpy(x, mol, L, centers, targets, radius, dr, exclude):
+    """Independent restatement (vectorised over pairs, images -2..2) of the RDF pair count."""
+    r = _radii(radius, dr)
+    u = r + r * 0.01
+    R = u[-1]
+    counts = np.zeros(r.size, np.int64)
+    xc, xt = x[centers], x[targets]
+    base = xt[None, :, :] - xc[:, None, :]
+    keep = np.ones((len(centers), len(targets)), bool)
+    if exclude:
+        keep = mol[centers][:, None] != mol[targets][None, :]
+    for nx in range(-2, 3):
+        for ny in range(-2, 3):
+            for nz in range(-2, 3):
+                d = base + np.array([nx * L[0], ny * L[1], nz * L[2]])
+                inside = keep & (np.abs(d) < R).all(-1)
+                dis = np.sqrt(d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1] + d[..., 2] * d[..., 2])[inside]
+                counts += ((dis[:, None] > r[None, :]) & (dis[:, None] < u[None, :])).sum(0)
+    return counts
+
+
+@pytest.mark.parametrize("exclude", [True, False])
+def test_rdf_counts_match_independent_count(oracle_mod, exclude):
+    rng = np.random.default_rng(7)
+    n = 120
+    L = np.array([6.0, 7.0, 5.5])
+    x = rng.uniform(0, 1, (n, 3)) * L
+    mol = np.repeat(np.arange(n // 3), 3)
+    types = rng.integers(0, 2, n)
+    c, t = np.flatnonzero(types == 0), np.flatnonzero(types == 1)
+    got = oracle_mod.rdf_counts(x, mol, L, c, t, 3.0, 0.05, exclude)
+    assert np.array_equal(got, _rdf_numpy(x, mol, L, c, t, 3.0, 0.05, exclude))
+    # a radius beyond half the box reaches more than one image of a pair
+    got = oracle_mod.rdf_counts(x, mol, L, c, t, 4.5, 0.1, exclude)
+    assert np.array_equal(got, _rdf_numpy(x, mol, L, c, t, 4.5, 0.1, exclude))
+
+
+def test_rdf_ideal_gas_is_flat(oracle_mod):
+    """Uniform random points: the normalised RDF (OutPutWorklet.cpp:303-306) averages to 1."""
+    from rbmd_b200 import rdf_snapshot
+    rng = np.random.default_rng(3)
+    n, Lb = 400, 8.0
+    x = rng.uniform(0, Lb, (n, 3))
+    ids = np.arange(n)
+    radius, dr = 3.5, 0.05
+    counts = oracle_mod.rdf_counts(x, ids, [Lb] * 3, ids, ids, radius, dr, True)
+    g = rdf_snapshot(counts, _radii(radius, dr), n, n, Lb ** 3)
+    assert abs(g[20:].mean() - 1.0) < 0.03
+
+
+def test_msd_vacf_match_numpy(oracle_mod):
+    rng = np.random.default_rng(5)
+    n = 64
+    L = np.array([4.0, 5.0, 6.0])
+    x0, x = rng.uniform(0, 1, (n, 3)) * L, rng.uniform(0, 1, (n, 3)) * L
+    img0, img = rng.integers(-2, 3, (n, 3)), rng.integers(-2, 3, (n, 3))
+    v0, v = rng.normal(size=(n, 3)), rng.normal(size=(n, 3))
+    msd, vacf = oracle_mod.msd_vacf(x0, img0, v0, x, img, v, L)
+    d = x + (img - img0) * L - x0
+    assert np.allclose(msd, [*(d ** 2).mean(0), (d ** 2).sum(1).mean()], rtol=1e-13)
+    w = v0 * v
+    assert np.allclose(vacf, [*w.mean(0), w.sum(1).mean()], rtol=1e-13)
