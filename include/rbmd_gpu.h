@@ -364,6 +364,22 @@ int rbmd_rdf_counts(rbmd_ctx* ctx, int32_t sys_id, const int32_t* centers, int32
                     const int32_t* targets, int32_t n_targets, double radius, double dr,
                     int32_t exclude_same_molecule, int64_t* counts, double* volume);
 
+/* ---------------------------------------------------------------- asynchronous state snapshots */
+/* Outputs that must not stall the step pipeline (trajectory, checkpoints, progress of a served
+ * system).  rbmd_snapshot_begin packs the state of one system as of the work queued so far on the
+ * device and copies it to pinned host staging on a second stream while later steps run; it
+ * returns at once with a ticket.  rbmd_snapshot_wait blocks until that copy has landed, then fills
+ * the destinations given at begin (each may be NULL): x, v [3 n_atoms], image [3 n_atoms],
+ * box [6] (lo x y z, hi x y z: the current box, NPT included) and step.  The destinations must
+ * stay valid until the wait returns RBMD_OK.  timeout_s < 0 waits without limit; on
+ * RBMD_ERR_TIMEOUT the ticket stays pending.  rbmd_snapshot_poll sets *done (1: a wait will not
+ * block) without blocking.  One waiter per ticket.  No counterpart in the reference (its outputs
+ * read the fields synchronously, framework/output/TrajectoryOutput.cpp:45-85). */
+int rbmd_snapshot_begin(rbmd_ctx* ctx, int32_t sys_id, double* x, double* v, int32_t* image,
+                        double* box, int64_t* step, int64_t* ticket);
+int rbmd_snapshot_poll(rbmd_ctx* ctx, int64_t ticket, int32_t* done);
+int rbmd_snapshot_wait(rbmd_ctx* ctx, int64_t ticket, double timeout_s);
+
 /* ---------------------------------------------------------------- EAM input helpers (host only) */
 /* funcfl file contents after the header lines (ExecutionNVT::ReadPotentialFile,
  * framework/run/ExecutionNVT.cpp:899-931). */

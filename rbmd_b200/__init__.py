@@ -206,6 +206,19 @@ class Context:
                                           C.byref(vol)))
         return counts, vol.value
 
+    # ---- asynchronous snapshots
+    def snapshot_begin(self, sid):
+        """Queue a snapshot of the system's state as of the work queued so far; returns a Snapshot
+        whose wait() gives (x, v, image, box, step) once the copy has landed (later steps keep
+        running meanwhile)."""
+        n = self._sizes[sid][0]
+        snap = Snapshot(self, n)
+        t = C.c_int64()
+        self._check(lib().rbmd_snapshot_begin(self.h, sid, _dp(snap.x), _dp(snap.v), _ip(snap.image),
+                                              _dp(snap.box), snap.step.ctypes.data_as(A.lptr), C.byref(t)))
+        snap.ticket = t.value
+        return snap
+
     # ---- diagnostics
     def launch_count(self):
         v = C.c_int64()
@@ -276,6 +289,27 @@ class Context:
 
     def serve_stop(self):
         self._check(lib().rbmd_serve_stop(self.h))
+
+
+class Snapshot:
+    """Pending rbmd_snapshot_begin: the destination arrays live here until the wait returns."""
+
+    def __init__(self, ctx, n):
+        self.ctx = ctx
+        self.x, self.v = np.zeros((n, 3)), np.zeros((n, 3))
+        self.image = np.zeros((n, 3), np.int32)
+        self.box = np.zeros(6)
+        self.step = np.zeros(1, np.int64)
+        self.ticket = None
+
+    def done(self):
+        d = C.c_int32()
+        self.ctx._check(lib().rbmd_snapshot_poll(self.ctx.h, self.ticket, C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, timeout=-1.0):
+        self.ctx._check(lib().rbmd_snapshot_wait(self.ctx.h, self.ticket, float(timeout)))
+        return self.x, self.v, self.image, self.box.reshape(2, 3), int(self.step[0])
 
 
 def rdf_bins(radius, dr):

@@ -225,6 +225,9 @@ def declare(lib, prefix="rbmd"):
         "observe_reset": ([ctx, C.c_int32, C.c_int32], C.c_int),
         "observe": ([ctx, C.c_int32, dptr, dptr], C.c_int),
         "rdf_bins": ([C.c_double, C.c_double, dptr, C.c_int32, iptr], C.c_int),
+        "snapshot_begin": ([ctx, C.c_int32, dptr, dptr, iptr, dptr, lptr, lptr], C.c_int),
+        "snapshot_poll": ([ctx, C.c_int64, iptr], C.c_int),
+        "snapshot_wait": ([ctx, C.c_int64, C.c_double], C.c_int),
         "rdf_counts": ([ctx, C.c_int32, iptr, C.c_int32, iptr, C.c_int32, C.c_double, C.c_double, C.c_int32,
                         lptr, dptr], C.c_int),
     }
@@ -246,4 +249,5 @@ HEADER_FUNCTIONS = [
     "rbmd_serve_result", "rbmd_serve_stop", "rbmd_launch_count", "rbmd_profile_enable",
     "rbmd_profile_get", "rbmd_step_timed", "rbmd_fma_peak", "rbmd_autotune",
     "rbmd_observe_reset", "rbmd_observe", "rbmd_rdf_bins", "rbmd_rdf_counts",
+    "rbmd_snapshot_begin", "rbmd_snapshot_poll", "rbmd_snapshot_wait",
 ]

@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xptxas", "-warn-spills", "-diag-suppress", "128", "-I", os.path.join(ROOT, "include")] + ARCH
 CU_SOURCES = ["k_cells.cu", "k_pair.cu", "k_kspace.cu", "k_integrate.cu", "k_baro.cu", "k_diag.cu", "k_observe.cu", "engine.cu"]
-CPP_SOURCES = ["capi.cpp", "serve.cpp", "tune.cpp", "observe.cpp"]
+CPP_SOURCES = ["capi.cpp", "serve.cpp", "tune.cpp", "observe.cpp", "snapshot.cpp"]
 
 
 def nvcc():

@@ -210,6 +210,26 @@ int rbmd_rdf_counts(rbmd_ctx* ctx, int32_t id, const int32_t* centers, int32_t n
   return ctx->c->rdf_counts(id, centers, nc, targets, nt, radius, dr, exclude_same_molecule, counts, volume);
 }
 
+int rbmd_snapshot_begin(rbmd_ctx* ctx, int32_t id, double* x, double* v, int32_t* image, double* box, int64_t* step,
+                        int64_t* ticket) {
+  CTX_CHECK(ctx);
+  return ctx->c->snapshot_begin(id, x, v, image, box, step, ticket);
+}
+
+int rbmd_snapshot_poll(rbmd_ctx* ctx, int64_t ticket, int32_t* done) {
+  CTX_CHECK(ctx);
+  if (!done) return RBMD_ERR_ARG;
+  int d = 0;
+  const int rc = ctx->c->snapshot_poll(ticket, &d);
+  *done = d;
+  return rc;
+}
+
+int rbmd_snapshot_wait(rbmd_ctx* ctx, int64_t ticket, double timeout_s) {
+  CTX_CHECK(ctx);
+  return ctx->c->snapshot_wait(ticket, timeout_s);
+}
+
 // ------------------------------------------------------------------ EAM input (host)
 int rbmd_eam_read_funcfl(const char* path, rbmd_eam_file* out, double* frho, double* zr, double* rhor) {
   // ExecutionNVT::ReadPotentialFile, framework/run/ExecutionNVT.cpp:899-931: two comment lines,

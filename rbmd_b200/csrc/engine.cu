@@ -151,6 +151,7 @@ void Context::dfree(void* p) {
 
 Context::~Context() {
   cudaStreamSynchronize(stream);
+  snapshots_release();
   for (auto& kv : batch_cache_) {
     if (kv.second->graph) cudaGraphExecDestroy(kv.second->graph);
     for (void* p : kv.second->allocs) dfree(p);

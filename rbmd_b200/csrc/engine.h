@@ -86,6 +86,9 @@ class Context {
   int observe(int id, double* msd, double* vacf);
   int rdf_counts(int id, const int32_t* centers, int nc, const int32_t* targets, int nt, double radius, double dr,
                  int exclude_same_molecule, int64_t* counts, double* volume);
+  int snapshot_begin(int id, double* x, double* v, int32_t* image, double* box, int64_t* step, int64_t* ticket);
+  int snapshot_poll(int64_t ticket, int* done);
+  int snapshot_wait(int64_t ticket, double timeout_s);
 
   int fail(int code, const std::string& msg);
   std::string last_error;
@@ -131,6 +134,25 @@ class Context {
   int next_id_ = 0;
   std::map<std::vector<int>, BatchRec*> batch_cache_;
   std::map<std::vector<int64_t>, int> tune_cache_;  // autotuner decisions by group signature
+  // asynchronous snapshots: packed on `stream`, copied to pinned staging on copy_stream_
+  struct Snap {
+    int n = 0;
+    double *x = nullptr, *v = nullptr, *box = nullptr;
+    int32_t* image = nullptr;
+    int64_t* step = nullptr;
+    void* dbuf = nullptr;
+    void* hbuf = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t done = nullptr;
+  };
+  std::map<int64_t, Snap> snaps_;
+  int64_t next_ticket_ = 1;
+  cudaStream_t copy_stream_ = nullptr;
+  std::vector<std::pair<size_t, void*>> pinned_free_;  // pinned staging kept for reuse
+  void* pinned_get(size_t bytes, size_t* got);
+  void pinned_put(void* p, size_t bytes);
+  void snapshot_finish(int64_t ticket);
+  void snapshots_release();
 };
 
 }  // namespace rbmd

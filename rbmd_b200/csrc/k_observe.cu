@@ -215,3 +215,48 @@ void launch_rdf_count(const SysDev* sys, int slot, const int* centers, int nc, c
 }
 
 }  // namespace rbmd
+
+namespace rbmd {
+
+// ------------------------------------------------------------------------- asynchronous snapshot
+// Packs one system's state for a snapshot copied to the host while later steps run: step, box
+// (lo xyz, hi xyz), positions and velocities [3n] and image counters [3n], in that order.
+__global__ void k_snapshot_pack(const SysDev* __restrict__ sys, int slot, char* __restrict__ out) {
+  const SysDev& D = sys[slot];
+  const int n = D.n;
+  auto* step = (long long*)out;
+  auto* box = (double*)(out + 8);
+  auto* x = box + 6;
+  auto* v = x + 3 * (size_t)n;
+  auto* image = (int*)(v + 3 * (size_t)n);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid == 0) {
+    *step = (long long)D.st->step;
+    for (int k = 0; k < 3; ++k) {
+      box[k] = D.lo[k];
+      box[3 + k] = D.hi[k];
+    }
+  }
+  for (int i = tid; i < n; i += gridDim.x * blockDim.x) {
+    const double4 p = D.x[i], u = D.v[i];
+    x[3 * i] = p.x;
+    x[3 * i + 1] = p.y;
+    x[3 * i + 2] = p.z;
+    v[3 * i] = u.x;
+    v[3 * i + 1] = u.y;
+    v[3 * i + 2] = u.z;
+    image[3 * i] = D.image[3 * i];
+    image[3 * i + 1] = D.image[3 * i + 1];
+    image[3 * i + 2] = D.image[3 * i + 2];
+  }
+}
+
+size_t snapshot_bytes(int n) { return 56 + 60 * (size_t)n; }
+
+void launch_snapshot_pack(const SysDev* sys, int slot, int n, void* out, cudaStream_t s) {
+  const int blocks = obs_blocks(n);
+  k_snapshot_pack<<<blocks, kObsThreads, 0, s>>>(sys, slot, (char*)out);
+  note_launch();
+}
+
+}  // namespace rbmd

@@ -92,6 +92,11 @@ void launch_rdf_count(const SysDev* sys, int slot, const int* centers, int nc, c
                       const double* radii, const double* upper, int nb, double dr, int exclude_mol,
                       unsigned long long* counts, cudaStream_t s);
 
+// Asynchronous snapshot: packed layout step (8 B), box lo / hi (6 doubles), x, v [3n] doubles,
+// image [3n] ints; snapshot_bytes(n) in all.
+size_t snapshot_bytes(int n);
+void launch_snapshot_pack(const SysDev* sys, int slot, int n, void* out, cudaStream_t s);
+
 constexpr int kCellWarpsHost = 4;  // home cells per block of the tile pair kernel
 constexpr double kTileMinPerCell = 3.0;  // mean atoms per cell from which the tile kernel is used
 

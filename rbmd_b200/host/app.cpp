@@ -114,6 +114,7 @@ ModelFileInitCondition::ModelFileInitCondition(const Json& cfg, const std::strin
 void ModelFileInitCondition::Execute(Para& p) {
   const DataFile d = read_data_file(_file, _atom_style, p.unit);
   p.init_way = "read_data";
+  p.atom_style = _atom_style;
   p.n = d.n_atoms;
   p.n_types = d.n_types;
   for (int k = 0; k < 3; ++k) {
@@ -244,6 +245,24 @@ void ExecutionMD::State(std::vector<double>& x, std::vector<double>& v, std::vec
 
 void ExecutionNVT::Execute() { check(rbmd_step(_ctx, &_sys, 1, 1), "rbmd_step"); }
 
+int64_t ExecutionMD::SnapshotBegin(StateSnapshot& s) {
+  s.x.resize(3 * (size_t)_para.n);
+  s.v.resize(3 * (size_t)_para.n);
+  s.image.resize(3 * (size_t)_para.n);
+  int64_t t = 0;
+  check(rbmd_snapshot_begin(_ctx, _sys, s.x.data(), s.v.data(), s.image.data(), s.box, &s.step, &t),
+        "rbmd_snapshot_begin");
+  return t;
+}
+
+bool ExecutionMD::SnapshotDone(int64_t ticket) {
+  int32_t done = 0;
+  check(rbmd_snapshot_poll(_ctx, ticket, &done), "rbmd_snapshot_poll");
+  return done != 0;
+}
+
+void ExecutionMD::SnapshotWait(int64_t ticket) { check(rbmd_snapshot_wait(_ctx, ticket, -1.0), "rbmd_snapshot_wait"); }
+
 void ExecutionMD::ObserveReset(int which) { check(rbmd_observe_reset(_ctx, _sys, which), "rbmd_observe_reset"); }
 
 void ExecutionMD::Observe(double* msd, double* vacf) { check(rbmd_observe(_ctx, _sys, msd, vacf), "rbmd_observe"); }
@@ -261,23 +280,30 @@ double ExecutionMD::RdfCounts(const std::vector<int>& centers, const std::vector
 }
 
 // ------------------------------------------------------------------------------------- outputs
-ThermoOutput::ThermoOutput(int interval, const std::string& path, bool console)
+ThermoOutput::ThermoOutput(int interval, const std::string& path, const std::string& temp_path, bool console)
     : _interval(std::max(1, interval)), _console(console) {
   _file = std::fopen(path.c_str(), "w");
   if (!_file) throw std::runtime_error("cannot write " + path);
+  _temp = std::fopen(temp_path.c_str(), "w");
+  if (!_temp) throw std::runtime_error("cannot write " + temp_path);
 }
 
 ThermoOutput::~ThermoOutput() {
   if (_file) std::fclose(_file);
+  if (_temp) std::fclose(_temp);
 }
 
 void ThermoOutput::Execute(Executioner& ex) {
   const int64_t step = ex.CurrentStep();
-  if (step == 0)
+  if (step == 0) {
     std::fprintf(_file, "Step Time VanderWaalsEnergy NearCoulombicEnergy FarCoulombicEnergy KinticEnergy "
                         "PotentialEnergy TotalEnergy BondEnergy AngleEnergy DihedralEnergy Temperature Pressure\n");
+    std::fprintf(_temp, "Step Temperature Pressure\n");
+  }
   if (step % _interval != 0 && step != ex.NumStep()) return;
   const rbmd_thermo t = ex.Run().Thermo();
+  std::fprintf(_temp, "%lld %g %g\n", (long long)step, t.temperature, t.pressure);
+  std::fflush(_temp);
   const double vdw = t.e_lj + t.e_eam;
   std::fprintf(_file, "%lld %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g %.10g\n",
                (long long)step, ex.CurrentTime(), vdw, t.e_coul_near, t.e_coul_far, t.kinetic_energy,
@@ -289,7 +315,29 @@ void ThermoOutput::Execute(Executioner& ex) {
   if (t.status) throw std::runtime_error("device status word " + std::to_string(t.status) + " at step " + std::to_string(step));
 }
 
-TrajectoryOutput::TrajectoryOutput(int interval, const std::string& path) : _interval(std::max(1, interval)) {
+void SnapshotOutput::Execute(Executioner& ex) {
+  // write every snapshot that has landed, oldest first; make room when too many are in flight
+  while (!_pending.empty() && (ex.Run().SnapshotDone(_pending.front()->ticket) || _pending.size() >= kInFlight)) {
+    ex.Run().SnapshotWait(_pending.front()->ticket);
+    Write(*_pending.front());
+    _pending.erase(_pending.begin());
+  }
+  if (!ShouldOutput(ex)) return;
+  auto s = std::make_unique<StateSnapshot>();
+  s->ticket = ex.Run().SnapshotBegin(*s);
+  _pending.push_back(std::move(s));
+}
+
+void SnapshotOutput::Finish(Executioner& ex) {
+  for (auto& s : _pending) {
+    ex.Run().SnapshotWait(s->ticket);
+    Write(*s);
+  }
+  _pending.clear();
+}
+
+TrajectoryOutput::TrajectoryOutput(const Para& para, int interval, const std::string& path)
+    : _para(para), _interval(std::max(1, interval)) {
   _file = std::fopen(path.c_str(), "w");
   if (!_file) throw std::runtime_error("cannot write " + path);
 }
@@ -298,18 +346,100 @@ TrajectoryOutput::~TrajectoryOutput() {
   if (_file) std::fclose(_file);
 }
 
-void TrajectoryOutput::Execute(Executioner& ex) {
-  const int64_t step = ex.CurrentStep();
-  if (step % _interval != 0 && step != ex.NumStep()) return;
-  std::vector<double> x, v;
-  std::vector<int> img;
-  ex.Run().State(x, v, img);
-  const size_t n = x.size() / 3;
-  std::fprintf(_file, "step %lld atoms %zu\n", (long long)step, n);
+bool TrajectoryOutput::ShouldOutput(const Executioner& ex) const {
+  return ex.CurrentStep() >= 1 && ex.CurrentStep() % _interval == 0;
+}
+
+void TrajectoryOutput::Write(const StateSnapshot& s) {
+  const size_t n = s.x.size() / 3;
+  std::fprintf(_file, "ITEM: TIMESTEP\n%lld\nITEM: NUMBER OF ATOMS\n%zu\nITEM: BOX BOUNDS pp pp pp\n", (long long)s.step, n);
+  for (int k = 0; k < 3; ++k) std::fprintf(_file, "%g %g\n", s.box[k], s.box[3 + k]);
+  std::fprintf(_file, "ITEM: ATOMS id type x y z\n");
   for (size_t i = 0; i < n; ++i)
-    std::fprintf(_file, "%zu %.10g %.10g %.10g %d %d %d\n", i + 1, x[3 * i], x[3 * i + 1], x[3 * i + 2], img[3 * i],
-                 img[3 * i + 1], img[3 * i + 2]);
+    std::fprintf(_file, "%zu %d %g %g %g\n", i + 1, _para.type[i] + 1, s.x[3 * i], s.x[3 * i + 1], s.x[3 * i + 2]);
   std::fflush(_file);
+}
+
+CheckpointOutput::CheckpointOutput(const Para& para, int interval, const std::string& path)
+    : _para(para), _interval(std::max(1, interval)), _path(path) {}
+
+bool CheckpointOutput::ShouldOutput(const Executioner& ex) const {
+  return ex.CurrentStep() >= 1 && (ex.CurrentStep() % _interval == 0 || ex.CurrentStep() == ex.NumStep());
+}
+
+void CheckpointOutput::Write(const StateSnapshot& s) {
+  // written beside the previous checkpoint and renamed over it, so a crash never leaves half a file
+  const Para& p = _para;
+  const std::string tmp = _path + ".tmp";
+  FILE* f = std::fopen(tmp.c_str(), "w");
+  if (!f) throw std::runtime_error("cannot write " + tmp);
+  const int nb = (int)p.bond_type.size(), na = (int)p.angle_type.size(), nd = (int)p.dihedral_type.size();
+  std::fprintf(f, "LAMMPS data file: rbmd checkpoint at step %lld (atom_style %s)\n\n", (long long)s.step,
+               p.atom_style.c_str());
+  std::fprintf(f, "%d atoms\n%d atom types\n", p.n, p.n_types);
+  if (nb) std::fprintf(f, "%d bonds\n%zu bond types\n", nb, p.bond_k.size());
+  if (na) std::fprintf(f, "%d angles\n%zu angle types\n", na, p.angle_k.size());
+  if (nd) std::fprintf(f, "%d dihedrals\n%zu dihedral types\n", nd, p.dihedral_k.size());
+  const char* ax = "xyz";
+  std::fprintf(f, "\n");
+  for (int k = 0; k < 3; ++k) std::fprintf(f, "%.17g %.17g %clo %chi\n", s.box[k], s.box[3 + k], ax[k], ax[k]);
+  std::vector<double> tmass(p.n_types, 1.0);
+  for (int i = p.n - 1; i >= 0; --i) tmass[p.type[i]] = p.mass[i];
+  std::fprintf(f, "\nMasses\n\n");
+  for (int t = 0; t < p.n_types; ++t) std::fprintf(f, "%d %.17g\n", t + 1, tmass[t]);
+  std::fprintf(f, "\nPair Coeffs # lj/cut\n\n");
+  for (int t = 0; t < p.n_types; ++t) std::fprintf(f, "%d %.17g %.17g\n", t + 1, p.eps[t], p.sigma[t]);
+  if (nb) {
+    std::fprintf(f, "\nBond Coeffs # harmonic\n\n");
+    for (size_t t = 0; t < p.bond_k.size(); ++t) std::fprintf(f, "%zu %.17g %.17g\n", t + 1, p.bond_k[t], p.bond_r0[t]);
+  }
+  if (na) {
+    std::fprintf(f, "\nAngle Coeffs # harmonic\n\n");
+    for (size_t t = 0; t < p.angle_k.size(); ++t)
+      std::fprintf(f, "%zu %.17g %.17g\n", t + 1, p.angle_k[t], p.angle_theta0[t]);
+  }
+  if (nd) {
+    std::fprintf(f, "\nDihedral Coeffs # harmonic\n\n");
+    for (size_t t = 0; t < p.dihedral_k.size(); ++t)
+      std::fprintf(f, "%zu %.17g %d %d\n", t + 1, p.dihedral_k[t], p.dihedral_sign[t], p.dihedral_multiplicity[t]);
+  }
+  std::fprintf(f, "\nAtoms # %s\n\n", p.atom_style.c_str());
+  for (int i = 0; i < p.n; ++i) {
+    const double* x = &s.x[3 * (size_t)i];
+    const int* im = &s.image[3 * (size_t)i];
+    const double q = p.charge.empty() ? 0.0 : p.charge[i];
+    if (p.atom_style == "full")
+      std::fprintf(f, "%d %d %d %.17g %.17g %.17g %.17g %d %d %d\n", i + 1, (p.molecule.empty() ? i : p.molecule[i]) + 1,
+                   p.type[i] + 1, q, x[0], x[1], x[2], im[0], im[1], im[2]);
+    else if (p.atom_style == "charge")
+      std::fprintf(f, "%d %d %.17g %.17g %.17g %.17g %d %d %d\n", i + 1, p.type[i] + 1, q, x[0], x[1], x[2], im[0], im[1],
+                   im[2]);
+    else
+      std::fprintf(f, "%d %d %.17g %.17g %.17g %d %d %d\n", i + 1, p.type[i] + 1, x[0], x[1], x[2], im[0], im[1], im[2]);
+  }
+  std::fprintf(f, "\nVelocities\n\n");
+  for (int i = 0; i < p.n; ++i)
+    std::fprintf(f, "%d %.17g %.17g %.17g\n", i + 1, s.v[3 * (size_t)i], s.v[3 * (size_t)i + 1], s.v[3 * (size_t)i + 2]);
+  if (nb) {
+    std::fprintf(f, "\nBonds\n\n");
+    for (int b = 0; b < nb; ++b)
+      std::fprintf(f, "%d %d %d %d\n", b + 1, p.bond_type[b] + 1, p.bond_atoms[2 * b] + 1, p.bond_atoms[2 * b + 1] + 1);
+  }
+  if (na) {
+    std::fprintf(f, "\nAngles\n\n");
+    for (int a = 0; a < na; ++a)
+      std::fprintf(f, "%d %d %d %d %d\n", a + 1, p.angle_type[a] + 1, p.angle_atoms[3 * a] + 1, p.angle_atoms[3 * a + 1] + 1,
+                   p.angle_atoms[3 * a + 2] + 1);
+  }
+  if (nd) {
+    std::fprintf(f, "\nDihedrals\n\n");
+    for (int d = 0; d < nd; ++d)
+      std::fprintf(f, "%d %d %d %d %d %d\n", d + 1, p.dihedral_type[d] + 1, p.dihedral_atoms[4 * d] + 1,
+                   p.dihedral_atoms[4 * d + 1] + 1, p.dihedral_atoms[4 * d + 2] + 1, p.dihedral_atoms[4 * d + 3] + 1);
+  }
+  const bool ok = std::fflush(f) == 0;
+  std::fclose(f);
+  if (!ok || std::rename(tmp.c_str(), _path.c_str()) != 0) throw std::runtime_error("cannot write " + _path);
 }
 
 CorrelationOutput::CorrelationOutput(bool vacf, int interval, int64_t start_step, int64_t end_step,
@@ -440,6 +570,7 @@ void Executioner::Execute() {
     PreStep();
     TakeStep();
   }
+  for (auto& o : _outputs) o->Finish(*this);
 }
 
 // --------------------------------------------------------------------------------- application
@@ -653,7 +784,11 @@ void MDApplication::CreateActions() {
   }
   if (const Json* outs = _cfg.find("outputs")) {
     if (const Json* th = outs->find("thermo_out")) _thermo_interval = (int)th->number("interval", 1);
-    if (const Json* tr = outs->find("trajectory_out")) _traj_interval = (int)tr->number("interval", 100);
+    if (const Json* tr = outs->find("trajectory_out")) _traj_interval = (int)tr->number("interval", 1);
+    if (const Json* cp = outs->find("checkpoint_out")) {
+      _checkpoint_interval = (int)cp->number("interval", 1000);
+      _checkpoint_file = cp->string("file", _checkpoint_file);
+    }
     // msd_out / vacf_out: interval (default 1), start_step and end_step (required);
     // rdf_out: radius, dr, statistics_rdf_steps, atoms_pair (read_data) (MDApplication.cpp:221-235)
     auto need = [](const Json* o, const char* out, const char* key) {
@@ -754,8 +889,9 @@ void MDApplication::DumpSystem(const std::string& path) const {
   darr("special_weights", _para.sp_w);
   std::fprintf(f, "\"eam\": {\"nrho\": %d, \"nr\": %d, \"drho\": %.17g, \"dr\": %.17g, \"rhomax\": %.17g, \"cut\": %.17g},\n",
                _para.eam_nrho, _para.eam_nr, _para.eam_drho, _para.eam_dr, _para.eam_rhomax, _para.eam_cut);
-  std::fprintf(f, "\"outputs\": {\"thermo_interval\": %d, \"trajectory_interval\": %d", _thermo_interval,
-               _traj_interval);
+  std::fprintf(f, "\"outputs\": {\"thermo_interval\": %d, \"trajectory_interval\": %d, \"checkpoint_interval\": %d, "
+               "\"checkpoint_file\": \"%s\"", _thermo_interval, _traj_interval, _checkpoint_interval,
+               _checkpoint_file.c_str());
   for (const Correlation* c : {&_msd, &_vacf})
     if (c->on)
       std::fprintf(f, ", \"%s\": {\"interval\": %d, \"start_step\": %lld, \"end_step\": %lld}",
@@ -785,8 +921,11 @@ int MDApplication::Run() {
     }
     ExecutionNVT run(_para, _device);
     Executioner ex(run, _para.params.num_steps, _para.params.timestep);
-    if (_thermo_interval > 0) ex.AddOutput(std::unique_ptr<Output>(new ThermoOutput(_thermo_interval, "energy.rbmd", true)));
-    if (_traj_interval > 0) ex.AddOutput(std::unique_ptr<Output>(new TrajectoryOutput(_traj_interval, "trajectory.rbmd")));
+    if (_thermo_interval > 0)
+      ex.AddOutput(std::unique_ptr<Output>(new ThermoOutput(_thermo_interval, "energy.rbmd", "temperature.rbmd", true)));
+    if (_traj_interval > 0) ex.AddOutput(std::unique_ptr<Output>(new TrajectoryOutput(_para, _traj_interval, "rbmd.trj")));
+    if (_checkpoint_interval > 0)
+      ex.AddOutput(std::unique_ptr<Output>(new CheckpointOutput(_para, _checkpoint_interval, _checkpoint_file)));
     if (_rdf.on)
       ex.AddOutput(std::unique_ptr<Output>(
           new RDFOutput(_para, _rdf.radius, _rdf.dr, _rdf.statistics_steps, _rdf.pairs, "rdf.rbmd")));

@@ -28,6 +28,7 @@ namespace rbmd_host {
 struct Para {
   rbmd_params params{};
   std::string init_way;  // "read_data" or "inbuild"
+  std::string atom_style = "charge";  // of the data file read (inbuild: charge)
   std::string unit = "LJ";
   bool autotune = false;  // execution.autotune: time the pair layouts before the first step
   int n = 0, n_types = 0;
@@ -49,6 +50,15 @@ struct Para {
   std::vector<double> frho_spline, rhor_spline, z2r_spline;
 
   rbmd_system_desc desc() const;  // pointers into this object
+};
+
+// One rbmd_snapshot_begin in flight; heap-allocated so its buffers never move before the wait.
+struct StateSnapshot {
+  std::vector<double> x, v;
+  std::vector<int32_t> image;
+  double box[6] = {0, 0, 0, 0, 0, 0};
+  int64_t step = 0;
+  int64_t ticket = 0;
 };
 
 class InitCondition {
@@ -96,6 +106,9 @@ class ExecutionMD : public Execution {
   rbmd_thermo Thermo();
   void State(std::vector<double>& x, std::vector<double>& v, std::vector<int>& image);
   // trajectory observables (rbmd_observe_reset / rbmd_observe / rbmd_rdf_counts)
+  int64_t SnapshotBegin(StateSnapshot& s);
+  bool SnapshotDone(int64_t ticket);
+  void SnapshotWait(int64_t ticket);
   void ObserveReset(int which);
   void Observe(double* msd, double* vacf);
   double RdfCounts(const std::vector<int>& centers, const std::vector<int>& targets, double radius, double dr,
@@ -122,31 +135,72 @@ class Output {
  public:
   virtual ~Output() = default;
   virtual void Execute(Executioner& ex) = 0;
+  virtual void Finish(Executioner&) {}  // after the last step: complete pending work
+};
+
+// Outputs written from asynchronous snapshots: the state is queued for copy at the output step
+// and the file written once the copy has landed (at a later output call or at Finish), so the
+// steps in between are not held up.  At most kInFlight snapshots are pending.
+class SnapshotOutput : public Output {
+ public:
+  void Execute(Executioner& ex) override;
+  void Finish(Executioner& ex) override;
+
+ protected:
+  virtual bool ShouldOutput(const Executioner& ex) const = 0;
+  virtual void Write(const StateSnapshot& s) = 0;
+
+ private:
+  static constexpr size_t kInFlight = 4;
+  std::vector<std::unique_ptr<StateSnapshot>> _pending;
 };
 
 // energy.rbmd columns of output/ThermoOutput.cpp:223-291 plus temperature and pressure
 class ThermoOutput : public Output {
  public:
-  ThermoOutput(int interval, const std::string& path, bool console);
+  ThermoOutput(int interval, const std::string& path, const std::string& temp_path, bool console);
   ~ThermoOutput() override;
   void Execute(Executioner& ex) override;
 
  private:
   int _interval;
   FILE* _file = nullptr;
+  FILE* _temp = nullptr;  // temperature.rbmd (output/TempOutput.cpp:85-103): Step Temperature Pressure
   bool _console;
 };
 
-// positions every `interval` steps, one "step N" block of "id type x y z ix iy iz" lines
-class TrajectoryOutput : public Output {
+// rbmd.trj (output/TrajectoryOutput.cpp:33-85): a LAMMPS dump block ("ITEM: TIMESTEP" ... "ITEM:
+// ATOMS id type x y z") every `interval` steps from step 1.
+class TrajectoryOutput : public SnapshotOutput {
  public:
-  TrajectoryOutput(int interval, const std::string& path);
+  TrajectoryOutput(const Para& para, int interval, const std::string& path);
   ~TrajectoryOutput() override;
-  void Execute(Executioner& ex) override;
+
+ protected:
+  bool ShouldOutput(const Executioner& ex) const override;
+  void Write(const StateSnapshot& s) override;
 
  private:
+  const Para& _para;
   int _interval;
   FILE* _file = nullptr;
+};
+
+// A LAMMPS data file of the current state (positions with image flags, velocities, the topology
+// and coefficients the run was read with) every `interval` steps, replacing the previous one: the
+// checkpoint a read_data input restarts from.  The reference writes none.
+class CheckpointOutput : public SnapshotOutput {
+ public:
+  CheckpointOutput(const Para& para, int interval, const std::string& path);
+
+ protected:
+  bool ShouldOutput(const Executioner& ex) const override;
+  void Write(const StateSnapshot& s) override;
+
+ private:
+  const Para& _para;
+  int _interval;
+  std::string _path;
 };
 
 // msd.rbmd / vacf.rbmd (output/MSDOutput.cpp, output/VACFOutput.cpp): the reference configuration
@@ -244,7 +298,8 @@ class MDApplication : public Application {
   void DumpSystem(const std::string& path) const;
   Json _cfg;
   Para _para;
-  int _thermo_interval = 0, _traj_interval = 0;
+  int _thermo_interval = 0, _traj_interval = 0, _checkpoint_interval = 0;
+  std::string _checkpoint_file = "rbmd_checkpoint.data";
   struct Correlation {
     bool on = false;
     int interval = 1;

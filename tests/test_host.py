@@ -243,3 +243,15 @@ def test_observable_output_errors(rbmd_bin, tmp_path, outputs, message):
     r = subprocess.run([rbmd_bin, "-j", path, "--dump-system", str(tmp_path / "d.json")], capture_output=True,
                        text=True)
     assert r.returncode == 1 and message in r.stderr, r.stderr
+
+
+def test_checkpoint_and_trajectory_input(rbmd_bin, tmp_path):
+    """trajectory_out defaults to every step (TrajectoryOutput.cpp:36); checkpoint_out (no reference
+    counterpart) takes an interval and a file name."""
+    sd = synth.spce_water(n_mol=8)
+    path = synth.write_rbmd_input(sd, str(tmp_path))
+    cfg = json.load(open(path))
+    cfg["outputs"].update(trajectory_out={}, checkpoint_out={"interval": 50, "file": "x.data"})
+    json.dump(cfg, open(path, "w"))
+    o = dump(rbmd_bin, path, tmp_path)["outputs"]
+    assert o["trajectory_interval"] == 1 and o["checkpoint_interval"] == 50 and o["checkpoint_file"] == "x.data"
