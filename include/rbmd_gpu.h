@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBMD_ABI_VERSION 3
+#define RBMD_ABI_VERSION 4
 
 /* ---------------------------------------------------------------- status codes */
 enum rbmd_status {
@@ -195,6 +195,14 @@ typedef struct rbmd_system_desc {
   const double* dihedral_k;             /* [n_dihedral_types] K */
   const int32_t* dihedral_sign;         /* [n_dihedral_types] d: 1 (cos shift +1), else -1 */
   const int32_t* dihedral_multiplicity; /* [n_dihedral_types] n >= 0 */
+  /* EAM tables per atom type (setfl, LAMMPS eam/alloy; the reference reads funcfl only).  0: one
+   * table of each kind for every type (funcfl).  1: eam_frho_spline holds n_types embedding tables
+   * of (eam_nrho+1)*7 and eam_rhor_spline n_types density tables of (eam_nr+1)*7 (the density an
+   * atom of that type contributes to its neighbours), one after the other in type order, and
+   * eam_z2r_spline n_types (n_types+1)/2 pair tables of (eam_nr+1)*7 (r phi), the pair of types
+   * i >= j at index i (i+1)/2 + j. */
+  int32_t eam_per_type;
+  int32_t pad_eam;
 } rbmd_system_desc;
 
 /* ---------------------------------------------------------------- results */
@@ -398,6 +406,29 @@ int rbmd_eam_spline_sizes(const rbmd_eam_file* in, int32_t* nrho_out, int32_t* n
 int rbmd_eam_build_splines(const rbmd_eam_file* in, double* frho_spline, double* rhor_spline,
                            double* z2r_spline, int32_t* nrho_out, double* drho_out,
                            int32_t* nr_out, double* dr_out, double* rhomax_out);
+/* setfl file (LAMMPS eam/alloy format; the reference ships potentials/CuNi.eam.alloy but reads
+ * funcfl only): three comment lines; "n_elements name1 name2 ..."; "nrho drho nr dr cutoff"; per
+ * element a line "Z mass a lattice", F(rho) [nrho] and rho(r) [nr]; then r phi(r) [nr] for every
+ * element pair i >= j in the order (0,0), (1,0), (1,1), (2,0) ... */
+typedef struct rbmd_eam_setfl {
+  int32_t n_elements, nrho, nr, pad0;
+  double drho, dr, cut_off;
+} rbmd_eam_setfl;
+/* First call with every array NULL fills *out (sizes); the second fills names [n_elements * 16]
+ * chars (NUL-padded), mass [n_elements], frho [n_elements * nrho], rhor [n_elements * nr] and
+ * z2r [n_elements (n_elements + 1) / 2 * nr]. */
+int rbmd_eam_read_setfl(const char* path, rbmd_eam_setfl* out, char* names, double* mass, double* frho,
+                        double* rhor, double* z2r);
+/* Per-type spline tables of a setfl potential (eam_per_type = 1): type t takes element
+ * type_element[t].  The tables are splined on the file's own grid (nrho, drho, nr, dr; rhomax =
+ * (nrho - 1) drho) with the 7-coefficient rows of rbmd_eam_build_splines, as LAMMPS eam/alloy
+ * builds them (no resampling).  frho_spline needs n_types (nrho + 1) 7 doubles, rhor_spline
+ * n_types (nr + 1) 7, z2r_spline n_types (n_types + 1) / 2 (nr + 1) 7. */
+int rbmd_eam_build_setfl_splines(const rbmd_eam_setfl* in, const double* frho, const double* rhor,
+                                 const double* z2r, const int32_t* type_element, int32_t n_types,
+                                 double* frho_spline, double* rhor_spline, double* z2r_spline,
+                                 double* rhomax_out);
+
 /* Read a funcfl file: first call with arrays NULL to get nrho/nr, second call to fill. */
 int rbmd_eam_read_funcfl(const char* path, rbmd_eam_file* out_sizes, double* frho, double* zr,
                          double* rhor);

@@ -136,6 +136,14 @@ class System {
   int eam_nrho = 0, eam_nr = 0;
   double eam_drho = 0, eam_dr = 0, eam_rhomax = 0, eam_cut = 0;
   std::vector<double> frho_spline, rhor_spline, z2r_spline;
+  // setfl (LAMMPS eam/alloy): tables per type, z2r per type pair i >= j at i (i+1)/2 + j
+  int eam_per_type = 0;
+  const double* frho_of(int t) const { return &frho_spline[eam_per_type ? (size_t)t * 7 * (eam_nrho + 1) : 0]; }
+  const double* rhor_of(int t) const { return &rhor_spline[eam_per_type ? (size_t)t * 7 * (eam_nr + 1) : 0]; }
+  const double* z2r_of(int a, int b) const {
+    const int hi = a > b ? a : b, lo = a > b ? b : a;
+    return &z2r_spline[eam_per_type ? (size_t)(hi * (hi + 1) / 2 + lo) * 7 * (eam_nr + 1) : 0];
+  }
 
   rbmd_params p;
   Units u;
@@ -210,6 +218,12 @@ struct EamFile {
   std::vector<double> frho, zr, rhor;
 };
 bool read_funcfl(const std::string& path, EamFile& out);
+// setfl (LAMMPS eam/alloy PairEAMAlloy::file2array + array2spline): tables splined on the file's
+// grid, expanded to atom types (type t takes element type_element[t]); z2r per type pair i >= j at
+// i (i+1)/2 + j.  frho [ne][nrho], rhor [ne][nr], z2r [ne(ne+1)/2][nr] row-major.
+void build_setfl_splines(int ne, int nrho, double drho, int nr, double dr, const double* frho, const double* rhor,
+                         const double* z2r, const int* type_element, int n_types, std::vector<double>& frho_s,
+                         std::vector<double>& rhor_s, std::vector<double>& z2r_s, double& rhomax);
 void build_splines(const EamFile& in, std::vector<double>& frho_s, std::vector<double>& rhor_s,
                    std::vector<double>& z2r_s, int& nrho, double& drho, int& nr, double& dr,
                    double& rhomax);

@@ -199,6 +199,18 @@ int oracle_eam_read_funcfl(const char* path, int32_t* nrho, int32_t* nr, double*
   return 0;
 }
 
+int oracle_eam_build_setfl_splines(int32_t ne, int32_t nrho, double drho, int32_t nr, double dr, const double* frho,
+                                   const double* rhor, const double* z2r, const int32_t* type_element,
+                                   int32_t n_types, double* frho_s, double* rhor_s, double* z2r_s,
+                                   double* rhomax) {
+  std::vector<double> a, b, c;
+  oracle::build_setfl_splines(ne, nrho, drho, nr, dr, frho, rhor, z2r, type_element, n_types, a, b, c, *rhomax);
+  std::memcpy(frho_s, a.data(), sizeof(double) * a.size());
+  std::memcpy(rhor_s, b.data(), sizeof(double) * b.size());
+  std::memcpy(z2r_s, c.data(), sizeof(double) * c.size());
+  return 0;
+}
+
 int oracle_eam_build_splines(int32_t nrho_in, int32_t nr_in, double drho_in, double dr_in, double cut,
                              const double* frho, const double* zr, const double* rhor,
                              double* frho_s, double* rhor_s, double* z2r_s, int32_t* nrho,

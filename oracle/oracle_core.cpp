@@ -128,9 +128,11 @@ System::System(const rbmd_system_desc& d, const rbmd_params& prm) : p(prm) {
     eam_dr = d.eam_dr;
     eam_rhomax = d.eam_rhomax;
     eam_cut = d.eam_cut;
-    frho_spline.assign(d.eam_frho_spline, d.eam_frho_spline + 7 * (eam_nrho + 1));
-    rhor_spline.assign(d.eam_rhor_spline, d.eam_rhor_spline + 7 * (eam_nr + 1));
-    z2r_spline.assign(d.eam_z2r_spline, d.eam_z2r_spline + 7 * (eam_nr + 1));
+    eam_per_type = d.eam_per_type;
+    const size_t t = eam_per_type ? (size_t)d.n_types : 1, pairs = eam_per_type ? t * (t + 1) / 2 : 1;
+    frho_spline.assign(d.eam_frho_spline, d.eam_frho_spline + 7 * (eam_nrho + 1) * t);
+    rhor_spline.assign(d.eam_rhor_spline, d.eam_rhor_spline + 7 * (eam_nr + 1) * t);
+    z2r_spline.assign(d.eam_z2r_spline, d.eam_z2r_spline + 7 * (eam_nr + 1) * pairs);
   }
 
   // ---- derived parameters

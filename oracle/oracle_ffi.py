@@ -282,3 +282,27 @@ def rdf_counts(x, molecule, box_len, centers, targets, radius, dr, exclude_same_
     L.oracle_rdf_counts(_dp(x), _ip(mol), _dp(bl), _ip(c), c.size, _ip(t), t.size, float(radius), float(dr),
                         int(bool(exclude_same_molecule)), counts.ctypes.data_as(C.POINTER(C.c_int64)))
     return counts
+
+
+def setfl_splines(body, type_element):
+    """Per-type EAM tables of a setfl body, restated (checks rbmd_eam_build_setfl_splines)."""
+    L = lib()
+    P = C.POINTER
+    L.oracle_eam_build_setfl_splines.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_double,
+                                                 P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int32),
+                                                 C.c_int32, P(C.c_double), P(C.c_double), P(C.c_double),
+                                                 P(C.c_double)]
+    L.oracle_eam_build_setfl_splines.restype = C.c_int
+    te = np.ascontiguousarray(type_element, np.int32)
+    nt, nrho, nr = te.size, int(body["nrho"]), int(body["nr"])
+    fs, rs = np.zeros(7 * (nrho + 1) * nt), np.zeros(7 * (nr + 1) * nt)
+    zs = np.zeros(7 * (nr + 1) * nt * (nt + 1) // 2)
+    rhomax = np.zeros(1)
+    frho = np.ascontiguousarray(body["frho"], np.float64)
+    rhor = np.ascontiguousarray(body["rhor"], np.float64)
+    z2r = np.ascontiguousarray(body["z2r"], np.float64)
+    L.oracle_eam_build_setfl_splines(int(body["n_elements"]), nrho, float(body["drho"]), nr, float(body["dr"]),
+                                     _dp(frho), _dp(rhor), _dp(z2r), _ip(te), nt, _dp(fs), _dp(rs), _dp(zs),
+                                     _dp(rhomax))
+    return dict(nrho=nrho, nr=nr, drho=float(body["drho"]), dr=float(body["dr"]), rhomax=float(rhomax[0]),
+                cut=float(body["cut"]), frho_spline=fs, rhor_spline=rs, z2r_spline=zs, per_type=1)

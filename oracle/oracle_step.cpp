@@ -74,7 +74,7 @@ inline void add_virial(double v[6], const double r[3], const double F[3], double
 }
 
 // EAM spline evaluations, ExecForceFunction.h:896-1096
-inline double eam_rho(const std::vector<double>& sp, double r, double rdr, int nr) {
+inline double eam_rho(const double* sp, double r, double rdr, int nr) {
   double pp = r * rdr + 1.0;
   int mm = (int)pp;
   mm = std::min(mm, nr - 1);
@@ -113,7 +113,7 @@ void System::near_force(std::vector<double>& F) {
       const int i = (int)i_l;
       double rho = 0.0;
       int index_shell = rbl_offset(i);
-      traverse(i, [&](int, const double*, const double* r0, double d2) {
+      traverse(i, [&](int j, const double*, const double* r0, double d2) {
         bool core, shell = false;
         if (rbl) {
           shell = (rc_2 - d2 > 0.0001 && d2 - rs_2 > 0.0001);
@@ -130,10 +130,11 @@ void System::near_force(std::vector<double>& F) {
         double r[3] = {-r0[0], -r0[1], -r0[2]};  // MinDistanceVec(p_i, p_j)
         min_image(r);
         double rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+        // the density of the neighbour's type (LAMMPS eam/alloy type2rhor[jtype][itype])
         if (core) {
-          if (rsq < rc * rc && rsq > 0.01) rho += eam_rho(rhor_spline, std::sqrt(rsq), rdr, eam_nr);
+          if (rsq < rc * rc && rsq > 0.01) rho += eam_rho(rhor_of(type[j]), std::sqrt(rsq), rdr, eam_nr);
         } else {
-          if (rsq < rc * rc && rsq > rs_2) rho += pice * eam_rho(rhor_spline, std::sqrt(rsq), rdr, eam_nr);
+          if (rsq < rc * rc && rsq > rs_2) rho += pice * eam_rho(rhor_of(type[j]), std::sqrt(rsq), rdr, eam_nr);
         }
       });
       // ComputeEAMfp, ExecForceFunction.h:946-962
@@ -142,7 +143,7 @@ void System::near_force(std::vector<double>& F) {
       mm = std::max(1, std::min(mm, eam_nrho - 1));
       pp -= mm;
       pp = std::min(pp, 1.0);
-      const double* c = &frho_spline[7 * mm];
+      const double* c = frho_of(type[i]) + 7 * mm;
       fp[i] = (c[0] * pp + c[1]) * pp + c[2];
     });
     par_for((long)(N), [&](long i_l) {
@@ -175,10 +176,11 @@ void System::near_force(std::vector<double>& F) {
         mm = std::min(mm, eam_nr - 1);
         pp -= mm;
         pp = std::min(pp, 1.0);
-        const double* ci = &rhor_spline[7 * mm];
+        const double* ci = rhor_of(type[i]) + 7 * mm;
         double rhoip = (ci[0] * pp + ci[1]) * pp + ci[2];
-        double rhojp = rhoip;
-        const double* cz = &z2r_spline[7 * mm];
+        const double* cj = rhor_of(type[j]) + 7 * mm;
+        double rhojp = (cj[0] * pp + cj[1]) * pp + cj[2];
+        const double* cz = z2r_of(type[i], type[j]) + 7 * mm;
         double z2p = (cz[0] * pp + cz[1]) * pp + cz[2];
         double z2 = ((cz[3] * pp + cz[4]) * pp + cz[5]) * pp + cz[6];
         double recip = 1.0 / rr;
@@ -1143,19 +1145,19 @@ void System::energies(double& e_lj, double& e_coul, double& e_eam) const {
       const int i = (int)i_l;
       double rho = 0;
       double& pair = pair_i[i];
-      traverse(i, [&](int, const double*, const double* r0, double d2) {
+      traverse(i, [&](int j, const double*, const double* r0, double d2) {
         if (!(rc_2 - d2 > 0.0001 && d2 > 0.0001)) return;
         double r[3] = {-r0[0], -r0[1], -r0[2]};
         min_image(r);
         double rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
         if (rsq < cut * cut && rsq > 0.01) {
           double rr = std::sqrt(rsq);
-          rho += eam_rho(rhor_spline, rr, rdr, eam_nr);
+          rho += eam_rho(rhor_of(type[j]), rr, rdr, eam_nr);
           double pp = rr * rdr + 1.0;
           int mm = std::min((int)pp, eam_nr - 1);
           pp -= mm;
           pp = std::min(pp, 1.0);
-          const double* c = &z2r_spline[7 * mm];
+          const double* c = z2r_of(type[i], type[j]) + 7 * mm;
           double z2 = ((c[3] * pp + c[4]) * pp + c[5]) * pp + c[6];
           pair += 0.5 * (z2 * (1.0 / rr));
         }
@@ -1164,7 +1166,7 @@ void System::energies(double& e_lj, double& e_coul, double& e_eam) const {
       int mm = std::max(1, std::min((int)pp, eam_nrho - 1));
       pp -= mm;
       pp = std::min(pp, 1.0);
-      const double* c = &frho_spline[7 * mm];
+      const double* c = frho_of(type[i]) + 7 * mm;
       double fpv = (c[0] * pp + c[1]) * pp + c[2];
       double phi = ((c[3] * pp + c[4]) * pp + c[5]) * pp + c[6];
       if (rho > eam_rhomax) phi += fpv * (rho - eam_rhomax);
@@ -1297,6 +1299,34 @@ static void interpolate(int n, double delta, const std::vector<double>& f, std::
     S(mm, 1) = 2.0 * S(mm, 4) / delta;
     S(mm, 0) = 3.0 * S(mm, 3) / delta;
   }
+}
+
+void build_setfl_splines(int ne, int nrho, double drho, int nr, double dr, const double* frho, const double* rhor,
+                         const double* z2r, const int* type_element, int n_types, std::vector<double>& frho_s,
+                         std::vector<double>& rhor_s, std::vector<double>& z2r_s, double& rhomax) {
+  (void)ne;
+  const size_t rf = 7 * (size_t)(nrho + 1), rr = 7 * (size_t)(nr + 1);
+  frho_s.assign(rf * n_types, 0.0);
+  rhor_s.assign(rr * n_types, 0.0);
+  z2r_s.assign(rr * n_types * (n_types + 1) / 2, 0.0);
+  // one table: copy the values into rows 1..n and spline them in place of the output slice
+  auto table = [&](const double* src, int n, double delta, std::vector<double>& dst, size_t at) {
+    std::vector<double> f(n + 1, 0.0), sp(7 * (size_t)(n + 1), 0.0);
+    for (int mm = 1; mm <= n; ++mm) f[mm] = src[mm - 1];
+    interpolate(n, delta, f, sp);
+    std::copy(sp.begin(), sp.end(), dst.begin() + at);
+  };
+  for (int t = 0; t < n_types; ++t) {
+    const int e = type_element[t];
+    table(frho + (size_t)e * nrho, nrho, drho, frho_s, t * rf);
+    table(rhor + (size_t)e * nr, nr, dr, rhor_s, t * rr);
+  }
+  for (int i = 0; i < n_types; ++i)
+    for (int j = 0; j <= i; ++j) {
+      const int a = std::max(type_element[i], type_element[j]), b = std::min(type_element[i], type_element[j]);
+      table(z2r + (size_t)(a * (a + 1) / 2 + b) * nr, nr, dr, z2r_s, (size_t)(i * (i + 1) / 2 + j) * rr);
+    }
+  rhomax = (nrho - 1) * drho;
 }
 
 void build_splines(const EamFile& in, std::vector<double>& frho_s, std::vector<double>& rhor_s,

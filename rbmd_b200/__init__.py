@@ -312,6 +312,47 @@ class Snapshot:
         return self.x, self.v, self.image, self.box.reshape(2, 3), int(self.step[0])
 
 
+def read_setfl(path):
+    """Reads a setfl (LAMMPS eam/alloy) file into a dict: n_elements, names, mass, nrho, drho, nr,
+    dr, cut, frho [n_elements, nrho], rhor [n_elements, nr], z2r [pairs, nr]."""
+    f = A.EamSetfl()
+    rc = lib().rbmd_eam_read_setfl(str(path).encode(), C.byref(f), None, None, None, None, None)
+    if rc:
+        raise RbmdError(rc, f"cannot read setfl file {path}")
+    ne, nrho, nr = f.n_elements, f.nrho, f.nr
+    names = C.create_string_buffer(16 * ne)
+    mass, frho, rhor = np.zeros(ne), np.zeros((ne, nrho)), np.zeros((ne, nr))
+    z2r = np.zeros((ne * (ne + 1) // 2, nr))
+    rc = lib().rbmd_eam_read_setfl(str(path).encode(), C.byref(f), names, _dp(mass), _dp(frho), _dp(rhor), _dp(z2r))
+    if rc:
+        raise RbmdError(rc, f"cannot read setfl file {path}")
+    nm = [names.raw[16 * e:16 * (e + 1)].split(b"\0")[0].decode() for e in range(ne)]
+    return dict(n_elements=ne, names=nm, mass=mass, nrho=nrho, drho=f.drho, nr=nr, dr=f.dr, cut=f.cut_off,
+                frho=frho, rhor=rhor, z2r=z2r)
+
+
+def setfl_splines(body, type_element):
+    """Per-type EAM spline tables (eam_per_type = 1) of a setfl body: type t takes element
+    type_element[t] (rbmd_eam_build_setfl_splines)."""
+    f = A.EamSetfl(n_elements=body["n_elements"], nrho=body["nrho"], nr=body["nr"], drho=body["drho"],
+                   dr=body["dr"], cut_off=body["cut"])
+    te = np.ascontiguousarray(type_element, np.int32)
+    nt, nrho, nr = te.size, body["nrho"], body["nr"]
+    fs = np.zeros(7 * (nrho + 1) * nt)
+    rs = np.zeros(7 * (nr + 1) * nt)
+    zs = np.zeros(7 * (nr + 1) * nt * (nt + 1) // 2)
+    rhomax = C.c_double()
+    frho = np.ascontiguousarray(body["frho"], np.float64)
+    rhor = np.ascontiguousarray(body["rhor"], np.float64)
+    z2r = np.ascontiguousarray(body["z2r"], np.float64)
+    rc = lib().rbmd_eam_build_setfl_splines(C.byref(f), _dp(frho), _dp(rhor), _dp(z2r), _ip(te), nt, _dp(fs),
+                                            _dp(rs), _dp(zs), C.byref(rhomax))
+    if rc:
+        raise RbmdError(rc, "rbmd_eam_build_setfl_splines failed")
+    return dict(nrho=nrho, nr=nr, drho=float(body["drho"]), dr=float(body["dr"]), rhomax=rhomax.value,
+                cut=float(body["cut"]), frho_spline=fs, rhor_spline=rs, z2r_spline=zs, per_type=1)
+
+
 def rdf_bins(radius, dr):
     """RDF radii: (int)(radius / dr) bins at dr, 2 dr, ... accumulated (RDFOutput.cpp:42-53)."""
     n = C.c_int32()

@@ -5,7 +5,7 @@ a probe with the host compiler.
 """
 import ctypes as C
 
-RBMD_ABI_VERSION = 3
+RBMD_ABI_VERSION = 4
 
 # status
 OK, ERR_ARG, ERR_OOM, ERR_NUMERIC, ERR_TIMEOUT, ERR_CUDA, ERR_STATE, ERR_BUDGET, ERR_UNSUPPORTED, ERR_IO = range(10)
@@ -76,6 +76,7 @@ class SystemDesc(C.Structure):
         ("n_dihedrals", C.c_int32), ("n_dihedral_types", C.c_int32),
         ("dihedral_atoms", iptr), ("dihedral_type", iptr), ("dihedral_k", dptr), ("dihedral_sign", iptr),
         ("dihedral_multiplicity", iptr),
+        ("eam_per_type", C.c_int32), ("pad_eam", C.c_int32),
     ]
 
 
@@ -126,6 +127,11 @@ class TuneResult(C.Structure):
     def as_dict(self):
         return dict(n_systems=self.n_systems, layout=LAYOUT_NAMES[self.layout], atoms=self.atoms,
                     ms={LAYOUT_NAMES[k]: self.ms[k] for k in range(3)}, from_cache=bool(self.from_cache))
+
+
+class EamSetfl(C.Structure):
+    _fields_ = [("n_elements", C.c_int32), ("nrho", C.c_int32), ("nr", C.c_int32), ("pad0", C.c_int32),
+                ("drho", C.c_double), ("dr", C.c_double), ("cut_off", C.c_double)]
 
 
 class ServeCfg(C.Structure):
@@ -210,6 +216,9 @@ def declare(lib, prefix="rbmd"):
         "eam_spline_sizes": ([P(EamFile), iptr, iptr], C.c_int),
         "eam_build_splines": ([P(EamFile), dptr, dptr, dptr, iptr, dptr, iptr, dptr, dptr], C.c_int),
         "eam_read_funcfl": ([C.c_char_p, P(EamFile), dptr, dptr, dptr], C.c_int),
+        "eam_read_setfl": ([C.c_char_p, P(EamSetfl), C.c_char_p, dptr, dptr, dptr, dptr], C.c_int),
+        "eam_build_setfl_splines": ([P(EamSetfl), dptr, dptr, dptr, iptr, C.c_int32, dptr, dptr, dptr, dptr],
+                                    C.c_int),
         "serve_start": ([ctx, P(ServeCfg)], C.c_int),
         "serve_submit": ([ctx, P(SystemDesc), P(Params), C.c_int32, P(C.c_int64)], C.c_int),
         "serve_poll": ([ctx, C.c_int64, iptr], C.c_int),
@@ -250,4 +259,5 @@ HEADER_FUNCTIONS = [
     "rbmd_profile_get", "rbmd_step_timed", "rbmd_fma_peak", "rbmd_autotune",
     "rbmd_observe_reset", "rbmd_observe", "rbmd_rdf_bins", "rbmd_rdf_counts",
     "rbmd_snapshot_begin", "rbmd_snapshot_poll", "rbmd_snapshot_wait",
+    "rbmd_eam_read_setfl", "rbmd_eam_build_setfl_splines",
 ]

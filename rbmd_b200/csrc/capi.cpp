@@ -1,9 +1,11 @@
 // capi.cpp -- extern "C" entry points declared in include/rbmd_gpu.h.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <fstream>
 #include <limits>
 #include <new>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -288,6 +290,90 @@ static void eam_interpolate(int n, double delta, const std::vector<double>& f, d
     S(m, 1) = 2.0 * S(m, 4) / delta;
     S(m, 0) = 3.0 * S(m, 3) / delta;
   }
+}
+
+int rbmd_eam_read_setfl(const char* path, rbmd_eam_setfl* out, char* names, double* mass, double* frho,
+                        double* rhor, double* z2r) {
+  // LAMMPS pair eam/alloy read_file: 3 comment lines, elements line, grid line, per-element
+  // blocks, then the lower triangle of r phi tables.
+  if (!path || !out) return RBMD_ERR_ARG;
+  std::ifstream in(path);
+  if (!in.is_open()) return RBMD_ERR_IO;
+  for (int i = 0; i < 3; ++i) in.ignore(std::numeric_limits<std::streamsize>::max(), '\n');
+  std::string line;
+  if (!std::getline(in, line)) return RBMD_ERR_IO;
+  std::istringstream el(line);
+  int ne = 0;
+  el >> ne;
+  if (!el || ne < 1 || ne > 64) return RBMD_ERR_IO;
+  std::vector<std::string> nm(ne);
+  for (int e = 0; e < ne; ++e)
+    if (!(el >> nm[e])) return RBMD_ERR_IO;
+  int nrho = 0, nr = 0;
+  double drho = 0, dr = 0, cut = 0;
+  in >> nrho >> drho >> nr >> dr >> cut;
+  if (!in || nrho < 5 || nr < 5 || !(drho > 0) || !(dr > 0) || !(cut > 0)) return RBMD_ERR_IO;
+  out->n_elements = ne;
+  out->nrho = nrho;
+  out->nr = nr;
+  out->pad0 = 0;
+  out->drho = drho;
+  out->dr = dr;
+  out->cut_off = cut;
+  if (!names && !mass && !frho && !rhor && !z2r) return RBMD_OK;
+  if (!frho || !rhor || !z2r) return RBMD_ERR_ARG;
+  for (int e = 0; e < ne; ++e) {
+    int z = 0;
+    double m = 0, a = 0;
+    std::string lat;
+    in >> z >> m >> a >> lat;
+    if (!in) return RBMD_ERR_IO;
+    if (mass) mass[e] = m;
+    if (names) {
+      std::memset(names + 16 * e, 0, 16);
+      std::strncpy(names + 16 * e, nm[e].c_str(), 15);
+    }
+    for (int k = 0; k < nrho; ++k) in >> frho[(size_t)e * nrho + k];
+    for (int k = 0; k < nr; ++k) in >> rhor[(size_t)e * nr + k];
+    if (!in) return RBMD_ERR_IO;
+  }
+  const size_t pairs = (size_t)ne * (ne + 1) / 2;
+  for (size_t q = 0; q < pairs; ++q)
+    for (int k = 0; k < nr; ++k) in >> z2r[q * nr + k];
+  if (!in) return RBMD_ERR_IO;
+  return RBMD_OK;
+}
+
+int rbmd_eam_build_setfl_splines(const rbmd_eam_setfl* in, const double* frho, const double* rhor,
+                                 const double* z2r, const int32_t* type_element, int32_t n_types,
+                                 double* frho_s, double* rhor_s, double* z2r_s, double* rhomax_out) {
+  // LAMMPS PairEAMAlloy::file2array (the file's grid, arrays copied) then array2spline.
+  if (!in || !frho || !rhor || !z2r || !type_element || n_types < 1 || !frho_s || !rhor_s || !z2r_s)
+    return RBMD_ERR_ARG;
+  const int ne = in->n_elements, nrho = in->nrho, nr = in->nr;
+  if (ne < 1 || nrho < 5 || nr < 5) return RBMD_ERR_ARG;
+  for (int t = 0; t < n_types; ++t)
+    if (type_element[t] < 0 || type_element[t] >= ne) return RBMD_ERR_ARG;
+  const size_t rf = 7 * (size_t)(nrho + 1), rr = 7 * (size_t)(nr + 1);
+  std::vector<double> f(std::max(nrho, nr) + 1, 0.0);
+  auto spline = [&](const double* src, int n, double delta, double* dst) {
+    std::fill(f.begin(), f.end(), 0.0);
+    for (int m = 1; m <= n; ++m) f[m] = src[m - 1];
+    std::memset(dst, 0, sizeof(double) * 7 * (n + 1));
+    eam_interpolate(n, delta, f, dst);
+  };
+  for (int t = 0; t < n_types; ++t) {
+    const int e = type_element[t];
+    spline(frho + (size_t)e * nrho, nrho, in->drho, frho_s + t * rf);
+    spline(rhor + (size_t)e * nr, nr, in->dr, rhor_s + t * rr);
+  }
+  for (int i = 0; i < n_types; ++i)
+    for (int j = 0; j <= i; ++j) {
+      const int a = std::max(type_element[i], type_element[j]), b = std::min(type_element[i], type_element[j]);
+      spline(z2r + (size_t)(a * (a + 1) / 2 + b) * nr, nr, in->dr, z2r_s + (size_t)(i * (i + 1) / 2 + j) * rr);
+    }
+  if (rhomax_out) *rhomax_out = (nrho - 1) * in->drho;
+  return RBMD_OK;
 }
 
 int rbmd_eam_build_splines(const rbmd_eam_file* in, double* frho_s, double* rhor_s, double* z2r_s,

@@ -75,6 +75,8 @@ struct SysDev {
   int special, pice, nc, ncell, P, n_bonds, n_angles, nk_ewald;
   int dims[3];
   int eam_nrho, eam_nr;
+  int eam_per_type;  // EAM tables per type (setfl): frho / rhor by type, z2r by type pair
+  int eam_pad;
   int lean;   // segment-table traversal usable (every dimension holds >= 2 nc + 1 cells)
   int dense;  // pair kernel layout: tile (warp per home cell, dense systems) or warp per atom
   int blocks_pair, blocks_atom, blocks_rho, blocks_tri, rbe_mmax, rbe_slots, has_triples, n_triples;

@@ -255,7 +255,11 @@ int64_t Context::estimate_bytes(const rbmd_system_desc& d, const rbmd_params& p)
   b += (int64_t)(d.n_bonds * 2 + d.n_angles * 3 + d.n_dihedrals * 4) * 48 +
        (int64_t)(d.n_bonds + d.n_angles + d.n_dihedrals) * 76;
   if (d.special_offsets) b += (int64_t)d.special_offsets[n] * 12 + 4 * (n + 1);
-  if (p.force_field == RBMD_FF_EAM) b += (int64_t)(d.eam_nrho + 2 * d.eam_nr + 3) * 56;
+  if (p.force_field == RBMD_FF_EAM) {
+    size_t nf, nr, nz;
+    eam_table_sizes(d, &nf, &nr, &nz);
+    b += (int64_t)(nf + nr + nz) * 8;
+  }
   b += ((n + kPairWarps - 1) / kPairWarps) * 72 + ((n + kAtomBlock - 1) / kAtomBlock) * 64 + 4096;
   return b;
 }
@@ -304,6 +308,8 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   if (p.force_field == RBMD_FF_EAM &&
       (!d.eam_frho_spline || !d.eam_rhor_spline || !d.eam_z2r_spline || d.eam_nrho < 3 || d.eam_nr < 3))
     return fail(RBMD_ERR_ARG, "EAM needs the three spline tables");
+  if (p.force_field == RBMD_FF_EAM && (d.eam_per_type < 0 || d.eam_per_type > 1))
+    return fail(RBMD_ERR_ARG, "eam_per_type must be 0 or 1");
   if (d.n_bonds > 0 && (!d.bond_atoms || !d.bond_type || !d.bond_k || !d.bond_r0))
     return fail(RBMD_ERR_ARG, "bond arrays missing");
   if (d.n_angles > 0 && !d.angle_atoms) return fail(RBMD_ERR_ARG, "angle atoms missing");
@@ -693,13 +699,16 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
     D.eam_dr = d.eam_dr;
     D.eam_rhomax = d.eam_rhomax;
     D.eam_cut = d.eam_cut;
-    D.frho_s = (double*)dal(sizeof(double) * 7 * (d.eam_nrho + 1));
-    D.rhor_s = (double*)dal(sizeof(double) * 7 * (d.eam_nr + 1));
-    D.z2r_s = (double*)dal(sizeof(double) * 7 * (d.eam_nr + 1));
+    D.eam_per_type = d.eam_per_type;
+    size_t nf, nr, nz;
+    eam_table_sizes(d, &nf, &nr, &nz);
+    D.frho_s = (double*)dal(sizeof(double) * nf);
+    D.rhor_s = (double*)dal(sizeof(double) * nr);
+    D.z2r_s = (double*)dal(sizeof(double) * nz);
     D.eam_fp = (double*)dal(sizeof(double) * n);
-    up(D.frho_s, d.eam_frho_spline, sizeof(double) * 7 * (d.eam_nrho + 1));
-    up(D.rhor_s, d.eam_rhor_spline, sizeof(double) * 7 * (d.eam_nr + 1));
-    up(D.z2r_s, d.eam_z2r_spline, sizeof(double) * 7 * (d.eam_nr + 1));
+    up(D.frho_s, d.eam_frho_spline, sizeof(double) * nf);
+    up(D.rhor_s, d.eam_rhor_spline, sizeof(double) * nr);
+    up(D.z2r_s, d.eam_z2r_spline, sizeof(double) * nz);
   }
   D.atom_part = (double*)dal(sizeof(double) * 8 * D.blocks_atom);
   // pair-kernel partials: enough blocks for any layout the autotuner may switch to

@@ -39,6 +39,15 @@ struct System {
   int obs_have = 0;             // RBMD_OBS_* bits taken
 };
 
+// Doubles in each EAM spline array of a descriptor: frho, rhor and z2r (per type when
+// eam_per_type, one table each otherwise).
+inline void eam_table_sizes(const rbmd_system_desc& d, size_t* nf, size_t* nr, size_t* nz) {
+  const size_t t = d.eam_per_type ? (size_t)d.n_types : 1, pairs = d.eam_per_type ? t * (t + 1) / 2 : 1;
+  *nf = 7 * (size_t)(d.eam_nrho + 1) * t;
+  *nr = 7 * (size_t)(d.eam_nr + 1) * t;
+  *nz = 7 * (size_t)(d.eam_nr + 1) * pairs;
+}
+
 // RDF bins of radius / dr (RDFOutput.cpp:42-53): (int)(radius / dr) radii, dr accumulated by
 // repeated addition.  Returns the bin count, or -1 for a bad (radius, dr).
 int rdf_bins(double radius, double dr, std::vector<double>* radii);

@@ -88,6 +88,21 @@ __device__ inline void eam_row(const double* tab, double r, double rdr, int nr, 
   p = fmin(p, 1.0);
 }
 
+// EAM tables of a type and of a type pair: one table of each kind for every type (funcfl, the
+// reference's EAM), or per type (setfl): frho / rhor by type, z2r by pair i >= j at i (i+1)/2 + j
+// (LAMMPS pair eam/alloy's type2frho, type2rhor, type2z2r).
+__device__ inline const double* eam_frho(const SysDev& s, int t) {
+  return s.eam_per_type ? s.frho_s + (size_t)t * 7 * (s.eam_nrho + 1) : s.frho_s;
+}
+__device__ inline const double* eam_rhor(const SysDev& s, int t) {
+  return s.eam_per_type ? s.rhor_s + (size_t)t * 7 * (s.eam_nr + 1) : s.rhor_s;
+}
+__device__ inline const double* eam_z2r(const SysDev& s, int a, int b) {
+  if (!s.eam_per_type) return s.z2r_s;
+  const int hi = max(a, b), lo = min(a, b);
+  return s.z2r_s + (size_t)(hi * (hi + 1) / 2 + lo) * 7 * (s.eam_nr + 1);
+}
+
 struct PairAcc {
   double f[3];
   double g[3];    // Coulomb part before qqr2e (RBL Coulomb modes)
@@ -119,24 +134,27 @@ __device__ inline void eval_pair(const SysDev& s, int i, int ti, int moli, doubl
     double p;
     eam_row(s.rhor_s, rr, 1.0 / s.eam_dr, s.eam_nr, m, p);
     const double scale = core ? 1.0 : (double)pice;
+    const int tj = mj.y;
     if (MODE == kEAM_RHO || MODE == kEAM_ENERGY) {
-      const double* c = s.rhor_s + 7 * m;
+      const double* c = eam_rhor(s, tj) + 7 * m;  // the density the neighbour's type contributes
       a.rho += scale * (((__ldg(c + 3) * p + __ldg(c + 4)) * p + __ldg(c + 5)) * p + __ldg(c + 6));
       if (MODE == kEAM_ENERGY) {
-        const double* z = s.z2r_s + 7 * m;
+        const double* z = eam_z2r(s, ti, tj) + 7 * m;
         double z2 = ((__ldg(z + 3) * p + __ldg(z + 4)) * p + __ldg(z + 5)) * p + __ldg(z + 6);
         a.e1 += 0.5 * (z2 * (1.0 / rr));
       }
     } else {
-      const double* ci = s.rhor_s + 7 * m;
+      const double* ci = eam_rhor(s, ti) + 7 * m;
       const double rhoip = (__ldg(ci) * p + __ldg(ci + 1)) * p + __ldg(ci + 2);
-      const double* cz = s.z2r_s + 7 * m;
+      const double* cj = eam_rhor(s, tj) + 7 * m;
+      const double rhojp = (__ldg(cj) * p + __ldg(cj + 1)) * p + __ldg(cj + 2);
+      const double* cz = eam_z2r(s, ti, tj) + 7 * m;
       const double z2p = (__ldg(cz) * p + __ldg(cz + 1)) * p + __ldg(cz + 2);
       const double z2 = ((__ldg(cz + 3) * p + __ldg(cz + 4)) * p + __ldg(cz + 5)) * p + __ldg(cz + 6);
       const double recip = 1.0 / rr;
       const double phi = z2 * recip;
       const double phip = z2p * recip - phi * recip;
-      const double psip = fpi * rhoip + __ldg(&s.eam_fp[mj.x]) * rhoip + phip;
+      const double psip = fpi * rhojp + __ldg(&s.eam_fp[mj.x]) * rhoip + phip;
       const double fpair = -psip * recip;
       a.f[0] += scale * ((double)rx * fpair);
       a.f[1] += scale * ((double)ry * fpair);
@@ -498,7 +516,7 @@ k_pair(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int
       m = max(1, min(m, s.eam_nrho - 1));
       p -= m;
       p = fmin(p, 1.0);
-      const double* c = s.frho_s + 7 * m;
+      const double* c = eam_frho(s, s.meta[i].x) + 7 * m;
       s.eam_fp[i] = (c[0] * p + c[1]) * p + c[2];
     } else if (MODE == kEAM_ENERGY) {
       const double rho = r9[0];
@@ -507,7 +525,7 @@ k_pair(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int
       m = max(1, min(m, s.eam_nrho - 1));
       p -= m;
       p = fmin(p, 1.0);
-      const double* c = s.frho_s + 7 * m;
+      const double* c = eam_frho(s, s.meta[i].x) + 7 * m;
       const double fpv = (c[0] * p + c[1]) * p + c[2];
       double phi = ((c[3] * p + c[4]) * p + c[5]) * p + c[6];
       if (rho > s.eam_rhomax) phi += fpv * (rho - s.eam_rhomax);
@@ -921,7 +939,7 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
       m = max(1, min(m, s.eam_nrho - 1));
       p -= m;
       p = fmin(p, 1.0);
-      const double* c = s.frho_s + 7 * m;
+      const double* c = eam_frho(s, s.meta[i].x) + 7 * m;
       if (MODE == kEAM_RHO) {
         s.eam_fp[i] = (c[0] * p + c[1]) * p + c[2];
       } else {
@@ -1117,7 +1135,7 @@ __device__ inline void finish_atom(const SysDev& s, int i, double (&r9)[9]) {
     m = max(1, min(m, s.eam_nrho - 1));
     p -= m;
     p = fmin(p, 1.0);
-    const double* c = s.frho_s + 7 * m;
+    const double* c = eam_frho(s, s.meta[i].x) + 7 * m;
     if (MODE == kEAM_RHO) {
       s.eam_fp[i] = (c[0] * p + c[1]) * p + c[2];
     } else {

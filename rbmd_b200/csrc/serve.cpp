@@ -52,9 +52,16 @@ void OwnedDesc::copy_from(const rbmd_system_desc& s) {
   const size_t ns = s.special_offsets ? (size_t)s.special_offsets[n] : 0;
   cp(spi, s.special_ids, ns);
   cp(spw, s.special_weights, ns);
-  cp(frho, s.eam_frho_spline, s.eam_frho_spline ? 7 * (size_t)(s.eam_nrho + 1) : 0);
-  cp(rhor, s.eam_rhor_spline, s.eam_rhor_spline ? 7 * (size_t)(s.eam_nr + 1) : 0);
-  cp(z2r, s.eam_z2r_spline, s.eam_z2r_spline ? 7 * (size_t)(s.eam_nr + 1) : 0);
+  size_t nf, nr, nz;
+  eam_table_sizes(s, &nf, &nr, &nz);
+  cp(frho, s.eam_frho_spline, s.eam_frho_spline ? nf : 0);
+  cp(rhor, s.eam_rhor_spline, s.eam_rhor_spline ? nr : 0);
+  cp(z2r, s.eam_z2r_spline, s.eam_z2r_spline ? nz : 0);
+  cp(da, s.dihedral_atoms, 4 * (size_t)std::max(0, s.n_dihedrals));
+  cp(dt, s.dihedral_type, (size_t)std::max(0, s.n_dihedrals));
+  cp(dk, s.dihedral_k, (size_t)std::max(0, s.n_dihedral_types));
+  cp(dsg, s.dihedral_sign, (size_t)std::max(0, s.n_dihedral_types));
+  cp(dm, s.dihedral_multiplicity, (size_t)std::max(0, s.n_dihedral_types));
   auto P = [](auto& v) { return v.empty() ? nullptr : v.data(); };
   d.position = P(pos);
   d.velocity = P(vel);
@@ -79,6 +86,11 @@ void OwnedDesc::copy_from(const rbmd_system_desc& s) {
   d.eam_frho_spline = P(frho);
   d.eam_rhor_spline = P(rhor);
   d.eam_z2r_spline = P(z2r);
+  d.dihedral_atoms = P(da);
+  d.dihedral_type = P(dt);
+  d.dihedral_k = P(dk);
+  d.dihedral_sign = P(dsg);
+  d.dihedral_multiplicity = P(dm);
 }
 
 Server::Server(Context* c, const rbmd_serve_cfg& cfg) : ctx_(c), cfg_(cfg) {

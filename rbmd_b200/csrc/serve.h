@@ -17,8 +17,8 @@ namespace rbmd {
 // Deep copy of an rbmd_system_desc (the caller's arrays may be freed after submit).
 struct OwnedDesc {
   rbmd_system_desc d{};
-  std::vector<double> pos, vel, chg, mass, eps, sig, bk, br0, ak, at0, spw, frho, rhor, z2r;
-  std::vector<int32_t> type, mol, img, ba, bt, aa, at, spo, spi;
+  std::vector<double> pos, vel, chg, mass, eps, sig, bk, br0, ak, at0, spw, frho, rhor, z2r, dk;
+  std::vector<int32_t> type, mol, img, ba, bt, aa, at, spo, spi, da, dt, dsg, dm;
   void copy_from(const rbmd_system_desc& src);
 };
 

@@ -90,6 +90,7 @@ rbmd_system_desc Para::desc() const {
   d.eam_frho_spline = frho_spline.empty() ? nullptr : frho_spline.data();
   d.eam_rhor_spline = rhor_spline.empty() ? nullptr : rhor_spline.data();
   d.eam_z2r_spline = z2r_spline.empty() ? nullptr : z2r_spline.data();
+  d.eam_per_type = eam_per_type;
   if (!dihedral_type.empty()) {
     d.n_dihedrals = (int32_t)dihedral_type.size();
     d.n_dihedral_types = (int32_t)dihedral_k.size();
@@ -636,6 +637,17 @@ void MDApplication::ReadHyperParameters(const Json& hp) {
     else throw std::runtime_error("force_field type \"" + _ff_type + "\" is not supported");
     _potential_file = ff->string("potential_file", "");
     _dihedral_type = ff->string("dihedral_type", "");  // ForceField.cpp:49
+    // setfl (eam/alloy) potentials: "potential_format": "setfl", or a file named *.alloy / *.setfl;
+    // "elements": the file's element of each atom type (default: type t is element t)
+    _potential_format = ff->string("potential_format", "");
+    _eam_elements.clear();
+    if (const Json* el = ff->find("elements")) {
+      if (!el->is_array()) throw std::runtime_error("force_field.elements must be an array of element names");
+      for (const Json& e : el->arr) {
+        if (!e.is_string()) throw std::runtime_error("force_field.elements must be an array of element names");
+        _eam_elements.push_back(e.str);
+      }
+    }
   }
   if (const Json* nb = hp.find("neighbor")) {
     const std::string t = nb->string("type", "RBL");
@@ -762,6 +774,16 @@ void MDApplication::CreateActions() {
     if (_potential_file.empty()) throw std::runtime_error("EAM needs force_field.potential_file");
     std::string path = _potential_file;
     if (!exists(path) && exists(_base_dir + "/" + path)) path = _base_dir + "/" + path;
+    auto ends = [&](const char* suf) {
+      const size_t k = std::strlen(suf);
+      return _potential_file.size() >= k && _potential_file.compare(_potential_file.size() - k, k, suf) == 0;
+    };
+    const bool setfl = _potential_format == "setfl" || (_potential_format.empty() && (ends(".alloy") || ends(".setfl")));
+    if (!_potential_format.empty() && _potential_format != "setfl" && _potential_format != "funcfl")
+      throw std::runtime_error("potential_format must be \"funcfl\" or \"setfl\"");
+    if (setfl) {
+      ReadSetfl(path);
+    } else {
     rbmd_eam_file f;
     std::memset(&f, 0, sizeof(f));
     if (rbmd_eam_read_funcfl(path.c_str(), &f, nullptr, nullptr, nullptr) != RBMD_OK)
@@ -781,6 +803,7 @@ void MDApplication::CreateActions() {
                                &_para.eam_nrho, &_para.eam_drho, &_para.eam_nr, &_para.eam_dr, &_para.eam_rhomax) != RBMD_OK)
       throw std::runtime_error("cannot build EAM splines from " + path);
     _para.eam_cut = f.cut_off;
+    }
   }
   if (const Json* outs = _cfg.find("outputs")) {
     if (const Json* th = outs->find("thermo_out")) _thermo_interval = (int)th->number("interval", 1);
@@ -830,6 +853,48 @@ void MDApplication::CreateActions() {
         throw std::runtime_error("rdf_out: radius and dr must be positive with radius / dr >= 1");
     }
   }
+}
+
+void MDApplication::ReadSetfl(const std::string& path) {
+  rbmd_eam_setfl f;
+  std::memset(&f, 0, sizeof(f));
+  if (rbmd_eam_read_setfl(path.c_str(), &f, nullptr, nullptr, nullptr, nullptr, nullptr) != RBMD_OK)
+    throw std::runtime_error("cannot read setfl potential " + path);
+  const int ne = f.n_elements;
+  std::vector<char> names(16 * (size_t)ne);
+  std::vector<double> mass(ne), frho((size_t)ne * f.nrho), rhor((size_t)ne * f.nr), z2r((size_t)ne * (ne + 1) / 2 * f.nr);
+  if (rbmd_eam_read_setfl(path.c_str(), &f, names.data(), mass.data(), frho.data(), rhor.data(), z2r.data()) != RBMD_OK)
+    throw std::runtime_error("cannot read setfl potential " + path);
+  std::vector<int32_t> te(_para.n_types);
+  for (int t = 0; t < _para.n_types; ++t) {
+    if (_eam_elements.empty()) {
+      if (t >= ne)
+        throw std::runtime_error(path + " has " + std::to_string(ne) + " elements for " + std::to_string(_para.n_types) +
+                                 " atom types (map them with force_field.elements)");
+      te[t] = t;
+    } else {
+      if ((int)_eam_elements.size() != _para.n_types)
+        throw std::runtime_error("force_field.elements needs one element name per atom type");
+      te[t] = -1;
+      for (int e = 0; e < ne; ++e)
+        if (_eam_elements[t] == std::string(names.data() + 16 * e)) te[t] = e;
+      if (te[t] < 0) throw std::runtime_error("element " + _eam_elements[t] + " is not in " + path);
+    }
+  }
+  const size_t nt = _para.n_types;
+  _para.frho_spline.assign(7 * ((size_t)f.nrho + 1) * nt, 0.0);
+  _para.rhor_spline.assign(7 * ((size_t)f.nr + 1) * nt, 0.0);
+  _para.z2r_spline.assign(7 * ((size_t)f.nr + 1) * nt * (nt + 1) / 2, 0.0);
+  if (rbmd_eam_build_setfl_splines(&f, frho.data(), rhor.data(), z2r.data(), te.data(), (int32_t)nt,
+                                   _para.frho_spline.data(), _para.rhor_spline.data(), _para.z2r_spline.data(),
+                                   &_para.eam_rhomax) != RBMD_OK)
+    throw std::runtime_error("cannot build EAM splines from " + path);
+  _para.eam_nrho = f.nrho;
+  _para.eam_nr = f.nr;
+  _para.eam_drho = f.drho;
+  _para.eam_dr = f.dr;
+  _para.eam_cut = f.cut_off;
+  _para.eam_per_type = 1;
 }
 
 void MDApplication::DumpSystem(const std::string& path) const {
@@ -887,8 +952,13 @@ void MDApplication::DumpSystem(const std::string& path) const {
   iarr("special_offsets", _para.sp_off);
   iarr("special_ids", _para.sp_ids);
   darr("special_weights", _para.sp_w);
-  std::fprintf(f, "\"eam\": {\"nrho\": %d, \"nr\": %d, \"drho\": %.17g, \"dr\": %.17g, \"rhomax\": %.17g, \"cut\": %.17g},\n",
-               _para.eam_nrho, _para.eam_nr, _para.eam_drho, _para.eam_dr, _para.eam_rhomax, _para.eam_cut);
+  std::fprintf(f, "\"eam\": {\"nrho\": %d, \"nr\": %d, \"drho\": %.17g, \"dr\": %.17g, \"rhomax\": %.17g, \"cut\": %.17g, "
+               "\"per_type\": %d},\n",
+               _para.eam_nrho, _para.eam_nr, _para.eam_drho, _para.eam_dr, _para.eam_rhomax, _para.eam_cut,
+               _para.eam_per_type);
+  darr("eam_frho_spline", _para.frho_spline);
+  darr("eam_rhor_spline", _para.rhor_spline);
+  darr("eam_z2r_spline", _para.z2r_spline);
   std::fprintf(f, "\"outputs\": {\"thermo_interval\": %d, \"trajectory_interval\": %d, \"checkpoint_interval\": %d, "
                "\"checkpoint_file\": \"%s\"", _thermo_interval, _traj_interval, _checkpoint_interval,
                _checkpoint_file.c_str());

@@ -47,6 +47,7 @@ struct Para {
   // EAM
   int eam_nrho = 0, eam_nr = 0;
   double eam_drho = 0, eam_dr = 0, eam_rhomax = 0, eam_cut = 0;
+  int eam_per_type = 0;  // setfl: tables per atom type
   std::vector<double> frho_spline, rhor_spline, z2r_spline;
 
   rbmd_system_desc desc() const;  // pointers into this object
@@ -296,6 +297,7 @@ class MDApplication : public Application {
   void ReadHyperParameters(const Json& hp);
   void ReadExecution(const Json& ex);
   void DumpSystem(const std::string& path) const;
+  void ReadSetfl(const std::string& path);
   Json _cfg;
   Para _para;
   int _thermo_interval = 0, _traj_interval = 0, _checkpoint_interval = 0;
@@ -313,7 +315,8 @@ class MDApplication : public Application {
   } _rdf;
   bool _special_bonds = false;
   double _special_w[3] = {0, 0, 0};
-  std::string _ff_type, _potential_file, _base_dir, _dihedral_type;
+  std::string _ff_type, _potential_file, _base_dir, _dihedral_type, _potential_format;
+  std::vector<std::string> _eam_elements;
 };
 
 }  // namespace rbmd_host

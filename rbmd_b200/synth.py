@@ -121,6 +121,7 @@ class SystemData:
             d.eam_frho_spline = dp(e["frho_spline"])
             d.eam_rhor_spline = dp(e["rhor_spline"])
             d.eam_z2r_spline = dp(e["z2r_spline"])
+            d.eam_per_type = int(e.get("per_type", 0))
         if self.dihedral_atoms is not None:
             d.n_dihedrals = len(self.dihedral_type)
             d.n_dihedral_types = len(self.dihedral_k)
@@ -488,6 +489,84 @@ def eam_cu(cells=20, a=3.615, T=600.0, seed=1, build_splines=None, **kw):
                     params=params, name=f"eam_cu_{n}")
     if build_splines is not None:
         sd.eam = build_splines(johnson_funcfl())
+    return sd
+
+
+# A second Johnson-form element for two-element (setfl) tests: synthetic parameters, not fitted to
+# any metal.
+JOHNSON_B = dict(re=2.49, fe=1.15, beta=6.1, gamma=8.6, phi_e=0.52, E_c=4.1, rho_e=13.5)
+M_B = 58.69
+
+
+def johnson_setfl(elements=(JOHNSON_CU, JOHNSON_B), masses=(M_CU, M_B), names=("Cu", "B"), n=2000, cut=5.0):
+    """Tabulate Johnson functions of several elements as a setfl body: F_e on the nrho grid,
+    rho_e(r) on the nr grid, and r phi_ab(r) for every pair a >= b in setfl order, the cross pair
+    mixed as phi_ab = (f_b / f_a phi_a + f_a / f_b phi_b) / 2 (Johnson's alloy rule)."""
+    fs = [johnson_functions(par) for par in elements]
+    rho_max = 3.0 * max(par["rho_e"] for par in elements)
+    dr, drho = cut / (n - 1), rho_max / (n - 1)
+    r = np.arange(n) * dr
+    rr = np.where(r > 0, r, dr * 1e-3)
+    frho = np.stack([F(np.arange(n) * drho) for (_, _, F, *_) in fs])
+    rhor = np.stack([f(rr) for (f, *_) in fs])
+    z2r = []
+    for a in range(len(fs)):
+        for b in range(a + 1):
+            fa, pa = fs[a][0](rr), fs[a][1](rr)
+            fb, pb = fs[b][0](rr), fs[b][1](rr)
+            phi = pa if a == b else 0.5 * (fb / fa * pa + fa / fb * pb)
+            z2r.append(rr * phi)
+    return dict(n_elements=len(fs), names=list(names), mass=np.array(masses, np.float64), nrho=n, drho=drho,
+                nr=n, dr=dr, cut=cut, frho=frho, rhor=rhor, z2r=np.stack(z2r))
+
+
+def write_setfl(body, path):
+    """Writes a setfl body (johnson_setfl() or read_setfl() dict) as a LAMMPS eam/alloy file."""
+    with open(path, "w") as f:
+        f.write("setfl written by rbmd_b200.synth\n\n\n")
+        f.write(f"{body['n_elements']} " + " ".join(body["names"]) + "\n")
+        f.write(f"{int(body['nrho'])} {float(body['drho'])!r} {int(body['nr'])} {float(body['dr'])!r} "
+                f"{float(body['cut'])!r}\n")
+
+        def block(v):
+            v = np.asarray(v, np.float64)
+            for k in range(0, len(v), 5):
+                f.write(" ".join(repr(float(x)) for x in v[k:k + 5]) + "\n")
+
+        for e in range(body["n_elements"]):
+            f.write(f"{29 + e} {float(body['mass'][e])!r} 3.6 fcc\n")
+            block(body["frho"][e])
+            block(body["rhor"][e])
+        for q in range(len(body["z2r"])):
+            block(body["z2r"][q])
+    return path
+
+
+def eam_alloy(cells=6, a=3.6, frac_b=0.3, T=600.0, seed=1, build_splines=None, **kw):
+    """fcc lattice of two Johnson elements (johnson_setfl), a random fraction frac_b of type 1;
+    `build_splines(setfl_body, type_element) -> eam dict` makes the per-type tables
+    (rbmd_eam_build_setfl_splines)."""
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    g = np.arange(cells)
+    cell = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 1, 3)
+    pos = ((cell + base[None]) * a).reshape(-1, 3) + 0.25 * a
+    L = cells * a
+    n = pos.shape[0]
+    rng = np.random.default_rng(seed)
+    types = (rng.uniform(size=n) < frac_b).astype(np.int32)
+    mass = np.where(types == 1, M_B, M_CU)
+    kB, mvv2e = 8.617343e-5, 1.0364269e-4
+    vel = maxwell(mass, T, kB, mvv2e, rng)
+    params = A.default_params(force_field=A.FF_EAM, neighbor=A.NEIGH_RBL, cut_off=5.0, r_core=2.5,
+                              neighbor_sample_num=100, units=A.UNITS_METAL, timestep=0.002,
+                              temp_ctrl=A.TC_NOSE_HOOVER, temperature=(T, T, 0.1), num_steps=1000,
+                              seed=seed, precision=A.PREC_FP64)
+    for k, v in kw.items():
+        _set(params, k, v)
+    sd = SystemData(pos, mass, types, [0.0, 0.0], [0.0, 0.0], [0, 0, 0], [L, L, L], vel=vel,
+                    params=params, name=f"eam_alloy_{n}")
+    if build_splines is not None:
+        sd.eam = build_splines(johnson_setfl(), [0, 1])
     return sd
 
 

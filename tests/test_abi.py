@@ -43,7 +43,7 @@ def test_header_compiles_as_c():
 
 def test_host_only_entry_points():
     L = rbmd_b200.lib()
-    assert L.rbmd_abi_version() == A.RBMD_ABI_VERSION == 3
+    assert L.rbmd_abi_version() == A.RBMD_ABI_VERSION == 4
     p = A.Params()
     L.rbmd_params_default(C.byref(p))
     assert p.neighbor == A.NEIGH_RBL and p.precision == A.PREC_FP64 and p.fix_shake == A.SHAKE_NULL
@@ -55,13 +55,13 @@ def test_host_only_entry_points():
 
 def test_struct_sizes_match_header():
     """ctypes mirrors of the ABI structs have the C layout (sizes from a C compile of the header)."""
-    src = ('#include <stdio.h>\n#include "rbmd_gpu.h"\nint main(void) { printf("%zu %zu %zu %zu %zu %zu %zu\\n", '
+    src = ('#include <stdio.h>\n#include "rbmd_gpu.h"\nint main(void) { printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", '
            'sizeof(rbmd_params), sizeof(rbmd_system_desc), sizeof(rbmd_thermo), sizeof(rbmd_serve_cfg), '
-           'sizeof(rbmd_request_stats), sizeof(rbmd_device_cfg), sizeof(rbmd_tune_result)); return 0; }\n')
+           'sizeof(rbmd_request_stats), sizeof(rbmd_device_cfg), sizeof(rbmd_tune_result), sizeof(rbmd_eam_setfl)); return 0; }\n')
     exe = os.path.join(ROOT, "_work", "abi_sizes") if os.path.isdir(os.path.join(ROOT, "_work")) else "/tmp/abi_sizes"
     r = subprocess.run(["gcc", "-I", os.path.dirname(HEADER), "-x", "c", "-", "-o", exe], input=src,
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     sizes = list(map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split()))
     assert sizes == [C.sizeof(A.Params), C.sizeof(A.SystemDesc), C.sizeof(A.Thermo), C.sizeof(A.ServeCfg),
-                     C.sizeof(A.RequestStats), C.sizeof(A.DeviceCfg), C.sizeof(A.TuneResult)]
+                     C.sizeof(A.RequestStats), C.sizeof(A.DeviceCfg), C.sizeof(A.TuneResult), C.sizeof(A.EamSetfl)]

@@ -255,3 +255,45 @@ def test_checkpoint_and_trajectory_input(rbmd_bin, tmp_path):
     json.dump(cfg, open(path, "w"))
     o = dump(rbmd_bin, path, tmp_path)["outputs"]
     assert o["trajectory_interval"] == 1 and o["checkpoint_interval"] == 50 and o["checkpoint_file"] == "x.data"
+
+
+@pytest.mark.parametrize("how", ["extension", "format_key", "elements"])
+def test_setfl_potential_file(rbmd_bin, tmp_path, oracle_mod, how):
+    """setfl (eam/alloy) potentials: per-type tables equal to the oracle's restatement; atom types
+    map to the file's elements in order, or by force_field.elements."""
+    body = synth.johnson_setfl(n=600)
+    name = {"extension": "ab.eam.alloy", "format_key": "ab.pot", "elements": "ab.eam.alloy"}[how]
+    synth.write_setfl(body, str(tmp_path / name))
+    sd = synth.eam_alloy(cells=2)
+    path = synth.write_rbmd_input(sd, str(tmp_path), atom_style="atomic", potential_file=name)
+    cfg = json.load(open(path))
+    te = [0, 1]
+    if how == "format_key":
+        cfg["hyper_parameters"]["force_field"]["potential_format"] = "setfl"
+    if how == "elements":
+        cfg["hyper_parameters"]["force_field"]["elements"] = ["B", "Cu"]
+        te = [1, 0]
+    json.dump(cfg, open(path, "w"))
+    j = dump(rbmd_bin, path, tmp_path)
+    ref = oracle_mod.setfl_splines(body, te)
+    e = j["eam"]
+    assert e["per_type"] == 1 and (e["nrho"], e["nr"]) == (ref["nrho"], ref["nr"])
+    assert e["rhomax"] == ref["rhomax"] and e["cut"] == ref["cut"]
+    for k in ("frho_spline", "rhor_spline", "z2r_spline"):
+        assert np.array_equal(np.array(j["eam_" + k]), ref[k]), k
+
+
+def test_setfl_errors(rbmd_bin, tmp_path):
+    body = synth.johnson_setfl(n=600)
+    synth.write_setfl(body, str(tmp_path / "ab.eam.alloy"))
+    sd = synth.eam_alloy(cells=2)
+    path = synth.write_rbmd_input(sd, str(tmp_path), atom_style="atomic", potential_file="ab.eam.alloy")
+    cfg = json.load(open(path))
+    for ff, msg in (({"elements": ["Cu", "Zr"]}, "Zr"), ({"elements": ["Cu"]}, "one element name per atom type"),
+                    ({"potential_format": "tabulated"}, "potential_format")):
+        c = json.loads(json.dumps(cfg))
+        c["hyper_parameters"]["force_field"].update(ff)
+        json.dump(c, open(path, "w"))
+        r = subprocess.run([rbmd_bin, "-j", path, "--dump-system", str(tmp_path / "d.json")], capture_output=True,
+                           text=True)
+        assert r.returncode == 1 and msg in r.stderr, r.stderr

@@ -484,3 +484,74 @@ def test_msd_vacf_match_numpy(oracle_mod):
     assert np.allclose(msd, [*(d ** 2).mean(0), (d ** 2).sum(1).mean()], rtol=1e-13)
     w = v0 * v
     assert np.allclose(vacf, [*w.mean(0), w.sum(1).mean()], rtol=1e-13)
+
+
+# ------------------------------------------------------------------ setfl (eam/alloy) EAM
+def _row(tab, x, delta, n):
+    p = x / delta + 1.0
+    m = min(int(p), n - 1)
+    p = min(p - m, 1.0)
+    c = tab[m]
+    return ((c[3] * p + c[4]) * p + c[5]) * p + c[6], (c[0] * p + c[1]) * p + c[2]
+
+
+def test_setfl_splines_match_johnson(oracle_mod):
+    """setfl tables are splined on the file's grid with no resampling (LAMMPS eam/alloy
+    file2array), so unlike funcfl they reproduce f(r), r phi(r) and F(rho) at r itself; the
+    cross pair carries the mixing rule; type t takes element type_element[t]."""
+    body = synth.johnson_setfl(n=4000)
+    te = [1, 0]  # type 0 is element B, type 1 is Cu
+    eam = oracle_mod.setfl_splines(body, te)
+    nr, nrho, dr, drho = eam["nr"], eam["nrho"], eam["dr"], eam["drho"]
+    rs = eam["rhor_spline"].reshape(2, -1, 7)
+    zs = eam["z2r_spline"].reshape(3, -1, 7)
+    fs = eam["frho_spline"].reshape(2, -1, 7)
+    funcs = [synth.johnson_functions(synth.JOHNSON_B), synth.johnson_functions(synth.JOHNSON_CU)]
+    for r in np.linspace(1.8, 4.9, 13):
+        for t in range(2):
+            f, phi, F, df, dphi, dF = funcs[t]
+            rho, drho_dr = _row(rs[t], r, dr, nr)
+            assert rho == pytest.approx(f(r), rel=1e-7)
+            assert drho_dr == pytest.approx(df(r), rel=1e-4)
+            z2, _ = _row(zs[t * (t + 1) // 2 + t], r, dr, nr)
+            assert z2 == pytest.approx(r * phi(r), rel=1e-7)
+        fa, pa = funcs[0][0](r), funcs[0][1](r)
+        fb, pb = funcs[1][0](r), funcs[1][1](r)
+        z2, _ = _row(zs[1], r, dr, nr)  # types (1, 0)
+        assert z2 == pytest.approx(r * 0.5 * (fb / fa * pa + fa / fb * pb), rel=1e-7)
+    for t in range(2):
+        F = funcs[t][2]
+        for rho in (6.0, 12.0, 18.0):
+            v, _ = _row(fs[t], rho, drho, nrho)
+            assert v == pytest.approx(F(rho), rel=1e-6)
+    assert eam["rhomax"] == pytest.approx((nrho - 1) * drho)
+
+
+def test_setfl_alloy_forces_are_energy_gradients(oracle_mod):
+    """Per-type densities, embedding and pair tables: the oracle's forces are minus the gradient
+    of its EAM energy (Verlet neighbours, so every pair within the cutoff counts)."""
+    sd = synth.eam_alloy(cells=3, frac_b=0.4, build_splines=oracle_mod.setfl_splines,
+                         neighbor=A.NEIGH_VERLET, cut_off=4.9, r_core=4.9)
+    sd.eam["cut"] = 4.9
+    rng = np.random.default_rng(2)
+    sd.pos = sd.pos + rng.normal(scale=0.05, size=sd.pos.shape)
+    assert (sd.types == 1).any() and (sd.types == 0).any()
+    o = oracle_mod.Oracle(sd)
+    o.compute_forces()
+    f = o.forces()
+    n = sd.n
+
+    def energy(pos):
+        s2 = sd.copy()
+        s2.pos = pos
+        oo = oracle_mod.Oracle(s2)
+        oo.compute_forces()
+        return oo.thermo()["e_eam"] * n
+
+    h = 1e-5
+    for i, k in ((0, 0), (7, 1), (31, 2), (50, 0)):
+        p1, p2 = sd.pos.copy(), sd.pos.copy()
+        p1[i, k] += h
+        p2[i, k] -= h
+        g = -(energy(p1) - energy(p2)) / (2 * h)
+        assert f[i, k] == pytest.approx(g, rel=2e-5, abs=1e-6)
