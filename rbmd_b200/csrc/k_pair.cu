@@ -1066,32 +1066,6 @@ template <> __device__ inline float cls_thr<float>(const SysDev& s, int k) { ret
 __device__ inline double tile_d2(double x, double y, double z) { return add_rn(add_rn(mul_rn(x, x), mul_rn(y, y)), mul_rn(z, z)); }
 __device__ inline float tile_d2(float x, float y, float z) { return __fmaf_rn(z, z, __fmaf_rn(y, y, __fmul_rn(x, x))); }
 
-// Packed FP32 pairs (sm_100 f32x2 arithmetic): two lanes' worth of work per instruction, each half
-// rounded exactly as the scalar instruction rounds it, so tile_d2 of two atoms comes out bit for
-// bit as two scalar tile_d2 calls.
-__device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
-  unsigned long long r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-  return r;
-}
-__device__ __forceinline__ void f2_unpack(unsigned long long v, float& a, float& b) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-}
-__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
-  unsigned long long r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ unsigned long long f2_d2(unsigned long long x, unsigned long long y, unsigned long long z) {
-  unsigned long long r;
-  asm("{\n\t.reg .b64 t;\n\t"
-      "mul.rn.f32x2 t, %1, %1;\n\t"
-      "fma.rn.f32x2 t, %2, %2, t;\n\t"
-      "fma.rn.f32x2 %0, %3, %3, t;\n\t}"
-      : "=l"(r) : "l"(x), "l"(y), "l"(z));
-  return r;
-}
-
 // FP32 RBL classification against the band edges (SysDev::band), as two flags whose ballots
 // carry three outcomes out of the hot loop: x alone = core, y alone = shell, both = banded (to be
 // classified in FP64), neither = out (or the pair of an atom with itself).  Outside the bands the
@@ -1371,9 +1345,6 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
   // bit 15 set for a shell pair
   __shared__ unsigned short s_q[kCellWarps][kTileQ][32];
   __shared__ R4 s_pi[kCellWarps][32];          // chunk atom positions (far away for box-outside atoms)
-  // FP32 path: the same positions by coordinate, so that two neighbouring atoms' x (y, z) load as
-  // one packed pair for the f32x2 classification
-  __shared__ __align__(8) float s_pc[kCellWarps][3][32];
   // FP32 path: per chunk atom its type, molecule, special count and first special slot; the
   // concatenated-queue offsets; and its force accumulator
   __shared__ int4 s_ainfo[kCellWarps][32];
@@ -1478,11 +1449,6 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
         R4 q = p4;
         if (stray) q.x = q.y = q.z = far;
         s_pi[wid][lane] = q;
-        if constexpr (F32) {
-          s_pc[wid][0][lane] = (float)q.x;
-          s_pc[wid][1][lane] = (float)q.y;
-          s_pc[wid][2][lane] = (float)q.z;
-        }
         if constexpr (F32) {
           s_ainfo[wid][lane] = make_int4(ti, moli, nsp, SPECIAL ? s.sp_off[i] : 0);
           s_acc[wid][lane][0] = s_acc[wid][lane][1] = s_acc[wid][lane][2] = 0.0f;
@@ -1709,33 +1675,7 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
           // classified again from the FP64 positions (rare)
           constexpr bool kBandOnly = F32;  // no other classification compiled in
           if (kBandOnly || (sizeof(R) == 4 && rbl)) {
-            int ii = 0;
-            if constexpr (F32) {
-              // two atoms per iteration: packed differences and squared distances
-              const unsigned long long cx2 = f2_pack((float)cx, (float)cx), cy2 = f2_pack((float)cy, (float)cy);
-              const unsigned long long cz2 = f2_pack((float)cz, (float)cz);
-              for (; ii + 1 < nat; ii += 2) {
-                const unsigned long long qx = *reinterpret_cast<const unsigned long long*>(&s_pc[wid][0][ii]);
-                const unsigned long long qy = *reinterpret_cast<const unsigned long long*>(&s_pc[wid][1][ii]);
-                const unsigned long long qz = *reinterpret_cast<const unsigned long long*>(&s_pc[wid][2][ii]);
-                float dd0, dd1;
-                f2_unpack(f2_d2(f2_sub(cx2, qx), f2_sub(cy2, qy), f2_sub(cz2, qz)), dd0, dd1);
-                bool c0, h0, c1, h1;
-                band_classify(dd0, b0, b1, b2, b3, c0, h0);
-                band_classify(dd1, b0, b1, b2, b3, c1, h1);
-                const unsigned cm0 = __ballot_sync(FULL, c0), sm0 = __ballot_sync(FULL, h0);
-                const unsigned cm1 = __ballot_sync(FULL, c1), sm1 = __ballot_sync(FULL, h1);
-                if (lane == ii) {
-                  my_cm = cm0;
-                  my_sm = sm0;
-                }
-                if (lane == ii + 1) {
-                  my_cm = cm1;
-                  my_sm = sm1;
-                }
-              }
-            }
-            for (; ii < nat; ++ii) {
+            for (int ii = 0; ii < nat; ++ii) {
               const R4 q = s_pi[wid][ii];
               const float dd = tile_d2((float)cx - (float)q.x, (float)cy - (float)q.y, (float)cz - (float)q.z);
               bool core, shell;
