@@ -39,6 +39,16 @@ struct System {
   int obs_have = 0;             // RBMD_OBS_* bits taken
 };
 
+// The tile pair kernel's traversal: every dimension holds more than nc cells, so each stencil
+// offset needs one periodic image at most (a stencil may still repeat cells), and every edge is at
+// least 2 rc, so a pair within rc is at its nearest image (the reference evaluates forces at the
+// minimum image; the tile kernel's FP32 evaluation uses the traversal image as it is).
+inline bool tile_layout_ok(const SysDev& D) {
+  for (int k = 0; k < 3; ++k)
+    if (D.dims[k] < D.nc + 1 || D.L[k] < 2.0 * D.rc) return false;
+  return true;
+}
+
 // Doubles in each EAM spline array of a descriptor: frho, rhor and z2r (per type when
 // eam_per_type, one table each otherwise).
 inline void eam_table_sizes(const rbmd_system_desc& d, size_t* nf, size_t* nr, size_t* nz) {

@@ -1581,52 +1581,66 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
         __syncwarp();
       };
 
-      // ---- the home cell's candidate sequence, traversal rows in groups of 32 (one per lane)
-      for (int r0 = 0; r0 < nrows; r0 += 32) {
+      // ---- the home cell's candidate sequence, traversal rows in groups (one per lane).  A row's
+      // unwrapped z cells hz - nc .. hz + nc form one range, two around the periodic wrap, or, when
+      // the box holds fewer than 2 nc + 1 cells in z (but more than nc), three: below the box
+      // (image -L), inside, above (image +L); the segment table holds 64, so groups are 32 rows,
+      // or 21 rows when a row can have three ranges.
+      const int group = dz >= side ? 32 : 21;
+      for (int r0 = 0; r0 < nrows; r0 += group) {
         const int r = r0 + lane;
-        int nseg = 0, cnt = 0, sa0 = 0, sa1 = 0, n0c = 0, n1c = 0, code0 = 0, code1 = 0;
-        if (r < nrows) {
+        int nseg = 0, cnt = 0, sa0 = 0, sa1 = 0, sa2 = 0, n0c = 0, n1c = 0, n2c = 0, cxy = 0;
+        bool below = false, above = false;
+        if (lane < group && r < nrows) {
           const int da = r / side - nc, db = r % side - nc;
           const int n0 = hx + da, n1 = hy + db;  // the home cell is inside the grid and nc < dims
           const int w0 = n0 < 0 ? n0 + dx : (n0 >= dx ? n0 - dx : n0);
           const int w1 = n1 < 0 ? n1 + dy : (n1 >= dy ? n1 - dy : n1);
           const int t0 = n0 < 0 ? 2 : (n0 >= dx ? 0 : 1), t1 = n1 < 0 ? 2 : (n1 >= dy ? 0 : 1);
-          const int cxy = (t0 << kJsBits) | (t1 << (kJsBits + 2));
+          cxy = (t0 << kJsBits) | (t1 << (kJsBits + 2));
           const int base = dz * (w1 + dy * w0);
-          // unwrapped z cells hz - nc .. hz + nc: one range, or two around the periodic wrap
-          const int z0 = hz - nc;
-          const int zw = z0 < 0 ? z0 + dz : z0;
-          const int tz = z0 < 0 ? 2 : 1;
-          sa0 = __ldg(&s.cell_start[base + zw]);
-          code0 = cxy | (tz << (kJsBits + 4));
-          if (zw + side <= dz) {
-            n0c = __ldg(&s.cell_start[base + zw + side]) - sa0;
-            nseg = 1;
-          } else {
+          const int z0 = hz - nc, z1 = hz + nc;  // -dz < z0 <= hz <= z1 < 2 dz
+          below = z0 < 0;
+          above = z1 >= dz;
+          if (below) {  // cells z0 + dz .. dz - 1
+            sa0 = __ldg(&s.cell_start[base + z0 + dz]);
             n0c = __ldg(&s.cell_start[base + dz]) - sa0;
-            sa1 = __ldg(&s.cell_start[base]);
-            n1c = __ldg(&s.cell_start[base + zw + side - dz]) - sa1;
-            code1 = cxy | ((tz - 1) << (kJsBits + 4));
-            nseg = 2;
           }
-          cnt = n0c + (nseg == 2 ? n1c : 0);
+          {  // cells max(z0, 0) .. min(z1, dz - 1)
+            const int za = below ? 0 : z0, zb = above ? dz - 1 : z1;
+            sa1 = __ldg(&s.cell_start[base + za]);
+            n1c = __ldg(&s.cell_start[base + zb + 1]) - sa1;
+          }
+          if (above) {  // cells 0 .. z1 - dz
+            sa2 = __ldg(&s.cell_start[base]);
+            n2c = __ldg(&s.cell_start[base + z1 - dz + 1]) - sa2;
+          }
+          nseg = 1 + (below ? 1 : 0) + (above ? 1 : 0);
+          cnt = n0c + n1c + n2c;
         }
         const int seg_incl = warp_incl_scan(nseg, lane);
         const int cnt_incl = warp_incl_scan(cnt, lane);
         const int total = __shfl_sync(FULL, cnt_incl, 31);
-        {
-          const int slot = seg_incl - nseg, beg = cnt_incl - cnt;
-          if (nseg >= 1) {
+        if (nseg) {
+          int slot = seg_incl - nseg;
+          const int beg = cnt_incl - cnt;
+          if (below) {
             s_sa[wid][slot] = sa0;
             s_sb[wid][slot] = beg;
             s_se[wid][slot] = beg + n0c;
-            s_code[wid][slot] = code0;
+            s_code[wid][slot] = cxy | (2 << (kJsBits + 4));
+            ++slot;
           }
-          if (nseg == 2) {
-            s_sa[wid][slot + 1] = sa1;
-            s_sb[wid][slot + 1] = beg + n0c;
-            s_se[wid][slot + 1] = beg + n0c + n1c;
-            s_code[wid][slot + 1] = code1;
+          s_sa[wid][slot] = sa1;
+          s_sb[wid][slot] = beg + n0c;
+          s_se[wid][slot] = beg + n0c + n1c;
+          s_code[wid][slot] = cxy | (1 << (kJsBits + 4));
+          ++slot;
+          if (above) {
+            s_sa[wid][slot] = sa2;
+            s_sb[wid][slot] = beg + n0c + n1c;
+            s_se[wid][slot] = beg + n0c + n1c + n2c;
+            s_code[wid][slot] = cxy | (0 << (kJsBits + 4));
           }
         }
         __syncwarp();

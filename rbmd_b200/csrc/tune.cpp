@@ -21,7 +21,7 @@ std::vector<int> Context::usable_layouts(const System* s) const {
   if (D.npt) return {RBMD_LAYOUT_GENERAL};
   const bool stencil_ok = D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1;
   std::vector<int> out;
-  if (stencil_ok && D.n < (1 << 25)) out.push_back(RBMD_LAYOUT_TILE);
+  if (tile_layout_ok(D) && D.n < (1 << 25)) out.push_back(RBMD_LAYOUT_TILE);
   if (stencil_ok) out.push_back(RBMD_LAYOUT_LEAN);
   out.push_back(RBMD_LAYOUT_GENERAL);
   return out;
@@ -30,7 +30,8 @@ std::vector<int> Context::usable_layouts(const System* s) const {
 void Context::set_layout(System* s, int layout) {
   SysDev& D = s->dev;
   const int dense = layout == RBMD_LAYOUT_TILE ? 1 : 0;
-  const int lean = layout != RBMD_LAYOUT_GENERAL ? 1 : 0;
+  const bool stencil_ok = D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1;
+  const int lean = (layout != RBMD_LAYOUT_GENERAL && stencil_ok) ? 1 : 0;
   if (D.dense == dense && D.lean == lean) return;
   drop_batches_with(s->id);  // cached work tables and graphs hold the old layout
   D.dense = dense;

@@ -312,3 +312,36 @@ def test_mixed_precision_classification_is_exact_along_trajectories(oracle_mod):
             o.compute_forces()
             assert rel_rms(ctx.forces(sid), o.forces()) < 1e-4
         ctx.close()
+
+
+SMALL_BOXES = {
+    # boxes holding more than nc but fewer than 2 nc + 1 cells per dimension: the stencil repeats
+    # cells, and the tile kernel walks a row's z cells in up to three ranges
+    "water_dims4": lambda: synth.spce_water(n_mol=300),
+    "nacl_dims4": lambda: _jiggle(synth.nacl_melt(n_side=6), 0.15),
+    "lj_dims6_nc3": lambda: _jiggle(synth.lj_fcc(cells=3), 0.08),
+}
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED])
+@pytest.mark.parametrize("case", list(SMALL_BOXES))
+def test_small_box_tile_layout(ctx_factory, oracle_mod, case, prec):
+    sd = SMALL_BOXES[case]()
+    sd.params.precision = prec
+    ctx, sid, o = pair(ctx_factory, oracle_mod, sd, layout="cell")
+    d = ctx.derived(sid)
+    nc = d["num_cycles"]
+    assert all(nc < k for k in d["dims"]) and any(k < 2 * nc + 1 for k in d["dims"])
+    assert all(2 * sd.params.cut_off <= h - lo for h, lo in zip(sd.box_hi, sd.box_lo))
+    gn, gs, gi = ctx.rbl_lists(sid, cap=1024)
+    on, os_, oi = o.rbl_lists(cap=1024)
+    assert np.array_equal(gn, on) and np.array_equal(gs, os_)
+    for i in range(sd.n):
+        k = gn[i] + gs[i]
+        assert np.array_equal(gi[i, :k], oi[i, :k]), f"atom {i}"
+    ctx.compute_forces(sid)
+    ref = sd.copy()
+    ref.params.precision = A.PREC_FP64
+    o2 = oracle_mod.Oracle(ref)
+    o2.compute_forces()
+    assert rel_rms(ctx.forces(sid), o2.forces()) < (1e-9 if prec == A.PREC_FP64 else 1e-4)

@@ -67,14 +67,20 @@ def test_autotune_on_first_step_then_cache(ctx_factory, oracle_mod):
 
 
 def test_autotune_fixed_layouts(ctx_factory):
-    """NPT systems and boxes too small for the segment tables have a single usable layout."""
+    """NPT systems and boxes of nc cells per dimension (the least accepted) have a single usable layout; boxes
+    of nc + 1 to 2 nc cells (a stencil that repeats cells) have the tile and general layouts."""
     ctx = ctx_factory()
     npt = synth.lj_fcc(cells=6)
     p = npt.params
     p.ensemble, p.temp_ctrl, p.press_ctrl = A.ENS_NPT, A.TC_BERENDSEN, A.PC_BERENDSEN
     p.pressure[:] = (0.5, 0.5, 0.5)
-    small = synth.lj_fcc(cells=2, precision=A.PREC_MIXED)
-    ids = [ctx.add_system(npt), ctx.add_system(small)]
-    ctx.init(ids)
+    tiny = synth.lj_fcc(cells=2, rho=0.9, precision=A.PREC_MIXED)  # 3 cells per dimension = nc
+    small = synth.lj_fcc(cells=3, precision=A.PREC_MIXED)  # 6 cells per dimension, edges 2 rc
+    ids = [ctx.add_system(npt), ctx.add_system(tiny)]
+    sid = ctx.add_system(small)
+    ctx.init(ids + [sid])
     for r in ctx.autotune(ids):
         assert r["layout"] == "general" and all(v < 0 for v in r["ms"].values())
+    (r,) = ctx.autotune([sid])
+    assert r["layout"] in ("tile", "general") and r["ms"]["lean"] < 0
+    assert r["ms"]["tile"] > 0 and r["ms"]["general"] > 0
