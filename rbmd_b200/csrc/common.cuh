@@ -77,7 +77,7 @@ struct SysDev {
   int eam_nrho, eam_nr;
   int eam_per_type;  // EAM tables per type (setfl): frho / rhor by type, z2r by type pair
   int eam_pad;
-  int lean;   // segment-table traversal usable (every dimension holds >= 2 nc + 1 cells)
+  int lean;   // segment-table traversal usable (every dimension holds more than nc cells)
   int dense;  // pair kernel layout: tile (warp per home cell, dense systems) or warp per atom
   int blocks_pair, blocks_atom, blocks_rho, blocks_tri, rbe_mmax, rbe_slots, has_triples, n_triples;
   // NPT barostats (npt 1: Berendsen at the end of the step, 2: MTK around the integrator): the

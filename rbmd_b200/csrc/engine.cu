@@ -432,12 +432,13 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   // registers.  RBMD_PAIR_LAYOUT overrides the choice for tuning and tests: "atom" (general),
   // "lean", "cell" (tile).
   const bool stencil_ok = D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1;
-  // The tile kernel also walks stencils that repeat cells, as long as every dimension holds more
-  // than nc cells (one periodic image per offset).  It is not the default there: on the saline
-  // stream's 1000-1500-atom systems (4 cells per dimension) it took 1.76 ms per step against the
-  // general kernel's 1.41 ms, so only the autotuner or RBMD_PAIR_LAYOUT=cell selects it.
+  // The lean and tile kernels also walk stencils that repeat cells, as long as every dimension
+  // holds more than nc cells (one periodic image per offset; the tile kernel also needs edges of
+  // 2 rc).  There the lean kernel is the default: on the saline stream's 1000-1500-atom systems
+  // (4 cells per dimension) it took 0.85 ms per step, the general kernel 1.40 ms and the tile
+  // kernel 1.76 ms, so only the autotuner or RBMD_PAIR_LAYOUT=cell selects the tile kernel.
   const bool tile_ok = tile_layout_ok(D);
-  D.lean = stencil_ok ? 1 : 0;
+  D.lean = lean_layout_ok(D) ? 1 : 0;
   D.dense = (stencil_ok && p.precision == RBMD_PREC_MIXED && n < (1 << 25) &&
              (double)n >= kTileMinPerCell * (double)D.ncell) ? 1 : 0;
   const char* lay = std::getenv("RBMD_PAIR_LAYOUT");

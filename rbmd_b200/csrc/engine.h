@@ -48,6 +48,11 @@ inline bool tile_layout_ok(const SysDev& D) {
     if (D.dims[k] < D.nc + 1 || D.L[k] < 2.0 * D.rc) return false;
   return true;
 }
+// The lean kernel's (warp per atom over per-row segment tables): more than nc cells per dimension,
+// so a row's z cells take three ranges at most; it evaluates forces at the minimum image.
+inline bool lean_layout_ok(const SysDev& D) {
+  return D.dims[0] >= D.nc + 1 && D.dims[1] >= D.nc + 1 && D.dims[2] >= D.nc + 1;
+}
 
 // Doubles in each EAM spline array of a descriptor: frho, rhor and z2r (per type when
 // eam_per_type, one table each otherwise).

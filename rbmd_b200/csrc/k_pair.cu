@@ -756,13 +756,16 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
       qn -= cnt;
     };
 
-    for (int r0 = 0; r0 < nrows; r0 += 32) {
-      // ---- segment table of rows r0 .. r0 + 31 (one row per lane)
+    // rows per segment table: 32 of at most two ranges each, or 21 of at most three when the box
+    // holds fewer than 2 nc + 1 cells in z (the table holds 64)
+    const int group = dz >= side ? 32 : 21;
+    for (int r0 = 0; r0 < nrows; r0 += group) {
+      // ---- segment table of rows r0 .. r0 + group - 1 (one row per lane)
       const int r = r0 + lane;
       int nseg = 0, cnt = 0;
-      int sa0 = 0, sa1 = 0, n0c = 0, n1c = 0;
-      R oxv = R(0), oyv = R(0), oz0 = R(0), oz1 = R(0);
-      if (r < nrows) {
+      int sa0 = 0, sa1 = 0, sa2 = 0, n0c = 0, n1c = 0, n2c = 0;
+      R oxv = R(0), oyv = R(0), oz0 = R(0), oz1 = R(0), oz2 = R(0);
+      if (lane < group && r < nrows) {
         const int da = r / side - nc, db = r % side - nc;
         int n0 = c0 + da, n1 = c1 + db;
         int w0 = ((n0 % dx) + dx) % dx;
@@ -788,10 +791,11 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
             }
           }
           if (elo <= ehi) {
-            // unwrapped z cells [z0, z1] (at most dz of them, since dz >= 2 nc + 1) start in the
+            // unwrapped z cells [z0, z1] (len <= 2 nc + 1 <= 2 dz - 1 of them) start in the
             // periodic copy q = floor(z0 / dz); they map to wrapped cells [zw, zw + len) when that
-            // stays below dz, else to [zw, dz) then [0, zw + len - dz) of the next copy.  The
-            // shift of a cell is d * (wrapped - unwrapped) = -d dz q (first part), -d dz (q + 1).
+            // stays below dz, else to [zw, dz), then [0, rest) of the next copy, or [0, dz) and
+            // [0, rest - dz) of the two next when the stencil is longer than the box.  The shift of
+            // a cell is d * (wrapped - unwrapped) = -d dz q, -d dz (q + 1), -d dz (q + 2).
             const int base = dz * (w1 + dy * w0);
             const int z0 = c2 + elo, len = ehi - elo + 1;
             const int zw = ((z0 % dz) + dz) % dz;
@@ -803,12 +807,21 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
               nseg = 1;
             } else {
               n0c = __ldg(&s.cell_start[base + dz]) - sa0;
+              const int rest = zw + len - dz;
               sa1 = __ldg(&s.cell_start[base]);
-              n1c = __ldg(&s.cell_start[base + zw + len - dz]) - sa1;
               oz1 = (R)(-d2c * (double)dz * (double)(q + 1));
-              nseg = 2;
+              if (rest <= dz) {
+                n1c = __ldg(&s.cell_start[base + rest]) - sa1;
+                nseg = 2;
+              } else {
+                n1c = __ldg(&s.cell_start[base + dz]) - sa1;
+                sa2 = sa1;
+                n2c = __ldg(&s.cell_start[base + rest - dz]) - sa2;
+                oz2 = (R)(-d2c * (double)dz * (double)(q + 2));
+                nseg = 3;
+              }
             }
-            cnt = n0c + (nseg == 2 ? n1c : 0);
+            cnt = n0c + n1c + n2c;
           }
         }
       }
@@ -826,13 +839,21 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
           s_so[wid][1][slot] = oyv;
           s_so[wid][2][slot] = oz0;
         }
-        if (nseg == 2) {
+        if (nseg >= 2) {
           s_sa[wid][slot + 1] = sa1;
           s_sb[wid][slot + 1] = beg + n0c;
           s_se[wid][slot + 1] = beg + n0c + n1c;
           s_so[wid][0][slot + 1] = oxv;
           s_so[wid][1][slot + 1] = oyv;
           s_so[wid][2][slot + 1] = oz1;
+        }
+        if (nseg == 3) {
+          s_sa[wid][slot + 2] = sa2;
+          s_sb[wid][slot + 2] = beg + n0c + n1c;
+          s_se[wid][slot + 2] = beg + n0c + n1c + n2c;
+          s_so[wid][0][slot + 2] = oxv;
+          s_so[wid][1][slot + 2] = oyv;
+          s_so[wid][2][slot + 2] = oz2;
         }
       }
       __syncwarp();

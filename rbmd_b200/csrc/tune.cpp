@@ -19,10 +19,9 @@ namespace rbmd {
 std::vector<int> Context::usable_layouts(const System* s) const {
   const SysDev& D = s->dev;
   if (D.npt) return {RBMD_LAYOUT_GENERAL};
-  const bool stencil_ok = D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1;
   std::vector<int> out;
   if (tile_layout_ok(D) && D.n < (1 << 25)) out.push_back(RBMD_LAYOUT_TILE);
-  if (stencil_ok) out.push_back(RBMD_LAYOUT_LEAN);
+  if (lean_layout_ok(D)) out.push_back(RBMD_LAYOUT_LEAN);
   out.push_back(RBMD_LAYOUT_GENERAL);
   return out;
 }
@@ -30,8 +29,7 @@ std::vector<int> Context::usable_layouts(const System* s) const {
 void Context::set_layout(System* s, int layout) {
   SysDev& D = s->dev;
   const int dense = layout == RBMD_LAYOUT_TILE ? 1 : 0;
-  const bool stencil_ok = D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1;
-  const int lean = (layout != RBMD_LAYOUT_GENERAL && stencil_ok) ? 1 : 0;
+  const int lean = (layout != RBMD_LAYOUT_GENERAL && lean_layout_ok(D)) ? 1 : 0;
   if (D.dense == dense && D.lean == lean) return;
   drop_batches_with(s->id);  // cached work tables and graphs hold the old layout
   D.dense = dense;

@@ -316,23 +316,28 @@ def test_mixed_precision_classification_is_exact_along_trajectories(oracle_mod):
 
 SMALL_BOXES = {
     # boxes holding more than nc but fewer than 2 nc + 1 cells per dimension: the stencil repeats
-    # cells, and the tile kernel walks a row's z cells in up to three ranges
+    # cells, and the tile and lean kernels walk a row's z cells in up to three ranges
     "water_dims4": lambda: synth.spce_water(n_mol=300),
     "nacl_dims4": lambda: _jiggle(synth.nacl_melt(n_side=6), 0.15),
     "lj_dims6_nc3": lambda: _jiggle(synth.lj_fcc(cells=3), 0.08),
+    # edges below 2 rc: a pair within rc may not be at its nearest image (lean only)
+    "water_dims3": lambda: synth.spce_water(n_mol=120),
 }
 
 
 @pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED])
+@pytest.mark.parametrize("layout", ["cell", "lean"])
 @pytest.mark.parametrize("case", list(SMALL_BOXES))
-def test_small_box_tile_layout(ctx_factory, oracle_mod, case, prec):
+def test_small_box_layouts(ctx_factory, oracle_mod, case, layout, prec):
     sd = SMALL_BOXES[case]()
+    short = any(2 * sd.params.cut_off > h - lo for h, lo in zip(sd.box_hi, sd.box_lo))
+    if layout == "cell" and short:
+        pytest.skip("the tile layout needs edges of at least 2 rc")
     sd.params.precision = prec
-    ctx, sid, o = pair(ctx_factory, oracle_mod, sd, layout="cell")
+    ctx, sid, o = pair(ctx_factory, oracle_mod, sd, layout=layout)
     d = ctx.derived(sid)
     nc = d["num_cycles"]
     assert all(nc < k for k in d["dims"]) and any(k < 2 * nc + 1 for k in d["dims"])
-    assert all(2 * sd.params.cut_off <= h - lo for h, lo in zip(sd.box_hi, sd.box_lo))
     gn, gs, gi = ctx.rbl_lists(sid, cap=1024)
     on, os_, oi = o.rbl_lists(cap=1024)
     assert np.array_equal(gn, on) and np.array_equal(gs, os_)

@@ -67,8 +67,9 @@ def test_autotune_on_first_step_then_cache(ctx_factory, oracle_mod):
 
 
 def test_autotune_fixed_layouts(ctx_factory):
-    """NPT systems and boxes of nc cells per dimension (the least accepted) have a single usable layout; boxes
-    of nc + 1 to 2 nc cells (a stencil that repeats cells) have the tile and general layouts."""
+    """NPT systems and boxes of nc cells per dimension (the least accepted) have a single usable
+    layout; boxes of nc + 1 to 2 nc cells (a stencil that repeats cells) and edges of 2 rc have all
+    three."""
     ctx = ctx_factory()
     npt = synth.lj_fcc(cells=6)
     p = npt.params
@@ -82,5 +83,4 @@ def test_autotune_fixed_layouts(ctx_factory):
     for r in ctx.autotune(ids):
         assert r["layout"] == "general" and all(v < 0 for v in r["ms"].values())
     (r,) = ctx.autotune([sid])
-    assert r["layout"] in ("tile", "general") and r["ms"]["lean"] < 0
-    assert r["ms"]["tile"] > 0 and r["ms"]["general"] > 0
+    assert all(v > 0 for v in r["ms"].values())
