@@ -539,7 +539,10 @@ __global__ void __launch_bounds__(kAtomBlock) k_ke_thermostat(const SysDev* __re
 // ------------------------------------------------------------------ SHAKE / RATTLE
 __device__ inline double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
-__global__ void k_shake(const SysDev* __restrict__ S, const int2* __restrict__ work) {
+// One thread per triple.  The atoms' old state is read again after the multiplier iteration
+// instead of being kept in registers across it (the reads hit L1 / L2): fewer live registers,
+// four blocks per SM instead of two, and the same arithmetic in the same order.
+__global__ void __launch_bounds__(128, 4) k_shake(const SysDev* __restrict__ S, const int2* __restrict__ work) {
   // NewConstraintAWaterBondAngleWorklet, framework/run/worklet/MolecularWorklet.h:2367-2645
   const int2 wk = work[blockIdx.x];
   const SysDev& s = S[wk.x];
@@ -549,56 +552,80 @@ __global__ void k_shake(const SysDev* __restrict__ S, const int2* __restrict__ w
   if (a < s.n_triples) {
     const int id[3] = {s.angle_atoms[3 * a], s.angle_atoms[3 * a + 1], s.angle_atoms[3 * a + 2]};
     const double dt = s.dt, fm = s.fmt2v;
-    double ox[3][3], ov[3][3], fo[3][3], ms[3], sp[3][3];
-    for (int t = 0; t < 3; ++t) {
+    // old position, velocity, force and mass of atom t, and its unconstrained update
+    auto load = [&](int t, double* ox, double* ov, double* fo, double& m, double* sp) {
       const double4 x = s.xold[id[t]], v = s.vold[id[t]], f = s.f[id[t]];
-      ox[t][0] = x.x; ox[t][1] = x.y; ox[t][2] = x.z;
-      ov[t][0] = v.x; ov[t][1] = v.y; ov[t][2] = v.z;
-      fo[t][0] = f.x; fo[t][1] = f.y; fo[t][2] = f.z;
-      ms[t] = v.w;
-      for (int k = 0; k < 3; ++k) sp[t][k] = ox[t][k] + ov[t][k] * dt + 0.5 * dt * dt * fo[t][k] / ms[t] * fm;
-    }
+      ox[0] = x.x; ox[1] = x.y; ox[2] = x.z;
+      ov[0] = v.x; ov[1] = v.y; ov[2] = v.z;
+      fo[0] = f.x; fo[1] = f.y; fo[2] = f.z;
+      m = v.w;
+      for (int k = 0; k < 3; ++k) sp[k] = ox[k] + ov[k] * dt + 0.5 * dt * dt * fo[k] / m * fm;
+    };
     const double bond1 = 1.0, bond2 = 1.0;
     const double bond12 = sqrt(bond1 * bond1 + bond2 * bond2 - 2.0 * bond1 * bond2 * cos((109.4700 / 180.0) * kPif));
     auto mdv = [&](const double* p, const double* q, double* o) {
       o[0] = p[0] - q[0]; o[1] = p[1] - q[1]; o[2] = p[2] - q[2];
       min_image(o[0], o[1], o[2], s.L[0], s.L[1], s.L[2]);
     };
-    double r01[3], r12[3], r20[3], s10[3], s21[3], s02[3];
-    mdv(ox[1], ox[0], r01);
-    mdv(ox[2], ox[1], r12);
-    mdv(ox[0], ox[2], r20);
-    mdv(sp[0], sp[1], s10);
-    mdv(sp[1], sp[2], s21);
-    mdv(sp[2], sp[0], s02);
-    const double r01sq = dot3(r01, r01), r02sq = dot3(r20, r20), r12sq = dot3(r12, r12);
-    const double s01sq = dot3(s10, s10), s02sq = dot3(s02, s02), s12sq = dot3(s21, s21);
-    const double im0 = 1.0 / ms[0], im1 = 1.0 / ms[1], im2 = 1.0 / ms[2];
-    const double a11 = 2.0 * (im0 + im1) * dot3(s10, r01), a12 = -2.0 * im1 * dot3(s10, r12),
-                 a13 = -2.0 * im0 * dot3(s10, r20), a21 = -2.0 * im1 * dot3(s21, r01),
-                 a22 = 2.0 * (im1 + im2) * dot3(s21, r12), a23 = -2.0 * im2 * dot3(s21, r20),
-                 a31 = -2.0 * im0 * dot3(s02, r01), a32 = -2.0 * im2 * dot3(s02, r12),
-                 a33 = 2.0 * (im0 + im2) * (dot3(s02, r20));
-    const double determ = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a11 * a23 * a32 -
-                          a12 * a21 * a33 - a13 * a22 * a31;
+    double ms[3], r01[3], r12[3], r20[3];
+    double a11i, a12i, a13i, a21i, a22i, a23i, a31i, a32i, a33i, s01sq, s02sq, s12sq;
+    double q1_0101, q1_1212, q1_2020, q1_0120, q1_0112, q1_2012;
+    double q2_0101, q2_1212, q2_2020, q2_0120, q2_0112, q2_2012;
+    double q3_0101, q3_1212, q3_2020, q3_0120, q3_0112, q3_2012;
     int err = 0;
-    if (fabs(determ) < 0.0001) err |= kErrShakeSingular;
-    const double di = 1.0 / determ;
-    const double a11i = di * (a22 * a33 - a23 * a32), a12i = -di * (a12 * a33 - a13 * a32),
-                 a13i = di * (a12 * a23 - a13 * a22), a21i = -di * (a21 * a33 - a23 * a31),
-                 a22i = di * (a11 * a33 - a13 * a31), a23i = -di * (a11 * a23 - a13 * a21),
-                 a31i = di * (a21 * a32 - a22 * a31), a32i = -di * (a11 * a32 - a12 * a31),
-                 a33i = di * (a11 * a22 - a12 * a21);
-    const double r0120 = dot3(r01, r20), r0112 = dot3(r01, r12), r2012 = dot3(r20, r12);
-    const double q1_0101 = (im0 + im1) * (im0 + im1) * r01sq, q1_1212 = im1 * im1 * r12sq,
-                 q1_2020 = im0 * im0 * r02sq, q1_0120 = -2.0 * (im0 + im1) * im0 * r0120,
-                 q1_0112 = -2.0 * (im0 + im1) * im1 * r0112, q1_2012 = 2.0 * im0 * im1 * r2012;
-    const double q2_0101 = im1 * im1 * r01sq, q2_1212 = (im1 + im2) * (im1 + im2) * r12sq,
-                 q2_2020 = im2 * im2 * r02sq, q2_0120 = 2.0 * im1 * im2 * r0120,
-                 q2_0112 = -2.0 * (im1 + im2) * im1 * r0112, q2_2012 = -2.0 * (im1 + im2) * im2 * r2012;
-    const double q3_0101 = im0 * im0 * r01sq, q3_1212 = im2 * im2 * r12sq,
-                 q3_2020 = (im0 + im2) * (im0 + im2) * r02sq, q3_0120 = -2.0 * (im0 + im2) * im0 * r0120,
-                 q3_0112 = 2.0 * im0 * im2 * r0112, q3_2012 = -2.0 * (im0 + im2) * im2 * r2012;
+    {
+      double ox[3][3], ov[3][3], fo[3][3], sp[3][3];
+      for (int t = 0; t < 3; ++t) load(t, ox[t], ov[t], fo[t], ms[t], sp[t]);
+      double s10[3], s21[3], s02[3];
+      mdv(ox[1], ox[0], r01);
+      mdv(ox[2], ox[1], r12);
+      mdv(ox[0], ox[2], r20);
+      mdv(sp[0], sp[1], s10);
+      mdv(sp[1], sp[2], s21);
+      mdv(sp[2], sp[0], s02);
+      const double r01sq = dot3(r01, r01), r02sq = dot3(r20, r20), r12sq = dot3(r12, r12);
+      s01sq = dot3(s10, s10);
+      s02sq = dot3(s02, s02);
+      s12sq = dot3(s21, s21);
+      const double im0 = 1.0 / ms[0], im1 = 1.0 / ms[1], im2 = 1.0 / ms[2];
+      const double a11 = 2.0 * (im0 + im1) * dot3(s10, r01), a12 = -2.0 * im1 * dot3(s10, r12),
+                   a13 = -2.0 * im0 * dot3(s10, r20), a21 = -2.0 * im1 * dot3(s21, r01),
+                   a22 = 2.0 * (im1 + im2) * dot3(s21, r12), a23 = -2.0 * im2 * dot3(s21, r20),
+                   a31 = -2.0 * im0 * dot3(s02, r01), a32 = -2.0 * im2 * dot3(s02, r12),
+                   a33 = 2.0 * (im0 + im2) * (dot3(s02, r20));
+      const double determ = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a11 * a23 * a32 -
+                            a12 * a21 * a33 - a13 * a22 * a31;
+      if (fabs(determ) < 0.0001) err |= kErrShakeSingular;
+      const double di = 1.0 / determ;
+      a11i = di * (a22 * a33 - a23 * a32);
+      a12i = -di * (a12 * a33 - a13 * a32);
+      a13i = di * (a12 * a23 - a13 * a22);
+      a21i = -di * (a21 * a33 - a23 * a31);
+      a22i = di * (a11 * a33 - a13 * a31);
+      a23i = -di * (a11 * a23 - a13 * a21);
+      a31i = di * (a21 * a32 - a22 * a31);
+      a32i = -di * (a11 * a32 - a12 * a31);
+      a33i = di * (a11 * a22 - a12 * a21);
+      const double r0120 = dot3(r01, r20), r0112 = dot3(r01, r12), r2012 = dot3(r20, r12);
+      q1_0101 = (im0 + im1) * (im0 + im1) * r01sq;
+      q1_1212 = im1 * im1 * r12sq;
+      q1_2020 = im0 * im0 * r02sq;
+      q1_0120 = -2.0 * (im0 + im1) * im0 * r0120;
+      q1_0112 = -2.0 * (im0 + im1) * im1 * r0112;
+      q1_2012 = 2.0 * im0 * im1 * r2012;
+      q2_0101 = im1 * im1 * r01sq;
+      q2_1212 = (im1 + im2) * (im1 + im2) * r12sq;
+      q2_2020 = im2 * im2 * r02sq;
+      q2_0120 = 2.0 * im1 * im2 * r0120;
+      q2_0112 = -2.0 * (im1 + im2) * im1 * r0112;
+      q2_2012 = -2.0 * (im1 + im2) * im2 * r2012;
+      q3_0101 = im0 * im0 * r01sq;
+      q3_1212 = im2 * im2 * r12sq;
+      q3_2020 = (im0 + im2) * (im0 + im2) * r02sq;
+      q3_0120 = -2.0 * (im0 + im2) * im0 * r0120;
+      q3_0112 = 2.0 * im0 * im2 * r0112;
+      q3_2012 = -2.0 * (im0 + im2) * im2 * r2012;
+    }
     double l01 = 0.0, l20 = 0.0, l12 = 0.0;
     int niter = 0, done = 0;
     while (!done && niter < 5000) {  // bounded like the reference (max_iter 5000)
@@ -628,6 +655,7 @@ __global__ void k_shake(const SysDev* __restrict__ S, const int2* __restrict__ w
       niter++;
     }
     if (!done) err |= kErrShakeNoConverge;
+    const double im0 = 1.0 / ms[0], im1 = 1.0 / ms[1], im2 = 1.0 / ms[2];
     double pc[3][3];
     for (int k = 0; k < 3; ++k) {
       pc[0][k] = l01 * r01[k] * im0 - l20 * r20[k] * im0;
@@ -636,10 +664,12 @@ __global__ void k_shake(const SysDev* __restrict__ S, const int2* __restrict__ w
     }
     for (int t = 0; t < 3; ++t) {
       const int ii = id[t];
+      double ox[3], ov[3], fo[3], m, sp[3];
+      load(t, ox, ov, fo, m, sp);  // the same values as before the iteration
       double nv[3], nx[3];
       for (int k = 0; k < 3; ++k) {
-        nv[k] = (ov[t][k] + 0.5 * dt * fo[t][k] / ms[t] * fm) + pc[t][k] / dt;
-        double xx = sp[t][k] + pc[t][k];
+        nv[k] = (ov[k] + 0.5 * dt * fo[k] / m * fm) + pc[t][k] / dt;
+        double xx = sp[k] + pc[t][k];
         int img = s.image[3 * ii + k];
         if (xx < s.lo[k]) {
           xx += (s.hi[k] - s.lo[k]);
@@ -652,7 +682,7 @@ __global__ void k_shake(const SysDev* __restrict__ S, const int2* __restrict__ w
         nx[k] = xx;
         s.image[3 * ii + k] = img;
       }
-      s.v[ii] = make_double4(nv[0], nv[1], nv[2], ms[t]);
+      s.v[ii] = make_double4(nv[0], nv[1], nv[2], m);
       const double q = s.x[ii].w;
       s.x[ii] = make_double4(nx[0], nx[1], nx[2], q);
       // the cell list was built before the constraint (as the reference's locator is); refresh
