@@ -273,6 +273,7 @@ k_final(const SysDev* __restrict__ S, const int2* __restrict__ work, int mode) {
   __shared__ double2 s_r[256];
   __shared__ float4 s_kf[256];
   __shared__ float2 s_rf[256];
+  float4* s_kk = reinterpret_cast<float4*>(s_k);  // mixed precision: FP32 k vectors (s_k unused)
   __shared__ double s_part[kAtomBlock / 32][8];
 
   double4 xi = act ? s.x[i] : make_double4(0, 0, 0, 0);
@@ -307,7 +308,7 @@ k_final(const SysDev* __restrict__ S, const int2* __restrict__ work, int mode) {
           const int l = k0 + k;
           s_kf[k] = make_float4((float)s.km[3 * l], (float)s.km[3 * l + 1], (float)s.km[3 * l + 2], (float)kv.w);
           s_rf[k] = make_float2((float)re, (float)im);
-          s_k[k] = kv;
+          s_kk[k] = make_float4((float)kv.x, (float)kv.y, (float)kv.z, 0.0f);
         } else {
           s_k[k] = kv;
           s_r[k] = make_double2(re, im);
@@ -322,13 +323,13 @@ k_final(const SysDev* __restrict__ S, const int2* __restrict__ work, int mode) {
             float ph = m.x * ux + m.y * uy + m.z * uz;
             ph -= rintf(ph);
             float sn, cs;
-            sincospif(2.0f * ph, &sn, &cs);
+            __sincosf(6.28318531f * ph, &sn, &cs);  // hardware sin / cos: |2 pi ph| <= pi
             const float2 r = s_rf[k];
             const float Fs = m.w * q * (cs * r.y - sn * r.x);
-            const double4 kv = s_k[k];
-            gx += Fs * (float)kv.x;
-            gy += Fs * (float)kv.y;
-            gz += Fs * (float)kv.z;
+            const float4 kf = s_kk[k];
+            gx += Fs * kf.x;
+            gy += Fs * kf.y;
+            gz += Fs * kf.z;
           }
         } else {
           for (int k = 0; k < nch; ++k) {

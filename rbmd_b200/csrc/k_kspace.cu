@@ -146,14 +146,15 @@ __global__ void __launch_bounds__(256) k_rho(const SysDev* __restrict__ S, const
     const double4 k = kv[l];
     double re = 0.0, im = 0.0;
     if (MIXED && !ENERGY) {
-      // phase in turns m . (r / L), reduced to [-1/2, 1/2] before the FP32 sincos
+      // phase in turns m . (r / L), reduced to [-1/2, 1/2] before the FP32 sine and cosine (the
+      // SFU approximations, absolute error about 4e-7 on [-pi, pi])
       const float mxr = (float)s.km[3 * l], myr = (float)s.km[3 * l + 1], mzr = (float)s.km[3 * l + 2];
       for (int j = 0; j < na; ++j) {
         const float4 u = s_u[j];
         float ph = mxr * u.x + myr * u.y + mzr * u.z;
         ph -= rintf(ph);
         float sn, cs;
-        sincospif(2.0f * ph, &sn, &cs);
+        __sincosf(6.28318531f * ph, &sn, &cs);  // hardware sin / cos: |2 pi ph| <= pi
         re += (double)(u.w * cs);
         im += (double)(u.w * sn);
       }
