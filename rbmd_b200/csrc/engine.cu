@@ -1154,101 +1154,138 @@ int Context::set_step(int id, int64_t step) {
 }
 
 int Context::get_thermo(int id, rbmd_thermo* out) {
-  std::lock_guard<std::recursive_mutex> lk(mu);
-  System* s = find(id);
-  if (!s) return fail(RBMD_ERR_STATE, "unknown system id");
-  if (!out) return fail(RBMD_ERR_ARG, "null output");
-  int rc = refresh(s);
-  if (rc) return rc;
-  const SysDev& D = s->dev;
   int32_t one = id;
+  return get_thermo_many(&one, 1, out);
+}
+
+// Thermo of several systems with one force / energy evaluation per batch of compatible systems and
+// one synchronisation (the serving loop retires several systems per round).  Each system's
+// arithmetic is independent of the others in its batch, so the values equal get_thermo's alone.
+int Context::get_thermo_many(const int32_t* ids, int nsys, rbmd_thermo* outs) {
+  std::lock_guard<std::recursive_mutex> lk(mu);
+  if (!outs || nsys <= 0) return fail(RBMD_ERR_ARG, "null output");
+  struct Pending {
+    System* s = nullptr;
+    void* fsave = nullptr;
+    std::vector<double> te_step, te;
+    SysState st;
+  };
+  std::vector<Pending> ps(nsys);
+  int rc = RBMD_OK;
+  for (int q = 0; q < nsys; ++q) {
+    System* s = find(ids[q]);
+    if (!s) return fail(RBMD_ERR_STATE, "unknown system id");
+    rc = refresh(s);
+    if (rc) return rc;
+    ps[q].s = s;
+  }
   auto bs = [&] {
     rbmd_device_cfg saved = cfg;
-    cfg.batched = 0;
-    auto r = batches_for(&one, 1, rc);
+    cfg.batched = 1;
+    auto r = batches_for(ids, nsys, rc);
     cfg = saved;
     return r;
   }();
   if (rc) return rc;
-  const Batch& b = bs[0]->b;
-  // keep the step's forces: the pressure evaluation below recomputes them in FP64
-  void* fsave = dmalloc(sizeof(double4) * D.n);
-  if (!fsave) return fail(RBMD_ERR_OOM, "thermo scratch");
-  cudaMemcpyAsync(fsave, D.f, sizeof(double4) * D.n, cudaMemcpyDeviceToDevice, stream);
-  // NPT: bond and angle energies are those of the step's force evaluation, before the remap
-  // (PARA_BOND_ENERGY / PARA_ANGLE_ENERGY are set there and read by ThermoOutput::Execute)
-  std::vector<double> te_step(D.npt ? s->n_terms : 0);
-  if (!te_step.empty())
-    cudaMemcpyAsync(te_step.data(), D.term_energy, sizeof(double) * te_step.size(), cudaMemcpyDeviceToHost, stream);
-  cudaMemsetAsync(&D.st->virial[0], 0, sizeof(double) * 6, stream);
-  launch_cells(b, stream);
-  if (b.coul == RBMD_COUL_RBE) launch_rbe_sample(b, stream);
-  if (b.coul != RBMD_COUL_NONE) launch_rho(b, stream, b.coul == RBMD_COUL_EWALD);
-  if (b.has_bonded) launch_bonded(b, stream, 1);
-  launch_pair(b, stream, 1);
-  launch_final(b, stream, kFinalForceOnly, 1);
-  launch_energy(b, stream);
-  if (D.coul != RBMD_COUL_NONE) launch_ewald_energy(b, stream);
-  cudaMemcpyAsync(D.f, fsave, sizeof(double4) * D.n, cudaMemcpyDeviceToDevice, stream);
-  SysState st;
-  cudaMemcpyAsync(&st, D.st, sizeof(SysState), cudaMemcpyDeviceToHost, stream);
-  std::vector<double> te(s->n_terms);
-  if (s->n_terms) cudaMemcpyAsync(te.data(), D.term_energy, sizeof(double) * s->n_terms, cudaMemcpyDeviceToHost, stream);
-  dfree(fsave);
+  for (auto& p : ps) {
+    const SysDev& D = p.s->dev;
+    // keep the step's forces: the pressure evaluation below recomputes them in FP64
+    p.fsave = dmalloc(sizeof(double4) * D.n);
+    if (!p.fsave) {
+      for (auto& q : ps) dfree(q.fsave);
+      return fail(RBMD_ERR_OOM, "thermo scratch");
+    }
+    cudaMemcpyAsync(p.fsave, D.f, sizeof(double4) * D.n, cudaMemcpyDeviceToDevice, stream);
+    // NPT: bond and angle energies are those of the step's force evaluation, before the remap
+    // (PARA_BOND_ENERGY / PARA_ANGLE_ENERGY are set there and read by ThermoOutput::Execute)
+    p.te_step.resize(D.npt ? p.s->n_terms : 0);
+    if (!p.te_step.empty())
+      cudaMemcpyAsync(p.te_step.data(), D.term_energy, sizeof(double) * p.te_step.size(), cudaMemcpyDeviceToHost,
+                      stream);
+    cudaMemsetAsync(&D.st->virial[0], 0, sizeof(double) * 6, stream);
+  }
+  for (BatchRec* br : bs) {
+    const Batch& b = br->b;
+    launch_cells(b, stream);
+    if (b.coul == RBMD_COUL_RBE) launch_rbe_sample(b, stream);
+    if (b.coul != RBMD_COUL_NONE) launch_rho(b, stream, b.coul == RBMD_COUL_EWALD);
+    if (b.has_bonded) launch_bonded(b, stream, 1);
+    launch_pair(b, stream, 1);
+    launch_final(b, stream, kFinalForceOnly, 1);
+    launch_energy(b, stream);
+    if (b.coul != RBMD_COUL_NONE) launch_ewald_energy(b, stream);
+  }
+  for (auto& p : ps) {
+    const SysDev& D = p.s->dev;
+    cudaMemcpyAsync(D.f, p.fsave, sizeof(double4) * D.n, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(&p.st, D.st, sizeof(SysState), cudaMemcpyDeviceToHost, stream);
+    p.te.resize(p.s->n_terms);
+    if (p.s->n_terms)
+      cudaMemcpyAsync(p.te.data(), D.term_energy, sizeof(double) * p.s->n_terms, cudaMemcpyDeviceToHost, stream);
+    dfree(p.fsave);
+  }
   rc = sync();
   if (rc) return rc;
-  if (!te_step.empty() && st.step > 0) te.swap(te_step);
-  std::memset(out, 0, sizeof(*out));
-  const int n = D.n;
-  out->step = st.step;
-  out->temperature = st.temperature;
-  out->tempT_sum = st.tempT_sum;
-  out->kinetic_energy = st.tempT_sum / n * 0.5;
-  double eb = 0, ea = 0;
-  for (int t = 0; t < D.n_bonds; ++t) eb += te[t];
-  for (int t = 0; t < D.n_angles; ++t) ea += te[D.n_bonds + t];
-  double ed = 0;
-  for (int t = 0; t < D.n_dihedrals; ++t) ed += te[D.n_bonds + D.n_angles + t];
-  out->e_dihedral = D.n_dihedrals ? ed / D.n_dihedrals : 0.0;
-  out->e_bond = D.n_bonds ? eb / D.n_bonds : 0.0;
-  out->e_angle = D.n_angles ? ea / D.n_angles : 0.0;
-  if (D.ff == RBMD_FF_EAM) {
-    out->e_eam = (st.energy[2] + st.energy[3]) / n;
-  } else {
-    out->e_lj = st.energy[0] / n;
-    out->e_coul_near = st.energy[1] / n;
+  for (int q = 0; q < nsys; ++q) {
+    Pending& p = ps[q];
+    System* s = p.s;
+    const SysDev& D = s->dev;
+    const SysState& st = p.st;
+    std::vector<double>& te = p.te;
+    rbmd_thermo* out = outs + q;
+    if (!p.te_step.empty() && st.step > 0) te.swap(p.te_step);
+    std::memset(out, 0, sizeof(*out));
+    const int n = D.n;
+    out->step = st.step;
+    out->temperature = st.temperature;
+    out->tempT_sum = st.tempT_sum;
+    out->kinetic_energy = st.tempT_sum / n * 0.5;
+    double eb = 0, ea = 0;
+    for (int t = 0; t < D.n_bonds; ++t) eb += te[t];
+    for (int t = 0; t < D.n_angles; ++t) ea += te[D.n_bonds + t];
+    double ed = 0;
+    for (int t = 0; t < D.n_dihedrals; ++t) ed += te[D.n_bonds + D.n_angles + t];
+    out->e_dihedral = D.n_dihedrals ? ed / D.n_dihedrals : 0.0;
+    out->e_bond = D.n_bonds ? eb / D.n_bonds : 0.0;
+    out->e_angle = D.n_angles ? ea / D.n_angles : 0.0;
+    if (D.ff == RBMD_FF_EAM) {
+      out->e_eam = (st.energy[2] + st.energy[3]) / n;
+    } else {
+      out->e_lj = st.energy[0] / n;
+      out->e_coul_near = st.energy[1] / n;
+    }
+    if (D.coul != RBMD_COUL_NONE)
+      out->e_coul_far = D.qqr2e * st.energy[6] * ((2 * kPi / D.volume)) / n + s->self_energy;
+    if (D.ff == RBMD_FF_LJ_CUT) out->potential_energy = out->e_lj;
+    else if (D.ff == RBMD_FF_LJ_CUT_COUL_LONG) out->potential_energy = out->e_lj + out->e_coul_far + out->e_coul_near;
+    else if (D.ff == RBMD_FF_CVFF)
+      out->potential_energy =
+          out->e_lj + out->e_coul_far + out->e_coul_near + out->e_bond + out->e_angle + out->e_dihedral;
+    else out->potential_energy = out->e_eam;
+    out->total_energy = out->potential_energy + out->kinetic_energy;
+    double vir[6];
+    for (int k = 0; k < 6; ++k) vir[k] = st.virial[k];
+    if (s->p.fix_shake == RBMD_SHAKE_TRUE)
+      for (int k = 0; k < 6; ++k) vir[k] += st.shake_virial[k];
+    if (D.ff == RBMD_FF_EAM)
+      for (int k = 0; k < 6; ++k) vir[k] = 0;
+    out->pressure = (st.tdof * D.boltz * st.temperature + vir[0] + vir[1] + vir[2]) / 3.0 * (1.0 / D.volume) * D.nktv2p;
+    if (D.npt && st.step > 0) {
+      // NPT: the pressure of the step is the one the barostat used (PARA_PRESSURE,
+      // ExecutionNPT.cpp:1446), taken before the remap
+      out->pressure = st.baro_pressure;
+      for (int k = 0; k < 6; ++k) vir[k] = st.baro_virial[k];
+    }
+    for (int k = 0; k < 6; ++k) out->virial[k] = vir[k];
+    out->volume = D.volume;
+    for (int k = 0; k < 3; ++k) {
+      out->nhc_eta[k] = st.eta[k];
+      out->box_lo[k] = D.lo[k];
+      out->box_hi[k] = D.hi[k];
+    }
+    for (int k = 0; k < 4; ++k) out->nhc_eta_dot[k] = st.eta_dot[k];
+    out->status = st.status;
   }
-  if (D.coul != RBMD_COUL_NONE)
-    out->e_coul_far = D.qqr2e * st.energy[6] * ((2 * kPi / D.volume)) / n + s->self_energy;
-  if (D.ff == RBMD_FF_LJ_CUT) out->potential_energy = out->e_lj;
-  else if (D.ff == RBMD_FF_LJ_CUT_COUL_LONG) out->potential_energy = out->e_lj + out->e_coul_far + out->e_coul_near;
-  else if (D.ff == RBMD_FF_CVFF)
-    out->potential_energy =
-        out->e_lj + out->e_coul_far + out->e_coul_near + out->e_bond + out->e_angle + out->e_dihedral;
-  else out->potential_energy = out->e_eam;
-  out->total_energy = out->potential_energy + out->kinetic_energy;
-  double vir[6];
-  for (int k = 0; k < 6; ++k) vir[k] = st.virial[k];
-  if (s->p.fix_shake == RBMD_SHAKE_TRUE)
-    for (int k = 0; k < 6; ++k) vir[k] += st.shake_virial[k];
-  if (D.ff == RBMD_FF_EAM)
-    for (int k = 0; k < 6; ++k) vir[k] = 0;
-  out->pressure = (st.tdof * D.boltz * st.temperature + vir[0] + vir[1] + vir[2]) / 3.0 * (1.0 / D.volume) * D.nktv2p;
-  if (D.npt && st.step > 0) {
-    // NPT: the pressure of the step is the one the barostat used (PARA_PRESSURE,
-    // ExecutionNPT.cpp:1446), taken before the remap
-    out->pressure = st.baro_pressure;
-    for (int k = 0; k < 6; ++k) vir[k] = st.baro_virial[k];
-  }
-  for (int k = 0; k < 6; ++k) out->virial[k] = vir[k];
-  out->volume = D.volume;
-  for (int k = 0; k < 3; ++k) {
-    out->nhc_eta[k] = st.eta[k];
-    out->box_lo[k] = D.lo[k];
-    out->box_hi[k] = D.hi[k];
-  }
-  for (int k = 0; k < 4; ++k) out->nhc_eta_dot[k] = st.eta_dot[k];
-  out->status = st.status;
   return check_cuda("get_thermo");
 }
 

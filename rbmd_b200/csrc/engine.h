@@ -99,6 +99,7 @@ class Context {
   int set_state(int id, const double* x, const double* v, const int32_t* image);
   int set_step(int id, int64_t step);
   int get_thermo(int id, rbmd_thermo* out);
+  int get_thermo_many(const int32_t* ids, int n, rbmd_thermo* outs);
   int get_cells(int id, int32_t* dims, int32_t* coa, int32_t* sorted, int32_t* lo, int32_t* up);
   int get_rbl_lists(int id, int cap, int32_t* nc, int32_t* ns, int32_t* ids);
   int get_rbl_lists_static(int id, int cap, int32_t* nc, int32_t* ns, int32_t* ids);

@@ -306,28 +306,50 @@ void Server::loop() {
       round_steps_ += k;
     }
     lap(3);
-    // retire finished systems
-    std::vector<Request*> keep;
+    // retire finished systems: each one's state, then one thermo evaluation for all of them
+    std::vector<Request*> keep, retiring;
     for (Request* r : active_) {
-      if (r->remaining > 0 && !rc) {
-        keep.push_back(r);
-        continue;
-      }
+      if (r->remaining > 0 && !rc) keep.push_back(r);
+      else retiring.push_back(r);
+    }
+    std::vector<int> status(retiring.size(), rc);
+    for (size_t q = 0; q < retiring.size(); ++q) {
+      Request* r = retiring[q];
       const int n = r->desc.d.n_atoms;
       r->x.assign(3 * (size_t)n, 0.0);
       r->v.assign(3 * (size_t)n, 0.0);
-      int st = rc;
-      if (!st) st = ctx_->get_state(r->sys, r->x.data(), r->v.data(), nullptr);
-      lap(4);
-      if (!st) st = ctx_->get_thermo(r->sys, &r->thermo);
-      if (!st && r->thermo.status != 0) st = RBMD_ERR_NUMERIC;
-      lap(5);
+      if (!status[q]) status[q] = ctx_->get_state(r->sys, r->x.data(), r->v.data(), nullptr);
+    }
+    lap(4);
+    std::vector<int32_t> tids;
+    std::vector<size_t> tq;
+    for (size_t q = 0; q < retiring.size(); ++q)
+      if (!status[q]) {
+        tids.push_back(retiring[q]->sys);
+        tq.push_back(q);
+      }
+    if (!tids.empty()) {
+      std::vector<rbmd_thermo> th(tids.size());
+      const int trc = ctx_->get_thermo_many(tids.data(), (int)tids.size(), th.data());
+      for (size_t u = 0; u < tq.size(); ++u) {
+        Request* r = retiring[tq[u]];
+        if (trc) {
+          status[tq[u]] = trc;
+          continue;
+        }
+        r->thermo = th[u];
+        if (r->thermo.status != 0) status[tq[u]] = RBMD_ERR_NUMERIC;
+      }
+    }
+    lap(5);
+    for (size_t q = 0; q < retiring.size(); ++q) {
+      Request* r = retiring[q];
       ctx_->remove_system(r->sys);
-      lap(6);
       std::lock_guard<std::mutex> lk(mu_);
       used_ -= r->bytes;
-      finish(r, st);
+      finish(r, status[q]);
     }
+    lap(6);
     {
       std::lock_guard<std::mutex> lk(mu_);
       active_ = keep;

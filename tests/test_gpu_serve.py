@@ -34,8 +34,9 @@ def _alone(sd, nsteps):
     ctx.init(sid)
     ctx.step(sid, nsteps)
     x, v, _ = ctx.state(sid)
+    th = ctx.thermo(sid)
     ctx.close()
-    return x, v
+    return x, v, th
 
 
 @pytest.fixture(scope="module")
@@ -67,16 +68,20 @@ def _serve(mix, wait_between=None, **cfg):
 def test_serve_results_equal_alone(alone_results, cfg):
     mix = _mix()
     got = _serve(mix, **cfg)
-    for (sd, n), (xa, va), (x, v, th, st) in zip(mix, alone_results, got):
+    for (sd, n), (xa, va, tha), (x, v, th, st) in zip(mix, alone_results, got):
         assert st["status"] == 0 and th["status"] == 0
         assert st["atom_steps"] == sd.n * n
         assert np.array_equal(x, xa) and np.array_equal(v, va), sd.name
+        # the thermo of systems retired together (one batched evaluation) equals the thermo alone
+        for key in ("potential_energy", "kinetic_energy", "total_energy", "pressure", "e_lj", "e_coul_near",
+                    "e_coul_far", "e_bond", "e_angle", "temperature", "step"):
+            assert th[key] == tha[key], (sd.name, key)
 
 
 def test_serve_late_arrivals(alone_results):
     mix = _mix()
     got = _serve(mix, wait_between=1, steps_per_round=5)
-    for (xa, va), (x, v, _, st) in zip(alone_results, got):
+    for (xa, va, _), (x, v, _, st) in zip(alone_results, got):
         assert np.array_equal(x, xa) and np.array_equal(v, va)
 
 
@@ -88,7 +93,7 @@ def test_serve_hbm_budget_admission(alone_results):
     got = _serve(mix, hbm_budget_bytes=max(sizes) + min(sizes), steps_per_round=4)
     admits = [st["t_admit"] for _, _, _, st in got]
     assert admits == sorted(admits)
-    for (xa, va), (x, v, _, st) in zip(alone_results, got):
+    for (xa, va, _), (x, v, _, st) in zip(alone_results, got):
         assert np.array_equal(x, xa) and np.array_equal(v, va)
 
 
