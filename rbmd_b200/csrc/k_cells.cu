@@ -4,6 +4,8 @@
 // count (atomics) -> exclusive scan (one block per system) -> scatter (atomics) -> per-cell sort
 // by atom id (the stable order of the reference's sort of fresh 0..N-1 point ids) fused with the
 // gather of cell-ordered positions, charges and metadata that the pair kernel streams.
+#include <climits>
+
 #include "kernels.h"
 
 namespace rbmd {
@@ -75,32 +77,52 @@ __global__ void k_cells_scatter(const SysDev* __restrict__ S, const int2* __rest
   s.sorted[slot] = i;
 }
 
-// One thread per cell: order the cell's atoms by id (insertion sort; cells hold a few tens of
-// atoms) and write the cell-ordered copies of positions and metadata.
-__global__ void k_cells_sort_gather(const SysDev* __restrict__ S, const int2* __restrict__ work) {
+// One warp per cell (kSortWarps warps per block, each taking kCellBlock / kSortWarps cells of the
+// block's range): the cell's atom ids ranked by value with shuffles (cells of more than 32 atoms,
+// rare, are sorted by lane 0), then the cell-ordered copies of positions and metadata written by
+// consecutive lanes.  The order is the ids' ascending order, as before.
+constexpr int kSortWarps = 32;
+
+__global__ void __launch_bounds__(kSortWarps * 32) k_cells_sort_gather(const SysDev* __restrict__ S,
+                                                                     const int2* __restrict__ work) {
   const int2 w = work[blockIdx.x];
   const SysDev& s = S[w.x];
-  const int c = w.y + threadIdx.x;
-  if (c >= s.ncell) return;
-  const int b = s.cell_start[c], e = s.cell_start[c + 1];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned FULL = 0xffffffffu;
   int* ids = s.sorted;
-  for (int k = b + 1; k < e; ++k) {
-    const int key = ids[k];
-    int j = k - 1;
-    while (j >= b && ids[j] > key) {
-      ids[j + 1] = ids[j];
-      --j;
+  for (int cc = wid; cc < kCellBlock; cc += kSortWarps) {
+    const int c = w.y + cc;
+    if (c >= s.ncell) break;  // warp-uniform
+    const int b = s.cell_start[c], e = s.cell_start[c + 1], cnt = e - b;
+    if (cnt <= 32) {
+      const int id = lane < cnt ? ids[b + lane] : INT_MAX;
+      int rank = 0;
+      for (int j = 0; j < cnt; ++j) rank += __shfl_sync(FULL, id, j) < id ? 1 : 0;
+      __syncwarp();
+      if (lane < cnt) ids[b + rank] = id;
+      __syncwarp();
+    } else {
+      if (lane == 0)
+        for (int k = b + 1; k < e; ++k) {
+          const int key = ids[k];
+          int j = k - 1;
+          while (j >= b && ids[j] > key) {
+            ids[j + 1] = ids[j];
+            --j;
+          }
+          ids[j + 1] = key;
+        }
+      __syncwarp();
     }
-    ids[j + 1] = key;
-  }
-  for (int k = b; k < e; ++k) {
-    const int i = ids[k];
-    s.rank[i] = k;
-    const double4 p = s.x[i];
-    s.sx[k] = p;
-    s.sxf[k] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
-    const int4 m = s.meta[i];
-    s.smeta[k] = make_int4(i, m.x, m.y, m.z);
+    for (int k = b + lane; k < e; k += 32) {
+      const int i = ids[k];
+      s.rank[i] = k;
+      const double4 p = s.x[i];
+      s.sx[k] = p;
+      s.sxf[k] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
+      const int4 m = s.meta[i];
+      s.smeta[k] = make_int4(i, m.x, m.y, m.z);
+    }
   }
 }
 
@@ -109,7 +131,7 @@ void launch_cells(const Batch& b, cudaStream_t st) {
   k_cells_count<<<b.atom.n, kAtomBlock, 0, st>>>(b.sys, b.atom.d);
   k_cells_scan<<<b.nsys, 1024, 0, st>>>(b.sys, b.d_slots);
   k_cells_scatter<<<b.atom.n, kAtomBlock, 0, st>>>(b.sys, b.atom.d);
-  k_cells_sort_gather<<<b.cell.n, kCellBlock, 0, st>>>(b.sys, b.cell.d);
+  k_cells_sort_gather<<<b.cell.n, kSortWarps * 32, 0, st>>>(b.sys, b.cell.d);
   note_launch(5);
 }
 
