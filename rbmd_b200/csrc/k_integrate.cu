@@ -540,10 +540,12 @@ __global__ void __launch_bounds__(kAtomBlock) k_ke_thermostat(const SysDev* __re
 // ------------------------------------------------------------------ SHAKE / RATTLE
 __device__ inline double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
-// One thread per triple.  The atoms' old state is read again after the multiplier iteration
-// instead of being kept in registers across it (the reads hit L1 / L2): fewer live registers,
-// four blocks per SM instead of two, and the same arithmetic in the same order.
-__global__ void __launch_bounds__(128, 4) k_shake(const SysDev* __restrict__ S, const int2* __restrict__ work) {
+// One thread per triple.  The kernel waits on memory, not on arithmetic, so every load it needs
+// (old state, charge, image counters, cell rank) is issued up front, in one round, and only the
+// values the update needs after the multiplier iteration are kept (the unconstrained position and
+// the half-kicked velocity, formed as the update forms them); the arithmetic and its order are the
+// reference's.
+__global__ void __launch_bounds__(128, 3) k_shake(const SysDev* __restrict__ S, const int2* __restrict__ work) {
   // NewConstraintAWaterBondAngleWorklet, framework/run/worklet/MolecularWorklet.h:2367-2645
   const int2 wk = work[blockIdx.x];
   const SysDev& s = S[wk.x];
@@ -553,9 +555,21 @@ __global__ void __launch_bounds__(128, 4) k_shake(const SysDev* __restrict__ S, 
   if (a < s.n_triples) {
     const int id[3] = {s.angle_atoms[3 * a], s.angle_atoms[3 * a + 1], s.angle_atoms[3 * a + 2]};
     const double dt = s.dt, fm = s.fmt2v;
+    // every load of the triple in one round
+    double4 xo[3], vo[3], fo4[3];
+    double qa[3];
+    int img[3][3], rk[3];
+    for (int t = 0; t < 3; ++t) {
+      xo[t] = s.xold[id[t]];
+      vo[t] = s.vold[id[t]];
+      fo4[t] = s.f[id[t]];
+      qa[t] = s.x[id[t]].w;
+      rk[t] = s.rank[id[t]];
+      for (int k = 0; k < 3; ++k) img[t][k] = s.image[3 * id[t] + k];
+    }
     // old position, velocity, force and mass of atom t, and its unconstrained update
     auto load = [&](int t, double* ox, double* ov, double* fo, double& m, double* sp) {
-      const double4 x = s.xold[id[t]], v = s.vold[id[t]], f = s.f[id[t]];
+      const double4 x = xo[t], v = vo[t], f = fo4[t];
       ox[0] = x.x; ox[1] = x.y; ox[2] = x.z;
       ov[0] = v.x; ov[1] = v.y; ov[2] = v.z;
       fo[0] = f.x; fo[1] = f.y; fo[2] = f.z;
@@ -568,7 +582,7 @@ __global__ void __launch_bounds__(128, 4) k_shake(const SysDev* __restrict__ S, 
       o[0] = p[0] - q[0]; o[1] = p[1] - q[1]; o[2] = p[2] - q[2];
       min_image(o[0], o[1], o[2], s.L[0], s.L[1], s.L[2]);
     };
-    double ms[3], r01[3], r12[3], r20[3];
+    double ms[3], r01[3], r12[3], r20[3], spk[3][3], vh[3][3];
     double a11i, a12i, a13i, a21i, a22i, a23i, a31i, a32i, a33i, s01sq, s02sq, s12sq;
     double q1_0101, q1_1212, q1_2020, q1_0120, q1_0112, q1_2012;
     double q2_0101, q2_1212, q2_2020, q2_0120, q2_0112, q2_2012;
@@ -576,7 +590,13 @@ __global__ void __launch_bounds__(128, 4) k_shake(const SysDev* __restrict__ S, 
     int err = 0;
     {
       double ox[3][3], ov[3][3], fo[3][3], sp[3][3];
-      for (int t = 0; t < 3; ++t) load(t, ox[t], ov[t], fo[t], ms[t], sp[t]);
+      for (int t = 0; t < 3; ++t) {
+        load(t, ox[t], ov[t], fo[t], ms[t], sp[t]);
+        for (int k = 0; k < 3; ++k) {
+          spk[t][k] = sp[t][k];
+          vh[t][k] = ov[t][k] + 0.5 * dt * fo[t][k] / ms[t] * fm;  // the update's velocity before the correction
+        }
+      }
       double s10[3], s21[3], s02[3];
       mdv(ox[1], ox[0], r01);
       mdv(ox[2], ox[1], r12);
@@ -665,30 +685,29 @@ __global__ void __launch_bounds__(128, 4) k_shake(const SysDev* __restrict__ S, 
     }
     for (int t = 0; t < 3; ++t) {
       const int ii = id[t];
-      double ox[3], ov[3], fo[3], m, sp[3];
-      load(t, ox, ov, fo, m, sp);  // the same values as before the iteration
+      const double m = ms[t];
       double nv[3], nx[3];
       for (int k = 0; k < 3; ++k) {
-        nv[k] = (ov[k] + 0.5 * dt * fo[k] / m * fm) + pc[t][k] / dt;
-        double xx = sp[k] + pc[t][k];
-        int img = s.image[3 * ii + k];
+        nv[k] = vh[t][k] + pc[t][k] / dt;
+        double xx = spk[t][k] + pc[t][k];
+        int im = img[t][k];
         if (xx < s.lo[k]) {
           xx += (s.hi[k] - s.lo[k]);
-          img -= 1;
+          im -= 1;
         }
         if (xx > s.hi[k]) {
           xx -= (s.hi[k] - s.lo[k]);
-          img += 1;
+          im += 1;
         }
         nx[k] = xx;
-        s.image[3 * ii + k] = img;
+        s.image[3 * ii + k] = im;
       }
       s.v[ii] = make_double4(nv[0], nv[1], nv[2], m);
-      const double q = s.x[ii].w;
+      const double q = qa[t];
       s.x[ii] = make_double4(nx[0], nx[1], nx[2], q);
       // the cell list was built before the constraint (as the reference's locator is); refresh
       // the cell-ordered copies the pair kernel streams
-      const int k = s.rank[ii];
+      const int k = rk[t];
       s.sx[k] = make_double4(nx[0], nx[1], nx[2], q);
       s.sxf[k] = make_float4((float)nx[0], (float)nx[1], (float)nx[2], (float)q);
     }
