@@ -72,8 +72,9 @@ enum rbmd_units {            /* init_configuration.*.unit */
 };
 enum rbmd_precision {
   RBMD_PREC_FP64 = 0,        /* every kernel in FP64 */
-  RBMD_PREC_MIXED = 1        /* pair + RBE arithmetic FP32; positions, rho(k) sums, reductions,
-                                SHAKE, thermostat and barostat FP64 */
+  RBMD_PREC_MIXED = 1        /* pair + RBE arithmetic FP32; positions, rho(k) sums (of FP32
+                                partials over 32 atoms), reductions, SHAKE, thermostat and
+                                barostat FP64 */
 };
 enum rbmd_rbl_mode {
   RBMD_RBL_STRIDE = 0,       /* every pice-th shell atom in cell traversal order (reference) */

@@ -321,7 +321,7 @@ k_final(const SysDev* __restrict__ S, const int2* __restrict__ work, int mode) {
           for (int k = 0; k < nch; ++k) {
             const float4 m = s_kf[k];
             float ph = m.x * ux + m.y * uy + m.z * uz;
-            ph -= rintf(ph);
+            ph -= __fsub_rn(__fadd_rn(ph, 12582912.0f), 12582912.0f);  // rint on the FMA pipe, |ph| < 2^22
             float sn, cs;
             __sincosf(6.28318531f * ph, &sn, &cs);  // hardware sin / cos: |2 pi ph| <= pi
             const float2 r = s_rf[k];

@@ -149,14 +149,23 @@ __global__ void __launch_bounds__(256) k_rho(const SysDev* __restrict__ S, const
       // phase in turns m . (r / L), reduced to [-1/2, 1/2] before the FP32 sine and cosine (the
       // SFU approximations, absolute error about 4e-7 on [-pi, pi])
       const float mxr = (float)s.km[3 * l], myr = (float)s.km[3 * l + 1], mzr = (float)s.km[3 * l + 2];
-      for (int j = 0; j < na; ++j) {
-        const float4 u = s_u[j];
-        float ph = mxr * u.x + myr * u.y + mzr * u.z;
-        ph -= rintf(ph);
-        float sn, cs;
-        __sincosf(6.28318531f * ph, &sn, &cs);  // hardware sin / cos: |2 pi ph| <= pi
-        re += (double)(u.w * cs);
-        im += (double)(u.w * sn);
+      // FP32 partial sums over 32 atoms, added in FP64 (the SFU, which also converts FP32 to
+      // FP64, is this loop's bottleneck); the nearest integer of the phase by the 1.5 * 2^23
+      // addition (round to nearest even, |ph| < 2^22), on the FMA pipe
+      for (int j0 = 0; j0 < na; j0 += 32) {
+        const int j1 = min(na, j0 + 32);
+        float pr = 0.0f, pm = 0.0f;
+        for (int j = j0; j < j1; ++j) {
+          const float4 u = s_u[j];
+          float ph = mxr * u.x + myr * u.y + mzr * u.z;
+          ph -= __fsub_rn(__fadd_rn(ph, 12582912.0f), 12582912.0f);
+          float sn, cs;
+          __sincosf(6.28318531f * ph, &sn, &cs);  // hardware sin / cos: |2 pi ph| <= pi
+          pr += u.w * cs;
+          pm += u.w * sn;
+        }
+        re += (double)pr;
+        im += (double)pm;
       }
     } else {
       for (int j = 0; j < na; ++j) {
