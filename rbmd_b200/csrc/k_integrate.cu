@@ -262,7 +262,7 @@ __global__ void k_bonded(const SysDev* __restrict__ S, const int2* __restrict__ 
 
 // ------------------------------------------------------------------ final force + kick
 template <bool MIXED, bool VIRIAL>
-__global__ void __launch_bounds__(kAtomBlock)
+__global__ void __launch_bounds__(kAtomBlock, 4)
 k_final(const SysDev* __restrict__ S, const int2* __restrict__ work, int mode) {
   const int2 wk = work[blockIdx.x];
   const SysDev& s = S[wk.x];
