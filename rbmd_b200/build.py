@@ -67,7 +67,9 @@ def build(verbose=False, jobs=None):
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
     host_srcs = sorted(os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".cpp")) if os.path.isdir(HOST) else []
-    if host_srcs and _newer(host_srcs + [LIB] + [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".h")], BIN):
+    host_deps = [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith((".h", ".hpp"))] if host_srcs else []
+    host_deps.append(os.path.join(ROOT, "include", "rbmd_gpu.h"))
+    if host_srcs and _newer(host_srcs + [LIB] + host_deps, BIN):
         cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-o", BIN] + host_srcs + \
               ["-L", OUT, "-lrbmd_b200", "-Wl,-rpath,$ORIGIN", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)

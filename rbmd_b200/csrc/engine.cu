@@ -1401,7 +1401,18 @@ int Context::get_rbl_lists_static(int id, int cap, int32_t* nc, int32_t* ns, int
                                   " need " + std::to_string(need) + " ints of scratch; the static scratch holds " +
                                   std::to_string(kStaticListInts) + " (8 MiB)");
   int* scratch = nullptr;
-  cudaSetDevice(cfg.device);
+  // The scratch lookup needs the context's device current; the caller's current device is put
+  // back on every return, so an observer thread's own later CUDA work stays where it was.
+  struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+      if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+      if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+      if (prev >= 0) cudaSetDevice(prev);
+    }
+  } guard(cfg.device);
   const int e = static_list_scratch(&scratch);
   if (e) return fail(RBMD_ERR_CUDA, std::string("static list scratch: ") + cudaGetErrorString((cudaError_t)e));
   StaticLists L;

@@ -666,10 +666,15 @@ void MDApplication::ReadHyperParameters(const Json& hp) {
     else throw std::runtime_error("coulomb type \"" + t + "\" is not supported");
     P.coulomb_sample_num = (int32_t)cl->number("coulomb_sample_num", P.coulomb_sample_num);
     P.alpha = cl->number("alpha", P.alpha);
-    const std::vector<double> km = cl->numbers("kmax");
-    if (km.size() == 1) P.kmax[0] = P.kmax[1] = P.kmax[2] = (int32_t)km[0];
-    else if (km.size() == 3)
-      for (int k = 0; k < 3; ++k) P.kmax[k] = (int32_t)km[k];
+    // Coulomb::Execute (hyperparameters/Coulomb.cpp:40) reads kmax with GetVectorValue, which stops
+    // the run when the value is not an array (parser/Configuration.h:142-163), and the k loops index
+    // it per dimension: a scalar or a list of other than three entries is refused here too.
+    if (const Json* km = cl->find("kmax")) {
+      if (!km->is_array()) throw std::runtime_error("coulomb.kmax must be an array of three integers, e.g. [2, 2, 2]");
+      const std::vector<double> v = cl->numbers("kmax");
+      if (v.size() != 3) throw std::runtime_error("coulomb.kmax must hold three integers (one per dimension)");
+      for (int k = 0; k < 3; ++k) P.kmax[k] = (int32_t)v[k];
+    }
   }
   P.fix_shake = RBMD_SHAKE_NULL;
   if (const Json* ex = hp.find("extend")) {

@@ -53,12 +53,12 @@ def test_host_only_entry_points():
     assert L.rbmd_eam_read_funcfl(b"/nonexistent/file.eam", C.byref(A.EamFile()), None, None, None) == A.ERR_IO
 
 
-def test_struct_sizes_match_header():
+def test_struct_sizes_match_header(tmp_path):
     """ctypes mirrors of the ABI structs have the C layout (sizes from a C compile of the header)."""
     src = ('#include <stdio.h>\n#include "rbmd_gpu.h"\nint main(void) { printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", '
            'sizeof(rbmd_params), sizeof(rbmd_system_desc), sizeof(rbmd_thermo), sizeof(rbmd_serve_cfg), '
            'sizeof(rbmd_request_stats), sizeof(rbmd_device_cfg), sizeof(rbmd_tune_result), sizeof(rbmd_eam_setfl)); return 0; }\n')
-    exe = os.path.join(ROOT, "_work", "abi_sizes") if os.path.isdir(os.path.join(ROOT, "_work")) else "/tmp/abi_sizes"
+    exe = str(tmp_path / "abi_sizes")
     r = subprocess.run(["gcc", "-I", os.path.dirname(HEADER), "-x", "c", "-", "-o", exe], input=src,
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

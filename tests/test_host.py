@@ -51,7 +51,7 @@ def test_json_dialect_and_inbuild(rbmd_bin, tmp_path):
   "hyper_parameters": {
     "force_field": { "type": "LJ/CUT/COUL/LONG" },
     "neighbor": { "type": "RBL", "cut_off": 1.9, "r_core": 1.0, "neighbor_sample_num": 20, },
-    "coulomb": { "type": "RBE", "coulomb_sample_num": 50, "alpha": 0.7, "kmax": 2 },
+    "coulomb": { "type": "RBE", "coulomb_sample_num": 50, "alpha": 0.7, "kmax": [ 2, 2, 2 ] },
     "extend": { },
   },
   "execution": { "ensemble": "NVT", "temperature": [ 1.5, 1.5, 0.2 ], "temp_ctrl_type": "BERENDSEN",
@@ -149,6 +149,9 @@ def test_eam_potential_file(rbmd_bin, tmp_path, oracle_mod):
     (lambda cfg: cfg["init_configuration"]["read_data"].update(atom_style="molecular"), "atom_style"),
     (lambda cfg: cfg["init_configuration"]["read_data"].update(file="missing.data"), "missing.data"),
     (lambda cfg: cfg["hyper_parameters"]["force_field"].update(type="OPLS-AA"), "OPLS-AA"),
+    # Coulomb::Execute reads kmax as an array (hyperparameters/Coulomb.cpp:40) and stops otherwise
+    (lambda cfg: cfg["hyper_parameters"]["coulomb"].update(kmax=2), "kmax"),
+    (lambda cfg: cfg["hyper_parameters"]["coulomb"].update(kmax=[2, 2]), "kmax"),
 ])
 def test_errors_are_reported(rbmd_bin, tmp_path, mutate, message):
     sd = synth.spce_water(n_mol=8)
