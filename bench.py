@@ -195,7 +195,7 @@ def kernel_profile(ctx, ids, systems):
     ctx.step(ids, 2)
     ctx.sync()
     out = {}
-    for name in ("nhc", "kick_drift", "cells", "shake", "rbe_sample", "rho", "bonded", "pair_tile", "pair_lean",
+    for name in ("nhc", "kick_drift", "cells", "shake", "rbe_sample", "rho", "bonded", "pair_col", "pair_tile", "pair_lean",
                  "pair_atom", "final", "rattle"):
         ms, n, units = ctx.profile_get(name)
         if n:
@@ -298,6 +298,139 @@ def measure_traj_accuracy(device, sizes=(1000, 4000, 16000, 64000), checkpoints=
     return {"aggregate_rel_rms": (num / den) ** 0.5, "systems": per, "steps_between": every}
 
 
+def ewald_kspace_forces(x, q, L, alpha, kmax, qqr2e=1.0, chunk=4096):
+    """The reciprocal-space Ewald force alone, F_i = (4 pi / V) qqr2e q_i sum_k exp(-k^2 / 4 alpha)
+    / k^2 k Im(exp(i k.r_i) conj(rho_k)), rho_k = sum_j q_j exp(i k.r_j), over m in
+    [-kmax, kmax]^3 without 0 (the k-space part of ExecutionMD::ComputeChargeStructureFactorEwald +
+    ComputeNewFarElectrostaticsWorklet, RunWorklet.cpp:2492-2540), in numpy: the denominator of the
+    k-space-only RBE error."""
+    L = np.asarray(L, np.float64)
+    g = [np.arange(-k, k + 1) for k in kmax]
+    m = np.stack(np.meshgrid(*g, indexing="ij"), -1).reshape(-1, 3)
+    m = m[(m != 0).any(1)]
+    kv = 2 * np.pi * m / L
+    k2 = (kv * kv).sum(1)
+    w = np.exp(-k2 / (4 * alpha)) / k2
+    V = float(np.prod(L))
+    F = np.zeros_like(x)
+    for a in range(0, len(kv), chunk):
+        kk, ww = kv[a:a + chunk], w[a:a + chunk]
+        e = np.exp(1j * (x @ kk.T))                     # [n, k]
+        rho = (q[:, None] * e).sum(0)                   # [k]
+        im = (e * np.conj(rho)[None, :]).imag * ww[None, :]
+        F += im @ kk
+    return F * (4 * np.pi / V) * qqr2e * q[:, None]
+
+
+def converged_kmax(L, alpha, tol=1e-12):
+    """Smallest |m| per dimension with exp(-k^2 / 4 alpha) < tol beyond it."""
+    kc = math.sqrt(-4.0 * alpha * math.log(tol))
+    return [int(math.ceil(kc * l / (2 * math.pi))) for l in L]
+
+
+def measure_rbe_curve(device, n=1000, Ps=(100, 400, 1600, 6400), seeds=(1, 2, 3)):
+    """RBE against full Ewald on one saline system of the stream's parameters (FP64 on both sides,
+    converged Ewald kmax, the same RBL picks): total-force relative RMS ||F_rbe - F_ewald|| /
+    ||F_ewald|| and k-space-only ||F_rbe - F_ewald|| / ||F_k|| (F_k the reciprocal-space Ewald force
+    alone) at P = 100 ... 6400 k samples, averaged over Philox seeds, with the least-squares slope of
+    log(error) against log(P) (-0.5 for a variance-limited estimator) and the P at which the
+    total-force error would reach 1e-3 on that line."""
+    import rbmd_b200
+    from rbmd_b200 import _abi as A, synth
+    sd = synth.saline(n, seed=11, precision=A.PREC_FP64)
+    L = sd.box_hi - sd.box_lo
+    km = converged_kmax(L, sd.params.alpha)
+    ctx = rbmd_b200.Context(device=device)
+    ew = sd.copy()
+    ew.params.coulomb = A.COUL_EWALD
+    ew.params.kmax[:] = km
+    sid = ctx.add_system(ew)
+    ctx.compute_forces(sid)
+    f_ew = ctx.forces(sid)
+    ctx.remove_system(sid)
+    f_k = ewald_kspace_forces(sd.pos, sd.charge, L, sd.params.alpha, km, qqr2e=332.06371)
+    rows = []
+    for P in Ps:
+        tot, ks = [], []
+        for seed in seeds:
+            s2 = sd.copy()
+            s2.params.coulomb_sample_num = P
+            s2.params.seed = seed
+            sid = ctx.add_system(s2)
+            ctx.compute_forces(sid)
+            d = ctx.forces(sid) - f_ew
+            ctx.remove_system(sid)
+            tot.append(float(np.sqrt((d * d).sum() / (f_ew * f_ew).sum())))
+            ks.append(float(np.sqrt((d * d).sum() / (f_k * f_k).sum())))
+        rows.append({"P": P, "total_rel_rms": float(np.mean(tot)), "kspace_rel_rms": float(np.mean(ks)),
+                     "seeds": len(seeds)})
+    ctx.close()
+    lp = np.log([r["P"] for r in rows])
+    slope, icpt = np.polyfit(lp, np.log([r["total_rel_rms"] for r in rows]), 1)
+    kslope, _ = np.polyfit(lp, np.log([r["kspace_rel_rms"] for r in rows]), 1)
+    p_needed = float(math.exp((math.log(1e-3) - icpt) / slope)) if slope < 0 else None
+    return {"atoms": sd.n, "ewald_kmax": km, "curve": rows, "slope_total": float(slope), "slope_kspace": float(kslope),
+            "P_for_1e-3_total": p_needed}
+
+
+def measure_saline_energy(device, n=4000, steps=1000, every=50):
+    """Energies of the served configuration (saline, RBE P = 100 + RBL, SHAKE, dt 1 fs), per atom in
+    kcal/mol: (i) NVT (Nose-Hoover, the served ensemble) in mixed precision against FP64 on the same
+    Philox stream: the largest |E_mixed - E_fp64| along the run, absolute and relative to |PE_0| (the
+    mixed path's energy error; the two trajectories decorrelate chaotically over the run);
+    (ii) NVE drift E_end - E_0 for RBE + RBL in mixed precision and in FP64 (same draws: the mixed
+    path's drift must match the FP64 one) and for FP64 full Ewald with Verlet lists, a force that is
+    the gradient of the reported energy (the integrator and SHAKE alone).  RBL's sampled shells and
+    RBE's sampled k vectors make the served force a random estimate of that gradient, so its NVE
+    energy is not conserved: that heating is the method's, equal in both precisions."""
+    import rbmd_b200
+    from rbmd_b200 import _abi as A, synth
+    base = synth.saline(n, seed=21)
+    base.params.seed = 5
+    L = base.box_hi - base.box_lo
+
+    def run(prec, coul, nve, verlet=False):
+        sd = base.copy()
+        sd.params.precision = prec
+        if nve:
+            sd.params.temp_ctrl = A.TC_NONE
+            sd.params.ensemble = A.ENS_NVE
+        if coul == A.COUL_EWALD:
+            sd.params.coulomb = A.COUL_EWALD
+            sd.params.kmax[:] = converged_kmax(L, sd.params.alpha)
+        if verlet:
+            sd.params.neighbor = A.NEIGH_VERLET
+        ctx = rbmd_b200.Context(device=device)
+        sid = ctx.add_system(sd)
+        ctx.init(sid)
+        th = ctx.thermo(sid)
+        e, pe0 = [th["total_energy"]], th["potential_energy"]
+        for _ in range(steps // every):
+            ctx.step(sid, every)
+            e.append(ctx.thermo(sid)["total_energy"])
+        st = ctx.thermo(sid)["status"]
+        ctx.close()
+        return np.array(e), pe0, st
+
+    ps = steps * float(base.params.timestep) * 1e-3
+    out = {"atoms": base.n, "steps": steps, "every": every, "ps": ps, "unit": "kcal/mol per atom"}
+    e_m, pe0, s1 = run(A.PREC_MIXED, A.COUL_RBE, False)
+    e_d, _, s2 = run(A.PREC_FP64, A.COUL_RBE, False)
+    d = float(np.abs(e_m - e_d).max())
+    out["nvt_mixed_vs_fp64"] = {"max_abs": d, "rel_to_pe0": d / abs(pe0), "pe0": pe0, "e0": float(e_d[0])}
+    drift = {}
+    for tag, prec, coul, verlet in (("rbe_rbl_mixed", A.PREC_MIXED, A.COUL_RBE, False),
+                                    ("rbe_rbl_fp64", A.PREC_FP64, A.COUL_RBE, False),
+                                    ("ewald_verlet_fp64", A.PREC_FP64, A.COUL_EWALD, True)):
+        e, _, st = run(prec, coul, True, verlet)
+        drift[tag] = {"drift": float(e[-1] - e[0]), "per_ps": float((e[-1] - e[0]) / ps),
+                      "max_excursion": float(np.abs(e - e[0]).max()), "status": int(st)}
+    out["nve"] = drift
+    out["nve_drift_mixed_minus_fp64"] = drift["rbe_rbl_mixed"]["drift"] - drift["rbe_rbl_fp64"]["drift"]
+    out["status"] = [int(s1), int(s2)]
+    return out
+
+
 def measure_drift(device, steps=1000, every=100):
     """Energy conservation of the LJ fluid (4000 atoms, RBL rs 1.2 with 100 shell samples, NVE,
     dt 0.005): total energy per atom every `every` steps in FP64 and in mixed precision.  Reports
@@ -357,48 +490,101 @@ def measure_e2e(systems, arrivals, args, device):
                 atom_steps=atom_steps)
 
 
-def cpu_port_rate(seconds, threads=None):
-    """The FP64 CPU restatement of the reference algorithm on a sample of the workload: one 1000-atom
-    saline system stepped until `seconds` of CPU time."""
+STRATA = ((1000, 4000), (4000, 16000), (16000, 64001))  # log-thirds of the stream's size range
+
+
+def stream_strata(n_requests, seed=7):
+    """The serving stream's sizes in three log-size strata: per stratum the request nearest its
+    median size (the system the CPU runs) and the stratum's share of the stream's atoms (its
+    weight in the throughput)."""
+    from rbmd_b200 import synth
+    sizes, _ = synth.serving_stream(n_requests=n_requests, seed=seed)
+    out = []
+    for lo, hi in STRATA:
+        s = np.sort(sizes[(sizes >= lo) & (sizes < hi)])
+        if s.size == 0:
+            continue
+        out.append(dict(lo=lo, hi=hi, requests=int(s.size), atoms=int(s.sum()), size=int(s[s.size // 2])))
+    return out
+
+
+def cpu_stream_rate(n_requests, steps=None, warmup=1, seconds=None, threads=None):
+    """The FP64 CPU restatement of the reference algorithm on a size-stratified sample of the
+    serving stream: one system per stratum (the stratum's median size, the stream's own
+    parameters), `warmup` untimed then `steps` timed steps of each (or steps until `seconds` of
+    wall time), on `threads` host threads.  The stream's throughput follows from the per-stratum
+    rates r_k weighted by the strata's atoms w_k: sum(w) / sum(w / r), the rate at which the CPU
+    would work through the stream's atom-steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_ffi
     from rbmd_b200 import _abi as A, synth
     # the oracle's loops run on RBMD_ORACLE_THREADS std::threads, fixed at its first parallel loop
     threads = threads or (os.cpu_count() or 1)
     os.environ["RBMD_ORACLE_THREADS"] = str(threads)
-    sd = synth.saline(1000, seed=3)
-    sd.params.precision = A.PREC_FP64
-    o = oracle_ffi.Oracle(sd)
-    o.init()
-    o.step(1)
-    t0 = time.perf_counter()
-    steps = 0
-    while time.perf_counter() - t0 < seconds:
-        o.step(1)
-        steps += 1
-    dt = time.perf_counter() - t0
-    return dict(value=sd.n * steps / dt, unit=UNIT, cores=threads, kind="port",
-                sample=f"one {sd.n}-atom saline system of the stream's parameters, {steps} NVT steps in {dt:.1f} s")
+    strata = stream_strata(n_requests)
+    systems = []
+    for k, st in enumerate(strata):
+        sd = synth.saline(st["size"], seed=3 + k)
+        sd.params.precision = A.PREC_FP64
+        o = oracle_ffi.Oracle(sd)
+        o.init()
+        o.step(warmup)
+        systems.append((sd, o))
+    per_step = [0.0] * len(systems)
+    done = 0
+    t_all = time.perf_counter()
+    while True:
+        for k, (sd, o) in enumerate(systems):
+            t0 = time.perf_counter()
+            o.step(1)
+            per_step[k] += time.perf_counter() - t0
+        done += 1
+        if steps is not None and done >= steps:
+            break
+        if steps is None and time.perf_counter() - t_all >= (seconds or 10.0) and done >= 2:
+            break
+    rates = [sd.n * done / t for (sd, _), t in zip(systems, per_step)]
+    w = [st["atoms"] for st in strata]
+    value = sum(w) / sum(wk / rk for wk, rk in zip(w, rates))
+    desc = ", ".join(f"{sd.n} atoms for [{st['lo']}, {st['hi']}) ({st['requests']} requests, "
+                     f"{r:.3g} atom-steps/s)" for (sd, _), st, r in zip(systems, strata, rates))
+    return dict(value=value, unit=UNIT, cores=threads, kind="port",
+                sample=f"size-stratified sample of the stream: {done} FP64 NVT steps each of {desc}; "
+                       "throughput weighted by each stratum's atoms",
+                strata=[dict(st, rate=r) for st, r in zip(strata, rates)], steps=done)
 
 
-PAIR_KERNELS = {"pair_tile": "k_pair_tile (warp per home cell: shared candidate batches, RBL picks, LJ + erfc)",
+PAIR_KERNELS = {"pair_col": "k_pair_col (warp per column of home cells, lane per atom over a staged row: RBL picks, LJ + erfc)",
+                "pair_tile": "k_pair_tile (warp per home cell: shared candidate batches, RBL picks, LJ + erfc)",
                 "pair_lean": "k_pair2 (warp per atom with segment tables)", "pair_atom": "k_pair (general warp per atom)"}
 
 
-def profiled_traffic(name):
-    """DRAM bytes (read + write) per atom of a pair kernel, from its committed ncu summary
-    profiles/k_<name>_saline_small.md (line "traffic_bytes_per_atom: X"); None without one."""
+def profiled_figures(name):
+    """Machine-readable figures ("key: value" lines) of a pair kernel's committed ncu summary
+    profiles/k_<name>_saline_small.md: traffic_bytes_per_atom, issue_active_pct,
+    warp_inst_per_atom; {} without one."""
     path = os.path.join(ROOT, "profiles", f"k_{name}_saline_small.md")
+    out = {}
     if not os.path.exists(path):
-        return None
+        return out
     for line in open(path):
-        if line.strip().startswith("traffic_bytes_per_atom:"):
-            return float(line.split(":", 1)[1])
-    return None
+        key, sep, val = line.strip().partition(":")
+        if sep and key in ("traffic_bytes_per_atom", "issue_active_pct", "warp_inst_per_atom"):
+            try:
+                out[key] = float(val)
+            except ValueError:
+                pass
+    out["source"] = f"profiles/k_{name}_saline_small.md"
+    return out
 
 
 def roofline(prof, pairs_per_atom, peaks, fp32_peak):
-    """Roofline of the dominant pair kernel (largest device time over the profiled steps)."""
+    """Roofline of the dominant pair kernel (largest device time over the profiled steps).  Its
+    bound is the FP32 pipe (the pair arithmetic and the selection around it are FP32 / integer
+    issue; SFU ops -- rsqrt, ex2, rcp -- are counted as one flop each, not separately weighted):
+    achieved = 40 flops per selected pair (26 LJ + 14 real-space Coulomb) x pairs per atom x
+    atoms per launch / the launch's CUDA-event time.  The HBM view (64 algorithmic bytes per atom)
+    is the secondary entry."""
     recs = {k: v for k, v in prof.items() if k in PAIR_KERNELS}
     if not recs:
         return None, None
@@ -412,39 +598,70 @@ def roofline(prof, pairs_per_atom, peaks, fp32_peak):
     flops = (26 + 14) * pairs_per_atom * atoms  # LJ + Coulomb pair convention (flops per pair)
     hbm = peaks.get("hbm_gbs", 6650.0)
     achieved_gbs = bytes_alg / secs / 1e9
-    tpa = profiled_traffic(name)
-    r_hbm = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s", "frac": achieved_gbs / hbm,
-             "traffic": None if tpa is None else tpa * atoms, "kernel": PAIR_KERNELS[name],
-             "launch_ms": p["avg_ms"], "atoms_per_launch": atoms, "bytes_alg_per_atom": 64.0,
-             "traffic_source": None if tpa is None else f"profiles/k_{name}_saline_small.md, scaled by atoms",
-             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+    fig = profiled_figures(name)
+    tpa = fig.get("traffic_bytes_per_atom")
+    traffic = None if tpa is None else tpa * atoms
+    traffic_src = None if tpa is None else \
+        f"{fig['source']} (ncu dram__bytes_read.sum + dram__bytes_write.sum on 64 stream systems), scaled by atoms"
     tf = flops / secs / 1e12
     r_fp32 = {"bound": "fp32", "achieved": tf, "peak": fp32_peak, "unit": "TFLOP/s",
-              "frac": tf / fp32_peak if fp32_peak else None,
-              "peak_source": "FFMA-chain microbenchmark in this run (rbmd_fma_peak)",
-              "flops_per_pair": 40, "pairs_per_atom": pairs_per_atom}
-    return r_hbm, r_fp32
+              "frac": tf / fp32_peak if fp32_peak else None, "traffic": traffic, "traffic_source": traffic_src,
+              "kernel": PAIR_KERNELS[name], "launch_ms": p["avg_ms"], "atoms_per_launch": atoms,
+              "peak_source": "FFMA-chain microbenchmark in this run (rbmd_fma_peak), of measured",
+              "flops_per_pair": 40, "pairs_per_atom": pairs_per_atom,
+              "issue_active_pct": fig.get("issue_active_pct"), "warp_inst_per_atom": fig.get("warp_inst_per_atom"),
+              "issue_source": fig.get("source")}
+    r_hbm = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s", "frac": achieved_gbs / hbm,
+             "traffic": traffic, "traffic_source": traffic_src, "bytes_alg_per_atom": 64.0,
+             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+    return r_fp32, r_hbm
 
 
 def run_reference(args, dist):
-    """--impl reference: the CPU restatement of the reference algorithm on all host cores."""
+    """--impl reference: the CPU restatement of the reference algorithm on all host cores, on a
+    size-stratified sample of the same stream (each step one FP64 step of each stratum's system)."""
     if dist.rank != 0:
         return
     cores = os.cpu_count() or 1
-    r = cpu_port_rate(max(5.0, args.cpu_seconds), threads=cores)
+    r = cpu_stream_rate(args.requests, steps=args.steps, warmup=args.warmup, threads=cores)
     line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "impl": "reference", "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "parallelism": "cpu"},
+            "config": {"workload": WORKLOAD + "; CPU: size-stratified sample (one system per log-size third, "
+                       "weighted by the stream's atoms in it)", "parallelism": "cpu"},
             "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port",
                              "sample": r["sample"]},
+            "strata": r["strata"],
             "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "reference binary needs VTK-m 1.9 (absent); this is the FP64 C++ restatement of its algorithm"}
     print(json.dumps(line), flush=True)
 
 
+def launch_ranks(args):
+    """`--gpus N` without a torchrun environment: start N ranks (one process per GPU, rendezvous on
+    127.0.0.1) through torch.distributed.run and return its exit code; None when this process is
+    already a rank (or N is 1).  A rank whose WORLD_SIZE differs from --gpus is an error."""
+    world = os.environ.get("WORLD_SIZE")
+    if world is not None:
+        if int(world) != args.gpus:
+            raise SystemExit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}")
+        return None
+    if args.gpus <= 1:
+        return None
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
+    rc = launch_ranks(args)
+    if rc is not None:
+        sys.exit(rc)
     dist = Dist()
     if args.impl == "reference":
         run_reference(args, dist)
@@ -468,13 +685,15 @@ def main():
     for sid in ids:
         ctx.remove_system(sid)
     ctx.close()
-    r_hbm, r_fp32 = roofline(prof, ppa, peaks, fp32_peak)
+    r_fp32, r_hbm = roofline(prof, ppa, peaks, fp32_peak)
     extra = {}
     if dist.rank == 0:
         if not args.skip_accuracy:
             extra["accuracy"] = measure_accuracy(device)
             extra["accuracy"]["trajectory_mixed_vs_fp64"] = measure_traj_accuracy(device)
             extra["drift"] = measure_drift(device)
+            extra["rbe_curve"] = measure_rbe_curve(device)
+            extra["saline_energy"] = measure_saline_energy(device)
         if not args.skip_plain:
             extra["plain_fp64"] = measure_plain(systems, args, device)
     e2e = None
@@ -483,7 +702,7 @@ def main():
         e2e_val = dist.reduce(e2e["value"], "sum")
     dist.barrier()
     if dist.rank == 0:
-        cpu = None if args.skip_cpu else cpu_port_rate(args.cpu_seconds, threads=1)
+        cpu = None if args.skip_cpu else cpu_stream_rate(args.requests, seconds=args.cpu_seconds)
         plain = extra.get("plain_fp64")
         line = {
             "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
@@ -493,7 +712,7 @@ def main():
             "config": {"workload": WORKLOAD, "n_systems_per_gpu": len(systems), "atoms_per_gpu": res["atoms_rank"],
                        "atoms_total": res["atoms_all"], "batched_step_per_launch": True, "parallelism": f"dp{dist.world} (independent systems)",
                        "l2": "inputs larger than L2 (all systems resident, >1 GB)"},
-            "roofline": r_hbm, "roofline_fp32": r_fp32,
+            "roofline": r_fp32, "roofline_hbm": r_hbm,
             "pipe_peaks_tflops": {"fp32": fp32_peak, "fp64": fp64_peak},
             "cpu_baseline": cpu,
             "clocks": res["clocks"],
@@ -508,6 +727,8 @@ def main():
         if "accuracy" in extra:
             line["force_rel_rms"] = extra["accuracy"]
             line["energy_drift"] = extra["drift"]
+            line["rbe_vs_ewald_curve"] = extra["rbe_curve"]
+            line["served_config_energy"] = extra["saline_energy"]
         if e2e is not None:
             line["e2e"] = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"],
                            "d2h_bytes_per_step": e2e["d2h"], "wall_s": e2e["wall_s"], "p50_latency_s": e2e["p50_s"],

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBMD_ABI_VERSION 4
+#define RBMD_ABI_VERSION 5
 
 /* ---------------------------------------------------------------- status codes */
 enum rbmd_status {
@@ -484,13 +484,16 @@ int rbmd_step_timed(rbmd_ctx* ctx, const int32_t* sys_ids, int32_t n, int32_t ns
 enum rbmd_pair_layout {
   RBMD_LAYOUT_TILE = 0,     /* warp per home cell, candidate batches shared by the cell's atoms */
   RBMD_LAYOUT_LEAN = 1,     /* warp per atom over per-row segment tables (dims >= 2 nc + 1) */
-  RBMD_LAYOUT_GENERAL = 2   /* warp per atom, any box */
+  RBMD_LAYOUT_GENERAL = 2,  /* warp per atom, any box */
+  RBMD_LAYOUT_COLUMN = 3    /* warp per column of home cells, lane per atom walking its own candidate
+                               window of a shared staged row (mixed-precision RBL forces of LJ/CUT,
+                               LJ/CUT/COUL/LONG and CVFF; the tile layout's boxes) */
 };
 typedef struct rbmd_tune_result {
   int32_t n_systems;        /* systems of the group (grouped as rbmd_step batches them) */
   int32_t layout;           /* chosen enum rbmd_pair_layout */
   int64_t atoms;            /* atoms of the group */
-  double ms[3];             /* measured pair-kernel time per layout (index = layout); -1: unusable or
+  double ms[4];             /* measured pair-kernel time per layout (index = layout); -1: unusable or
                                not timed */
   int32_t from_cache;       /* 1: taken from an earlier decision for the same signature */
   int32_t pad0;

@@ -5,7 +5,7 @@ a probe with the host compiler.
 """
 import ctypes as C
 
-RBMD_ABI_VERSION = 4
+RBMD_ABI_VERSION = 5
 
 # status
 OK, ERR_ARG, ERR_OOM, ERR_NUMERIC, ERR_TIMEOUT, ERR_CUDA, ERR_STATE, ERR_BUDGET, ERR_UNSUPPORTED, ERR_IO = range(10)
@@ -116,17 +116,17 @@ class DeviceCfg(C.Structure):
                 ("autotune", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
 
 
-LAYOUT_TILE, LAYOUT_LEAN, LAYOUT_GENERAL = 0, 1, 2
-LAYOUT_NAMES = {LAYOUT_TILE: "tile", LAYOUT_LEAN: "lean", LAYOUT_GENERAL: "general"}
+LAYOUT_TILE, LAYOUT_LEAN, LAYOUT_GENERAL, LAYOUT_COLUMN = 0, 1, 2, 3
+LAYOUT_NAMES = {LAYOUT_TILE: "tile", LAYOUT_LEAN: "lean", LAYOUT_GENERAL: "general", LAYOUT_COLUMN: "column"}
 
 
 class TuneResult(C.Structure):
-    _fields_ = [("n_systems", C.c_int32), ("layout", C.c_int32), ("atoms", C.c_int64), ("ms", C.c_double * 3),
+    _fields_ = [("n_systems", C.c_int32), ("layout", C.c_int32), ("atoms", C.c_int64), ("ms", C.c_double * 4),
                 ("from_cache", C.c_int32), ("pad0", C.c_int32)]
 
     def as_dict(self):
         return dict(n_systems=self.n_systems, layout=LAYOUT_NAMES[self.layout], atoms=self.atoms,
-                    ms={LAYOUT_NAMES[k]: self.ms[k] for k in range(3)}, from_cache=bool(self.from_cache))
+                    ms={LAYOUT_NAMES[k]: self.ms[k] for k in range(4)}, from_cache=bool(self.from_cache))
 
 
 class EamSetfl(C.Structure):

@@ -35,6 +35,10 @@ enum : uint32_t {
   kTagRbeGauss = 0x52424531u, kTagRbeAccept = 0x52424532u, kTagRblOffset = 0x52424c31u
 };
 
+// Binned cells of atoms that SHAKE wrapped across the box after the cell list was built, kept per
+// step; beyond this many the culling pair kernels walk whole stencils for the step.
+constexpr int kMaxMigrated = 16;
+
 // Per-system scalar state that kernels read and update on the device (thermostat chain,
 // reductions, step counter).  One record per system, in device memory.
 struct SysState {
@@ -67,6 +71,14 @@ struct SysState {
   int status;              // error word
   int pad;
   unsigned counter[8];     // last-block arrival counters
+  // Positions SHAKE changed since this step's cell list was built (the reference's locator keeps
+  // the cells of before the constraint, ExecutionNVT.cpp:843-870): the largest displacement (FP32
+  // bits, non-negative) and the binned cells of atoms it wrapped across the box.  Reset with the
+  // cell list.  The pair kernels that cull cells geometrically widen by the displacement and never
+  // cull a recorded cell (an atom there sits on the far side of the box).
+  unsigned shake_disp_bits;
+  int mig_n;
+  int mig_cell[kMaxMigrated];
 };
 
 struct SysDev {
@@ -78,8 +90,11 @@ struct SysDev {
   int eam_per_type;  // EAM tables per type (setfl): frho / rhor by type, z2r by type pair
   int eam_pad;
   int lean;   // segment-table traversal usable (every dimension holds more than nc cells)
-  int dense;  // pair kernel layout: tile (warp per home cell, dense systems) or warp per atom
+  int dense;  // pair kernel layout: 0 warp per atom, 1 tile (warp per home cell), 2 column (warp per
+              // column of home cells, lane per atom; FP32 RBL forces only, the tile kernel otherwise)
   int blocks_pair, blocks_atom, blocks_rho, blocks_tri, rbe_mmax, rbe_slots, has_triples, n_triples;
+  int blocks_col;  // blocks of the column kernel per system (dense == 2)
+  int col_pad;
   // NPT barostats (npt 1: Berendsen at the end of the step, 2: MTK around the integrator): the
   // box changes on the device every step.  Cell arrays and the cell work table hold ncell_cap cells
   // (the box at kBoxGrow x L0); kmax indexes the Ewald k lists.

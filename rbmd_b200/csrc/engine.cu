@@ -92,7 +92,9 @@ static void derive(const rbmd_system_desc& d, const rbmd_params& p, rbmd_derived
 // ------------------------------------------------------------------------------ context
 namespace {
 // Profiler record of a batch's pair launch, by traversal layout.
-const char* pair_name(const Batch& b) { return b.dense ? "pair_tile" : (b.lean ? "pair_lean" : "pair_atom"); }
+const char* pair_name(const Batch& b) {
+  return b.dense == 2 ? "pair_col" : (b.dense ? "pair_tile" : (b.lean ? "pair_lean" : "pair_atom"));
+}
 
 // Exact thresholds for the reference's window tests.  fl(c - x) is non-increasing in x, so
 // {x : fl(c - x) > e} is a down-set of the floats and thr_below returns its largest element;
@@ -429,8 +431,9 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   // tile kernel (warp per home cell, candidates shared by the cell's atoms) pays off in mixed
   // precision once cells hold a few atoms on average; the lean kernel (warp per atom) is faster
   // below that and in FP64, where the tile kernel's per-lane FP64 state no longer fits in
-  // registers.  RBMD_PAIR_LAYOUT overrides the choice for tuning and tests: "atom" (general),
-  // "lean", "cell" (tile).
+  // registers.  In mixed precision the column kernel (warp per column of home cells, lane per
+  // atom) takes the tile kernel's systems for the RBL forces.  RBMD_PAIR_LAYOUT overrides the
+  // choice for tuning and tests: "atom" (general), "lean", "cell" (tile), "column".
   const bool stencil_ok = D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1;
   // The lean and tile kernels also walk stencils that repeat cells, as long as every dimension
   // holds more than nc cells (one periodic image per offset; the tile kernel also needs edges of
@@ -441,6 +444,8 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   D.lean = lean_layout_ok(D) ? 1 : 0;
   D.dense = (stencil_ok && p.precision == RBMD_PREC_MIXED && n < (1 << 25) &&
              (double)n >= kTileMinPerCell * (double)D.ncell) ? 1 : 0;
+  // dense mixed-precision RBL forces: the column kernel in place of the tile kernel
+  if (D.dense == 1 && column_layout_ok(D)) D.dense = 2;
   const char* lay = std::getenv("RBMD_PAIR_LAYOUT");
   s->tuned = lay != nullptr && lay[0] != '\0' && std::strcmp(lay, "auto") != 0;  // a forced layout is not retuned
   if (lay) {
@@ -451,6 +456,8 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
       D.dense = 0;
     } else if (std::strcmp(lay, "cell") == 0) {
       D.dense = (tile_ok && n < (1 << 25)) ? 1 : 0;
+    } else if (std::strcmp(lay, "column") == 0) {
+      D.dense = column_layout_ok(D) ? 2 : ((tile_ok && n < (1 << 25)) ? 1 : 0);
     }
   }
   if (p.ensemble == RBMD_ENS_NPT) {
@@ -473,7 +480,8 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   } else {
     D.ncell_cap = D.ncell;
   }
-  D.blocks_pair = D.dense ? (D.ncell + kCellWarpsHost - 1) / kCellWarpsHost : (n + kPairWarps - 1) / kPairWarps;
+  D.blocks_pair = D.dense ? tile_blocks(D) : (n + kPairWarps - 1) / kPairWarps;
+  D.blocks_col = column_blocks(D);
   D.blocks_atom = (n + kAtomBlock - 1) / kAtomBlock;
   D.blocks_rho = (n + kRhoChunk - 1) / kRhoChunk;
   D.blocks_tri = (D.n_triples + 127) / 128;
@@ -822,7 +830,7 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
   b.lean = g.lean;
   b.npt = g.npt;
   std::vector<int> slots;
-  std::vector<int2> wa, wp, wc, wr, wt, wm;
+  std::vector<int2> wa, wp, wc, wr, wt, wm, wpc;
   for (int k = 0; k < 4; ++k) b.band[k] = g.band[k];
   for (System* s : group) {
     const SysDev& D = s->dev;
@@ -835,7 +843,10 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
     b.max_P = std::max(b.max_P, std::max(D.P, D.nk_ewald));
     b.natoms += D.n;
     for (int k = 0; k < D.n; k += kAtomBlock) wa.push_back(make_int2(s->slot, k));
-    if (D.dense)
+    if (D.dense == 2) {
+      for (int k = 0; k < D.dims[0] * D.dims[1]; k += kColWarpsHost) wp.push_back(make_int2(s->slot, k));
+      for (int k = 0; k < D.ncell; k += kCellWarpsHost) wpc.push_back(make_int2(s->slot, k));
+    } else if (D.dense)
       for (int k = 0; k < D.ncell; k += kCellWarpsHost) wp.push_back(make_int2(s->slot, k));
     else
       for (int k = 0; k < D.n; k += kPairWarps) wp.push_back(make_int2(s->slot, k));
@@ -858,6 +869,7 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
   };
   mk(wa, b.atom);
   mk(wp, b.pair);
+  mk(wpc, b.pair_cells);
   mk(wc, b.cell);
   mk(wr, b.rho);
   mk(wt, b.tri);

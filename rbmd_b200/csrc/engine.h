@@ -53,6 +53,17 @@ inline bool tile_layout_ok(const SysDev& D) {
 inline bool lean_layout_ok(const SysDev& D) {
   return D.dims[0] >= D.nc + 1 && D.dims[1] >= D.nc + 1 && D.dims[2] >= D.nc + 1;
 }
+// The column kernel's (warp per column of home cells, lane per atom): the tile kernel's boxes, FP32
+// RBL forces of LJ/CUT, LJ/CUT/COUL/LONG and CVFF; every other pass of such a system runs the tile
+// kernel over its cell table.
+inline bool column_layout_ok(const SysDev& D) {
+  return tile_layout_ok(D) && D.n < (1 << 25) && D.prec == RBMD_PREC_MIXED && D.neigh == RBMD_NEIGH_RBL &&
+         D.ff != RBMD_FF_EAM;
+}
+// Blocks per system of the pair kernels: tile (4 home cells per block; also the column layout's
+// cell table), column (4 columns per block), warp per atom (8 atoms per block).
+inline int tile_blocks(const SysDev& D) { return (D.ncell + 3) / 4; }
+inline int column_blocks(const SysDev& D) { return (D.dims[0] * D.dims[1] + 3) / 4; }
 
 // Doubles in each EAM spline array of a descriptor: frho, rhor and z2r (per type when
 // eam_per_type, one table each otherwise).

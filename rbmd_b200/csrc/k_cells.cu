@@ -15,6 +15,10 @@ __global__ void k_cells_zero(const SysDev* __restrict__ S, const int2* __restric
   const SysDev& s = S[w.x];
   const int c = w.y + threadIdx.x;
   if (c < s.ncell) s.cell_count[c] = 0;
+  if (c == 0) {  // a new cell list: nothing has moved since
+    s.st->shake_disp_bits = 0u;
+    s.st->mig_n = 0;
+  }
 }
 
 __global__ void k_cells_count(const SysDev* __restrict__ S, const int2* __restrict__ work) {

@@ -683,10 +683,14 @@ __global__ void __launch_bounds__(128, 3) k_shake(const SysDev* __restrict__ S, 
       pc[1][k] = l12 * r12[k] * im1 - l01 * r01[k] * im1;
       pc[2][k] = l20 * r20[k] * im2 - l12 * r12[k] * im2;
     }
+    float disp_max = 0.0f;  // largest displacement of the triple's atoms since the cell list
     for (int t = 0; t < 3; ++t) {
       const int ii = id[t];
       const double m = ms[t];
       double nv[3], nx[3];
+      const double4 xb = s.x[ii];  // the position the cell list was built from
+      double disp2 = 0.0;
+      bool crossed = false;  // wrapped across the box relative to that position
       for (int k = 0; k < 3; ++k) {
         nv[k] = vh[t][k] + pc[t][k] / dt;
         double xx = spk[t][k] + pc[t][k];
@@ -701,6 +705,15 @@ __global__ void __launch_bounds__(128, 3) k_shake(const SysDev* __restrict__ S, 
         }
         nx[k] = xx;
         s.image[3 * ii + k] = im;
+        const double L = s.hi[k] - s.lo[k], dk = xx - (&xb.x)[k];
+        const double dm = fabs(dk) > 0.5 * L ? fabs(dk) - L : dk;  // nearest image
+        crossed |= fabs(dk) > 0.5 * L;
+        disp2 += dm * dm;
+      }
+      disp_max = fmaxf(disp_max, (float)(sqrt(disp2) * (1.0 + 1e-6)));
+      if (crossed) {
+        const int slot = atomicAdd(&s.st->mig_n, 1);
+        if (slot < kMaxMigrated) s.st->mig_cell[slot] = s.cell_of_atom[ii];
       }
       s.v[ii] = make_double4(nv[0], nv[1], nv[2], m);
       const double q = qa[t];
@@ -710,6 +723,11 @@ __global__ void __launch_bounds__(128, 3) k_shake(const SysDev* __restrict__ S, 
       const int k = rk[t];
       s.sx[k] = make_double4(nx[0], nx[1], nx[2], q);
       s.sxf[k] = make_float4((float)nx[0], (float)nx[1], (float)nx[2], (float)q);
+    }
+    {  // one atomic per converged group of lanes (a block's triples belong to one system)
+      const unsigned am = __activemask();
+      const unsigned mx = __reduce_max_sync(am, __float_as_uint(disp_max));  // non-negative: bits order as values
+      if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1)) atomicMax(&s.st->shake_disp_bits, mx);
     }
     const double dtfsq = 0.5 * dt * dt * fm;
     l01 = l01 / dtfsq;

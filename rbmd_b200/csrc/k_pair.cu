@@ -26,6 +26,8 @@
 
 #include "kernels.h"
 
+#include <type_traits>
+
 namespace rbmd {
 
 enum PairMode {
@@ -726,8 +728,11 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
     const R rc2 = (R)s.rc2, rs2 = (R)s.rs2;
     const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
     // conservative culling radius: cells farther than rc from i (with a margin for atoms that
-    // moved since binning) cannot hold a core or shell atom
-    const double margin = 0.1 * fmin(d0, fmin(d1, d2c));
+    // moved since binning: at least the largest SHAKE displacement since the cell list was built)
+    // cannot hold a core or shell atom; cells of atoms SHAKE wrapped across the box (they sit on
+    // the far side of it) are never culled, and beyond kMaxMigrated of them nothing is
+    const double margin = fmax(0.1 * fmin(d0, fmin(d1, d2c)), 1.001 * (double)__uint_as_float(s.st->shake_disp_bits));
+    const int mig_n = s.st->mig_n;
     const double cut2 = s.rc2;
     const double lo0 = s.lo[0], lo1 = s.lo[1], lo2 = s.lo[2];
     const float spice = (float)pice;
@@ -779,8 +784,8 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
         const double gx = fmax(0.0, fmax(bx0 - xi.x, xi.x - bx1));
         const double gy = fmax(0.0, fmax(by0 - xi.y, xi.y - by1));
         const double gxy = gx * gx + gy * gy;
+        int elo = nc + 1, ehi = -nc - 1;
         if (gxy < cut2) {
-          int elo = nc + 1, ehi = -nc - 1;
           for (int de = -nc; de <= nc; ++de) {
             const int n2 = c2 + de;
             const double bz0 = lo2 + n2 * d2c - margin, bz1 = lo2 + (n2 + 1) * d2c + margin;
@@ -790,6 +795,22 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
               ehi = max(ehi, de);
             }
           }
+        }
+        if (mig_n > kMaxMigrated) {
+          elo = -nc;
+          ehi = nc;
+        } else {
+          for (int m = 0; m < mig_n; ++m) {
+            const int cm = __ldg(&s.st->mig_cell[m]) - dz * (w1 + dy * w0);
+            if (cm < 0 || cm >= dz) continue;  // not in this row's column
+            for (int de = -nc; de <= nc; ++de)
+              if ((((c2 + de) % dz) + dz) % dz == cm) {
+                elo = min(elo, de);
+                ehi = max(ehi, de);
+              }
+          }
+        }
+        {
           if (elo <= ehi) {
             // unwrapped z cells [z0, z1] (len <= 2 nc + 1 <= 2 dz - 1 of them) start in the
             // periodic copy q = floor(z0 / dz); they map to wrapped cells [zw, zw + len) when that
@@ -1856,11 +1877,458 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
   }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Column variant (mixed-precision RBL forces: LJ/CUT and LJ + real-space Coulomb).  One warp per
+// column of home cells -- fixed x and y cell, all z -- whose atoms are contiguous in the cell-ordered
+// arrays (cells are numbered z fastest), taken 32 at a time: one lane per home atom.  The chunk's
+// atoms sit in a few consecutive z cells, so for a traversal row (x and y cell offset) their
+// candidate windows -- the row's z cells from the atom's own cell - nc to + nc -- are overlapping
+// sub-ranges of one contiguous union, which the warp stages once in shared memory, shifted into
+// the home frame.  Each lane then walks its own window in lock step with the others (step t: every
+// lane reads entry t of its own window): one shared load, the FP32 squared distance, the band
+// compares of the exact classification, a shell counter and a predicated queue append -- no
+// ballots and no cross-lane traffic.  A lane's window is trimmed to the z cells that can hold an
+// atom within rc of it (an x/y gap to the row's column of g leaves a z half-width sqrt(rc^2 - g^2));
+// cells dropped that way hold no core or shell atom, so the shell ranks, and the RBL picks, stay
+// exactly those of the full traversal.  Reading past the end of its window (the lanes step
+// together) a lane meets only cells beyond rc, which classify as out.  The selected pairs of a row
+// are evaluated by their own lane at the end of the row, so an atom's force is summed in traversal
+// order by one lane.  Atoms outside the box walk their own neighbourhood with the whole warp first
+// (tile_stray), as in the tile kernel.
+constexpr int kColWarps = 4;     // columns per block (kColWarpsHost on the host side)
+constexpr int kColStage = 192;   // staged candidates per warp
+constexpr int kColQ = 64;        // queued pairs per lane, and the most steps between evaluations
+constexpr float kColFar = 1e30f;
+#ifndef RBMD_COL_MIN_BLOCKS
+#define RBMD_COL_MIN_BLOCKS 5
+#endif
+
+// Rare paths of the column kernel, kept out of line so that their registers do not weigh on the
+// walk: the FP64 classification of a banded pair (bit 0 core, bit 1 shell) ...
+__device__ __noinline__ unsigned col_classify_fp64(const SysDev* __restrict__ sp, int si, int js, int mx, int my,
+                                                   int mz) {
+  const SysDev& s = *sp;
+  const double4 xd = ldg4(&s.sx[si]);
+  bool core, shell;
+  classify_fp64(s, xd.x, xd.y, xd.z, js, mx, my, mz, true, core, shell);
+  return (core ? 1u : 0u) | (shell ? 2u : 0u);
+}
+
+// ... and one atom outside the box, walked by the whole warp (every lane calls it): its force is
+// written and its three force components returned in every lane.
+template <int MODE, bool SPECIAL>
+__device__ __noinline__ double3 col_stray(const SysDev* __restrict__ sp, int si, int skip, const float* s_tab,
+                                         int owner_lane, int i) {
+  const SysDev& s = *sp;
+  float ff[6];
+  PairAcc acc;
+  acc_zero(ff, acc);
+  tile_stray<float, MODE, SPECIAL, false>(s, si, skip, s.pice, true, s_tab, 0, nullptr, nullptr, nullptr, nullptr, ff,
+                                          acc);
+  double cmb[6], r9[9];
+  acc_warp_total<true>(ff, acc, cmb);
+  acc_to_r9<MODE, true, false>(s, cmb, acc, r9);
+  if ((int)(threadIdx.x & 31) == owner_lane) finish_atom<MODE>(s, i, r9);
+  return make_double3(r9[0], r9[1], r9[2]);
+}
+
+template <int MODE, bool SPECIAL>
+__global__ void __launch_bounds__(kColWarps * 32, RBMD_COL_MIN_BLOCKS)
+k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, float4 band) {
+  static_assert(MODE == kLJ_RBL || MODE == kCOUL_RBL, "column layout: FP32 RBL forces only");
+  static_assert(kColStage < 0x8000, "queue entries hold a stage index below bit 15");
+  __shared__ float4 s_c[kColWarps][kColStage];      // candidate position - image shift, charge
+  __shared__ int s_id[kColWarps][kColStage];        // atom id (LJ/CUT: molecule) | type << kJsBits
+  __shared__ unsigned short s_q[kColWarps][kColQ * 32];  // slot k of lane l at k * 32 + l: stage entry | shell << 15
+  // per lane (home atom): what the evaluation needs, kept out of registers during the walk
+  __shared__ int4 s_ai[kColWarps][32];    // type, molecule, special partners, first special slot
+  __shared__ int2 s_sp[kColWarps][32];    // first two special partners
+  __shared__ float2 s_sw[kColWarps][32];  // and their weights
+  __shared__ float4 s_f[kColWarps][32];   // force accumulated so far (x, y, z), charge in w
+  __shared__ float s_shift[3][3];         // per dimension: d (w - n) for w - n = -dims, 0, +dims
+  __shared__ float s_tab[2 * kMaxF32Types * kMaxF32Types];
+  __shared__ double s_red[kColWarps][3];
+
+  const int2 wk = work[blockIdx.x];
+  const SysDev& s = S[wk.x];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  const int dx = s.dims[0], dy = s.dims[1], dz = s.dims[2];
+  const int ntypes = s.ntypes;
+  if (threadIdx.x < 9) {
+    const int dim = threadIdx.x / 3, t = threadIdx.x % 3;
+    s_shift[dim][t] = (float)(s.d[dim] * (double)((t - 1) * s.dims[dim]));
+  }
+  for (int t = threadIdx.x; t < ntypes * ntypes && t < kMaxF32Types * kMaxF32Types; t += blockDim.x) {
+    const int a = t / ntypes, b = t % ntypes;
+    const double sg = (s.sig[a] + s.sig[b]) / 2;
+    s_tab[2 * t] = (float)(-24.0 * sqrt(s.eps[a] * s.eps[b]));
+    s_tab[2 * t + 1] = (float)(sg * sg * sg * sg * sg * sg);
+  }
+  __syncthreads();
+
+  // FP32 band edges of the launch (the union of its systems' bands; a batch shares rc and rs)
+  const float b0 = band.x, b1 = band.y, b2 = band.z, b3 = band.w;
+  const int pice = s.pice;
+  // stride picks: with pice dividing 32, a 32-bit pattern of the picked shell ranks rotated by one
+  // per shell; otherwise a countdown of the shells still to skip
+  const bool rot = (32 % pice) == 0;
+  unsigned pat0 = 0u;
+  for (int k = 0; k < 32; k += pice) pat0 |= 1u << k;
+  const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
+  const float fdx = (float)s.d[0], fdy = (float)s.d[1], fdz = (float)s.d[2];
+  const float frc2 = (float)s.rc2;
+  // trimming margins: 1e-3 of a cell (far above the FP32 rounding of the coordinates involved) plus
+  // the largest distance SHAKE moved an atom since the cell list was built; cells of atoms it wrapped
+  // across the box are never trimmed, and beyond kMaxMigrated of them nothing is
+  const float mdisp = __uint_as_float(s.st->shake_disp_bits);
+  const int mig_n = s.st->mig_n;
+  const float mgx = 1e-3f * fdx + mdisp, mgy = 1e-3f * fdy + mdisp, mgz = 1e-3f * fdz + mdisp;
+  double red0 = 0.0, red1 = 0.0, red2 = 0.0;  // this lane's atoms' forces (the RBL mean)
+
+  const int col = wk.y + wid;
+  if (col < dx * dy) {
+    const int hx = col / dy, hy = col % dy;
+    const int cbase = dz * (hy + dy * hx);
+    const int a0 = __ldg(&s.cell_start[cbase]), a1 = __ldg(&s.cell_start[cbase + dz]);
+    for (int g0 = a0; g0 < a1; g0 += 32) {
+      const int si = g0 + lane;
+      const bool valid = si < a1;
+      int i = 0, zl = 0;
+      float4 p4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      bool stray = false;
+      int c = 0;  // shells still to skip before the next pick
+      __syncwarp();  // the previous chunk's evaluation has read the per-lane records
+      if (valid) {
+        const int4 mi = __ldg(&s.smeta[si]);
+        i = mi.x;
+        p4 = __ldg(&s.sxf[si]);
+        zl = __ldg(&s.cell_of_atom[i]) - cbase;  // internal cell id iz + dz (iy + dy ix), this column
+        const double4 xd = ldg4(&s.sx[si]);
+        stray = (int)((xd.x - s.lo[0]) / s.d[0]) != hx || (int)((xd.y - s.lo[1]) / s.d[1]) != hy ||
+                (int)((xd.z - s.lo[2]) / s.d[2]) != zl;
+        if (s.rbl_mode == RBMD_RBL_PHILOX && pice > 1) {
+          uint32_t o[4];
+          philox4x32_10((uint32_t)i, 0u, (uint32_t)s.st->step, kTagRblOffset, s.seed_lo, s.seed_hi, o);
+          const int nm = (int)(o[0] % (uint32_t)pice);
+          c = nm == 0 ? 0 : pice - nm;
+        }
+        int nsp = 0, spb = 0, sp0 = -1, sp1 = -1;
+        float w0 = 1.0f, w1 = 1.0f;
+        if (SPECIAL) {  // special partners: the first two cached, the rest read from the CSR lists
+          spb = __ldg(&s.sp_off[i]);
+          nsp = __ldg(&s.sp_off[i + 1]) - spb;
+          if (nsp > 0) {
+            sp0 = __ldg(&s.sp_ids[spb]);
+            w0 = (float)__ldg(&s.sp_w[spb]);
+          }
+          if (nsp > 1) {
+            sp1 = __ldg(&s.sp_ids[spb + 1]);
+            w1 = (float)__ldg(&s.sp_w[spb + 1]);
+          }
+        }
+        s_ai[wid][lane] = make_int4(mi.y, mi.z, nsp, spb);
+        s_sp[wid][lane] = make_int2(sp0, sp1);
+        s_sw[wid][lane] = make_float2(w0, w1);
+      } else {  // a lane without an atom still runs the evaluation rounds (adding nothing): its
+                // record must hold valid indices (type 0, no special partners)
+        s_ai[wid][lane] = make_int4(0, -1, 0, 0);
+        s_sp[wid][lane] = make_int2(-1, -1);
+        s_sw[wid][lane] = make_float2(1.0f, 1.0f);
+      }
+      s_f[wid][lane] = make_float4(0.0f, 0.0f, 0.0f, p4.w);
+
+      // ---- atoms outside the box: the whole warp walks each one's own neighbourhood
+      unsigned strays = __ballot_sync(FULL, valid && stray);
+      while (strays) {
+        const int as = __ffs(strays) - 1;
+        strays &= strays - 1;
+        const int sk = __shfl_sync(FULL, c, as);
+        const double3 r = col_stray<MODE, SPECIAL>(&s, g0 + as, sk, s_tab, as, i);
+        if (lane == as) {
+          red0 += r.x;
+          red1 += r.y;
+          red2 += r.z;
+        }
+      }
+
+      // ---- the chunk's own atoms, row by row
+      const bool act = valid && !stray;
+      const int zmin = __reduce_min_sync(FULL, act ? zl : 0x7fffffff);
+      const int zmax = __reduce_max_sync(FULL, act ? zl : -1);
+      const float pix = p4.x, piy = p4.y, piz = p4.z;
+      unsigned pat = rot ? ((pat0 << c) | (c ? pat0 >> (32 - c) : 0u)) : 0u;  // picks at ranks c, c + pice, ...
+      int qo = 0;  // queued pairs of this lane times 32 (the offset of its next slot)
+
+      // evaluates this lane's queued pairs (their candidates are in the stage)
+      auto flush = [&]() {
+        const int qn = qo >> 5;
+        const int rounds = __reduce_max_sync(FULL, qn);
+        if (rounds == 0) return;
+        const int4 ai = s_ai[wid][lane];
+        const int2 sp = s_sp[wid][lane];
+        const float2 sw = s_sw[wid][lane];
+        float4 fa = s_f[wid][lane];
+        const float spice = (float)pice, fsa = (float)sqrt(s.alpha);
+        const float falpha_l2 = (float)(s.alpha * 1.4426950408889634), fqq = (float)s.qqr2e;  // alpha log2(e)
+        for (int k = 0; k < rounds; ++k) {
+          if (k < qn) {
+            const unsigned h = s_q[wid][k * 32 + lane];
+            const int e = (int)(h & 0x7fffu);
+            const float4 pj = s_c[wid][e];
+            const float rx = pj.x - pix, ry = pj.y - piy, rz = pj.z - piz;
+            const float d2 = tile_d2(rx, ry, rz);
+            if (d2 > 0.0001f) {  // the pair of an atom with itself is queued as core and dropped here
+              const int idt = s_id[wid][e];
+              const int idj = idt & kJsMask, tj = idt >> kJsBits;
+              float w = 1.0f;
+              if (SPECIAL) {
+                if (ai.z <= 2) {
+                  w = (idj == sp.x) ? sw.x : w;
+                  w = (idj == sp.y) ? sw.y : w;
+                } else {
+                  for (int t2 = 0; t2 < ai.z; ++t2)
+                    if (__ldg(&s.sp_ids[ai.w + t2]) == idj) w = (float)__ldg(&s.sp_w[ai.w + t2]);
+                }
+              }
+              // LJ/CUT skips pairs of one molecule (its staged id is the molecule)
+              if (MODE != kLJ_RBL || idj != ai.y) {
+                const float f = tile_pair_f32<MODE>((h & 0x8000u) == 0u, d2, fa.w, pj.w, ai.x * ntypes + tj, w,
+                                                    spice, fsa, falpha_l2, fqq, s_tab);
+                fa.x += f * rx;
+                fa.y += f * ry;
+                fa.z += f * rz;
+              }
+            }
+          }
+        }
+        s_f[wid][lane] = fa;
+        qo = 0;
+      };
+
+      if (zmax >= 0) {
+        const float xr = pix - (float)s.lo[0], yr = piy - (float)s.lo[1], zr = piz - (float)s.lo[2];
+        const int u0 = zmin - nc, u1 = zmax + nc;  // the chunk's z cells, unwrapped, -dz < u0, u1 < 2 dz
+        for (int r = 0; r < nrows; ++r) {
+          const int da = r / side - nc, db = r % side - nc;
+          const int n0 = hx + da, n1 = hy + db;  // unwrapped column of the row (nc < dims)
+          const int w0c = n0 < 0 ? n0 + dx : (n0 >= dx ? n0 - dx : n0);
+          const int w1c = n1 < 0 ? n1 + dy : (n1 >= dy ? n1 - dy : n1);
+          const int t0c = n0 < 0 ? 2 : (n0 >= dx ? 0 : 1), t1c = n1 < 0 ? 2 : (n1 >= dy ? 0 : 1);
+          const int base = dz * (w1c + dy * w0c);
+          // the row's union: unwrapped z cells u0 .. u1 in up to three segments (images -1, 0, +1:
+          // below the box, inside, above), segment k holding sorted indices sa_k .., union entries ob_k ..
+          int sa0 = 0, sa1, sa2 = 0, ob1, ob2, len = 0;
+          if (u0 < 0) {  // below the box: cells u0 + dz .. dz - 1
+            sa0 = __ldg(&s.cell_start[base + u0 + dz]);
+            len = __ldg(&s.cell_start[base + dz]) - sa0;
+          }
+          ob1 = len;
+          {  // inside: cells max(u0, 0) .. min(u1, dz - 1)
+            sa1 = __ldg(&s.cell_start[base + max(u0, 0)]);
+            len += __ldg(&s.cell_start[base + min(u1, dz - 1) + 1]) - sa1;
+          }
+          ob2 = len;
+          if (u1 >= dz) {  // above the box: cells 0 .. u1 - dz
+            sa2 = __ldg(&s.cell_start[base]);
+            len += __ldg(&s.cell_start[base + u1 - dz + 1]) - sa2;
+          }
+          // union entries before unwrapped cell u (u0 <= u <= u1 + 1)
+          auto ucount = [&](int u) -> int {
+            if (u > u1) return len;
+            if (u < 0) return __ldg(&s.cell_start[base + u + dz]) - sa0;
+            if (u < dz) return ob1 + __ldg(&s.cell_start[base + u]) - sa1;
+            return ob2 + __ldg(&s.cell_start[base + u - dz]) - sa2;
+          };
+          // this lane's window, trimmed to the z cells that can hold an atom within rc: the x / y
+          // gaps to the row's column (shrunk by the margin) leave a z half-width sqrt(rc^2 - g^2)
+          // (grown by it)
+          int wb = 0, wl = 0;
+          if (act) {
+            int zlo = zl + nc + 1, zhi = zl - nc - 1;  // empty
+            const float gx = fmaxf(0.0f, fmaxf((float)n0 * fdx - xr, xr - (float)(n0 + 1) * fdx) - mgx);
+            const float gy = fmaxf(0.0f, fmaxf((float)n1 * fdy - yr, yr - (float)(n1 + 1) * fdy) - mgy);
+            const float g2 = __fmaf_rn(gx, gx, gy * gy);
+            if (g2 < frc2) {
+              const float h = sqrtf(frc2 - g2) + mgz;
+              zlo = max((int)floorf((zr - h) / fdz), zl - nc);
+              zhi = min((int)floorf((zr + h) / fdz), zl + nc);
+            }
+            if (mig_n > kMaxMigrated) {
+              zlo = zl - nc;
+              zhi = zl + nc;
+            } else {
+              for (int m = 0; m < mig_n; ++m) {  // the stencil's visits of a recorded cell stay in
+                const int zm = __ldg(&s.st->mig_cell[m]) - base;
+                if (zm < 0 || zm >= dz) continue;  // not in this row's column
+                for (int u = zm - dz; u <= zm + dz; u += dz)
+                  if (u >= zl - nc && u <= zl + nc) {
+                    zlo = min(zlo, u);
+                    zhi = max(zhi, u);
+                  }
+              }
+            }
+            if (zlo <= zhi) {
+              wb = ucount(zlo);
+              wl = ucount(zhi + 1) - wb;
+            }
+          }
+          if (__reduce_max_sync(FULL, wl) == 0) continue;
+          // walks the windows of the lanes `in`; their starts lie within kColStage - 32 entries of
+          // each other, so every staged tile covers at least 32 steps
+          auto walk = [&](bool in) {
+            const int ml = __reduce_max_sync(FULL, in ? wl : 0);
+            if (ml == 0) return;
+            const int gbb = __reduce_min_sync(FULL, in ? wb : 0x7fffffff);
+            const int spr = __reduce_max_sync(FULL, in ? wb : gbb) - gbb;
+            const int T = kColStage - spr;  // steps per staged tile
+            const float shx = s_shift[0][t0c], shy = s_shift[1][t1c];
+            // lanes not walking step through the stage too, from a position that matches nothing
+            const float wpx = in ? pix : -kColFar, wpy = in ? piy : -kColFar, wpz = in ? piz : -kColFar;
+            const int i0 = in ? wb - gbb : 0;
+            for (int t0 = 0; t0 < ml; t0 += T) {
+              const int tl = min(T, ml - t0);
+              const int need = spr + tl;  // entries any lane reads in this tile (<= kColStage)
+              const int ub = gbb + t0;    // union index of stage entry 0
+              for (int e = lane; e < need; e += 32) {
+                const int g = ub + e;
+                float4 cv = make_float4(kColFar, kColFar, kColFar, 0.0f);
+                int idt = 0;
+                if (g < len) {
+                  const int zc = g < ob1 ? 2 : (g < ob2 ? 1 : 0);  // z shift code: below 2, inside 1, above 0
+                  const int js = g < ob1 ? sa0 + g : (g < ob2 ? sa1 + (g - ob1) : sa2 + (g - ob2));
+                  const float4 pj = __ldg(&s.sxf[js]);
+                  const int4 mj = __ldg(&s.smeta[js]);
+                  cv = make_float4(pj.x - shx, pj.y - shy, pj.z - s_shift[2][zc], pj.w);
+                  idt = (MODE == kLJ_RBL ? mj.z : mj.x) | (mj.y << kJsBits);
+                }
+                s_c[wid][e] = cv;
+                s_id[wid][e] = idt;
+              }
+              __syncwarp();
+              // the walk, with the pick rule fixed at compile time (ROT: rotating pattern)
+              auto steps = [&](auto rot_tag) {
+                constexpr bool ROT = decltype(rot_tag)::value;
+                for (int q0 = 0; q0 < tl; q0 += kColQ) {  // at most kColQ steps between evaluations
+                  const int te = min(kColQ, tl - q0);
+                  const int ib = i0 + q0;
+#pragma unroll 4
+                  for (int t = 0; t < te; ++t) {
+                    const int ix = ib + t;
+                    const float4 cj = s_c[wid][ix];
+                    const float ex = cj.x - wpx, ey = cj.y - wpy, ez = cj.z - wpz;
+                    const float dd = tile_d2(ex, ey, ez);
+                    // x alone: core (or the atom itself, dropped at evaluation); y alone: shell;
+                    // both: within a rounding band of rs^2 or rc^2, classified again in FP64
+                    bool core = ((dd <= b1) | (dd >= b2)) & (dd <= b3);
+                    bool shell = (dd >= b0) & (dd <= b3);
+                    if (core & shell) {
+                      // the candidate from its stage slot: union index, segment, sorted index, image
+                      const int g = ub + ix;
+                      const int zc = g < ob1 ? 2 : (g < ob2 ? 1 : 0);
+                      const int js = g < ob1 ? sa0 + g : (g < ob2 ? sa1 + (g - ob1) : sa2 + (g - ob2));
+                      const unsigned cs2 =
+                          col_classify_fp64(&s, si, js, (t0c - 1) * dx, (t1c - 1) * dy, (zc - 1) * dz);
+                      core = (cs2 & 1u) != 0u;
+                      shell = (cs2 & 2u) != 0u;
+                    }
+                    bool pick;
+                    if constexpr (ROT) {
+                      pick = shell & ((pat & 1u) != 0u);
+                      pat = shell ? __funnelshift_r(pat, pat, 1) : pat;
+                    } else {
+                      pick = shell & (c == 0);
+                      c = shell ? ((c == 0) ? pice - 1 : c - 1) : c;
+                    }
+                    // branch-free: the slot is always written and kept only when the pair is
+                    // selected (at most kColQ steps since the last evaluation)
+                    s_q[wid][qo + lane] = (unsigned short)(ix | (pick ? 0x8000 : 0));
+                    qo += (core | pick) ? 32 : 0;
+                  }
+                  flush();
+                }
+              };
+              if (rot) steps(std::true_type{});
+              else steps(std::false_type{});
+              __syncwarp();  // the stage is rewritten by the next tile or row
+            }
+          };
+          const int gmin = __reduce_min_sync(FULL, wl > 0 ? wb : 0x7fffffff);
+          const int gmax = __reduce_max_sync(FULL, wl > 0 ? wb : -1);
+          if (gmax - gmin <= kColStage - 32) {
+            walk(wl > 0);
+          } else {
+            // windows far apart (a sparse home column next to dense ones): the chunk's home cells
+            // take turns, and single lanes where one cell's trimmed windows are still too far apart
+            for (int zg = zmin; zg <= zmax; ++zg) {
+              const bool in = wl > 0 && zl == zg;
+              const int lo = __reduce_min_sync(FULL, in ? wb : 0x7fffffff);
+              const int hi = __reduce_max_sync(FULL, in ? wb : -1);
+              if (hi < 0) continue;
+              if (hi - lo <= kColStage - 32) {
+                walk(in);
+              } else {
+                for (unsigned m = __ballot_sync(FULL, in); m; m &= m - 1) walk(in && lane == __ffs(m) - 1);
+              }
+            }
+          }
+        }
+      }
+      if (act) {
+        const float4 fa = s_f[wid][lane];  // Coulomb already scaled by qqr2e inside the pair factor
+        double r9[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) r9[q] = 0.0;
+        r9[0] = (double)fa.x;
+        r9[1] = (double)fa.y;
+        r9[2] = (double)fa.z;
+        finish_atom<MODE>(s, i, r9);
+        red0 += r9[0];
+        red1 += r9[1];
+        red2 += r9[2];
+      }
+    }
+  }
+  // RBL mean force: warp totals, block partials, the last block of the system reduces them in order
+  red0 = warp_sum(red0);
+  red1 = warp_sum(red1);
+  red2 = warp_sum(red2);
+  if (lane == 0) {
+    s_red[wid][0] = red0;
+    s_red[wid][1] = red1;
+    s_red[wid][2] = red2;
+  }
+  __syncthreads();
+  const int blk = wk.y / kColWarps;
+  if (threadIdx.x < 9) {
+    double t = 0.0;
+    if (threadIdx.x < 3)
+      for (int w = 0; w < kColWarps; ++w) t += s_red[w][threadIdx.x];
+    s.vir_part[(size_t)blk * 9 + threadIdx.x] = t;
+  }
+  if (arrive_last(&s.st->counter[0], (unsigned)s.blocks_col)) {
+    if (threadIdx.x < 3) {
+      double t = 0.0;
+      for (int b = 0; b < s.blocks_col; ++b) t += __ldcg(&s.vir_part[(size_t)b * 9 + threadIdx.x]);
+      s.st->fmean[threadIdx.x] = t / s.n;
+    }
+  }
+}
+
 template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
 static void go(const Batch& b, cudaStream_t st) {
-  if (b.dense)
-    k_pair_tile<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kCellWarps * 32, 0, st>>>(
-        b.sys, b.pair.d, 0, nullptr, nullptr, nullptr, nullptr, make_float4(b.band[0], b.band[1], b.band[2], b.band[3]));
+  constexpr bool kColumn = sizeof(R) == 4 && (MODE == kLJ_RBL || MODE == kCOUL_RBL) && !VIRIAL;
+  const float4 band = make_float4(b.band[0], b.band[1], b.band[2], b.band[3]);
+  if constexpr (kColumn) {
+    if (b.dense == 2) {
+      k_pair_col<MODE, SPECIAL><<<b.pair.n, kColWarps * 32, 0, st>>>(b.sys, b.pair.d, band);
+      note_launch();
+      return;
+    }
+  }
+  if (b.dense)  // the column layout keeps the tile kernel's cell table for every other pass
+    k_pair_tile<R, MODE, SPECIAL, VIRIAL><<<b.dense == 2 ? b.pair_cells.n : b.pair.n, kCellWarps * 32, 0, st>>>(
+        b.sys, b.dense == 2 ? b.pair_cells.d : b.pair.d, 0, nullptr, nullptr, nullptr, nullptr, band);
   else if (b.lean)
     k_pair2<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kPairWarps * 32, 0, st>>>(b.sys, b.pair.d);
   else

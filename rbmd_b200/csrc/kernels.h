@@ -19,10 +19,11 @@ struct Batch {
   int* d_slots = nullptr;    // slots of this batch
   int nsys = 0;
   Work atom, pair, cell, rho, tri, term, kred, draw;
+  Work pair_cells;           // column layout: the tile kernel's cell table (energies, other modes)
   // uniform switches of the batch (a batch never mixes them)
   int ff = 0, neigh = 0, coul = 0, prec = 0, temp_ctrl = 0, special = 0;
   int has_shake = 0, has_bonded = 0;
-  int dense = 0;             // pair kernel: 1 = warp per home cell, 0 = warp per atom
+  int dense = 0;             // pair kernel: 0 = warp per atom, 1 = warp per home cell, 2 = warp per column
   int lean = 0;              // warp per atom with segment tables (dims >= 2 nc + 1 everywhere)
   int npt = 0;               // NPT barostat: 0 none, 1 Berendsen (end of step), 2 MTK (around the integrator)
   int max_P = 0;             // largest P (or Ewald nk) in the batch
@@ -98,6 +99,7 @@ size_t snapshot_bytes(int n);
 void launch_snapshot_pack(const SysDev* sys, int slot, int n, void* out, cudaStream_t s);
 
 constexpr int kCellWarpsHost = 4;  // home cells per block of the tile pair kernel
+constexpr int kColWarpsHost = 4;   // columns of home cells per block of the column pair kernel
 constexpr double kTileMinPerCell = 3.0;  // mean atoms per cell from which the tile kernel is used
 
 double fma_peak_tflops(int fp64, cudaStream_t s);

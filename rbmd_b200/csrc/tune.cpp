@@ -20,6 +20,7 @@ std::vector<int> Context::usable_layouts(const System* s) const {
   const SysDev& D = s->dev;
   if (D.npt) return {RBMD_LAYOUT_GENERAL};
   std::vector<int> out;
+  if (column_layout_ok(D)) out.push_back(RBMD_LAYOUT_COLUMN);
   if (tile_layout_ok(D) && D.n < (1 << 25)) out.push_back(RBMD_LAYOUT_TILE);
   if (lean_layout_ok(D)) out.push_back(RBMD_LAYOUT_LEAN);
   out.push_back(RBMD_LAYOUT_GENERAL);
@@ -28,13 +29,14 @@ std::vector<int> Context::usable_layouts(const System* s) const {
 
 void Context::set_layout(System* s, int layout) {
   SysDev& D = s->dev;
-  const int dense = layout == RBMD_LAYOUT_TILE ? 1 : 0;
+  const int dense = layout == RBMD_LAYOUT_COLUMN ? 2 : (layout == RBMD_LAYOUT_TILE ? 1 : 0);
   const int lean = (layout != RBMD_LAYOUT_GENERAL && lean_layout_ok(D)) ? 1 : 0;
   if (D.dense == dense && D.lean == lean) return;
   drop_batches_with(s->id);  // cached work tables and graphs hold the old layout
   D.dense = dense;
   D.lean = lean;
-  D.blocks_pair = dense ? (D.ncell + kCellWarpsHost - 1) / kCellWarpsHost : (D.n + kPairWarps - 1) / kPairWarps;
+  D.blocks_pair = dense ? tile_blocks(D) : (D.n + kPairWarps - 1) / kPairWarps;
+  D.blocks_col = column_blocks(D);
   upload_record(s);
 }
 

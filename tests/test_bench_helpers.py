@@ -1,0 +1,43 @@
+"""bench.py's measurement helpers that need no GPU: the reciprocal-space Ewald force used as the
+denominator of the k-space-only RBE error (against the oracle's far force), the converged kmax,
+and the serving stream's size strata behind the CPU baselines."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from rbmd_b200 import _abi as A
+from rbmd_b200 import synth
+
+from conftest import rel_rms
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+
+def test_ewald_kspace_matches_oracle_far_force(oracle_mod):
+    sd = synth.nacl_melt(n_side=6, coulomb=A.COUL_EWALD, kmax=(5, 5, 5), precision=A.PREC_FP64)
+    rng = np.random.default_rng(3)
+    sd.pos = np.ascontiguousarray((sd.pos + rng.normal(scale=0.1, size=sd.pos.shape)) % sd.box_hi[0])
+    o = oracle_mod.Oracle(sd)
+    o.compute_forces()
+    f = bench.ewald_kspace_forces(sd.pos, sd.charge, sd.box_hi - sd.box_lo, sd.params.alpha, (5, 5, 5))
+    assert rel_rms(f, o.force_part(1)) < 1e-10
+
+
+def test_converged_kmax():
+    km = bench.converged_kmax([21.7, 21.7, 30.0], 0.09)
+    kc = np.sqrt(-4 * 0.09 * np.log(1e-12))
+    assert km[0] == int(np.ceil(kc * 21.7 / (2 * np.pi))) and km[2] > km[0]
+    k = 2 * np.pi * km[0] / 21.7
+    assert np.exp(-k * k / (4 * 0.09)) < 1e-12
+
+
+def test_stream_strata_cover_the_stream():
+    st = bench.stream_strata(512)
+    sizes, _ = synth.serving_stream(n_requests=512)
+    assert sum(s["requests"] for s in st) == 512 and sum(s["atoms"] for s in st) == int(sizes.sum())
+    for s in st:
+        assert s["lo"] <= s["size"] < s["hi"]

@@ -42,7 +42,8 @@ def eam_small(oracle_mod, **kw):
 def pair(ctx_factory, oracle_mod, sd, layout="auto", **ctxkw):
     """GPU context + system and the oracle twin.  `layout` selects the pair kernel: "auto" (the
     library's choice), "atom" (general warp-per-atom traversal), "lean" (warp per atom with segment
-    tables), "cell" (tile: warp per home cell, candidates shared by the cell's atoms)."""
+    tables), "cell" (tile: warp per home cell, candidates shared by the cell's atoms), "column"
+    (warp per column of home cells, lane per atom; mixed-precision RBL forces, else as "cell")."""
     import os
     ctx = ctx_factory(**ctxkw)
     old = os.environ.get("RBMD_PAIR_LAYOUT")
@@ -58,7 +59,7 @@ def pair(ctx_factory, oracle_mod, sd, layout="auto", **ctxkw):
     return ctx, sid, o
 
 
-LAYOUTS = ["auto", "atom", "lean", "cell"]
+LAYOUTS = ["auto", "atom", "lean", "cell", "column"]
 
 
 CASES = {
@@ -326,12 +327,12 @@ SMALL_BOXES = {
 
 
 @pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED])
-@pytest.mark.parametrize("layout", ["cell", "lean"])
+@pytest.mark.parametrize("layout", ["cell", "lean", "column"])
 @pytest.mark.parametrize("case", list(SMALL_BOXES))
 def test_small_box_layouts(ctx_factory, oracle_mod, case, layout, prec):
     sd = SMALL_BOXES[case]()
     short = any(2 * sd.params.cut_off > h - lo for h, lo in zip(sd.box_hi, sd.box_lo))
-    if layout == "cell" and short:
+    if layout in ("cell", "column") and short:
         pytest.skip("the tile layout needs edges of at least 2 rc")
     sd.params.precision = prec
     ctx, sid, o = pair(ctx_factory, oracle_mod, sd, layout=layout)

@@ -31,7 +31,7 @@ def test_autotune_picks_the_fastest_and_keeps_state(ctx_factory, oracle_mod):
     assert len(res) == 2 and sorted(r["n_systems"] for r in res) == [1, 3]
     for r in res:
         timed = {k: v for k, v in r["ms"].items() if v >= 0}
-        assert set(timed) == {"tile", "lean", "general"} and not r["from_cache"]
+        assert set(timed) == {"column", "tile", "lean", "general"} and not r["from_cache"]
         assert r["layout"] == min(timed, key=timed.get)
     for i, ((x, v, img), f) in zip(ids, before):
         x2, v2, img2 = ctx.state(i)

@@ -69,3 +69,32 @@ def test_single_rank_needs_no_process_group():
     assert d.world == 1 and d.reduce(3.5, "max") == 3.5
     d.barrier()
     d.close()
+
+
+def test_gpus_flag_starts_ranks():
+    """`bench.py --gpus 2` without a torchrun environment starts two ranks itself (torch's launcher,
+    rendezvous on 127.0.0.1); under --impl reference rank 0 alone works and prints the line, the
+    other rank exits 0.  gloo stands in for NCCL on the CPU."""
+    import json
+    import subprocess
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR",
+                                                            "MASTER_PORT")}
+    env["RBMD_DIST_BACKEND"] = "gloo"
+    env["RBMD_ORACLE_THREADS"] = "2"
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--steps", "1", "--warmup", "0", "--requests", "12"], capture_output=True, text=True,
+                       timeout=600, env=env, cwd=ROOT)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
+    lines = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    line = lines[0]
+    assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+
+
+def test_gpus_flag_must_match_world_size():
+    import subprocess
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2"], capture_output=True,
+                       text=True, timeout=120, env=env, cwd=ROOT)
+    assert r.returncode != 0 and "WORLD_SIZE" in r.stderr
