@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--requests", type=int, default=512)
     ap.add_argument("--request-steps", type=int, default=1000)
     ap.add_argument("--rate", type=float, default=50.0)
+    ap.add_argument("--round-atoms", type=int, default=4_000_000,
+                    help="serving rounds step the requests with the least remaining work up to this many atoms "
+                         "(0: every active request each round)")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
@@ -462,7 +465,7 @@ def measure_e2e(systems, arrivals, args, device):
     """The stream through rbmd_serve_*: submissions at the Poisson times, results back to host."""
     import rbmd_b200
     ctx = rbmd_b200.Context(device=device)
-    ctx.serve_start(steps_per_round=50)
+    ctx.serve_start(steps_per_round=50, round_atoms=args.round_atoms)
     rids = []
     h2d = 0
     t0 = time.monotonic()
@@ -472,22 +475,30 @@ def measure_e2e(systems, arrivals, args, device):
             time.sleep(ta - now)
         rids.append(ctx.serve_submit(sd, args.request_steps))
         h2d += desc_bytes(sd)
-    lat, d2h, atom_steps = [], 0, 0
+    lat, d2h, atom_steps, sizes = [], 0, 0, []
     for rid, sd in zip(rids, systems):
         rc = ctx.serve_wait(rid, 3600.0)
         x, v, th, st = ctx.serve_result(rid)
         if rc or st["status"]:
             raise RuntimeError(f"request {rid} failed with {rc}/{st['status']}")
         lat.append(st["t_done"] - st["t_submit"])
+        sizes.append(sd.n)
         d2h += x.nbytes + v.nbytes
         atom_steps += st["atom_steps"]
     wall = time.monotonic() - t0
     ctx.serve_stop()
     ctx.close()
     total_steps = len(systems) * args.request_steps
+    lat, sizes = np.array(lat), np.array(sizes)
+    bands = {}
+    for lo, hi in STRATA:
+        m = (sizes >= lo) & (sizes < hi)
+        if m.any():
+            bands[f"{lo}-{hi - 1}"] = {"requests": int(m.sum()), "p50_s": float(np.percentile(lat[m], 50)),
+                                      "p99_s": float(np.percentile(lat[m], 99))}
     return dict(value=atom_steps / wall, wall_s=wall, p50_s=float(np.percentile(lat, 50)),
                 p99_s=float(np.percentile(lat, 99)), h2d=h2d / total_steps, d2h=d2h / total_steps,
-                atom_steps=atom_steps)
+                atom_steps=atom_steps, bands=bands)
 
 
 STRATA = ((1000, 4000), (4000, 16000), (16000, 64001))  # log-thirds of the stream's size range
@@ -732,7 +743,10 @@ def main():
         if e2e is not None:
             line["e2e"] = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"],
                            "d2h_bytes_per_step": e2e["d2h"], "wall_s": e2e["wall_s"], "p50_latency_s": e2e["p50_s"],
-                           "p99_latency_s": e2e["p99_s"], "request_steps": args.request_steps,
+                           "p99_latency_s": e2e["p99_s"], "latency_by_size": e2e["bands"],
+                           "round_policy": ("every active request each round" if args.round_atoms <= 0 else
+                                            f"least remaining work first, {args.round_atoms} atoms per round"),
+                           "request_steps": args.request_steps,
                            "step": "one MD step of one request; bytes averaged over all request-steps"}
         s = json.dumps(line)
         print(s, flush=True)

@@ -440,7 +440,10 @@ typedef struct rbmd_serve_cfg {
   int32_t max_systems;          /* slots (0 = unlimited) */
   int32_t steps_per_round;      /* MD steps run per batched launch sequence between admissions */
   int32_t use_graphs;
-  int32_t pad0;
+  int32_t round_atoms;          /* atoms stepped per round: 0 = every active request each round;
+                                   > 0 = the requests with the least remaining work (remaining
+                                   steps x atoms, then arrival order) until their atoms reach this
+                                   (at least one request), so small requests finish in few rounds */
 } rbmd_serve_cfg;
 
 typedef struct rbmd_request_stats {

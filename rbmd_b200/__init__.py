@@ -255,9 +255,9 @@ class Context:
         return ms.value, n.value, u.value
 
     # ---- serving
-    def serve_start(self, hbm_budget_bytes=0, max_systems=0, steps_per_round=10, graphs=True):
+    def serve_start(self, hbm_budget_bytes=0, max_systems=0, steps_per_round=10, graphs=True, round_atoms=0):
         cfg = A.ServeCfg(hbm_budget_bytes=int(hbm_budget_bytes), max_systems=max_systems,
-                         steps_per_round=steps_per_round, use_graphs=int(graphs))
+                         steps_per_round=steps_per_round, use_graphs=int(graphs), round_atoms=int(round_atoms))
         self._check(lib().rbmd_serve_start(self.h, C.byref(cfg)))
 
     def serve_submit(self, sd, nsteps, params=None):

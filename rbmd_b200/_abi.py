@@ -136,7 +136,7 @@ class EamSetfl(C.Structure):
 
 class ServeCfg(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_systems", C.c_int32),
-                ("steps_per_round", C.c_int32), ("use_graphs", C.c_int32), ("pad0", C.c_int32)]
+                ("steps_per_round", C.c_int32), ("use_graphs", C.c_int32), ("round_atoms", C.c_int32)]
 
 
 class RequestStats(C.Structure):

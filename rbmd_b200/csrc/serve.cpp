@@ -2,8 +2,11 @@
 //
 // Requests arrive at any time.  Between rounds of batched steps the loop admits queued requests
 // in arrival order while the HBM budget and the slot limit allow, runs `steps_per_round` steps
-// of every active system in one segment-indexed launch sequence (replayed as a CUDA graph while
-// the active set is unchanged), and retires systems whose step count is reached.  Positions,
+// of the round's systems in one segment-indexed launch sequence (replayed as a CUDA graph while
+// the set is unchanged), and retires systems whose step count is reached.  A round takes every
+// active system, or with `round_atoms` > 0 the systems with the least remaining work (remaining
+// steps x atoms) up to that many atoms: small requests then finish in a few rounds instead of
+// waiting for the largest ones, and the rounds stay large enough to fill the GPU.  Positions,
 // velocities and thermostat state stay resident on the device for the whole request.  Each
 // system's arithmetic is independent of the others in the batch (per-system work tables and
 // per-system fixed-order reductions), so a result is the same alone and in the mix.
@@ -287,16 +290,29 @@ void Server::loop() {
         if (r->state == RBMD_REQ_RUNNING) active_.push_back(r);
     }
     if (active_.empty()) continue;
-    // one round of batched steps over every active system
-    int k = cfg_.steps_per_round;
-    for (Request* r : active_) k = std::min(k, std::max(r->remaining, 0));
-    std::vector<int32_t> ids;
+    // one round of batched steps: every active system, or the least remaining work first up
+    // to round_atoms atoms (at least one system)
     std::vector<Request*> stepping;
     for (Request* r : active_)
-      if (r->remaining > 0) {
-        ids.push_back(r->sys);
-        stepping.push_back(r);
+      if (r->remaining > 0) stepping.push_back(r);
+    if (cfg_.round_atoms > 0 && !stepping.empty()) {
+      std::stable_sort(stepping.begin(), stepping.end(), [](const Request* a, const Request* b) {
+        const double wa = (double)a->remaining * a->desc.d.n_atoms, wb = (double)b->remaining * b->desc.d.n_atoms;
+        return wa != wb ? wa < wb : a->id < b->id;
+      });
+      int64_t atoms = 0;
+      size_t take = 0;
+      while (take < stepping.size() && (take == 0 || atoms + stepping[take]->desc.d.n_atoms <= cfg_.round_atoms)) {
+        atoms += stepping[take]->desc.d.n_atoms;
+        ++take;
       }
+      stepping.resize(take);
+      std::sort(stepping.begin(), stepping.end(), [](const Request* a, const Request* b) { return a->id < b->id; });
+    }
+    int k = cfg_.steps_per_round;
+    for (Request* r : stepping) k = std::min(k, r->remaining);
+    std::vector<int32_t> ids;
+    for (Request* r : stepping) ids.push_back(r->sys);
     int rc = RBMD_OK;
     if (!ids.empty() && k > 0) {
       rc = ctx_->step(ids.data(), (int)ids.size(), k);

@@ -63,8 +63,9 @@ def _serve(mix, wait_between=None, **cfg):
 
 
 @pytest.mark.parametrize("cfg", [dict(steps_per_round=4), dict(steps_per_round=50, max_systems=2),
-                                 dict(steps_per_round=3, max_systems=1)],
-                         ids=["all_at_once", "two_slots", "one_slot"])
+                                 dict(steps_per_round=3, max_systems=1),
+                                 dict(steps_per_round=4, round_atoms=3500)],
+                         ids=["all_at_once", "two_slots", "one_slot", "least_work_first"])
 def test_serve_results_equal_alone(alone_results, cfg):
     mix = _mix()
     got = _serve(mix, **cfg)
@@ -121,3 +122,23 @@ def test_serve_poll_states():
     assert th["step"] == 6 and st["t_done"] >= st["t_admit"] >= st["t_submit"]
     ctx.serve_stop()
     ctx.close()
+
+
+def test_serve_least_work_first_rounds():
+    """round_atoms: a round steps the requests with the least remaining work up to that many atoms,
+    so a small request submitted with large ones finishes first; results stay the alone ones."""
+    big = [synth.saline(3000, seed=20 + k) for k in range(3)]
+    small = synth.saline(1000, seed=30)
+    ctx = rbmd_b200.Context()
+    ctx.serve_start(steps_per_round=5, round_atoms=3500)
+    rids = [ctx.serve_submit(sd, 30) for sd in big] + [ctx.serve_submit(small, 30)]
+    out = []
+    for rid in rids:
+        assert ctx.serve_wait(rid, 300.0) == 0
+        out.append(ctx.serve_result(rid))
+    ctx.serve_stop()
+    ctx.close()
+    done = [st["t_done"] for _, _, _, st in out]
+    assert done[3] < min(done[:3])
+    xa, va, _ = _alone(small, 30)
+    assert np.array_equal(out[3][0], xa) and np.array_equal(out[3][1], va)
