@@ -6,7 +6,8 @@
  * four Cont* and Exec* device objects:
  *   - point locator      framework/locator/ContPointLocator.cxx:70-115, ExecPointLocator.h:38-382
  *   - force function     framework/forceFunction/ContForceFunction.cpp:30-45, ExecForceFunction.h
- *   - static erfc table  framework/staticTable/ContStaticTable.cpp:30-44 (replaced by analytic erfc)
+ *   - static erfc table  framework/staticTable/ContStaticTable.cpp:30-44 (analytic erfc by default;
+ *                        the table lookup on request, rbmd_params.near_table)
  *   - topology           framework/topology/ContTopology.cpp:31-42, ExecTopology.h:35-97
  * and the worklet library framework/run/worklet/RunWorklet.h:40-502 plus the water constraint and
  * bonded worklets of framework/run/worklet/MolecularWorklet.h.
@@ -29,7 +30,7 @@
 extern "C" {
 #endif
 
-#define RBMD_ABI_VERSION 5
+#define RBMD_ABI_VERSION 6
 
 /* ---------------------------------------------------------------- status codes */
 enum rbmd_status {
@@ -100,6 +101,22 @@ enum rbmd_press_ctrl {
                                 NOSE_HOOVER */
 };
 
+/* Real-space Coulomb kernel G(r) of the RBL near forces (ComputeNearEnergyForceERF[_box],
+ * ExecForceFunction.h:581-596, 665-680: F = -qi qj G(r) r_ij / r). */
+enum rbmd_near_coulomb {
+  RBMD_NEAR_ANALYTIC = 0,    /* G(r) = erfc(sqrt(a) r)/r^2 + 2 sqrt(a) exp(-a r^2)/(sqrt(pi) r) at the
+                                system's alpha (the form of ExecForceFunction::Gnear, :682-689) */
+  RBMD_NEAR_TABLE = 1        /* the reference's lookup (ExecStaticTable::Extract / TableGnearValue,
+                                staticTable/ExecStaticTable.h:96-135): G of alpha = 0.1 whatever the
+                                system's alpha, read without interpolation at the 11-bit key of
+                                the FP32 distance (rbmd_near_table_key); from
+                                rbmd_system_desc.near_table_values, else rbmd_near_table_default.
+                                RBL near forces only (Verlet forces and every energy stay analytic,
+                                as in the reference); needs cut_off <= 12, where the reference's
+                                table ends; pairs closer than 0.1 (before its first entry, where
+                                the reference reads outside the table) take the entry of r = 0.1 */
+};
+
 /* ---------------------------------------------------------------- run parameters */
 /* Mirrors the JSON keys that framework/hyperparameters/{ForceField,Neighbor,Coulomb,Extend}.cpp
  * and ExecutionMD::SetParameters (framework/run/ExecutionMD.cpp:144-153) copy into Para. */
@@ -126,7 +143,7 @@ typedef struct rbmd_params {
                                    pressure for temp_ctrl / press_ctrl BERENDSEN / BERENDSEN and
                                    NOSE_HOOVER / NOSE_HOOVER, the two pairs accepted here) */
   int32_t press_ctrl;           /* enum rbmd_press_ctrl */
-  int32_t pad0;
+  int32_t near_table;           /* enum rbmd_near_coulomb (default RBMD_NEAR_ANALYTIC) */
   double timestep;
   int64_t num_steps;            /* length of the run, used for temperature ramps */
   double special_bonds[3];      /* 1-2, 1-3, 1-4 LJ weights */
@@ -204,6 +221,11 @@ typedef struct rbmd_system_desc {
    * i >= j at index i (i+1)/2 + j. */
   int32_t eam_per_type;
   int32_t pad_eam;
+  /* RBMD_NEAR_TABLE: G by key, [RBMD_NEAR_TABLE_KEYS] (the reference's tables
+   * res/json_files/Gnear_table_{leq,geq}2_2.txt, column 4 at the key of column 1, fill keys
+   * 921-2047 and 0-639); NULL: rbmd_near_table_default.  Keys the reference's table does not
+   * cover should hold G at the key's lower edge, as the default table does. */
+  const float* near_table_values;
 } rbmd_system_desc;
 
 /* ---------------------------------------------------------------- results */
@@ -361,6 +383,21 @@ int rbmd_observe(rbmd_ctx* ctx, int32_t sys_id, double* msd, double* vacf);
  * bins at dr, 2 dr, ... accumulated by repeated addition.  radii may be NULL (count only); at most
  * cap values are written.  RBMD_ERR_ARG unless radius > 0, dr > 0 and radius / dr >= 1. */
 int rbmd_rdf_bins(double radius, double dr, double* radii, int32_t cap, int32_t* n_bins);
+
+/* ---------------------------------------------------------------- near-Coulomb table */
+#define RBMD_NEAR_TABLE_KEYS 2048
+/* The key of a distance: bits 15-25 of its FP32 pattern (the exponent's low three bits and the
+ * mantissa's top eight; ExecStaticTable::Extract, MASK 2^26 - 2^15 and MANTISSA_BITS 8,
+ * ExecStaticTable.h:38-39, 125-133).  Distances in [0.1, 2) give keys 921-2047, [2, 12) 0-639. */
+int32_t rbmd_near_table_key(float r);
+/* The library's table, [RBMD_NEAR_TABLE_KEYS] floats: G of alpha = 0.1 in FP64, rounded to FP32,
+ * at the points the reference tabulates -- for each key the first r of the walks
+ * r = 0.1 + 0.0001 m (r < 2) and r = 2 + 0.001 m (r < 12) that has that key (column 2 of its
+ * table files) -- and at the key's lower edge for the keys those walks do not reach.  The
+ * reference's files print G to six digits; below r = 8 they equal these values to that
+ * precision, above it they drift from the FP64 G, to about 1% at r = 12 (as 1 - erf taken in
+ * single precision would). */
+int rbmd_near_table_default(float* out);
 /* RDF pair counts of the current configuration (RDFOutput::ComputeRDF,
  * framework/output/RDFOutput.cpp:181-262; ComputeRDFWorklet,
  * framework/output/worklet/OutPutWorklet.cpp:230-310 and :578-640): counts[b] (n_bins of

@@ -115,6 +115,11 @@ struct Barostat {  // ExecutionNPT MTK state, ExecutionNPT.cpp:145-232, 1545-160
   double p_hydro = 0, p_current = 0, mtk_term1 = 0, mtk_term2 = 0;
 };
 
+// The reference's near-Coulomb table for alpha = 0.1 (model/ERFTable.h; the points its files
+// res/json_files/Gnear_table_{leq,geq}2_2.txt list), [2048] by key; see oracle_core.cpp.
+int near_key(float r);
+void near_table(float* out);
+
 class System {
  public:
   System(const rbmd_system_desc& desc, const rbmd_params& params);
@@ -144,6 +149,11 @@ class System {
     const int hi = a > b ? a : b, lo = a > b ? b : a;
     return &z2r_spline[eam_per_type ? (size_t)(hi * (hi + 1) / 2 + lo) * 7 * (eam_nr + 1) : 0];
   }
+
+  // RBMD_NEAR_TABLE (RBL near Coulomb): G by the 11-bit key of the FP32 distance,
+  // ExecStaticTable::Extract / TableGnearValue (staticTable/ExecStaticTable.h:96-135)
+  std::vector<float> near_tab;
+  double near_g(double dis) const;
 
   rbmd_params p;
   Units u;

@@ -179,6 +179,14 @@ int oracle_get_derived(void* h, rbmd_derived* out) {
 
 int oracle_status(void* h) { return static_cast<System*>(h)->status; }
 
+int oracle_near_key(float r) { return oracle::near_key(r); }
+
+int oracle_near_table(float* out) {
+  if (!out) return 1;
+  oracle::near_table(out);
+  return 0;
+}
+
 int oracle_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
   oracle::philox4x32_10(ctr, key, out);
   return 0;

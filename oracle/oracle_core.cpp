@@ -56,6 +56,48 @@ double u01(uint32_t hi, uint32_t lo) {
 }
 
 // ------------------------------------------------------------------ set-up
+// ExecStaticTable::Extract (staticTable/ExecStaticTable.h:125-133): (bits & MASK) >> (23 - 8) with
+// MASK = 2^26 - 2^15 (:38-39), i.e. the exponent's low three bits over the mantissa's top eight.
+int near_key(float r) {
+  uint32_t bits;
+  std::memcpy(&bits, &r, 4);
+  return (int)((bits & (67108864u - 32768u)) >> 15);
+}
+
+// G(r) = erfc(sqrt(a) r) / r^2 + 2 sqrt(a) exp(-a r^2) / (sqrt(pi) r), a = 0.1 (the Gnear form,
+// ExecForceFunction.h:682-689).  The tabulated points are, for each key, the first point of the
+// walk r = 0.1, 0.1001, ... (below 2) or r = 2, 2.001, ... (below 12) with that key (column 2 of the
+// table files); keys no walk reaches hold G at the smallest distance with that key.
+void near_table(float* out) {
+  const double a = 0.1;
+  auto G = [a](double r) {
+    return std::erfc(std::sqrt(a) * r) / (r * r) + 2 * std::sqrt(a) * std::exp(-a * r * r) / (std::sqrt(kPi) * r);
+  };
+  for (int k = 0; k < 2048; ++k) {
+    // exponent bits 0-2 -> 2^1..2^3 (distances 2..16), bits 3-7 -> 2^-4..2^0 (1/16..2)
+    const int low3 = k / 256;
+    const double base = low3 < 3 ? std::pow(2.0, 1 + low3) : std::pow(2.0, low3 - 7);
+    out[k] = (float)G(base * (1.0 + (k % 256) / 256.0));
+  }
+  std::vector<bool> done(2048, false);
+  const double start[2] = {0.1, 2.0}, stride[2] = {1e-4, 1e-3}, stop[2] = {2.0, 12.0};
+  for (int w = 0; w < 2; ++w)
+    for (long m = 0; start[w] + (double)m * stride[w] < stop[w]; ++m) {
+      const double r = start[w] + (double)m * stride[w];
+      const int k = near_key((float)r);
+      if (done[k]) continue;
+      done[k] = true;
+      out[k] = (float)G(r);
+    }
+}
+
+// TableGnearValue (ExecStaticTable.h:96-123): the entry at the key, no interpolation.  The
+// reference indexes before its table for r < 0.1; the entry of r = 0.1 stands in there.
+double System::near_g(double dis) const {
+  const float d = (float)dis;
+  return (double)near_tab[d < 0.1f ? 921 : near_key(d)];
+}
+
 System::System(const rbmd_system_desc& d, const rbmd_params& prm) : p(prm) {
   N = d.n_atoms;
   ntypes = d.n_types;
@@ -82,6 +124,11 @@ System::System(const rbmd_system_desc& d, const rbmd_params& prm) : p(prm) {
   for (int i = 0; i < N; ++i) mol[i] = d.molecule ? d.molecule[i] : i;
   eps.assign(d.epsilon, d.epsilon + ntypes);
   sig.assign(d.sigma, d.sigma + ntypes);
+  if (p.near_table == RBMD_NEAR_TABLE) {
+    near_tab.resize(2048);
+    if (d.near_table_values) near_tab.assign(d.near_table_values, d.near_table_values + 2048);
+    else near_table(near_tab.data());
+  }
   if (d.n_bonds > 0) {
     bond_atoms.assign(d.bond_atoms, d.bond_atoms + 2 * d.n_bonds);
     bond_type.assign(d.bond_type, d.bond_type + d.n_bonds);

@@ -70,6 +70,25 @@ def philox_kat(ctr, key):
     return list(o)
 
 
+def near_table():
+    """The oracle's near-Coulomb table (2048 float32 G values by key, alpha = 0.1)."""
+    import numpy as np
+    out = np.zeros(2048, np.float32)
+    L = lib()
+    L.oracle_near_table.argtypes = [C.POINTER(C.c_float)]
+    L.oracle_near_table.restype = C.c_int
+    assert L.oracle_near_table(out.ctypes.data_as(C.POINTER(C.c_float))) == 0
+    return out
+
+
+def near_key(r):
+    """Key of a distance (bits 15-25 of its float32 pattern)."""
+    L = lib()
+    L.oracle_near_key.argtypes = [C.c_float]
+    L.oracle_near_key.restype = C.c_int
+    return L.oracle_near_key(float(r))
+
+
 def _dp(a):
     from rbmd_b200 import _abi as A
     return a.ctypes.data_as(A.dptr)

@@ -243,7 +243,7 @@ void System::near_force(std::vector<double>& F) {
           bool in = core ? (dis_2 < rc_2 && dis_2 > 0.0001)
                          : (special ? (dis_2 < rc_2 && dis_2 > rs_2) : (dis_2 < rc_2 && dis_2 > 0.0001));
           if (in) {
-            double g = gnear(p.alpha, dis);
+            double g = near_tab.empty() ? gnear(p.alpha, dis) : near_g(dis);
             double fs_ = -q[i] * q[j] * g;
             for (int k = 0; k < 3; ++k) {
               double val = fs_ * r[k] / dis;

@@ -5,7 +5,7 @@ a probe with the host compiler.
 """
 import ctypes as C
 
-RBMD_ABI_VERSION = 5
+RBMD_ABI_VERSION = 6
 
 # status
 OK, ERR_ARG, ERR_OOM, ERR_NUMERIC, ERR_TIMEOUT, ERR_CUDA, ERR_STATE, ERR_BUDGET, ERR_UNSUPPORTED, ERR_IO = range(10)
@@ -19,6 +19,7 @@ STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_OOM", 3: "ERR_NUMERIC", 4: "ERR_T
 FF_LJ_CUT, FF_LJ_CUT_COUL_LONG, FF_CVFF, FF_EAM = 0, 1, 2, 3
 NEIGH_RBL, NEIGH_VERLET = 0, 1
 COUL_NONE, COUL_RBE, COUL_EWALD = 0, 1, 2
+NEAR_ANALYTIC, NEAR_TABLE = 0, 1
 TC_NOSE_HOOVER, TC_BERENDSEN, TC_RESCALE, TC_NONE = 0, 1, 2, 3
 UNITS_LJ, UNITS_REAL, UNITS_METAL = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
@@ -51,7 +52,7 @@ class Params(C.Structure):
         ("cut_off", C.c_double), ("r_core", C.c_double),
         ("coulomb_sample_num", C.c_int32), ("kmax", C.c_int32 * 3),
         ("alpha", C.c_double), ("temperature", C.c_double * 3), ("pressure", C.c_double * 3),
-        ("press_ctrl", C.c_int32), ("pad0", C.c_int32),
+        ("press_ctrl", C.c_int32), ("near_table", C.c_int32),
         ("timestep", C.c_double), ("num_steps", C.c_int64),
         ("special_bonds", C.c_double * 3), ("seed", C.c_uint64), ("bulk_modulus", C.c_double),
     ]
@@ -77,6 +78,7 @@ class SystemDesc(C.Structure):
         ("dihedral_atoms", iptr), ("dihedral_type", iptr), ("dihedral_k", dptr), ("dihedral_sign", iptr),
         ("dihedral_multiplicity", iptr),
         ("eam_per_type", C.c_int32), ("pad_eam", C.c_int32),
+        ("near_table_values", C.POINTER(C.c_float)),
     ]
 
 
@@ -234,6 +236,8 @@ def declare(lib, prefix="rbmd"):
         "observe_reset": ([ctx, C.c_int32, C.c_int32], C.c_int),
         "observe": ([ctx, C.c_int32, dptr, dptr], C.c_int),
         "rdf_bins": ([C.c_double, C.c_double, dptr, C.c_int32, iptr], C.c_int),
+        "near_table_key": ([C.c_float], C.c_int32),
+        "near_table_default": ([C.POINTER(C.c_float)], C.c_int),
         "snapshot_begin": ([ctx, C.c_int32, dptr, dptr, iptr, dptr, lptr, lptr], C.c_int),
         "snapshot_poll": ([ctx, C.c_int64, iptr], C.c_int),
         "snapshot_wait": ([ctx, C.c_int64, C.c_double], C.c_int),
@@ -259,5 +263,5 @@ HEADER_FUNCTIONS = [
     "rbmd_profile_get", "rbmd_step_timed", "rbmd_fma_peak", "rbmd_autotune",
     "rbmd_observe_reset", "rbmd_observe", "rbmd_rdf_bins", "rbmd_rdf_counts",
     "rbmd_snapshot_begin", "rbmd_snapshot_poll", "rbmd_snapshot_wait",
-    "rbmd_eam_read_setfl", "rbmd_eam_build_setfl_splines",
+    "rbmd_eam_read_setfl", "rbmd_eam_build_setfl_splines", "rbmd_near_table_key", "rbmd_near_table_default",
 ]

@@ -206,6 +206,14 @@ int rbmd_rdf_bins(double radius, double dr, double* radii, int32_t cap, int32_t*
   return RBMD_OK;
 }
 
+int32_t rbmd_near_table_key(float r) { return rbmd::near_table_key(r); }
+
+int rbmd_near_table_default(float* out) {
+  if (!out) return RBMD_ERR_ARG;
+  rbmd::near_table_default(out);
+  return RBMD_OK;
+}
+
 int rbmd_rdf_counts(rbmd_ctx* ctx, int32_t id, const int32_t* centers, int32_t nc, const int32_t* targets, int32_t nt,
                     double radius, double dr, int32_t exclude_same_molecule, int64_t* counts, double* volume) {
   CTX_CHECK(ctx);

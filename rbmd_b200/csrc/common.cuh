@@ -93,8 +93,6 @@ struct SysDev {
   int dense;  // pair kernel layout: 0 warp per atom, 1 tile (warp per home cell), 2 column (warp per
               // column of home cells, lane per atom; FP32 RBL forces only, the tile kernel otherwise)
   int blocks_pair, blocks_atom, blocks_rho, blocks_tri, rbe_mmax, rbe_slots, has_triples, n_triples;
-  int blocks_col;  // blocks of the column kernel per system (dense == 2)
-  int col_pad;
   // NPT barostats (npt 1: Berendsen at the end of the step, 2: MTK around the integrator): the
   // box changes on the device every step.  Cell arrays and the cell work table hold ncell_cap cells
   // (the box at kBoxGrow x L0); kmax indexes the Ewald k lists.
@@ -143,6 +141,9 @@ struct SysDev {
   // per-type tables
   double* eps;
   double* sig;
+  float2* ljf;  // mixed precision, [ntypes^2] by type pair a ntypes + b: -24 sqrt(eps_a eps_b) and
+                // ((sig_a + sig_b) / 2)^6, each rounded once from FP64
+  float* near_tab;  // RBMD_NEAR_TABLE with RBL Coulomb: G by key [kNearKeys]; nullptr: analytic G
   // special-bond CSR and molecules
   int* sp_off;
   int* sp_ids;

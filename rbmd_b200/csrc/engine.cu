@@ -262,6 +262,8 @@ int64_t Context::estimate_bytes(const rbmd_system_desc& d, const rbmd_params& p)
     eam_table_sizes(d, &nf, &nr, &nz);
     b += (int64_t)(nf + nr + nz) * 8;
   }
+  if (p.precision == RBMD_PREC_MIXED) b += (int64_t)d.n_types * d.n_types * 8;  // FP32 LJ factors
+  if (p.near_table == RBMD_NEAR_TABLE) b += (int64_t)kNearKeys * 4;
   b += ((n + kPairWarps - 1) / kPairWarps) * 72 + ((n + kAtomBlock - 1) / kAtomBlock) * 64 + 4096;
   return b;
 }
@@ -290,6 +292,11 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
     if (!(p.pressure[2] > 0)) return fail(RBMD_ERR_ARG, "NPT needs a pressure damping time pressure[2] > 0");
     if (ber && !(p.bulk_modulus > 0)) return fail(RBMD_ERR_ARG, "NPT Berendsen needs bulk_modulus > 0");
   }
+  if (p.near_table != RBMD_NEAR_ANALYTIC && p.near_table != RBMD_NEAR_TABLE)
+    return fail(RBMD_ERR_ARG, "near_table must be RBMD_NEAR_ANALYTIC or RBMD_NEAR_TABLE");
+  if (p.near_table == RBMD_NEAR_TABLE && p.cut_off > 12.0)
+    return fail(RBMD_ERR_UNSUPPORTED, "near_table: the reference's table ends at r = 12, cut_off is " +
+                                          std::to_string(p.cut_off));
   if (p.precision == RBMD_PREC_MIXED && d.n_types > kMaxF32Types)
     return fail(RBMD_ERR_UNSUPPORTED, "mixed precision supports at most " + std::to_string(kMaxF32Types) +
                                           " atom types");
@@ -481,7 +488,6 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
     D.ncell_cap = D.ncell;
   }
   D.blocks_pair = D.dense ? tile_blocks(D) : (n + kPairWarps - 1) / kPairWarps;
-  D.blocks_col = column_blocks(D);
   D.blocks_atom = (n + kAtomBlock - 1) / kAtomBlock;
   D.blocks_rho = (n + kRhoChunk - 1) / kRhoChunk;
   D.blocks_tri = (D.n_triples + 127) / 128;
@@ -637,6 +643,24 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   D.smeta = (int4*)dal(sizeof(int4) * n);
   D.eps = (double*)dal(sizeof(double) * d.n_types);
   D.sig = (double*)dal(sizeof(double) * d.n_types);
+  std::vector<float2> hlj;
+  if (D.prec == RBMD_PREC_MIXED) {  // at most kMaxF32Types types (checked above)
+    hlj.resize((size_t)d.n_types * d.n_types);
+    for (int a = 0; a < d.n_types; ++a)
+      for (int b = 0; b < d.n_types; ++b) {
+        const double sg = (d.sigma[a] + d.sigma[b]) / 2;
+        hlj[(size_t)a * d.n_types + b] =
+            make_float2((float)(-24.0 * std::sqrt(d.epsilon[a] * d.epsilon[b])), (float)(sg * sg * sg * sg * sg * sg));
+      }
+    D.ljf = (float2*)dal(sizeof(float2) * hlj.size());
+  }
+  std::vector<float> hnear;
+  if (p.near_table == RBMD_NEAR_TABLE && D.coul != RBMD_COUL_NONE && D.neigh == RBMD_NEIGH_RBL) {
+    hnear.resize(kNearKeys);
+    if (d.near_table_values) std::memcpy(hnear.data(), d.near_table_values, sizeof(float) * kNearKeys);
+    else near_table_default(hnear.data());
+    D.near_tab = (float*)dal(sizeof(float) * kNearKeys);
+  }
   D.mol_off = (int*)dal(sizeof(int) * mol_off.size());
   D.mol_atoms = (int*)dal(sizeof(int) * n);
   std::vector<int> sp_off;
@@ -741,6 +765,8 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   up(D.image, himg.data(), sizeof(int) * 3 * n);
   up(D.eps, d.epsilon, sizeof(double) * d.n_types);
   up(D.sig, d.sigma, sizeof(double) * d.n_types);
+  up(D.ljf, hlj.data(), sizeof(float2) * hlj.size());
+  up(D.near_tab, hnear.data(), sizeof(float) * hnear.size());
   up(D.mol_off, mol_off.data(), sizeof(int) * mol_off.size());
   up(D.mol_atoms, mol_atoms.data(), sizeof(int) * n);
   SysState st0;
@@ -801,13 +827,48 @@ int Context::remove_system(int id) {
   return RBMD_OK;
 }
 
+// ------------------------------------------------------------------------------ near-Coulomb table
+int near_table_key(float r) {
+  uint32_t b;
+  std::memcpy(&b, &r, sizeof(b));
+  return (int)((b & 0x03FF8000u) >> 15);
+}
+
+void near_table_default(float* out) {
+  const double a = 0.1, sa = std::sqrt(a);
+  auto g = [&](double r) {
+    return std::erfc(sa * r) / (r * r) + 2.0 * sa * std::exp(-a * r * r) / (std::sqrt(kPi) * r);
+  };
+  // every key: G at its lower edge, 2^e (1 + m / 256) for mantissa top bits m and an exponent e whose
+  // low three bits are the key's (e in [-4, 3] for the distances 1/16 .. 16 this covers)
+  for (int k = 0; k < kNearKeys; ++k) {
+    const int e3 = k >> 8, e = e3 <= 2 ? 1 + e3 : e3 - 7;
+    out[k] = (float)g(std::ldexp(1.0 + (k & 255) / 256.0, e));
+  }
+  // the reference's tabulated points: the first r of each walk with a given key
+  std::vector<char> seen(kNearKeys, 0);
+  auto walk = [&](double r0, double dr, double r1) {
+    for (long m = 0;; ++m) {
+      const double r = r0 + (double)m * dr;
+      if (r >= r1) break;
+      const int k = near_table_key((float)r);
+      if (!seen[k]) {
+        seen[k] = 1;
+        out[k] = (float)g(r);
+      }
+    }
+  };
+  walk(0.1, 1e-4, 2.0);
+  walk(2.0, 1e-3, 12.0);
+}
+
 // ------------------------------------------------------------------------------ batches
 bool same_group(const System* a, const System* b, bool layout) {
   const SysDev &x = a->dev, &y = b->dev;
   return x.ff == y.ff && x.neigh == y.neigh && x.coul == y.coul && x.prec == y.prec &&
          x.temp_ctrl == y.temp_ctrl && x.special == y.special && x.has_triples == y.has_triples &&
          ((x.n_bonds + x.n_angles + x.n_dihedrals) > 0) == ((y.n_bonds + y.n_angles + y.n_dihedrals) > 0) &&
-         x.npt == y.npt && x.rc2 == y.rc2 &&
+         x.npt == y.npt && x.rc2 == y.rc2 && (x.near_tab != nullptr) == (y.near_tab != nullptr) &&
          x.rs2 == y.rs2 &&
          (!layout || (x.dense == y.dense && x.lean == y.lean));
 }
@@ -829,8 +890,10 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
   b.dense = g.dense;
   b.lean = g.lean;
   b.npt = g.npt;
+  b.near = g.near_tab != nullptr;
   std::vector<int> slots;
   std::vector<int2> wa, wp, wc, wr, wt, wm, wpc;
+  std::vector<std::pair<double, int2>> cols;  // column layout: (atoms per column, (slot, column))
   for (int k = 0; k < 4; ++k) b.band[k] = g.band[k];
   for (System* s : group) {
     const SysDev& D = s->dev;
@@ -844,7 +907,8 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
     b.natoms += D.n;
     for (int k = 0; k < D.n; k += kAtomBlock) wa.push_back(make_int2(s->slot, k));
     if (D.dense == 2) {
-      for (int k = 0; k < D.dims[0] * D.dims[1]; k += kColWarpsHost) wp.push_back(make_int2(s->slot, k));
+      const int nxy = D.dims[0] * D.dims[1];
+      for (int k = 0; k < nxy; ++k) cols.push_back({(double)D.n / nxy, make_int2(s->slot, k)});
       for (int k = 0; k < D.ncell; k += kCellWarpsHost) wpc.push_back(make_int2(s->slot, k));
     } else if (D.dense)
       for (int k = 0; k < D.ncell; k += kCellWarpsHost) wp.push_back(make_int2(s->slot, k));
@@ -855,6 +919,11 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
     for (int k = 0; k < D.n_triples; k += 128) wt.push_back(make_int2(s->slot, k));
     for (int k = 0; k < D.n_bonds + D.n_angles + D.n_dihedrals; k += 128) wm.push_back(make_int2(s->slot, k));
   }
+  // the longest columns first, so that the persistent kernel's last columns are short ones
+  std::stable_sort(cols.begin(), cols.end(), [](const std::pair<double, int2>& a, const std::pair<double, int2>& c) {
+    return a.first > c.first;
+  });
+  for (const auto& c : cols) wp.push_back(c.second);
   auto mk = [&](const std::vector<int2>& h, Work& w) {
     w.n = (int)h.size();
     if (h.empty()) return;
@@ -870,6 +939,15 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
   mk(wa, b.atom);
   mk(wp, b.pair);
   mk(wpc, b.pair_cells);
+  if (b.dense == 2 && b.pair.n > 0) {
+    b.col_ctr = (unsigned*)dmalloc(2 * sizeof(unsigned));
+    if (!b.col_ctr) rc = RBMD_ERR_OOM;
+    else {
+      br->allocs.push_back(b.col_ctr);
+      cudaMemsetAsync(b.col_ctr, 0, 2 * sizeof(unsigned), stream);
+    }
+    b.col_grid = pair_col_grid(b.pair.n, b.ff, b.special, b.near);
+  }
   mk(wc, b.cell);
   mk(wr, b.rho);
   mk(wt, b.tri);

@@ -60,10 +60,9 @@ inline bool column_layout_ok(const SysDev& D) {
   return tile_layout_ok(D) && D.n < (1 << 25) && D.prec == RBMD_PREC_MIXED && D.neigh == RBMD_NEIGH_RBL &&
          D.ff != RBMD_FF_EAM;
 }
-// Blocks per system of the pair kernels: tile (4 home cells per block; also the column layout's
-// cell table), column (4 columns per block), warp per atom (8 atoms per block).
+// Blocks per system of the tile pair kernel (4 home cells per block; also the column layout's cell
+// table for the passes the column kernel does not run).
 inline int tile_blocks(const SysDev& D) { return (D.ncell + 3) / 4; }
-inline int column_blocks(const SysDev& D) { return (D.dims[0] * D.dims[1] + 3) / 4; }
 
 // Doubles in each EAM spline array of a descriptor: frho, rhor and z2r (per type when
 // eam_per_type, one table each otherwise).
@@ -73,6 +72,12 @@ inline void eam_table_sizes(const rbmd_system_desc& d, size_t* nf, size_t* nr, s
   *nr = 7 * (size_t)(d.eam_nr + 1) * t;
   *nz = 7 * (size_t)(d.eam_nr + 1) * pairs;
 }
+
+// The reference's near-Coulomb lookup table (ExecStaticTable.h:96-135, ERFTable.h): the key of a
+// distance and the library's table of G for alpha = 0.1 by key (include/rbmd_gpu.h documents both).
+constexpr int kNearKeys = RBMD_NEAR_TABLE_KEYS;
+int near_table_key(float r);
+void near_table_default(float* out);
 
 // RDF bins of radius / dr (RDFOutput.cpp:42-53): (int)(radius / dr) radii, dr accumulated by
 // repeated addition.  Returns the bin count, or -1 for a bad (radius, dr).

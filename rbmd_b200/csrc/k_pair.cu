@@ -81,6 +81,14 @@ __device__ inline float r_exp(float x) { return __expf(x); }
 __device__ inline double r_erfc(double x) { return erfc(x); }
 __device__ inline float r_erfc(float x) { return erfcf(x); }
 
+// The reference's near-Coulomb table (ExecStaticTable::Extract + TableGnearValue,
+// staticTable/ExecStaticTable.h:96-135): G at the key of the FP32 distance, bits 15-25 of its
+// pattern; closer than 0.1, before the reference's first entry, the entry of r = 0.1 (key 921).
+__device__ __forceinline__ float near_table_g(const float* __restrict__ tab, float dis) {
+  const unsigned k = dis < 0.1f ? 921u : ((__float_as_uint(dis) & 0x03FF8000u) >> 15);
+  return __ldg(&tab[k]);
+}
+
 // EAM spline row evaluation (ExecForceFunction::ComputeEAMrho / ComputeEAMforce)
 __device__ inline void eam_row(const double* tab, double r, double rdr, int nr, int& m, double& p) {
   p = r * rdr + 1.0;
@@ -113,7 +121,7 @@ struct PairAcc {
   double vir[6];
 };
 
-template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
+template <typename R, int MODE, bool SPECIAL, bool VIRIAL, bool NEAR = false>
 __device__ inline void eval_pair(const SysDev& s, int i, int ti, int moli, double qi, double fpi,
                                  int js, bool core, R rx, R ry, R rz, const int* spi, const double* spw,
                                  int nsp, R pice, PairAcc& a) {
@@ -204,8 +212,13 @@ __device__ inline void eval_pair(const SysDev& s, int i, int ti, int moli, doubl
                          : (SPECIAL ? (d2 < rc2 && d2 > rs2) : (d2 < rc2 && d2 > R(0.0001)));
     if (in) {
       const R dis = r_sqrt(d2);
-      const R sa = r_sqrt(alpha);
-      const R g = r_erfc(sa * dis) / d2 + R(2) * sa * r_exp(-alpha * d2) / ((R)sqrt(kPif) * dis);
+      R g;
+      if constexpr (NEAR) {  // RBMD_NEAR_TABLE
+        g = (R)near_table_g(s.near_tab, (float)dis);
+      } else {
+        const R sa = r_sqrt(alpha);
+        g = r_erfc(sa * dis) / d2 + R(2) * sa * r_exp(-alpha * d2) / ((R)sqrt(kPif) * dis);
+      }
       R fc = -(R)qi * qj * g / dis;
       if (!core) fc *= pice;
       a.g[0] += (double)(fc * rx);
@@ -270,7 +283,7 @@ __device__ inline void eval_pair(const SysDev& s, int i, int ti, int moli, doubl
   }
 }
 
-template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
+template <typename R, int MODE, bool SPECIAL, bool VIRIAL, bool NEAR = false>
 __global__ void __launch_bounds__(kPairWarps * 32)
 k_pair(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int* out_nc,
        int* out_ns, int* out_core, int* out_shell) {
@@ -347,7 +360,7 @@ k_pair(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int
         const bool core = js >= 0;
         if (!core) js = ~js;
         const R rx = s_qr[wid][0][lane], ry = s_qr[wid][1][lane], rz = s_qr[wid][2][lane];
-        eval_pair<R, MODE, SPECIAL, VIRIAL>(s, i, ti, moli, xi.w, fpi, js, core, rx, ry, rz, spi, spw,
+        eval_pair<R, MODE, SPECIAL, VIRIAL, NEAR>(s, i, ti, moli, xi.w, fpi, js, core, rx, ry, rz, spi, spw,
                                             nsp, (R)pice, a);
       }
       if (MODE == kLIST) {
@@ -591,12 +604,12 @@ __device__ inline float erfc_as_times(float x, float e) {
 // FP32 pair arithmetic of the RBL modes on preloaded data of j (type tj, molecule molj, charge qj)
 // and the special-bond weight w of the pair.  IMG applies the minimum image; callers whose
 // displacement is already the nearest image (|r| < rc < L / 2) skip it.
-template <int MODE, bool IMG = true>
+template <int MODE, bool IMG = true, bool NEAR = false>
 __device__ inline void eval_pair_f32_pre(int moli, float qi, bool core, float rx, float ry, float rz, int ti, int tj,
                                          int molj, float qj, float w, float pice, float rc2, float rs2, float sa,
                                          float alpha, const float* tab, int ntypes, float Lx, float Ly, float Lz,
                                          float& fx, float& fy, float& fz, float& gx, float& gy, float& gz,
-                                         bool special) {
+                                         bool special, const float* ntab) {
   if (MODE == kLJ_RBL && moli == molj) return;
   if (IMG) min_image(rx, ry, rz, Lx, Ly, Lz);
   const float d2 = rx * rx + ry * ry + rz * rz;
@@ -621,10 +634,15 @@ __device__ inline void eval_pair_f32_pre(int moli, float qi, bool core, float rx
     const bool in = core ? (d2 < rc2 && d2 > 0.0001f)
                          : (special ? (d2 < rc2 && d2 > rs2) : (d2 < rc2 && d2 > 0.0001f));
     if (in) {
-      const float r = d2 * inv_r;
-      const float x = sa * r;
-      const float e = __expf(-alpha * d2);
-      const float g = erfc_as_times(x, e) * inv_d2 + 1.1283791671f * sa * e * inv_r;  // 2/sqrt(pi)
+      float g;
+      if constexpr (NEAR) {  // RBMD_NEAR_TABLE
+        g = near_table_g(ntab, __fsqrt_rn(d2));
+      } else {
+        const float r = d2 * inv_r;
+        const float x = sa * r;
+        const float e = __expf(-alpha * d2);
+        g = erfc_as_times(x, e) * inv_d2 + 1.1283791671f * sa * e * inv_r;  // 2/sqrt(pi)
+      }
       float fc = -qi * qj * g * inv_r;
       if (!core) fc *= pice;
       gx += fc * rx;
@@ -634,7 +652,7 @@ __device__ inline void eval_pair_f32_pre(int moli, float qi, bool core, float rx
   }
 }
 
-template <int MODE, bool SPECIAL>
+template <int MODE, bool SPECIAL, bool NEAR = false>
 __device__ inline void eval_pair_f32(const SysDev& s, int moli, float qi, int js, bool core, float rx, float ry,
                                      float rz, int ti, const int* spi, const double* spw, int nsp, float pice,
                                      float rc2, float rs2, float sa, float alpha, const float* tab, int ntypes,
@@ -647,11 +665,11 @@ __device__ inline void eval_pair_f32(const SysDev& s, int moli, float qi, int js
     for (int k = 0; k < nsp; ++k)
       if (spi[k] == mj.x) w = (float)spw[k];
   const float qj = (MODE == kCOUL_RBL) ? __ldg(&s.sxf[js].w) : 0.0f;
-  eval_pair_f32_pre<MODE>(moli, qi, core, rx, ry, rz, ti, mj.y, mj.z, qj, w, pice, rc2, rs2, sa, alpha, tab, ntypes,
-                          Lx, Ly, Lz, fx, fy, fz, gx, gy, gz, SPECIAL);
+  eval_pair_f32_pre<MODE, true, NEAR>(moli, qi, core, rx, ry, rz, ti, mj.y, mj.z, qj, w, pice, rc2, rs2, sa, alpha, tab,
+                                      ntypes, Lx, Ly, Lz, fx, fy, fz, gx, gy, gz, SPECIAL, s.near_tab);
 }
 
-template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
+template <typename R, int MODE, bool SPECIAL, bool VIRIAL, bool NEAR = false>
 __global__ void __launch_bounds__(kPairWarps * 32, 3)
 k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
   using R4 = typename Vec4<R>::T;
@@ -748,12 +766,12 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
         const bool core = js >= 0;
         if (!core) js = ~js;
         if (F32) {
-          eval_pair_f32<MODE, SPECIAL>(s, moli, (float)xi.w, js, core, (float)s_qr[wid][0][slot],
+          eval_pair_f32<MODE, SPECIAL, NEAR>(s, moli, (float)xi.w, js, core, (float)s_qr[wid][0][slot],
                                        (float)s_qr[wid][1][slot], (float)s_qr[wid][2][slot], ti, spi, spw, nsp,
                                        spice, frc2, frs2, fsa, falpha, s_tab, ntypes, fLx, fLy, fLz, ffx, ffy, ffz,
                                        fgx, fgy, fgz);
         } else {
-          eval_pair<R, MODE, SPECIAL, VIRIAL>(s, i, ti, moli, xi.w, fpi, js, core, s_qr[wid][0][slot],
+          eval_pair<R, MODE, SPECIAL, VIRIAL, NEAR>(s, i, ti, moli, xi.w, fpi, js, core, s_qr[wid][0][slot],
                                               s_qr[wid][1][slot], s_qr[wid][2][slot], spi, spw, nsp, (R)pice, a);
         }
       }
@@ -1047,25 +1065,30 @@ __device__ inline float rcp_approx(float x) {
 // FP32 force of one RBL pair as a single vector factor: LJ (cutoff rs for core pairs of the
 // Coulomb modes, rc for LJ/CUT, shell pairs x pice) plus qqr2e times the real-space Coulomb term
 // (erfc by Abramowitz & Stegun 7.1.26, |error| <= 1.5e-7), the same windows as eval_pair_f32_pre.
-// alpha_l2 = alpha log2(e), so exp(-alpha d2) = 2^(-alpha_l2 d2).
-template <int MODE>
+// alpha_l2 = alpha log2(e), so exp(-alpha d2) = 2^(-alpha_l2 d2); clj = -24 sqrt(eps_i eps_j) and
+// s6 = sigma_ij^6 are the type pair's FP32 LJ factors.
 // The pair's class is exact (the FP64 decision, with the reference's 1e-4 margins around rs^2
 // and rc^2), and it implies every cutoff test of the reference's force functions (core: d2 < rs^2
 // and > 1e-4; shell: rs^2 < d2 < rc^2), so none is repeated here on the FP32 d2.
-__device__ inline float tile_pair_f32(bool core, float d2, float qi, float qj, int tp, float w, float pice, float sa,
-                                      float alpha_l2, float qq, const float* tab) {
-  const float clj = tab[2 * tp], s6 = tab[2 * tp + 1];
+template <int MODE, bool NEAR>
+__device__ inline float tile_pair_f32_lj(bool core, float d2, float qi, float qj, float clj, float s6, float w,
+                                         float pice, float sa, float alpha_l2, float qq, const float* ntab) {
   const float inv_r = rsqrt_approx(d2);
   const float inv_d2 = inv_r * inv_r;
   const float sd6 = s6 * inv_d2 * inv_d2 * inv_d2;
   const float ljf = clj * (2.0f * sd6 - 1.0f) * sd6 * inv_d2;
   if (MODE == kLJ_RBL) return core ? ljf : pice * ljf;
   const float fl = core ? w * ljf : w * (pice * ljf);
-  const float x = sa * (d2 * inv_r);
-  const float e = ex2_approx(-alpha_l2 * d2);
-  const float t = rcp_approx(1.0f + 0.3275911f * x);
-  const float erfc = t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f)))) * e;
-  const float g = erfc * inv_d2 + 1.1283791671f * sa * e * inv_r;  // 2/sqrt(pi)
+  float g;
+  if constexpr (NEAR) {  // RBMD_NEAR_TABLE
+    g = near_table_g(ntab, __fsqrt_rn(d2));
+  } else {
+    const float x = sa * (d2 * inv_r);
+    const float e = ex2_approx(-alpha_l2 * d2);
+    const float t = rcp_approx(1.0f + 0.3275911f * x);
+    const float erfc = t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f)))) * e;
+    g = erfc * inv_d2 + 1.1283791671f * sa * e * inv_r;  // 2/sqrt(pi)
+  }
   float fc = -qi * qj * g * inv_r;
   if (!core) fc *= pice;
   return fl + qq * fc;
@@ -1287,7 +1310,7 @@ __device__ inline void acc_warp_total(float (&ff)[6], PairAcc& a, double (&c)[6]
 // cells around its unclamped cell, each wrapped by a true modulo (ExecPointLocator::InWhichCell
 // and PeriodicIndexOffset), candidates 32 at a time.  Selected pairs are evaluated in place into
 // the lanes' accumulators (zero on entry); list mode writes the rows directly.
-template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
+template <typename R, int MODE, bool SPECIAL, bool VIRIAL, bool NEAR = false>
 __device__ void tile_stray(const SysDev& s, int si, int skip, int pice, bool rbl, const float* s_tab, int cap,
                            int* out_nc, int* out_ns, int* out_core, int* out_shell, float (&ff)[6],
                            PairAcc& acc) {
@@ -1360,12 +1383,12 @@ __device__ void tile_stray(const SysDev& s, int si, int skip, int pice, bool rbl
             n_shell += __popc(pk);
           } else if (sel) {
             if (F32)
-              eval_pair_f32<MODE, SPECIAL>(s, moli, (float)xd.w, kk, core, (float)rx, (float)ry, (float)rz, ti, spi,
+              eval_pair_f32<MODE, SPECIAL, NEAR>(s, moli, (float)xd.w, kk, core, (float)rx, (float)ry, (float)rz, ti, spi,
                                            spw, nsp, spice, (float)s.rc2, (float)s.rs2, fsa, falpha, s_tab,
                                            s.ntypes, (float)s.L[0], (float)s.L[1], (float)s.L[2], ff[0], ff[1],
                                            ff[2], ff[3], ff[4], ff[5]);
             else
-              eval_pair<R, MODE, SPECIAL, VIRIAL>(s, i, ti, moli, xd.w, fpi, kk, core, rx, ry, rz, spi, spw, nsp,
+              eval_pair<R, MODE, SPECIAL, VIRIAL, NEAR>(s, i, ti, moli, xd.w, fpi, kk, core, rx, ry, rz, spi, spw, nsp,
                                                   (R)pice, acc);
           }
         }
@@ -1376,7 +1399,7 @@ __device__ void tile_stray(const SysDev& s, int si, int skip, int pice, bool rbl
   }
 }
 
-template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
+template <typename R, int MODE, bool SPECIAL, bool VIRIAL, bool NEAR = false>
 __global__ void __launch_bounds__(kCellWarps * 32, RBMD_TILE_MIN_BLOCKS)
 k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap, int* out_nc, int* out_ns,
             int* out_core, int* out_shell, float4 band) {
@@ -1437,6 +1460,7 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
   const float b0 = band.x, b1 = band.y, b2 = band.z, b3 = band.w;
   const float spice = (float)pice, fsa = (float)sqrt(s.alpha);
   const float falpha_l2 = (float)(s.alpha * 1.4426950408889634), fqq = (float)s.qqr2e;  // alpha log2(e)
+  const float* const ntab = s.near_tab;  // RBMD_NEAR_TABLE: the reference's G table
   const R far = R(1e30);
   const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
   if (lane < 9) s_red[wid][lane] = 0.0;  // per-warp reduction values, added in a fixed order
@@ -1514,7 +1538,7 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
         const int as = __ffs(strays) - 1;
         strays &= strays - 1;
         const int sk = __shfl_sync(FULL, skip, as);
-        tile_stray<R, MODE, SPECIAL, VIRIAL>(s, g0 + as, sk, pice, rbl, s_tab, cap, out_nc, out_ns, out_core,
+        tile_stray<R, MODE, SPECIAL, VIRIAL, NEAR>(s, g0 + as, sk, pice, rbl, s_tab, cap, out_nc, out_ns, out_core,
                                              out_shell, ff, acc);
         if (MODE != kLIST) {
           acc_warp_total<F32>(ff, acc, cmb);
@@ -1576,8 +1600,9 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
               }
               if (!skip_pair) {
                 const float d2 = tile_d2(rx, ry, rz);
-                const float f = tile_pair_f32<MODE>((h & 0x8000u) == 0u, d2, pa.w, pj.w, ai.x * ntypes + tj, w, spice,
-                                                    fsa, falpha_l2, fqq, s_tab);
+                const int tp = ai.x * ntypes + tj;
+                const float f = tile_pair_f32_lj<MODE, NEAR>((h & 0x8000u) == 0u, d2, pa.w, pj.w, s_tab[2 * tp],
+                                                             s_tab[2 * tp + 1], w, spice, fsa, falpha_l2, fqq, ntab);
                 fx = f * rx;
                 fy = f * ry;
                 fz = f * rz;
@@ -1613,7 +1638,7 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
               const R rx = (pj.x - s_shift[0][(e >> kJsBits) & 3]) - pix;
               const R ry = (pj.y - s_shift[1][(e >> (kJsBits + 2)) & 3]) - piy;
               const R rz = (pj.z - s_shift[2][(e >> (kJsBits + 4)) & 3]) - piz;
-              eval_pair<R, MODE, SPECIAL, VIRIAL>(s, i, ti, moli, qi, fpi, js, core, rx, ry, rz, spi, spw, nsp,
+              eval_pair<R, MODE, SPECIAL, VIRIAL, NEAR>(s, i, ti, moli, qi, fpi, js, core, rx, ry, rz, spi, spw, nsp,
                                                   (R)pice, acc);
             }
           }
@@ -1895,12 +1920,18 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
 // are evaluated by their own lane at the end of the row, so an atom's force is summed in traversal
 // order by one lane.  Atoms outside the box walk their own neighbourhood with the whole warp first
 // (tile_stray), as in the tile kernel.
-constexpr int kColWarps = 4;     // columns per block (kColWarpsHost on the host side)
+// The kernel is persistent: one grid of resident blocks, each warp taking the batch's columns one at
+// a time from a work counter, longest columns first, so no warp waits for another and the launch's
+// tail is short columns.  The RBL mean force is summed per column and the system's last column
+// adds the partials in column order: the result does not depend on which warp took which column.
+constexpr int kColWarps = 4;     // warps per block
 constexpr int kColStage = 192;   // staged candidates per warp
-constexpr int kColQ = 64;        // queued pairs per lane, and the most steps between evaluations
+constexpr int kColQ = 96;        // queued pairs per lane, and the most steps between evaluations
 constexpr float kColFar = 1e30f;
+// resident blocks per SM: 4 (128 registers per thread) ran the saline stream's column launch in
+// 34.2 ms against 36.1 ms at 5 (96 registers, twice the local-memory traffic of spills)
 #ifndef RBMD_COL_MIN_BLOCKS
-#define RBMD_COL_MIN_BLOCKS 5
+#define RBMD_COL_MIN_BLOCKS 4
 #endif
 
 // Rare paths of the column kernel, kept out of line so that their registers do not weigh on the
@@ -1916,14 +1947,14 @@ __device__ __noinline__ unsigned col_classify_fp64(const SysDev* __restrict__ sp
 
 // ... and one atom outside the box, walked by the whole warp (every lane calls it): its force is
 // written and its three force components returned in every lane.
-template <int MODE, bool SPECIAL>
+template <int MODE, bool SPECIAL, bool NEAR>
 __device__ __noinline__ double3 col_stray(const SysDev* __restrict__ sp, int si, int skip, const float* s_tab,
                                          int owner_lane, int i) {
   const SysDev& s = *sp;
   float ff[6];
   PairAcc acc;
   acc_zero(ff, acc);
-  tile_stray<float, MODE, SPECIAL, false>(s, si, skip, s.pice, true, s_tab, 0, nullptr, nullptr, nullptr, nullptr, ff,
+  tile_stray<float, MODE, SPECIAL, false, NEAR>(s, si, skip, s.pice, true, s_tab, 0, nullptr, nullptr, nullptr, nullptr, ff,
                                           acc);
   double cmb[6], r9[9];
   acc_warp_total<true>(ff, acc, cmb);
@@ -1932,10 +1963,12 @@ __device__ __noinline__ double3 col_stray(const SysDev* __restrict__ sp, int si,
   return make_double3(r9[0], r9[1], r9[2]);
 }
 
-template <int MODE, bool SPECIAL>
+template <int MODE, bool SPECIAL, bool NEAR>
 __global__ void __launch_bounds__(kColWarps * 32, RBMD_COL_MIN_BLOCKS)
-k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, float4 band) {
+k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwork, unsigned* __restrict__ ctr,
+           float4 band) {
   static_assert(MODE == kLJ_RBL || MODE == kCOUL_RBL, "column layout: FP32 RBL forces only");
+  static_assert(!NEAR || MODE == kCOUL_RBL, "the near-Coulomb table applies to the Coulomb mode");
   static_assert(kColStage < 0x8000, "queue entries hold a stage index below bit 15");
   __shared__ float4 s_c[kColWarps][kColStage];      // candidate position - image shift, charge
   __shared__ int s_id[kColWarps][kColStage];        // atom id (LJ/CUT: molecule) | type << kJsBits
@@ -1945,396 +1978,444 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, float4 b
   __shared__ int2 s_sp[kColWarps][32];    // first two special partners
   __shared__ float2 s_sw[kColWarps][32];  // and their weights
   __shared__ float4 s_f[kColWarps][32];   // force accumulated so far (x, y, z), charge in w
-  __shared__ float s_shift[3][3];         // per dimension: d (w - n) for w - n = -dims, 0, +dims
-  __shared__ float s_tab[2 * kMaxF32Types * kMaxF32Types];
-  __shared__ double s_red[kColWarps][3];
+  __shared__ float s_shift[kColWarps][3][3];  // per dimension: d (w - n) for w - n = -dims, 0, +dims
 
-  const int2 wk = work[blockIdx.x];
-  const SysDev& s = S[wk.x];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
-  const int dx = s.dims[0], dy = s.dims[1], dz = s.dims[2];
-  const int ntypes = s.ntypes;
-  if (threadIdx.x < 9) {
-    const int dim = threadIdx.x / 3, t = threadIdx.x % 3;
-    s_shift[dim][t] = (float)(s.d[dim] * (double)((t - 1) * s.dims[dim]));
-  }
-  for (int t = threadIdx.x; t < ntypes * ntypes && t < kMaxF32Types * kMaxF32Types; t += blockDim.x) {
-    const int a = t / ntypes, b = t % ntypes;
-    const double sg = (s.sig[a] + s.sig[b]) / 2;
-    s_tab[2 * t] = (float)(-24.0 * sqrt(s.eps[a] * s.eps[b]));
-    s_tab[2 * t + 1] = (float)(sg * sg * sg * sg * sg * sg);
-  }
-  __syncthreads();
-
   // FP32 band edges of the launch (the union of its systems' bands; a batch shares rc and rs)
   const float b0 = band.x, b1 = band.y, b2 = band.z, b3 = band.w;
-  const int pice = s.pice;
-  // stride picks: with pice dividing 32, a 32-bit pattern of the picked shell ranks rotated by one
-  // per shell; otherwise a countdown of the shells still to skip
-  const bool rot = (32 % pice) == 0;
-  unsigned pat0 = 0u;
-  for (int k = 0; k < 32; k += pice) pat0 |= 1u << k;
-  const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
-  const float fdx = (float)s.d[0], fdy = (float)s.d[1], fdz = (float)s.d[2];
-  const float frc2 = (float)s.rc2;
-  // trimming margins: 1e-3 of a cell (far above the FP32 rounding of the coordinates involved) plus
-  // the largest distance SHAKE moved an atom since the cell list was built; cells of atoms it wrapped
-  // across the box are never trimmed, and beyond kMaxMigrated of them nothing is
-  const float mdisp = __uint_as_float(s.st->shake_disp_bits);
-  const int mig_n = s.st->mig_n;
-  const float mgx = 1e-3f * fdx + mdisp, mgy = 1e-3f * fdy + mdisp, mgz = 1e-3f * fdz + mdisp;
-  double red0 = 0.0, red1 = 0.0, red2 = 0.0;  // this lane's atoms' forces (the RBL mean)
-
-  const int col = wk.y + wid;
-  if (col < dx * dy) {
-    const int hx = col / dy, hy = col % dy;
-    const int cbase = dz * (hy + dy * hx);
-    const int a0 = __ldg(&s.cell_start[cbase]), a1 = __ldg(&s.cell_start[cbase + dz]);
-    for (int g0 = a0; g0 < a1; g0 += 32) {
-      const int si = g0 + lane;
-      const bool valid = si < a1;
-      int i = 0, zl = 0;
-      float4 p4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      bool stray = false;
-      int c = 0;  // shells still to skip before the next pick
-      __syncwarp();  // the previous chunk's evaluation has read the per-lane records
-      if (valid) {
-        const int4 mi = __ldg(&s.smeta[si]);
-        i = mi.x;
-        p4 = __ldg(&s.sxf[si]);
-        zl = __ldg(&s.cell_of_atom[i]) - cbase;  // internal cell id iz + dz (iy + dy ix), this column
-        const double4 xd = ldg4(&s.sx[si]);
-        stray = (int)((xd.x - s.lo[0]) / s.d[0]) != hx || (int)((xd.y - s.lo[1]) / s.d[1]) != hy ||
-                (int)((xd.z - s.lo[2]) / s.d[2]) != zl;
-        if (s.rbl_mode == RBMD_RBL_PHILOX && pice > 1) {
-          uint32_t o[4];
-          philox4x32_10((uint32_t)i, 0u, (uint32_t)s.st->step, kTagRblOffset, s.seed_lo, s.seed_hi, o);
-          const int nm = (int)(o[0] % (uint32_t)pice);
-          c = nm == 0 ? 0 : pice - nm;
-        }
-        int nsp = 0, spb = 0, sp0 = -1, sp1 = -1;
-        float w0 = 1.0f, w1 = 1.0f;
-        if (SPECIAL) {  // special partners: the first two cached, the rest read from the CSR lists
-          spb = __ldg(&s.sp_off[i]);
-          nsp = __ldg(&s.sp_off[i + 1]) - spb;
-          if (nsp > 0) {
-            sp0 = __ldg(&s.sp_ids[spb]);
-            w0 = (float)__ldg(&s.sp_w[spb]);
-          }
-          if (nsp > 1) {
-            sp1 = __ldg(&s.sp_ids[spb + 1]);
-            w1 = (float)__ldg(&s.sp_w[spb + 1]);
-          }
-        }
-        s_ai[wid][lane] = make_int4(mi.y, mi.z, nsp, spb);
-        s_sp[wid][lane] = make_int2(sp0, sp1);
-        s_sw[wid][lane] = make_float2(w0, w1);
-      } else {  // a lane without an atom still runs the evaluation rounds (adding nothing): its
-                // record must hold valid indices (type 0, no special partners)
-        s_ai[wid][lane] = make_int4(0, -1, 0, 0);
-        s_sp[wid][lane] = make_int2(-1, -1);
-        s_sw[wid][lane] = make_float2(1.0f, 1.0f);
+  int cur = -1;  // slot of the system whose image shifts s_shift holds
+  for (;;) {
+    int wi = 0;
+    if (lane == 0) wi = (int)atomicAdd(&ctr[0], 1u);
+    wi = __shfl_sync(FULL, wi, 0);
+    if (wi >= nwork) break;
+    const int2 wk = __ldg(&work[wi]);
+    const SysDev& s = S[wk.x];
+    const int dx = s.dims[0], dy = s.dims[1], dz = s.dims[2];
+    const int ntypes = s.ntypes;
+    if (wk.x != cur) {
+      cur = wk.x;
+      __syncwarp();  // the previous column's reads are done
+      if (lane < 9) {
+        const int dim = lane / 3, t = lane % 3;
+        s_shift[wid][dim][t] = (float)(s.d[dim] * (double)((t - 1) * s.dims[dim]));
       }
-      s_f[wid][lane] = make_float4(0.0f, 0.0f, 0.0f, p4.w);
+      __syncwarp();
+    }
+    const int pice = s.pice;
+    // stride picks: with pice dividing 32, a 32-bit pattern of the picked shell ranks rotated by one
+    // per shell; otherwise a countdown of the shells still to skip
+    const bool rot = (32 % pice) == 0;
+    unsigned pat0 = 0u;
+    for (int k = 0; k < 32; k += pice) pat0 |= 1u << k;
+    const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
+    const float fdx = (float)s.d[0], fdy = (float)s.d[1], fdz = (float)s.d[2];
+    const float frc2 = (float)s.rc2;
+    // trimming margins: 1e-3 of a cell (far above the FP32 rounding of the coordinates involved) plus
+    // the largest distance SHAKE moved an atom since the cell list was built; cells of atoms it wrapped
+    // across the box are never trimmed, and beyond kMaxMigrated of them nothing is
+    const float mdisp = __uint_as_float(s.st->shake_disp_bits);
+    const int mig_n = s.st->mig_n;
+    const float mgx = 1e-3f * fdx + mdisp, mgy = 1e-3f * fdy + mdisp, mgz = 1e-3f * fdz + mdisp;
+    double red0 = 0.0, red1 = 0.0, red2 = 0.0;  // this lane's atoms' forces (the RBL mean)
 
-      // ---- atoms outside the box: the whole warp walks each one's own neighbourhood
-      unsigned strays = __ballot_sync(FULL, valid && stray);
-      while (strays) {
-        const int as = __ffs(strays) - 1;
-        strays &= strays - 1;
-        const int sk = __shfl_sync(FULL, c, as);
-        const double3 r = col_stray<MODE, SPECIAL>(&s, g0 + as, sk, s_tab, as, i);
-        if (lane == as) {
-          red0 += r.x;
-          red1 += r.y;
-          red2 += r.z;
+    const int col = wk.y;
+    {
+      const int hx = col / dy, hy = col % dy;
+      const int cbase = dz * (hy + dy * hx);
+      const int a0 = __ldg(&s.cell_start[cbase]), a1 = __ldg(&s.cell_start[cbase + dz]);
+      for (int g0 = a0; g0 < a1; g0 += 32) {
+        const int si = g0 + lane;
+        const bool valid = si < a1;
+        int i = 0, zl = 0;
+        float4 p4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        bool stray = false;
+        int c = 0;  // shells still to skip before the next pick
+        __syncwarp();  // the previous chunk's evaluation has read the per-lane records
+        if (valid) {
+          const int4 mi = __ldg(&s.smeta[si]);
+          i = mi.x;
+          p4 = __ldg(&s.sxf[si]);
+          zl = __ldg(&s.cell_of_atom[i]) - cbase;  // internal cell id iz + dz (iy + dy ix), this column
+          const double4 xd = ldg4(&s.sx[si]);
+          stray = (int)((xd.x - s.lo[0]) / s.d[0]) != hx || (int)((xd.y - s.lo[1]) / s.d[1]) != hy ||
+                  (int)((xd.z - s.lo[2]) / s.d[2]) != zl;
+          if (s.rbl_mode == RBMD_RBL_PHILOX && pice > 1) {
+            uint32_t o[4];
+            philox4x32_10((uint32_t)i, 0u, (uint32_t)s.st->step, kTagRblOffset, s.seed_lo, s.seed_hi, o);
+            const int nm = (int)(o[0] % (uint32_t)pice);
+            c = nm == 0 ? 0 : pice - nm;
+          }
+          int nsp = 0, spb = 0, sp0 = -1, sp1 = -1;
+          float w0 = 1.0f, w1 = 1.0f;
+          if (SPECIAL) {  // special partners: the first two cached, the rest read from the CSR lists
+            spb = __ldg(&s.sp_off[i]);
+            nsp = __ldg(&s.sp_off[i + 1]) - spb;
+            if (nsp > 0) {
+              sp0 = __ldg(&s.sp_ids[spb]);
+              w0 = (float)__ldg(&s.sp_w[spb]);
+            }
+            if (nsp > 1) {
+              sp1 = __ldg(&s.sp_ids[spb + 1]);
+              w1 = (float)__ldg(&s.sp_w[spb + 1]);
+            }
+          }
+          s_ai[wid][lane] = make_int4(mi.y, mi.z, nsp, spb);
+          s_sp[wid][lane] = make_int2(sp0, sp1);
+          s_sw[wid][lane] = make_float2(w0, w1);
+        } else {  // a lane without an atom still runs the evaluation rounds (adding nothing): its
+                  // record must hold valid indices (type 0, no special partners)
+          s_ai[wid][lane] = make_int4(0, -1, 0, 0);
+          s_sp[wid][lane] = make_int2(-1, -1);
+          s_sw[wid][lane] = make_float2(1.0f, 1.0f);
         }
-      }
+        s_f[wid][lane] = make_float4(0.0f, 0.0f, 0.0f, p4.w);
 
-      // ---- the chunk's own atoms, row by row
-      const bool act = valid && !stray;
-      const int zmin = __reduce_min_sync(FULL, act ? zl : 0x7fffffff);
-      const int zmax = __reduce_max_sync(FULL, act ? zl : -1);
-      const float pix = p4.x, piy = p4.y, piz = p4.z;
-      unsigned pat = rot ? ((pat0 << c) | (c ? pat0 >> (32 - c) : 0u)) : 0u;  // picks at ranks c, c + pice, ...
-      int qo = 0;  // queued pairs of this lane times 32 (the offset of its next slot)
-
-      // evaluates this lane's queued pairs (their candidates are in the stage)
-      auto flush = [&]() {
-        const int qn = qo >> 5;
-        const int rounds = __reduce_max_sync(FULL, qn);
-        if (rounds == 0) return;
-        const int4 ai = s_ai[wid][lane];
-        const int2 sp = s_sp[wid][lane];
-        const float2 sw = s_sw[wid][lane];
-        float4 fa = s_f[wid][lane];
-        const float spice = (float)pice, fsa = (float)sqrt(s.alpha);
-        const float falpha_l2 = (float)(s.alpha * 1.4426950408889634), fqq = (float)s.qqr2e;  // alpha log2(e)
-        for (int k = 0; k < rounds; ++k) {
-          if (k < qn) {
-            const unsigned h = s_q[wid][k * 32 + lane];
-            const int e = (int)(h & 0x7fffu);
-            const float4 pj = s_c[wid][e];
-            const float rx = pj.x - pix, ry = pj.y - piy, rz = pj.z - piz;
-            const float d2 = tile_d2(rx, ry, rz);
-            if (d2 > 0.0001f) {  // the pair of an atom with itself is queued as core and dropped here
-              const int idt = s_id[wid][e];
-              const int idj = idt & kJsMask, tj = idt >> kJsBits;
-              float w = 1.0f;
-              if (SPECIAL) {
-                if (ai.z <= 2) {
-                  w = (idj == sp.x) ? sw.x : w;
-                  w = (idj == sp.y) ? sw.y : w;
-                } else {
-                  for (int t2 = 0; t2 < ai.z; ++t2)
-                    if (__ldg(&s.sp_ids[ai.w + t2]) == idj) w = (float)__ldg(&s.sp_w[ai.w + t2]);
-                }
-              }
-              // LJ/CUT skips pairs of one molecule (its staged id is the molecule)
-              if (MODE != kLJ_RBL || idj != ai.y) {
-                const float f = tile_pair_f32<MODE>((h & 0x8000u) == 0u, d2, fa.w, pj.w, ai.x * ntypes + tj, w,
-                                                    spice, fsa, falpha_l2, fqq, s_tab);
-                fa.x += f * rx;
-                fa.y += f * ry;
-                fa.z += f * rz;
-              }
-            }
+        // ---- atoms outside the box: the whole warp walks each one's own neighbourhood
+        unsigned strays = __ballot_sync(FULL, valid && stray);
+        while (strays) {
+          const int as = __ffs(strays) - 1;
+          strays &= strays - 1;
+          const int sk = __shfl_sync(FULL, c, as);
+          const double3 r = col_stray<MODE, SPECIAL, NEAR>(&s, g0 + as, sk, (const float*)s.ljf, as, i);
+          if (lane == as) {
+            red0 += r.x;
+            red1 += r.y;
+            red2 += r.z;
           }
         }
-        s_f[wid][lane] = fa;
-        qo = 0;
-      };
 
-      if (zmax >= 0) {
-        const float xr = pix - (float)s.lo[0], yr = piy - (float)s.lo[1], zr = piz - (float)s.lo[2];
-        const int u0 = zmin - nc, u1 = zmax + nc;  // the chunk's z cells, unwrapped, -dz < u0, u1 < 2 dz
-        for (int r = 0; r < nrows; ++r) {
-          const int da = r / side - nc, db = r % side - nc;
-          const int n0 = hx + da, n1 = hy + db;  // unwrapped column of the row (nc < dims)
-          const int w0c = n0 < 0 ? n0 + dx : (n0 >= dx ? n0 - dx : n0);
-          const int w1c = n1 < 0 ? n1 + dy : (n1 >= dy ? n1 - dy : n1);
-          const int t0c = n0 < 0 ? 2 : (n0 >= dx ? 0 : 1), t1c = n1 < 0 ? 2 : (n1 >= dy ? 0 : 1);
-          const int base = dz * (w1c + dy * w0c);
-          // the row's union: unwrapped z cells u0 .. u1 in up to three segments (images -1, 0, +1:
-          // below the box, inside, above), segment k holding sorted indices sa_k .., union entries ob_k ..
-          int sa0 = 0, sa1, sa2 = 0, ob1, ob2, len = 0;
-          if (u0 < 0) {  // below the box: cells u0 + dz .. dz - 1
-            sa0 = __ldg(&s.cell_start[base + u0 + dz]);
-            len = __ldg(&s.cell_start[base + dz]) - sa0;
-          }
-          ob1 = len;
-          {  // inside: cells max(u0, 0) .. min(u1, dz - 1)
-            sa1 = __ldg(&s.cell_start[base + max(u0, 0)]);
-            len += __ldg(&s.cell_start[base + min(u1, dz - 1) + 1]) - sa1;
-          }
-          ob2 = len;
-          if (u1 >= dz) {  // above the box: cells 0 .. u1 - dz
-            sa2 = __ldg(&s.cell_start[base]);
-            len += __ldg(&s.cell_start[base + u1 - dz + 1]) - sa2;
-          }
-          // union entries before unwrapped cell u (u0 <= u <= u1 + 1)
-          auto ucount = [&](int u) -> int {
-            if (u > u1) return len;
-            if (u < 0) return __ldg(&s.cell_start[base + u + dz]) - sa0;
-            if (u < dz) return ob1 + __ldg(&s.cell_start[base + u]) - sa1;
-            return ob2 + __ldg(&s.cell_start[base + u - dz]) - sa2;
-          };
-          // this lane's window, trimmed to the z cells that can hold an atom within rc: the x / y
-          // gaps to the row's column (shrunk by the margin) leave a z half-width sqrt(rc^2 - g^2)
-          // (grown by it)
-          int wb = 0, wl = 0;
-          if (act) {
-            int zlo = zl + nc + 1, zhi = zl - nc - 1;  // empty
-            const float gx = fmaxf(0.0f, fmaxf((float)n0 * fdx - xr, xr - (float)(n0 + 1) * fdx) - mgx);
-            const float gy = fmaxf(0.0f, fmaxf((float)n1 * fdy - yr, yr - (float)(n1 + 1) * fdy) - mgy);
-            const float g2 = __fmaf_rn(gx, gx, gy * gy);
-            if (g2 < frc2) {
-              const float h = sqrtf(frc2 - g2) + mgz;
-              zlo = max((int)floorf((zr - h) / fdz), zl - nc);
-              zhi = min((int)floorf((zr + h) / fdz), zl + nc);
-            }
-            if (mig_n > kMaxMigrated) {
-              zlo = zl - nc;
-              zhi = zl + nc;
-            } else {
-              for (int m = 0; m < mig_n; ++m) {  // the stencil's visits of a recorded cell stay in
-                const int zm = __ldg(&s.st->mig_cell[m]) - base;
-                if (zm < 0 || zm >= dz) continue;  // not in this row's column
-                for (int u = zm - dz; u <= zm + dz; u += dz)
-                  if (u >= zl - nc && u <= zl + nc) {
-                    zlo = min(zlo, u);
-                    zhi = max(zhi, u);
+        // ---- the chunk's own atoms, row by row
+        const bool act = valid && !stray;
+        const int zmin = __reduce_min_sync(FULL, act ? zl : 0x7fffffff);
+        const int zmax = __reduce_max_sync(FULL, act ? zl : -1);
+        const float pix = p4.x, piy = p4.y, piz = p4.z;
+        unsigned pat = rot ? ((pat0 << c) | (c ? pat0 >> (32 - c) : 0u)) : 0u;  // picks at ranks c, c + pice, ...
+        int qo = 0;  // queued pairs of this lane times 32 (the offset of its next slot)
+
+        // evaluates this lane's queued pairs (their candidates are in the stage)
+        auto flush = [&]() {
+          const int qn = qo >> 5;
+          const int rounds = __reduce_max_sync(FULL, qn);
+          if (rounds == 0) return;
+          const int4 ai = s_ai[wid][lane];
+          const int2 sp = s_sp[wid][lane];
+          const float2 sw = s_sw[wid][lane];
+          float4 fa = s_f[wid][lane];
+          const float spice = (float)pice, fsa = (float)sqrt(s.alpha);
+          const float falpha_l2 = (float)(s.alpha * 1.4426950408889634), fqq = (float)s.qqr2e;  // alpha log2(e)
+          const float* const ntab = s.near_tab;  // RBMD_NEAR_TABLE: the reference's G table
+          for (int k = 0; k < rounds; ++k) {
+            if (k < qn) {
+              const unsigned h = s_q[wid][k * 32 + lane];
+              const int e = (int)(h & 0x7fffu);
+              const float4 pj = s_c[wid][e];
+              const float rx = pj.x - pix, ry = pj.y - piy, rz = pj.z - piz;
+              const float d2 = tile_d2(rx, ry, rz);
+              if (d2 > 0.0001f) {  // the pair of an atom with itself is queued as core and dropped here
+                const int idt = s_id[wid][e];
+                const int idj = idt & kJsMask, tj = idt >> kJsBits;
+                float w = 1.0f;
+                if (SPECIAL) {
+                  if (ai.z <= 2) {
+                    w = (idj == sp.x) ? sw.x : w;
+                    w = (idj == sp.y) ? sw.y : w;
+                  } else {
+                    for (int t2 = 0; t2 < ai.z; ++t2)
+                      if (__ldg(&s.sp_ids[ai.w + t2]) == idj) w = (float)__ldg(&s.sp_w[ai.w + t2]);
                   }
+                }
+                // LJ/CUT skips pairs of one molecule (its staged id is the molecule)
+                if (MODE != kLJ_RBL || idj != ai.y) {
+                  const float2 lj = __ldg(&s.ljf[ai.x * ntypes + tj]);
+                  const float f = tile_pair_f32_lj<MODE, NEAR>((h & 0x8000u) == 0u, d2, fa.w, pj.w, lj.x, lj.y, w,
+                                                               spice, fsa, falpha_l2, fqq, ntab);
+                  fa.x += f * rx;
+                  fa.y += f * ry;
+                  fa.z += f * rz;
+                }
               }
             }
-            if (zlo <= zhi) {
-              wb = ucount(zlo);
-              wl = ucount(zhi + 1) - wb;
-            }
           }
-          if (__reduce_max_sync(FULL, wl) == 0) continue;
-          // walks the windows of the lanes `in`; their starts lie within kColStage - 32 entries of
-          // each other, so every staged tile covers at least 32 steps
-          auto walk = [&](bool in) {
-            const int ml = __reduce_max_sync(FULL, in ? wl : 0);
-            if (ml == 0) return;
-            const int gbb = __reduce_min_sync(FULL, in ? wb : 0x7fffffff);
-            const int spr = __reduce_max_sync(FULL, in ? wb : gbb) - gbb;
-            const int T = kColStage - spr;  // steps per staged tile
-            const float shx = s_shift[0][t0c], shy = s_shift[1][t1c];
-            // lanes not walking step through the stage too, from a position that matches nothing
-            const float wpx = in ? pix : -kColFar, wpy = in ? piy : -kColFar, wpz = in ? piz : -kColFar;
-            const int i0 = in ? wb - gbb : 0;
-            for (int t0 = 0; t0 < ml; t0 += T) {
-              const int tl = min(T, ml - t0);
-              const int need = spr + tl;  // entries any lane reads in this tile (<= kColStage)
-              const int ub = gbb + t0;    // union index of stage entry 0
-              for (int e = lane; e < need; e += 32) {
-                const int g = ub + e;
-                float4 cv = make_float4(kColFar, kColFar, kColFar, 0.0f);
-                int idt = 0;
-                if (g < len) {
-                  const int zc = g < ob1 ? 2 : (g < ob2 ? 1 : 0);  // z shift code: below 2, inside 1, above 0
-                  const int js = g < ob1 ? sa0 + g : (g < ob2 ? sa1 + (g - ob1) : sa2 + (g - ob2));
-                  const float4 pj = __ldg(&s.sxf[js]);
-                  const int4 mj = __ldg(&s.smeta[js]);
-                  cv = make_float4(pj.x - shx, pj.y - shy, pj.z - s_shift[2][zc], pj.w);
-                  idt = (MODE == kLJ_RBL ? mj.z : mj.x) | (mj.y << kJsBits);
-                }
-                s_c[wid][e] = cv;
-                s_id[wid][e] = idt;
-              }
-              __syncwarp();
-              // the walk, with the pick rule fixed at compile time (ROT: rotating pattern)
-              auto steps = [&](auto rot_tag) {
-                constexpr bool ROT = decltype(rot_tag)::value;
-                for (int q0 = 0; q0 < tl; q0 += kColQ) {  // at most kColQ steps between evaluations
-                  const int te = min(kColQ, tl - q0);
-                  const int ib = i0 + q0;
-#pragma unroll 4
-                  for (int t = 0; t < te; ++t) {
-                    const int ix = ib + t;
-                    const float4 cj = s_c[wid][ix];
-                    const float ex = cj.x - wpx, ey = cj.y - wpy, ez = cj.z - wpz;
-                    const float dd = tile_d2(ex, ey, ez);
-                    // x alone: core (or the atom itself, dropped at evaluation); y alone: shell;
-                    // both: within a rounding band of rs^2 or rc^2, classified again in FP64
-                    bool core = ((dd <= b1) | (dd >= b2)) & (dd <= b3);
-                    bool shell = (dd >= b0) & (dd <= b3);
-                    if (core & shell) {
-                      // the candidate from its stage slot: union index, segment, sorted index, image
-                      const int g = ub + ix;
-                      const int zc = g < ob1 ? 2 : (g < ob2 ? 1 : 0);
-                      const int js = g < ob1 ? sa0 + g : (g < ob2 ? sa1 + (g - ob1) : sa2 + (g - ob2));
-                      const unsigned cs2 =
-                          col_classify_fp64(&s, si, js, (t0c - 1) * dx, (t1c - 1) * dy, (zc - 1) * dz);
-                      core = (cs2 & 1u) != 0u;
-                      shell = (cs2 & 2u) != 0u;
-                    }
-                    bool pick;
-                    if constexpr (ROT) {
-                      pick = shell & ((pat & 1u) != 0u);
-                      pat = shell ? __funnelshift_r(pat, pat, 1) : pat;
-                    } else {
-                      pick = shell & (c == 0);
-                      c = shell ? ((c == 0) ? pice - 1 : c - 1) : c;
-                    }
-                    // branch-free: the slot is always written and kept only when the pair is
-                    // selected (at most kColQ steps since the last evaluation)
-                    s_q[wid][qo + lane] = (unsigned short)(ix | (pick ? 0x8000 : 0));
-                    qo += (core | pick) ? 32 : 0;
-                  }
-                  flush();
-                }
-              };
-              if (rot) steps(std::true_type{});
-              else steps(std::false_type{});
-              __syncwarp();  // the stage is rewritten by the next tile or row
+          s_f[wid][lane] = fa;
+          qo = 0;
+        };
+
+        if (zmax >= 0) {
+          const float xr = pix - (float)s.lo[0], yr = piy - (float)s.lo[1], zr = piz - (float)s.lo[2];
+          const int u0 = zmin - nc, u1 = zmax + nc;  // the chunk's z cells, unwrapped, -dz < u0, u1 < 2 dz
+          for (int r = 0; r < nrows; ++r) {
+            const int da = r / side - nc, db = r % side - nc;
+            const int n0 = hx + da, n1 = hy + db;  // unwrapped column of the row (nc < dims)
+            const int w0c = n0 < 0 ? n0 + dx : (n0 >= dx ? n0 - dx : n0);
+            const int w1c = n1 < 0 ? n1 + dy : (n1 >= dy ? n1 - dy : n1);
+            const int t0c = n0 < 0 ? 2 : (n0 >= dx ? 0 : 1), t1c = n1 < 0 ? 2 : (n1 >= dy ? 0 : 1);
+            const int base = dz * (w1c + dy * w0c);
+            // the row's union: unwrapped z cells u0 .. u1 in up to three segments (images -1, 0, +1:
+            // below the box, inside, above), segment k holding sorted indices sa_k .., union entries ob_k ..
+            int sa0 = 0, sa1, sa2 = 0, ob1, ob2, len = 0;
+            if (u0 < 0) {  // below the box: cells u0 + dz .. dz - 1
+              sa0 = __ldg(&s.cell_start[base + u0 + dz]);
+              len = __ldg(&s.cell_start[base + dz]) - sa0;
             }
-          };
-          const int gmin = __reduce_min_sync(FULL, wl > 0 ? wb : 0x7fffffff);
-          const int gmax = __reduce_max_sync(FULL, wl > 0 ? wb : -1);
-          if (gmax - gmin <= kColStage - 32) {
-            walk(wl > 0);
-          } else {
-            // windows far apart (a sparse home column next to dense ones): the chunk's home cells
-            // take turns, and single lanes where one cell's trimmed windows are still too far apart
-            for (int zg = zmin; zg <= zmax; ++zg) {
-              const bool in = wl > 0 && zl == zg;
-              const int lo = __reduce_min_sync(FULL, in ? wb : 0x7fffffff);
-              const int hi = __reduce_max_sync(FULL, in ? wb : -1);
-              if (hi < 0) continue;
-              if (hi - lo <= kColStage - 32) {
-                walk(in);
+            ob1 = len;
+            {  // inside: cells max(u0, 0) .. min(u1, dz - 1)
+              sa1 = __ldg(&s.cell_start[base + max(u0, 0)]);
+              len += __ldg(&s.cell_start[base + min(u1, dz - 1) + 1]) - sa1;
+            }
+            ob2 = len;
+            if (u1 >= dz) {  // above the box: cells 0 .. u1 - dz
+              sa2 = __ldg(&s.cell_start[base]);
+              len += __ldg(&s.cell_start[base + u1 - dz + 1]) - sa2;
+            }
+            // union entries before unwrapped cell u (u0 <= u <= u1 + 1)
+            auto ucount = [&](int u) -> int {
+              if (u > u1) return len;
+              if (u < 0) return __ldg(&s.cell_start[base + u + dz]) - sa0;
+              if (u < dz) return ob1 + __ldg(&s.cell_start[base + u]) - sa1;
+              return ob2 + __ldg(&s.cell_start[base + u - dz]) - sa2;
+            };
+            // this lane's window, trimmed to the z cells that can hold an atom within rc: the x / y
+            // gaps to the row's column (shrunk by the margin) leave a z half-width sqrt(rc^2 - g^2)
+            // (grown by it)
+            int wb = 0, wl = 0;
+            if (act) {
+              int zlo = zl + nc + 1, zhi = zl - nc - 1;  // empty
+              const float gx = fmaxf(0.0f, fmaxf((float)n0 * fdx - xr, xr - (float)(n0 + 1) * fdx) - mgx);
+              const float gy = fmaxf(0.0f, fmaxf((float)n1 * fdy - yr, yr - (float)(n1 + 1) * fdy) - mgy);
+              const float g2 = __fmaf_rn(gx, gx, gy * gy);
+              if (g2 < frc2) {
+                const float h = sqrtf(frc2 - g2) + mgz;
+                zlo = max((int)floorf((zr - h) / fdz), zl - nc);
+                zhi = min((int)floorf((zr + h) / fdz), zl + nc);
+              }
+              if (mig_n > kMaxMigrated) {
+                zlo = zl - nc;
+                zhi = zl + nc;
               } else {
-                for (unsigned m = __ballot_sync(FULL, in); m; m &= m - 1) walk(in && lane == __ffs(m) - 1);
+                for (int m = 0; m < mig_n; ++m) {  // the stencil's visits of a recorded cell stay in
+                  const int zm = __ldg(&s.st->mig_cell[m]) - base;
+                  if (zm < 0 || zm >= dz) continue;  // not in this row's column
+                  for (int u = zm - dz; u <= zm + dz; u += dz)
+                    if (u >= zl - nc && u <= zl + nc) {
+                      zlo = min(zlo, u);
+                      zhi = max(zhi, u);
+                    }
+                }
+              }
+              if (zlo <= zhi) {
+                wb = ucount(zlo);
+                wl = ucount(zhi + 1) - wb;
+              }
+            }
+            if (__reduce_max_sync(FULL, wl) == 0) continue;
+            // walks the windows of the lanes `in`; their starts lie within kColStage - 32 entries of
+            // each other, so every staged tile covers at least 32 steps
+            auto walk = [&](bool in) {
+              const int ml = __reduce_max_sync(FULL, in ? wl : 0);
+              if (ml == 0) return;
+              const int gbb = __reduce_min_sync(FULL, in ? wb : 0x7fffffff);
+              const int spr = __reduce_max_sync(FULL, in ? wb : gbb) - gbb;
+              const int T = kColStage - spr;  // steps per staged tile
+              const float shx = s_shift[wid][0][t0c], shy = s_shift[wid][1][t1c];
+              // lanes not walking step through the stage too, from a position that matches nothing
+              const float wpx = in ? pix : -kColFar, wpy = in ? piy : -kColFar, wpz = in ? piz : -kColFar;
+              const int i0 = in ? wb - gbb : 0;
+              for (int t0 = 0; t0 < ml; t0 += T) {
+                const int tl = min(T, ml - t0);
+                const int need = spr + tl;  // entries any lane reads in this tile (<= kColStage)
+                const int ub = gbb + t0;    // union index of stage entry 0
+                for (int e = lane; e < need; e += 32) {
+                  const int g = ub + e;
+                  float4 cv = make_float4(kColFar, kColFar, kColFar, 0.0f);
+                  int idt = 0;
+                  if (g < len) {
+                    const int zc = g < ob1 ? 2 : (g < ob2 ? 1 : 0);  // z shift code: below 2, inside 1, above 0
+                    const int js = g < ob1 ? sa0 + g : (g < ob2 ? sa1 + (g - ob1) : sa2 + (g - ob2));
+                    const float4 pj = __ldg(&s.sxf[js]);
+                    const int4 mj = __ldg(&s.smeta[js]);
+                    cv = make_float4(pj.x - shx, pj.y - shy, pj.z - s_shift[wid][2][zc], pj.w);
+                    idt = (MODE == kLJ_RBL ? mj.z : mj.x) | (mj.y << kJsBits);
+                  }
+                  s_c[wid][e] = cv;
+                  s_id[wid][e] = idt;
+                }
+                __syncwarp();
+                // the walk, with the pick rule fixed at compile time (ROT: rotating pattern)
+                auto steps = [&](auto rot_tag) {
+                  constexpr bool ROT = decltype(rot_tag)::value;
+                  for (int q0 = 0; q0 < tl; q0 += kColQ) {  // at most kColQ steps between evaluations
+                    const int te = min(kColQ, tl - q0);
+                    const int ib = i0 + q0;
+  #pragma unroll 4
+                    for (int t = 0; t < te; ++t) {
+                      const int ix = ib + t;
+                      const float4 cj = s_c[wid][ix];
+                      const float ex = cj.x - wpx, ey = cj.y - wpy, ez = cj.z - wpz;
+                      const float dd = tile_d2(ex, ey, ez);
+                      // x alone: core (or the atom itself, dropped at evaluation); y alone: shell;
+                      // both: within a rounding band of rs^2 or rc^2, classified again in FP64
+                      bool core = ((dd <= b1) | (dd >= b2)) & (dd <= b3);
+                      bool shell = (dd >= b0) & (dd <= b3);
+                      if (core & shell) {
+                        // the candidate from its stage slot: union index, segment, sorted index, image
+                        const int g = ub + ix;
+                        const int zc = g < ob1 ? 2 : (g < ob2 ? 1 : 0);
+                        const int js = g < ob1 ? sa0 + g : (g < ob2 ? sa1 + (g - ob1) : sa2 + (g - ob2));
+                        const unsigned cs2 =
+                            col_classify_fp64(&s, si, js, (t0c - 1) * dx, (t1c - 1) * dy, (zc - 1) * dz);
+                        core = (cs2 & 1u) != 0u;
+                        shell = (cs2 & 2u) != 0u;
+                      }
+                      bool pick;
+                      if constexpr (ROT) {
+                        pick = shell & ((pat & 1u) != 0u);
+                        pat = shell ? __funnelshift_r(pat, pat, 1) : pat;
+                      } else {
+                        pick = shell & (c == 0);
+                        c = shell ? ((c == 0) ? pice - 1 : c - 1) : c;
+                      }
+                      // branch-free: the slot is always written and kept only when the pair is
+                      // selected (at most kColQ steps since the last evaluation)
+                      s_q[wid][qo + lane] = (unsigned short)(ix | (pick ? 0x8000 : 0));
+                      qo += (core | pick) ? 32 : 0;
+                    }
+                    flush();
+                  }
+                };
+                if (rot) steps(std::true_type{});
+                else steps(std::false_type{});
+                __syncwarp();  // the stage is rewritten by the next tile or row
+              }
+            };
+            const int gmin = __reduce_min_sync(FULL, wl > 0 ? wb : 0x7fffffff);
+            const int gmax = __reduce_max_sync(FULL, wl > 0 ? wb : -1);
+            if (gmax - gmin <= kColStage - 32) {
+              walk(wl > 0);
+            } else {
+              // windows far apart (a sparse home column next to dense ones): the chunk's home cells
+              // take turns, and single lanes where one cell's trimmed windows are still too far apart
+              for (int zg = zmin; zg <= zmax; ++zg) {
+                const bool in = wl > 0 && zl == zg;
+                const int lo = __reduce_min_sync(FULL, in ? wb : 0x7fffffff);
+                const int hi = __reduce_max_sync(FULL, in ? wb : -1);
+                if (hi < 0) continue;
+                if (hi - lo <= kColStage - 32) {
+                  walk(in);
+                } else {
+                  for (unsigned m = __ballot_sync(FULL, in); m; m &= m - 1) walk(in && lane == __ffs(m) - 1);
+                }
               }
             }
           }
         }
-      }
-      if (act) {
-        const float4 fa = s_f[wid][lane];  // Coulomb already scaled by qqr2e inside the pair factor
-        double r9[9];
-#pragma unroll
-        for (int q = 0; q < 9; ++q) r9[q] = 0.0;
-        r9[0] = (double)fa.x;
-        r9[1] = (double)fa.y;
-        r9[2] = (double)fa.z;
-        finish_atom<MODE>(s, i, r9);
-        red0 += r9[0];
-        red1 += r9[1];
-        red2 += r9[2];
+        if (act) {
+          const float4 fa = s_f[wid][lane];  // Coulomb already scaled by qqr2e inside the pair factor
+          double r9[9];
+  #pragma unroll
+          for (int q = 0; q < 9; ++q) r9[q] = 0.0;
+          r9[0] = (double)fa.x;
+          r9[1] = (double)fa.y;
+          r9[2] = (double)fa.z;
+          finish_atom<MODE>(s, i, r9);
+          red0 += r9[0];
+          red1 += r9[1];
+          red2 += r9[2];
+        }
       }
     }
-  }
-  // RBL mean force: warp totals, block partials, the last block of the system reduces them in order
-  red0 = warp_sum(red0);
-  red1 = warp_sum(red1);
-  red2 = warp_sum(red2);
-  if (lane == 0) {
-    s_red[wid][0] = red0;
-    s_red[wid][1] = red1;
-    s_red[wid][2] = red2;
-  }
-  __syncthreads();
-  const int blk = wk.y / kColWarps;
-  if (threadIdx.x < 9) {
-    double t = 0.0;
-    if (threadIdx.x < 3)
-      for (int w = 0; w < kColWarps; ++w) t += s_red[w][threadIdx.x];
-    s.vir_part[(size_t)blk * 9 + threadIdx.x] = t;
-  }
-  if (arrive_last(&s.st->counter[0], (unsigned)s.blocks_col)) {
-    if (threadIdx.x < 3) {
-      double t = 0.0;
-      for (int b = 0; b < s.blocks_col; ++b) t += __ldcg(&s.vir_part[(size_t)b * 9 + threadIdx.x]);
-      s.st->fmean[threadIdx.x] = t / s.n;
+    // RBL mean force: a partial per column; the column of the system that completes last adds them
+    // in column order (lane k takes columns k, k + 32, ..., then the fixed butterfly)
+    red0 = warp_sum(red0);
+    red1 = warp_sum(red1);
+    red2 = warp_sum(red2);
+    const int ncols = dx * dy;
+    int last = 0;
+    if (lane == 0) {
+      s.vir_part[(size_t)col * 3 + 0] = red0;
+      s.vir_part[(size_t)col * 3 + 1] = red1;
+      s.vir_part[(size_t)col * 3 + 2] = red2;
+      __threadfence();
+      last = atomicAdd(&s.st->counter[0], 1u) == (unsigned)(ncols - 1);
+      if (last) s.st->counter[0] = 0u;
     }
+    if (__shfl_sync(FULL, last, 0)) {
+      __threadfence();
+      double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+      for (int c = lane; c < ncols; c += 32) {
+        t0 += __ldcg(&s.vir_part[(size_t)c * 3 + 0]);
+        t1 += __ldcg(&s.vir_part[(size_t)c * 3 + 1]);
+        t2 += __ldcg(&s.vir_part[(size_t)c * 3 + 2]);
+      }
+      t0 = warp_sum(t0);
+      t1 = warp_sum(t1);
+      t2 = warp_sum(t2);
+      if (lane == 0) {
+        s.st->fmean[0] = t0 / s.n;
+        s.st->fmean[1] = t1 / s.n;
+        s.st->fmean[2] = t2 / s.n;
+      }
+    }
+  }  // next column
+  // the last warp of the launch to finish resets the work counters for the next launch
+  if (lane == 0 && atomicAdd(&ctr[1], 1u) == gridDim.x * (unsigned)kColWarps - 1u) {
+    ctr[0] = 0u;
+    ctr[1] = 0u;
   }
 }
 
-template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
-static void go(const Batch& b, cudaStream_t st) {
+// NEAR: RBL Coulomb with the reference's near-Coulomb table (a batch never mixes it with the
+// analytic form); a compile-time switch, so that the analytic kernels carry none of its code.
+template <typename R, int MODE, bool SPECIAL, bool VIRIAL, bool NEAR>
+static void go_near(const Batch& b, cudaStream_t st) {
+  static_assert(!NEAR || MODE == kCOUL_RBL, "the near-Coulomb table applies to the RBL Coulomb mode");
   constexpr bool kColumn = sizeof(R) == 4 && (MODE == kLJ_RBL || MODE == kCOUL_RBL) && !VIRIAL;
   const float4 band = make_float4(b.band[0], b.band[1], b.band[2], b.band[3]);
   if constexpr (kColumn) {
     if (b.dense == 2) {
-      k_pair_col<MODE, SPECIAL><<<b.pair.n, kColWarps * 32, 0, st>>>(b.sys, b.pair.d, band);
-      note_launch();
+      if (b.pair.n > 0) {
+        k_pair_col<MODE, SPECIAL, NEAR><<<b.col_grid, kColWarps * 32, 0, st>>>(b.sys, b.pair.d, b.pair.n, b.col_ctr,
+                                                                               band);
+        note_launch();
+      }
       return;
     }
   }
   if (b.dense)  // the column layout keeps the tile kernel's cell table for every other pass
-    k_pair_tile<R, MODE, SPECIAL, VIRIAL><<<b.dense == 2 ? b.pair_cells.n : b.pair.n, kCellWarps * 32, 0, st>>>(
+    k_pair_tile<R, MODE, SPECIAL, VIRIAL, NEAR><<<b.dense == 2 ? b.pair_cells.n : b.pair.n, kCellWarps * 32, 0, st>>>(
         b.sys, b.dense == 2 ? b.pair_cells.d : b.pair.d, 0, nullptr, nullptr, nullptr, nullptr, band);
   else if (b.lean)
-    k_pair2<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kPairWarps * 32, 0, st>>>(b.sys, b.pair.d);
+    k_pair2<R, MODE, SPECIAL, VIRIAL, NEAR><<<b.pair.n, kPairWarps * 32, 0, st>>>(b.sys, b.pair.d);
   else
-    k_pair<R, MODE, SPECIAL, VIRIAL><<<b.pair.n, kPairWarps * 32, 0, st>>>(b.sys, b.pair.d, 0, nullptr,
-                                                                          nullptr, nullptr, nullptr);
+    k_pair<R, MODE, SPECIAL, VIRIAL, NEAR><<<b.pair.n, kPairWarps * 32, 0, st>>>(b.sys, b.pair.d, 0, nullptr,
+                                                                                nullptr, nullptr, nullptr);
   note_launch();
+}
+
+template <typename R, int MODE, bool SPECIAL, bool VIRIAL>
+static void go(const Batch& b, cudaStream_t st) {
+  if constexpr (MODE == kCOUL_RBL) {
+    if (b.near) {
+      go_near<R, MODE, SPECIAL, VIRIAL, true>(b, st);
+      return;
+    }
+  }
+  go_near<R, MODE, SPECIAL, VIRIAL, false>(b, st);
+}
+
+int pair_col_grid(int ncols, int ff, int special, int near) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const void* fn = ff == RBMD_FF_LJ_CUT ? (const void*)k_pair_col<kLJ_RBL, false, false>
+                   : special ? (near ? (const void*)k_pair_col<kCOUL_RBL, true, true>
+                                     : (const void*)k_pair_col<kCOUL_RBL, true, false>)
+                             : (near ? (const void*)k_pair_col<kCOUL_RBL, false, true>
+                                     : (const void*)k_pair_col<kCOUL_RBL, false, false>);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kColWarps * 32, 0);
+  const int need = (ncols + kColWarps - 1) / kColWarps;
+  return std::max(1, std::min(need, std::max(1, sms) * std::max(1, per_sm)));
 }
 
 template <typename R, bool VIRIAL>

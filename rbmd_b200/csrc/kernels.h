@@ -20,12 +20,18 @@ struct Batch {
   int nsys = 0;
   Work atom, pair, cell, rho, tri, term, kred, draw;
   Work pair_cells;           // column layout: the tile kernel's cell table (energies, other modes)
+  // column layout: pair.d lists every column (slot, column index), most atoms per column first;
+  // the persistent column kernel's warps take them in that order from col_ctr[0] (col_ctr[1] counts
+  // the warps that are done; the last one resets both), col_grid blocks
+  unsigned* col_ctr = nullptr;
+  int col_grid = 0;
   // uniform switches of the batch (a batch never mixes them)
   int ff = 0, neigh = 0, coul = 0, prec = 0, temp_ctrl = 0, special = 0;
   int has_shake = 0, has_bonded = 0;
   int dense = 0;             // pair kernel: 0 = warp per atom, 1 = warp per home cell, 2 = warp per column
   int lean = 0;              // warp per atom with segment tables (dims >= 2 nc + 1 everywhere)
   int npt = 0;               // NPT barostat: 0 none, 1 Berendsen (end of step), 2 MTK (around the integrator)
+  int near = 0;              // RBL Coulomb with the reference's near-Coulomb table (RBMD_NEAR_TABLE)
   int max_P = 0;             // largest P (or Ewald nk) in the batch
   float band[4] = {0, 0, 0, 0};  // FP32 classification bands: union over the batch (same rc, rs)
   long long natoms = 0;      // atoms over all systems of the batch
@@ -42,6 +48,9 @@ void launch_rbe_sample(const Batch& b, cudaStream_t s);
 void launch_rho(const Batch& b, cudaStream_t s, int ewald);
 void launch_bonded(const Batch& b, cudaStream_t s, int virial);
 void launch_pair(const Batch& b, cudaStream_t s, int virial);
+// Blocks of the persistent column kernel for `ncols` columns: resident blocks per SM x SMs of the
+// current device, fewer when the columns do not fill them (4 warps per block, a column per warp).
+int pair_col_grid(int ncols, int ff, int special, int near);
 void launch_final(const Batch& b, cudaStream_t s, FinalMode mode, int virial);
 void launch_ke_thermostat(const Batch& b, cudaStream_t s);
 void launch_flush_vscale(const Batch& b, cudaStream_t s);
@@ -99,7 +108,6 @@ size_t snapshot_bytes(int n);
 void launch_snapshot_pack(const SysDev* sys, int slot, int n, void* out, cudaStream_t s);
 
 constexpr int kCellWarpsHost = 4;  // home cells per block of the tile pair kernel
-constexpr int kColWarpsHost = 4;   // columns of home cells per block of the column pair kernel
 constexpr double kTileMinPerCell = 3.0;  // mean atoms per cell from which the tile kernel is used
 
 double fma_peak_tflops(int fp64, cudaStream_t s);

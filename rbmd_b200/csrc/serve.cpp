@@ -65,6 +65,7 @@ void OwnedDesc::copy_from(const rbmd_system_desc& s) {
   cp(dk, s.dihedral_k, (size_t)std::max(0, s.n_dihedral_types));
   cp(dsg, s.dihedral_sign, (size_t)std::max(0, s.n_dihedral_types));
   cp(dm, s.dihedral_multiplicity, (size_t)std::max(0, s.n_dihedral_types));
+  cp(near, s.near_table_values, s.near_table_values ? (size_t)kNearKeys : 0);
   auto P = [](auto& v) { return v.empty() ? nullptr : v.data(); };
   d.position = P(pos);
   d.velocity = P(vel);
@@ -94,6 +95,7 @@ void OwnedDesc::copy_from(const rbmd_system_desc& s) {
   d.dihedral_k = P(dk);
   d.dihedral_sign = P(dsg);
   d.dihedral_multiplicity = P(dm);
+  d.near_table_values = P(near);
 }
 
 Server::Server(Context* c, const rbmd_serve_cfg& cfg) : ctx_(c), cfg_(cfg) {

@@ -19,6 +19,7 @@ struct OwnedDesc {
   rbmd_system_desc d{};
   std::vector<double> pos, vel, chg, mass, eps, sig, bk, br0, ak, at0, spw, frho, rhor, z2r, dk;
   std::vector<int32_t> type, mol, img, ba, bt, aa, at, spo, spi, da, dt, dsg, dm;
+  std::vector<float> near;
   void copy_from(const rbmd_system_desc& src);
 };
 

@@ -36,7 +36,6 @@ void Context::set_layout(System* s, int layout) {
   D.dense = dense;
   D.lean = lean;
   D.blocks_pair = dense ? tile_blocks(D) : (D.n + kPairWarps - 1) / kPairWarps;
-  D.blocks_col = column_blocks(D);
   upload_record(s);
 }
 

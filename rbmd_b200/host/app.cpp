@@ -91,6 +91,7 @@ rbmd_system_desc Para::desc() const {
   d.eam_rhor_spline = rhor_spline.empty() ? nullptr : rhor_spline.data();
   d.eam_z2r_spline = z2r_spline.empty() ? nullptr : z2r_spline.data();
   d.eam_per_type = eam_per_type;
+  d.near_table_values = near_table.empty() ? nullptr : near_table.data();
   if (!dihedral_type.empty()) {
     d.n_dihedrals = (int32_t)dihedral_type.size();
     d.n_dihedral_types = (int32_t)dihedral_k.size();
@@ -626,6 +627,31 @@ int Application::Run() {
   return 0;
 }
 
+// The reference's G tables for the RBL near Coulomb force (res/json_files/Gnear_table_leq2_2.txt and
+// Gnear_table_geq2_2.txt, compiled into model/ERFTable.h): rows "key r dr G dG", G stored at its
+// key.  A row whose key is not that of its distance is refused; keys the files do not list keep
+// the library's values.
+static std::vector<float> read_near_tables(const std::vector<std::string>& paths) {
+  std::vector<float> tab(RBMD_NEAR_TABLE_KEYS);
+  rbmd_near_table_default(tab.data());
+  for (const std::string& path : paths) {
+    std::ifstream in(path);
+    if (!in.is_open()) throw std::runtime_error("cannot open near-Coulomb table file " + path);
+    long key;
+    double r, dr, g, dg;
+    int rows = 0;
+    while (in >> key >> r >> dr >> g >> dg) {
+      if (key < 0 || key >= RBMD_NEAR_TABLE_KEYS || rbmd_near_table_key((float)r) != key)
+        throw std::runtime_error(path + ": the row of key " + std::to_string(key) + " holds r = " + std::to_string(r) +
+                                 ", whose key differs");
+      tab[key] = (float)g;
+      ++rows;
+    }
+    if (!in.eof() || rows == 0) throw std::runtime_error(path + ": expected rows of five numbers (key r dr G dG)");
+  }
+  return tab;
+}
+
 void MDApplication::ReadHyperParameters(const Json& hp) {
   rbmd_params& P = _para.params;
   if (const Json* ff = hp.find("force_field")) {
@@ -674,6 +700,26 @@ void MDApplication::ReadHyperParameters(const Json& hp) {
       const std::vector<double> v = cl->numbers("kmax");
       if (v.size() != 3) throw std::runtime_error("coulomb.kmax must hold three integers (one per dimension)");
       for (int k = 0; k < 3; ++k) P.kmax[k] = (int32_t)v[k];
+    }
+    // "near_table": true takes the reference's alpha = 0.1 lookup for the RBL near Coulomb force
+    // (its only form there, RunWorklet.cpp:1046-1047, 1171-1172) with the library's table; a list of
+    // the reference's two Gnear_table files takes their values (this key is not the reference's:
+    // its RBL runs always use the table, the library defaults to the analytic form)
+    if (const Json* nt = cl->find("near_table")) {
+      std::vector<std::string> files;
+      if (nt->is_bool()) {
+        P.near_table = nt->b ? RBMD_NEAR_TABLE : RBMD_NEAR_ANALYTIC;
+      } else if (nt->is_array()) {
+        P.near_table = RBMD_NEAR_TABLE;
+        for (const Json& e : nt->arr) {
+          if (!e.is_string()) throw std::runtime_error("coulomb.near_table: file names must be strings");
+          files.push_back(e.str);
+        }
+        if (files.empty()) throw std::runtime_error("coulomb.near_table: an empty list of files");
+      } else {
+        throw std::runtime_error("coulomb.near_table must be true, false or a list of Gnear_table files");
+      }
+      _para.near_table = files.empty() ? std::vector<float>() : read_near_tables(files);
     }
   }
   P.fix_shake = RBMD_SHAKE_NULL;
@@ -926,13 +972,13 @@ void MDApplication::DumpSystem(const std::string& path) const {
                "\"init_inbuild\": %d, \"neighbor_sample_num\": %d, \"cut_off\": %.17g, \"r_core\": %.17g, "
                "\"coulomb_sample_num\": %d, \"kmax\": [%d,%d,%d], \"alpha\": %.17g, \"temperature\": [%.17g,%.17g,%.17g], "
                "\"timestep\": %.17g, \"num_steps\": %lld, \"special_bonds\": [%.17g,%.17g,%.17g], \"seed\": %llu, "
-               "\"pressure\": [%.17g,%.17g,%.17g], \"bulk_modulus\": %.17g, \"press_ctrl\": %d},\n",
+               "\"pressure\": [%.17g,%.17g,%.17g], \"bulk_modulus\": %.17g, \"press_ctrl\": %d, \"near_table\": %d},\n",
                P.force_field, P.neighbor, P.coulomb, P.ensemble, P.temp_ctrl, P.units, P.precision, P.rbl_mode,
                P.fix_shake, P.init_inbuild, P.neighbor_sample_num, P.cut_off, P.r_core, P.coulomb_sample_num,
                P.kmax[0], P.kmax[1], P.kmax[2], P.alpha, P.temperature[0], P.temperature[1], P.temperature[2],
                P.timestep, (long long)P.num_steps, P.special_bonds[0], P.special_bonds[1], P.special_bonds[2],
                (unsigned long long)P.seed, P.pressure[0], P.pressure[1], P.pressure[2], P.bulk_modulus,
-               P.press_ctrl);
+               P.press_ctrl, P.near_table);
   darr("position", _para.position);
   darr("velocity", _para.velocity);
   darr("charge", _para.charge);
@@ -964,6 +1010,7 @@ void MDApplication::DumpSystem(const std::string& path) const {
   darr("eam_frho_spline", _para.frho_spline);
   darr("eam_rhor_spline", _para.rhor_spline);
   darr("eam_z2r_spline", _para.z2r_spline);
+  darr("near_table_values", std::vector<double>(_para.near_table.begin(), _para.near_table.end()));
   std::fprintf(f, "\"outputs\": {\"thermo_interval\": %d, \"trajectory_interval\": %d, \"checkpoint_interval\": %d, "
                "\"checkpoint_file\": \"%s\"", _thermo_interval, _traj_interval, _checkpoint_interval,
                _checkpoint_file.c_str());

@@ -49,6 +49,8 @@ struct Para {
   double eam_drho = 0, eam_dr = 0, eam_rhomax = 0, eam_cut = 0;
   int eam_per_type = 0;  // setfl: tables per atom type
   std::vector<double> frho_spline, rhor_spline, z2r_spline;
+  // coulomb.near_table given as the reference's two Gnear_table files: G by key (empty: the library's table)
+  std::vector<float> near_table;
 
   rbmd_system_desc desc() const;  // pointers into this object
 };

@@ -12,6 +12,7 @@ Workloads (sizes exactly as named):
   * eam_cu        fcc Cu 20^3 x 4 = 32000 atoms, Johnson-form EAM tabulated to 5.0 A
   * saline        SPC/E + 0.15 M NaCl (Joung-Cheatham 2008 SPC/E ion parameters)
 """
+import ctypes as C
 import math
 
 import numpy as np
@@ -54,6 +55,7 @@ class SystemData:
         self.dihedral_atoms = self.dihedral_type = self.dihedral_k = None
         self.dihedral_sign = self.dihedral_multiplicity = None
         self.eam = None
+        self.near_table_values = None  # float32 [2048] G by key (params.near_table), or None: the library's
         self.params = params if params is not None else A.default_params()
         self._desc = None
 
@@ -122,6 +124,11 @@ class SystemData:
             d.eam_rhor_spline = dp(e["rhor_spline"])
             d.eam_z2r_spline = dp(e["z2r_spline"])
             d.eam_per_type = int(e.get("per_type", 0))
+        if self.near_table_values is not None:
+            tab = np.ascontiguousarray(self.near_table_values, dtype=np.float32)
+            assert tab.shape == (2048,)
+            self.near_table_values = tab
+            d.near_table_values = tab.ctypes.data_as(C.POINTER(C.c_float))
         if self.dihedral_atoms is not None:
             d.n_dihedrals = len(self.dihedral_type)
             d.n_dihedral_types = len(self.dihedral_k)

@@ -152,6 +152,8 @@ def load(j):
         sd.special_offsets = _arr(j, "special_offsets", np.int32)
         sd.special_ids = _arr(j, "special_ids", np.int32)
         sd.special_weights = _arr(j, "special_weights", np.float64)
+    if j.get("near_table_values"):
+        sd.near_table_values = _arr(j, "near_table_values", np.float32)
     e = j.get("eam") or {}
     if e.get("nrho"):
         sd.eam = dict(nrho=e["nrho"], nr=e["nr"], drho=e["drho"], dr=e["dr"], rhomax=e["rhomax"], cut=e["cut"],

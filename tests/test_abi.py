@@ -43,7 +43,7 @@ def test_header_compiles_as_c():
 
 def test_host_only_entry_points():
     L = rbmd_b200.lib()
-    assert L.rbmd_abi_version() == A.RBMD_ABI_VERSION == 5
+    assert L.rbmd_abi_version() == A.RBMD_ABI_VERSION == 6
     p = A.Params()
     L.rbmd_params_default(C.byref(p))
     assert p.neighbor == A.NEIGH_RBL and p.precision == A.PREC_FP64 and p.fix_shake == A.SHAKE_NULL
