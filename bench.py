@@ -14,7 +14,7 @@ Lines printed by rank 0 (one JSON line):
   e2e    -- the same stream through the public serving API (rbmd_serve_submit with host arrays at
             the Poisson arrival times; results read back to host), wall clock, with p50/p99
             request latency.
-  plain_fp64 -- the same size distribution (every 32nd request) run FP64, one system per launch.
+  plain_fp64 -- the same size distribution (every 4th request) run FP64, one system per launch.
   --impl reference -- the CPU restatement of the reference's algorithm (the reference itself needs
             VTK-m, which this environment lacks) on a bounded sample of the same workload.
 """
@@ -217,16 +217,16 @@ def measure_plain(systems, args, device):
     """FP64, one system per launch, eager: the plain path the batched mixed path is compared to."""
     import rbmd_b200
     from rbmd_b200 import _abi as A
-    sample = systems[::32]
+    sample = systems[::4]
     ctx = rbmd_b200.Context(device=device, batched=False, graphs=False)
     tot_ms, tot_as = 0.0, 0
-    steps = 5
+    steps = 20
     for sd in sample:
         s2 = sd.copy()
         s2.params.precision = A.PREC_FP64
         sid = ctx.add_system(s2)
         ctx.init(sid)
-        ctx.step(sid, 1)
+        ctx.step(sid, 2)
         ms = ctx.step_timed(sid, steps)
         tot_ms += ms
         tot_as += s2.n * steps

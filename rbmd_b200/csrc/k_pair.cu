@@ -1189,6 +1189,30 @@ __device__ inline unsigned pick_shells(unsigned sm, int pice, int& r) {
   return pk;
 }
 
+// The same picks for pice = 2^lg without a loop: bit k of each shell's rank (the shells before it
+// in the mask) is the exclusive prefix parity of the shells whose rank has bits 0..k-1 all set, so
+// the shells of rank r = c (mod pice) are an AND of lg such parities; c becomes (c - shells) mod
+// pice.  Every lane runs the same lg steps.
+__device__ __forceinline__ unsigned prefix_parity_excl(unsigned m) {
+  unsigned x = m << 1;
+  x ^= x << 1;
+  x ^= x << 2;
+  x ^= x << 4;
+  x ^= x << 8;
+  x ^= x << 16;
+  return x;
+}
+__device__ __forceinline__ unsigned pick_shells_pow2(unsigned sm, int lg, int& c) {
+  unsigned pm = sm, carry = sm;
+  for (int k = 0; k < lg; ++k) {
+    const unsigned bit_k = prefix_parity_excl(carry);
+    pm &= ((c >> k) & 1) ? bit_k : ~bit_k;
+    carry &= bit_k;
+  }
+  c = (c - __popc(sm)) & ((1 << lg) - 1);
+  return pm;
+}
+
 // Per-atom result of a pair pass: forces written (or the EAM embedding derivative); r9 leaves as
 // the atom's nine reduction values.
 template <int MODE>
@@ -1910,14 +1934,16 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
 // candidate windows -- the row's z cells from the atom's own cell - nc to + nc -- are overlapping
 // sub-ranges of one contiguous union, which the warp stages once in shared memory, shifted into
 // the home frame.  Each lane then walks its own window in lock step with the others (step t: every
-// lane reads entry t of its own window): one shared load, the FP32 squared distance, the band
-// compares of the exact classification, a shell counter and a predicated queue append -- no
-// ballots and no cross-lane traffic.  A lane's window is trimmed to the z cells that can hold an
-// atom within rc of it (an x/y gap to the row's column of g leaves a z half-width sqrt(rc^2 - g^2));
+// lane reads entry t of its own window), in blocks of 32 steps: a step is one shared load, the FP32
+// squared distance and the band compares of the exact classification, setting bit t of a core and
+// a shell mask -- no ballots, no cross-lane traffic and no bookkeeping.  Once per block the masks
+// are cut to the lane's own window (the lanes step together), the banded candidates (both bits)
+// are classified again in FP64, and the RBL picks -- every pice-th shell in traversal order -- are
+// taken from the shell mask.  A lane's window is trimmed to the z cells that can hold an atom
+// within rc of it (an x/y gap to the row's column of g leaves a z half-width sqrt(rc^2 - g^2));
 // cells dropped that way hold no core or shell atom, so the shell ranks, and the RBL picks, stay
-// exactly those of the full traversal.  Reading past the end of its window (the lanes step
-// together) a lane meets only cells beyond rc, which classify as out.  The selected pairs of a row
-// are evaluated by their own lane at the end of the row, so an atom's force is summed in traversal
+// exactly those of the full traversal.  The selected candidates of up to kColQ steps are evaluated
+// by their own lane from the masks, in traversal order, so an atom's force is summed in a fixed
 // order by one lane.  Atoms outside the box walk their own neighbourhood with the whole warp first
 // (tile_stray), as in the tile kernel.
 // The kernel is persistent: one grid of resident blocks, each warp taking the batch's columns one at
@@ -1926,7 +1952,8 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
 // adds the partials in column order: the result does not depend on which warp took which column.
 constexpr int kColWarps = 4;     // warps per block
 constexpr int kColStage = 192;   // staged candidates per warp
-constexpr int kColQ = 96;        // queued pairs per lane, and the most steps between evaluations
+constexpr int kColQ = 96;        // the most steps between evaluations
+constexpr int kColQW = kColQ / 32;  // 32-step blocks between evaluations
 constexpr float kColFar = 1e30f;
 // resident blocks per SM: 4 (128 registers per thread) ran the saline stream's column launch in
 // 34.2 ms against 36.1 ms at 5 (96 registers, twice the local-memory traffic of spills)
@@ -1969,10 +1996,13 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
            float4 band) {
   static_assert(MODE == kLJ_RBL || MODE == kCOUL_RBL, "column layout: FP32 RBL forces only");
   static_assert(!NEAR || MODE == kCOUL_RBL, "the near-Coulomb table applies to the Coulomb mode");
-  static_assert(kColStage < 0x8000, "queue entries hold a stage index below bit 15");
+  static_assert(kColQ % 32 == 0 && kColStage % 32 == 0, "the walk runs in blocks of 32 steps");
   __shared__ float4 s_c[kColWarps][kColStage];      // candidate position - image shift, charge
   __shared__ int s_id[kColWarps][kColStage];        // atom id (LJ/CUT: molecule) | type << kJsBits
-  __shared__ unsigned short s_q[kColWarps][kColQ * 32];  // slot k of lane l at k * 32 + l: stage entry | shell << 15
+  // per lane and 32-step block since the last evaluation, bit t for step t: the selected candidates
+  // (core, or a picked shell) and the picked shells among them
+  __shared__ unsigned s_sel[kColWarps][kColQW][32];
+  __shared__ unsigned s_pk[kColWarps][kColQW][32];
   // per lane (home atom): what the evaluation needs, kept out of registers during the walk
   __shared__ int4 s_ai[kColWarps][32];    // type, molecule, special partners, first special slot
   __shared__ int2 s_sp[kColWarps][32];    // first two special partners
@@ -2004,11 +2034,7 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
       __syncwarp();
     }
     const int pice = s.pice;
-    // stride picks: with pice dividing 32, a 32-bit pattern of the picked shell ranks rotated by one
-    // per shell; otherwise a countdown of the shells still to skip
-    const bool rot = (32 % pice) == 0;
-    unsigned pat0 = 0u;
-    for (int k = 0; k < 32; k += pice) pat0 |= 1u << k;
+    const int lgp = (pice & (pice - 1)) == 0 ? __ffs(pice) - 1 : -1;  // log2 pice, -1 if not a power of 2
     const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
     const float fdx = (float)s.d[0], fdy = (float)s.d[1], fdz = (float)s.d[2];
     const float frc2 = (float)s.rc2;
@@ -2091,12 +2117,11 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
         const int zmin = __reduce_min_sync(FULL, act ? zl : 0x7fffffff);
         const int zmax = __reduce_max_sync(FULL, act ? zl : -1);
         const float pix = p4.x, piy = p4.y, piz = p4.z;
-        unsigned pat = rot ? ((pat0 << c) | (c ? pat0 >> (32 - c) : 0u)) : 0u;  // picks at ranks c, c + pice, ...
-        int qo = 0;  // queued pairs of this lane times 32 (the offset of its next slot)
-
-        // evaluates this lane's queued pairs (their candidates are in the stage)
-        auto flush = [&]() {
-          const int qn = qo >> 5;
+        // evaluates this lane's selected candidates of the last nblk blocks, whose first step read
+        // stage entry `base` (the candidates are still in the stage)
+        auto flush = [&](int nblk, int base) {
+          int qn = 0;
+          for (int bk = 0; bk < nblk; ++bk) qn += __popc(s_sel[wid][bk][lane]);
           const int rounds = __reduce_max_sync(FULL, qn);
           if (rounds == 0) return;
           const int4 ai = s_ai[wid][lane];
@@ -2106,14 +2131,23 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
           const float spice = (float)pice, fsa = (float)sqrt(s.alpha);
           const float falpha_l2 = (float)(s.alpha * 1.4426950408889634), fqq = (float)s.qqr2e;  // alpha log2(e)
           const float* const ntab = s.near_tab;  // RBMD_NEAR_TABLE: the reference's G table
+          int wc = 0;  // block of the next selected candidate, its remaining bits and its picks
+          unsigned mc = s_sel[wid][0][lane], pc = s_pk[wid][0][lane];
           for (int k = 0; k < rounds; ++k) {
             if (k < qn) {
-              const unsigned h = s_q[wid][k * 32 + lane];
-              const int e = (int)(h & 0x7fffu);
+              while (mc == 0u) {
+                ++wc;
+                mc = s_sel[wid][wc][lane];
+                pc = s_pk[wid][wc][lane];
+              }
+              const int b = __ffs(mc) - 1;
+              mc &= mc - 1u;
+              const int e = base + 32 * wc + b;
+              const bool core = ((pc >> b) & 1u) == 0u;
               const float4 pj = s_c[wid][e];
               const float rx = pj.x - pix, ry = pj.y - piy, rz = pj.z - piz;
               const float d2 = tile_d2(rx, ry, rz);
-              if (d2 > 0.0001f) {  // the pair of an atom with itself is queued as core and dropped here
+              if (d2 > 0.0001f) {  // the pair of an atom with itself is selected as core and dropped here
                 const int idt = s_id[wid][e];
                 const int idj = idt & kJsMask, tj = idt >> kJsBits;
                 float w = 1.0f;
@@ -2129,8 +2163,8 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
                 // LJ/CUT skips pairs of one molecule (its staged id is the molecule)
                 if (MODE != kLJ_RBL || idj != ai.y) {
                   const float2 lj = __ldg(&s.ljf[ai.x * ntypes + tj]);
-                  const float f = tile_pair_f32_lj<MODE, NEAR>((h & 0x8000u) == 0u, d2, fa.w, pj.w, lj.x, lj.y, w,
-                                                               spice, fsa, falpha_l2, fqq, ntab);
+                  const float f = tile_pair_f32_lj<MODE, NEAR>(core, d2, fa.w, pj.w, lj.x, lj.y, w, spice, fsa,
+                                                               falpha_l2, fqq, ntab);
                   fa.x += f * rx;
                   fa.y += f * ry;
                   fa.z += f * rz;
@@ -2139,7 +2173,6 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
             }
           }
           s_f[wid][lane] = fa;
-          qo = 0;
         };
 
         if (zmax >= 0) {
@@ -2211,26 +2244,29 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
             }
             if (__reduce_max_sync(FULL, wl) == 0) continue;
             // walks the windows of the lanes `in`; their starts lie within kColStage - 32 entries of
-            // each other, so every staged tile covers at least 32 steps
+            // each other, so every staged tile covers at least one block of 32 steps
             auto walk = [&](bool in) {
               const int ml = __reduce_max_sync(FULL, in ? wl : 0);
               if (ml == 0) return;
               const int gbb = __reduce_min_sync(FULL, in ? wb : 0x7fffffff);
               const int spr = __reduce_max_sync(FULL, in ? wb : gbb) - gbb;
-              const int T = kColStage - spr;  // steps per staged tile
+              const int T = (kColStage - spr) & ~31;  // steps per staged tile, whole blocks
               const float shx = s_shift[wid][0][t0c], shy = s_shift[wid][1][t1c];
               // lanes not walking step through the stage too, from a position that matches nothing
               const float wpx = in ? pix : -kColFar, wpy = in ? piy : -kColFar, wpz = in ? piz : -kColFar;
               const int i0 = in ? wb - gbb : 0;
+              const int wlen = in ? wl : 0;  // steps of this lane's own window
               for (int t0 = 0; t0 < ml; t0 += T) {
                 const int tl = min(T, ml - t0);
-                const int need = spr + tl;  // entries any lane reads in this tile (<= kColStage)
-                const int ub = gbb + t0;    // union index of stage entry 0
-                for (int e = lane; e < need; e += 32) {
+                const int nb = (tl + 31) >> 5;  // blocks of this tile
+                const int need = spr + tl;      // entries of the tile's windows; up to spr + 32 nb (<=
+                                                // kColStage) are read, the rest staged as far away
+                const int ub = gbb + t0;        // union index of stage entry 0
+                for (int e = lane; e < spr + 32 * nb; e += 32) {
                   const int g = ub + e;
                   float4 cv = make_float4(kColFar, kColFar, kColFar, 0.0f);
                   int idt = 0;
-                  if (g < len) {
+                  if (g < len && e < need) {
                     const int zc = g < ob1 ? 2 : (g < ob2 ? 1 : 0);  // z shift code: below 2, inside 1, above 0
                     const int js = g < ob1 ? sa0 + g : (g < ob2 ? sa1 + (g - ob1) : sa2 + (g - ob2));
                     const float4 pj = __ldg(&s.sxf[js]);
@@ -2242,50 +2278,56 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
                   s_id[wid][e] = idt;
                 }
                 __syncwarp();
-                // the walk, with the pick rule fixed at compile time (ROT: rotating pattern)
-                auto steps = [&](auto rot_tag) {
-                  constexpr bool ROT = decltype(rot_tag)::value;
-                  for (int q0 = 0; q0 < tl; q0 += kColQ) {  // at most kColQ steps between evaluations
-                    const int te = min(kColQ, tl - q0);
-                    const int ib = i0 + q0;
-  #pragma unroll 4
-                    for (int t = 0; t < te; ++t) {
-                      const int ix = ib + t;
-                      const float4 cj = s_c[wid][ix];
+                // the walk: blocks of 32 steps, each step a compare into two bit masks, the picks
+                // and the FP64 re-classification once per block
+                for (int q0 = 0; q0 < nb; q0 += kColQW) {  // at most kColQ steps between evaluations
+                  const int nblk = min(kColQW, nb - q0);
+                  for (int bk = 0; bk < nblk; ++bk) {
+                    const int ib = i0 + 32 * (q0 + bk);  // this lane's stage entry at the block's first step
+                    unsigned cm = 0u, sm = 0u;
+                    auto step = [&](int st) {
+                      const float4 cj = s_c[wid][ib + st];
                       const float ex = cj.x - wpx, ey = cj.y - wpy, ez = cj.z - wpz;
                       const float dd = tile_d2(ex, ey, ez);
                       // x alone: core (or the atom itself, dropped at evaluation); y alone: shell;
                       // both: within a rounding band of rs^2 or rc^2, classified again in FP64
-                      bool core = ((dd <= b1) | (dd >= b2)) & (dd <= b3);
-                      bool shell = (dd >= b0) & (dd <= b3);
-                      if (core & shell) {
-                        // the candidate from its stage slot: union index, segment, sorted index, image
-                        const int g = ub + ix;
-                        const int zc = g < ob1 ? 2 : (g < ob2 ? 1 : 0);
-                        const int js = g < ob1 ? sa0 + g : (g < ob2 ? sa1 + (g - ob1) : sa2 + (g - ob2));
-                        const unsigned cs2 =
-                            col_classify_fp64(&s, si, js, (t0c - 1) * dx, (t1c - 1) * dy, (zc - 1) * dz);
-                        core = (cs2 & 1u) != 0u;
-                        shell = (cs2 & 2u) != 0u;
-                      }
-                      bool pick;
-                      if constexpr (ROT) {
-                        pick = shell & ((pat & 1u) != 0u);
-                        pat = shell ? __funnelshift_r(pat, pat, 1) : pat;
-                      } else {
-                        pick = shell & (c == 0);
-                        c = shell ? ((c == 0) ? pice - 1 : c - 1) : c;
-                      }
-                      // branch-free: the slot is always written and kept only when the pair is
-                      // selected (at most kColQ steps since the last evaluation)
-                      s_q[wid][qo + lane] = (unsigned short)(ix | (pick ? 0x8000 : 0));
-                      qo += (core | pick) ? 32 : 0;
+                      const bool x = ((dd <= b1) | (dd >= b2)) & (dd <= b3);
+                      const bool y = (dd >= b0) & (dd <= b3);
+                      cm |= x ? (1u << st) : 0u;
+                      sm |= y ? (1u << st) : 0u;
+                    };
+                    const int rem = tl - 32 * (q0 + bk);  // steps of the block: 32 but in the tile's last
+                    if (rem >= 32) {
+#pragma unroll
+                      for (int st = 0; st < 32; ++st) step(st);
+                    } else {
+#pragma unroll 4
+                      for (int st = 0; st < rem; ++st) step(st);
                     }
-                    flush();
+                    // only this lane's own window counts: past its end (the lanes step together) lie
+                    // cells beyond rc or outside the stencil
+                    const int left = wlen - (t0 + 32 * (q0 + bk));
+                    const unsigned vm = left >= 32 ? 0xffffffffu : (left > 0 ? (1u << left) - 1u : 0u);
+                    cm &= vm;
+                    sm &= vm;
+                    for (unsigned bm = cm & sm; bm != 0u; bm &= bm - 1u) {
+                      // a banded candidate from its stage slot: union index, segment, sorted index, image
+                      const int st = __ffs(bm) - 1;
+                      const int g = ub + ib + st;
+                      const int zc = g < ob1 ? 2 : (g < ob2 ? 1 : 0);
+                      const int js = g < ob1 ? sa0 + g : (g < ob2 ? sa1 + (g - ob1) : sa2 + (g - ob2));
+                      const unsigned cs2 = col_classify_fp64(&s, si, js, (t0c - 1) * dx, (t1c - 1) * dy, (zc - 1) * dz);
+                      const unsigned bit = 1u << st;
+                      cm = (cs2 & 1u) ? (cm | bit) : (cm & ~bit);
+                      sm = (cs2 & 2u) ? (sm | bit) : (sm & ~bit);
+                    }
+                    // every pice-th shell in traversal order, c shells still to skip before the next
+                    const unsigned pm = lgp >= 0 ? pick_shells_pow2(sm, lgp, c) : pick_shells(sm, pice, c);
+                    s_sel[wid][bk][lane] = cm | pm;
+                    s_pk[wid][bk][lane] = pm;
                   }
-                };
-                if (rot) steps(std::true_type{});
-                else steps(std::false_type{});
+                  flush(nblk, i0 + 32 * q0);
+                }
                 __syncwarp();  // the stage is rewritten by the next tile or row
               }
             };
