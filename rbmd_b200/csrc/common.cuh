@@ -103,6 +103,9 @@ struct SysDev {
   double lo[3], hi[3], L[3], d[3];
   double rc, rs, rc2, rs2, alpha, volume, S;
   double qqr2e, fmt2v, mvv2e, kB, boltz, nktv2p;
+  // FP32 constants of the mixed-precision pair evaluation: sqrt(alpha), alpha log2(e) (so that
+  // exp(-alpha d2) = 2^(-falpha_l2 d2)) and qqr2e, each rounded once from FP64
+  float fsa, falpha_l2, fqq, fpad;
   double dt, t_start, t_stop, t_damp;
   int64_t num_steps;
   double eam_dr, eam_drho, eam_rhomax, eam_cut;

@@ -414,6 +414,9 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   D.volume = s->dv.volume;
   D.S = s->dv.S_rbe;
   D.qqr2e = u.qqr2e;
+  D.fsa = (float)std::sqrt(p.alpha);
+  D.falpha_l2 = (float)(p.alpha * 1.4426950408889634);
+  D.fqq = (float)u.qqr2e;
   D.fmt2v = u.fmt2v;
   D.mvv2e = u.mvv2e;
   D.kB = u.kB;
@@ -442,17 +445,20 @@ int Context::add_system(const rbmd_system_desc& d, const rbmd_params& p, int32_t
   // atom) takes the tile kernel's systems for the RBL forces.  RBMD_PAIR_LAYOUT overrides the
   // choice for tuning and tests: "atom" (general), "lean", "cell" (tile), "column".
   const bool stencil_ok = D.dims[0] >= 2 * D.nc + 1 && D.dims[1] >= 2 * D.nc + 1 && D.dims[2] >= 2 * D.nc + 1;
-  // The lean and tile kernels also walk stencils that repeat cells, as long as every dimension
-  // holds more than nc cells (one periodic image per offset; the tile kernel also needs edges of
-  // 2 rc).  There the lean kernel is the default: on the saline stream's 1000-1500-atom systems
-  // (4 cells per dimension) it took 0.85 ms per step, the general kernel 1.40 ms and the tile
-  // kernel 1.76 ms, so only the autotuner or RBMD_PAIR_LAYOUT=cell selects the tile kernel.
+  // The lean, tile and column kernels also walk stencils that repeat cells, as long as every
+  // dimension holds more than nc cells (one periodic image per offset; the tile and column kernels
+  // also need edges of 2 rc).  On the saline stream's 1000-1500-atom systems (4 cells per
+  // dimension) the lean kernel took 0.85 ms per step, the general kernel 1.40 ms and the tile
+  // kernel 1.76 ms; the column kernel takes them within the launch of the large systems for
+  // about 0.24 ms more, so it is their default for mixed-precision RBL forces, the lean kernel
+  // otherwise, and only the autotuner or RBMD_PAIR_LAYOUT=cell selects the tile kernel there.
   const bool tile_ok = tile_layout_ok(D);
   D.lean = lean_layout_ok(D) ? 1 : 0;
-  D.dense = (stencil_ok && p.precision == RBMD_PREC_MIXED && n < (1 << 25) &&
-             (double)n >= kTileMinPerCell * (double)D.ncell) ? 1 : 0;
-  // dense mixed-precision RBL forces: the column kernel in place of the tile kernel
-  if (D.dense == 1 && column_layout_ok(D)) D.dense = 2;
+  const bool dense_ok = p.precision == RBMD_PREC_MIXED && n < (1 << 25) &&
+                        (double)n >= kTileMinPerCell * (double)D.ncell;
+  D.dense = (stencil_ok && dense_ok) ? 1 : 0;
+  // dense mixed-precision RBL forces: the column kernel in place of the tile or lean kernel
+  if (dense_ok && column_layout_ok(D)) D.dense = 2;
   const char* lay = std::getenv("RBMD_PAIR_LAYOUT");
   s->tuned = lay != nullptr && lay[0] != '\0' && std::strcmp(lay, "auto") != 0;  // a forced layout is not retuned
   if (lay) {

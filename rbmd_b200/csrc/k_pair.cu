@@ -1482,8 +1482,7 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
   // FP32 band edges: one set for the whole launch, the union of its systems' bands (a batch's
   // systems share rc and rs)
   const float b0 = band.x, b1 = band.y, b2 = band.z, b3 = band.w;
-  const float spice = (float)pice, fsa = (float)sqrt(s.alpha);
-  const float falpha_l2 = (float)(s.alpha * 1.4426950408889634), fqq = (float)s.qqr2e;  // alpha log2(e)
+  const float spice = (float)pice, fsa = s.fsa, falpha_l2 = s.falpha_l2, fqq = s.fqq;
   const float* const ntab = s.near_tab;  // RBMD_NEAR_TABLE: the reference's G table
   const R far = R(1e30);
   const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
@@ -1951,8 +1950,8 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
 // tail is short columns.  The RBL mean force is summed per column and the system's last column
 // adds the partials in column order: the result does not depend on which warp took which column.
 constexpr int kColWarps = 4;     // warps per block
-constexpr int kColStage = 192;   // staged candidates per warp
-constexpr int kColQ = 96;        // the most steps between evaluations
+constexpr int kColStage = 256;   // staged candidates per warp
+constexpr int kColQ = kColStage;  // the most steps between evaluations: a staged tile
 constexpr int kColQW = kColQ / 32;  // 32-step blocks between evaluations
 constexpr float kColFar = 1e30f;
 // resident blocks per SM: 4 (128 registers per thread) ran the saline stream's column launch in
@@ -2128,8 +2127,7 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
           const int2 sp = s_sp[wid][lane];
           const float2 sw = s_sw[wid][lane];
           float4 fa = s_f[wid][lane];
-          const float spice = (float)pice, fsa = (float)sqrt(s.alpha);
-          const float falpha_l2 = (float)(s.alpha * 1.4426950408889634), fqq = (float)s.qqr2e;  // alpha log2(e)
+          const float spice = (float)pice, fsa = s.fsa, falpha_l2 = s.falpha_l2, fqq = s.fqq;
           const float* const ntab = s.near_tab;  // RBMD_NEAR_TABLE: the reference's G table
           int wc = 0;  // block of the next selected candidate, its remaining bits and its picks
           unsigned mc = s_sel[wid][0][lane], pc = s_pk[wid][0][lane];
