@@ -144,6 +144,13 @@ class Context {
   // admitting and retiring systems then costs no device-wide synchronisation.  dmalloc returns
   // nullptr (and clears the error) when the pool cannot grow.
   void* dmalloc(size_t bytes);
+  bool pooled() const { return pool_ != nullptr; }
+  // bytes of device memory the pool holds (in use or free for reuse)
+  int64_t pool_reserved() const {
+    uint64_t v = 0;
+    if (pool_) cudaMemPoolGetAttribute(pool_, cudaMemPoolAttrReservedMemCurrent, &v);
+    return (int64_t)v;
+  }
   void dfree(void* p);
 
  private:

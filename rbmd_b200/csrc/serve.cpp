@@ -252,6 +252,14 @@ void Server::loop() {
       }
     }
     lap(0);
+    // Keep the context's memory pool at twice the admitted footprint (capped by the budget), grown
+    // by one allocation freed at once (the pool keeps freed memory): the systems' own allocations,
+    // a few dozen each, then come from memory the pool holds.  Growing the pool allocation by
+    // allocation took up to 0.1 s per large system and 1.8 s of the saline stream's 37 s.
+    if (!admitted.empty() && ctx_->pooled()) {
+      const int64_t want = std::min<int64_t>(budget_, 2 * used_), have = ctx_->pool_reserved();
+      if (want > have) ctx_->dfree(ctx_->dmalloc((size_t)(want - have)));
+    }
     // upload + Init of the admitted systems (outside the queue lock)
     std::vector<int32_t> new_ids;
     for (Request* r : admitted) {
