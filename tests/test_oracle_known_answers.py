@@ -163,7 +163,10 @@ def test_eam_splines_match_johnson(oracle_mod):
 
 def test_rbe_mean_force_is_unbiased(oracle_mod):
     """The RBE k-space force averaged over independent Philox streams converges to the Ewald
-    k-space force (RBE is an unbiased estimator)."""
+    k-space force (RBE is an unbiased estimator).  For an unbiased estimator the squared error of
+    the mean of K samples is tr(Cov) / K, with tr(Cov) estimated from the samples' own spread, so
+    z = |mean - Ewald|^2 / (V / K) is about 1 (1.1 here); a bias b adds |b|^2 K / V, so z < 3 rejects
+    a bias of 1.5% of the Ewald force and more (a 2% scale error gives z = 4.8 at K = 2400)."""
     sd = synth.nacl_melt(n_side=4, rho=0.6, P=40, alpha=0.6)
     rng = np.random.default_rng(1)
     sd.pos += rng.normal(scale=0.2, size=sd.pos.shape)
@@ -173,17 +176,20 @@ def test_rbe_mean_force_is_unbiased(oracle_mod):
     ew = oracle_mod.Oracle(sd)
     ewald = ew.ewald_kspace_force()
     sd.params.coulomb = A.COUL_RBE
-    acc = np.zeros_like(ewald)
-    K = 600
+    K = 4000
+    samples = np.empty((K,) + ewald.shape)
     for k in range(K):
         sd2 = sd.copy()
         sd2.params.seed = 1000 + k
         o = oracle_mod.Oracle(sd2)
         o.compute_forces()
-        acc += o.force_part(1)
-    mean = acc / K
+        samples[k] = o.force_part(1)
+    mean = samples.mean(0)
+    var = ((samples - mean) ** 2).sum() / (K - 1)
+    z = ((mean - ewald) ** 2).sum() / (var / K)
+    assert z < 3.0, z
     err = np.sqrt(((mean - ewald) ** 2).sum() / (ewald ** 2).sum())
-    assert err < 0.08
+    assert err < 0.02, err
 
 
 def test_shake_holds_water_geometry(oracle_mod):
