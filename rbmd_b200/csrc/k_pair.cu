@@ -2131,6 +2131,8 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
           const float* const ntab = s.near_tab;  // RBMD_NEAR_TABLE: the reference's G table
           int wc = 0;  // block of the next selected candidate, its remaining bits and its picks
           unsigned mc = s_sel[wid][0][lane], pc = s_pk[wid][0][lane];
+          // two rounds per iteration: independent pairs for the scheduler to interleave
+#pragma unroll 2
           for (int k = 0; k < rounds; ++k) {
             if (k < qn) {
               while (mc == 0u) {
@@ -2145,29 +2147,28 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
               const float4 pj = s_c[wid][e];
               const float rx = pj.x - pix, ry = pj.y - piy, rz = pj.z - piz;
               const float d2 = tile_d2(rx, ry, rz);
-              if (d2 > 0.0001f) {  // the pair of an atom with itself is selected as core and dropped here
-                const int idt = s_id[wid][e];
-                const int idj = idt & kJsMask, tj = idt >> kJsBits;
-                float w = 1.0f;
-                if (SPECIAL) {
-                  if (ai.z <= 2) {
-                    w = (idj == sp.x) ? sw.x : w;
-                    w = (idj == sp.y) ? sw.y : w;
-                  } else {
-                    for (int t2 = 0; t2 < ai.z; ++t2)
-                      if (__ldg(&s.sp_ids[ai.w + t2]) == idj) w = (float)__ldg(&s.sp_w[ai.w + t2]);
-                  }
-                }
-                // LJ/CUT skips pairs of one molecule (its staged id is the molecule)
-                if (MODE != kLJ_RBL || idj != ai.y) {
-                  const float2 lj = __ldg(&s.ljf[ai.x * ntypes + tj]);
-                  const float f = tile_pair_f32_lj<MODE, NEAR>(core, d2, fa.w, pj.w, lj.x, lj.y, w, spice, fsa,
-                                                               falpha_l2, fqq, ntab);
-                  fa.x += f * rx;
-                  fa.y += f * ry;
-                  fa.z += f * rz;
+              const int idt = s_id[wid][e];
+              const int idj = idt & kJsMask, tj = idt >> kJsBits;
+              float w = 1.0f;
+              if (SPECIAL) {
+                if (ai.z <= 2) {
+                  w = (idj == sp.x) ? sw.x : w;
+                  w = (idj == sp.y) ? sw.y : w;
+                } else {
+                  for (int t2 = 0; t2 < ai.z; ++t2)
+                    if (__ldg(&s.sp_ids[ai.w + t2]) == idj) w = (float)__ldg(&s.sp_w[ai.w + t2]);
                 }
               }
+              const float2 lj = __ldg(&s.ljf[ai.x * ntypes + tj]);
+              float f = tile_pair_f32_lj<MODE, NEAR>(core, d2, fa.w, pj.w, lj.x, lj.y, w, spice, fsa, falpha_l2,
+                                                     fqq, ntab);
+              // without a branch: the pair of an atom with itself (selected as core, d2 = 0, f not
+              // finite) and, for LJ/CUT, pairs of one molecule (its staged id is the molecule) are
+              // dropped by the select
+              f = ((d2 > 0.0001f) & (MODE != kLJ_RBL || idj != ai.y)) ? f : 0.0f;
+              fa.x += f * rx;
+              fa.y += f * ry;
+              fa.z += f * rz;
             }
           }
           s_f[wid][lane] = fa;
