@@ -149,7 +149,7 @@ int oracle_get_kspace(void* h, int32_t* m, double* rhok) {
   return 0;
 }
 
-// Full Ewald k-space force (x qqr2e) at the current positions; the FP64 judge of RBE's own error.
+// Full Ewald k-space force (x qqr2e) at the current positions; the FP64 yardstick for RBE's own error.
 int oracle_ewald_kspace_force(void* h, double* f) {
   System* s = static_cast<System*>(h);
   std::vector<double> F;
