@@ -2131,9 +2131,9 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
           const float* const ntab = s.near_tab;  // RBMD_NEAR_TABLE: the reference's G table
           int wc = 0;  // block of the next selected candidate, its remaining bits and its picks
           unsigned mc = s_sel[wid][0][lane], pc = s_pk[wid][0][lane];
-          // (not unrolled: two rounds per iteration cut the instructions by 7%, but inside a step, where
-          // the out-of-line stray walk also runs, the larger code missed the instruction cache and
-          // the launch was no faster)
+          // (not unrolled: two rounds per iteration cut the instructions by 7% and force evaluations
+          // from the start ran 8% faster, but steps of the dynamics ran no faster, and the first
+          // step's launch stalled on instruction fetch)
           for (int k = 0; k < rounds; ++k) {
             if (k < qn) {
               while (mc == 0u) {
