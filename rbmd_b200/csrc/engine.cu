@@ -946,11 +946,11 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
   mk(wp, b.pair);
   mk(wpc, b.pair_cells);
   if (b.dense == 2 && b.pair.n > 0) {
-    b.col_ctr = (unsigned*)dmalloc(2 * sizeof(unsigned));
+    b.col_ctr = (unsigned*)dmalloc(4 * sizeof(unsigned));  // the column kernel's, then the stray pass's
     if (!b.col_ctr) rc = RBMD_ERR_OOM;
     else {
       br->allocs.push_back(b.col_ctr);
-      cudaMemsetAsync(b.col_ctr, 0, 2 * sizeof(unsigned), stream);
+      cudaMemsetAsync(b.col_ctr, 0, 4 * sizeof(unsigned), stream);
     }
     b.col_grid = pair_col_grid(b.pair.n, b.ff, b.special, b.near);
   }

@@ -1943,8 +1943,11 @@ k_pair_tile(const SysDev* __restrict__ S, const int2* __restrict__ work, int cap
 // cells dropped that way hold no core or shell atom, so the shell ranks, and the RBL picks, stay
 // exactly those of the full traversal.  The selected candidates of up to kColQ steps are evaluated
 // by their own lane from the masks, in traversal order, so an atom's force is summed in a fixed
-// order by one lane.  Atoms outside the box walk their own neighbourhood with the whole warp first
-// (tile_stray), as in the tile kernel.
+// order by one lane.  An atom outside its binned cell (SHAKE moves atoms after binning, and atoms
+// may lie outside the box) walks its own neighbourhood with the whole warp (tile_stray, as in the
+// tile kernel), in a pass of its own before the column kernel (k_pair_col_strays): its force is
+// written there, and the column kernel only reads it back for the RBL mean, so that the stray
+// walk's code does not share the instruction cache with the walk and the evaluation.
 // The kernel is persistent: one grid of resident blocks, each warp taking the batch's columns one at
 // a time from a work counter, longest columns first, so no warp waits for another and the launch's
 // tail is short columns.  The RBL mean force is summed per column and the system's last column
@@ -1971,22 +1974,72 @@ __device__ __noinline__ unsigned col_classify_fp64(const SysDev* __restrict__ sp
   return (core ? 1u : 0u) | (shell ? 2u : 0u);
 }
 
-// ... and one atom outside the box, walked by the whole warp (every lane calls it): its force is
-// written and its three force components returned in every lane.
+// Whether the atom at sorted index si, binned into home column (hx, hy) at z cell zl, lies outside
+// that cell: the unclamped cell of its FP64 position (ExecPointLocator::InWhichCell) is another.
+__device__ inline bool col_is_stray(const SysDev& s, int si, int hx, int hy, int zl) {
+  const double4 xd = ldg4(&s.sx[si]);
+  return (int)((xd.x - s.lo[0]) / s.d[0]) != hx || (int)((xd.y - s.lo[1]) / s.d[1]) != hy ||
+         (int)((xd.z - s.lo[2]) / s.d[2]) != zl;
+}
+
+// The first shell rank to pick of atom i (RBL Philox offset mode; 0 in stride mode): the count of
+// shells still to skip before its first pick.
+__device__ inline int col_first_skip(const SysDev& s, int i, int pice) {
+  if (s.rbl_mode != RBMD_RBL_PHILOX || pice <= 1) return 0;
+  uint32_t o[4];
+  philox4x32_10((uint32_t)i, 0u, (uint32_t)s.st->step, kTagRblOffset, s.seed_lo, s.seed_hi, o);
+  const int nm = (int)(o[0] % (uint32_t)pice);
+  return nm == 0 ? 0 : pice - nm;
+}
+
+// The stray atoms of the batch's columns, before the column kernel: each is walked by the whole
+// warp over its own neighbourhood and its force written (finish_atom), where the column kernel
+// reads it back.  Warps take columns from a work counter (ctr[0]; ctr[1] counts finished warps, and
+// the last one resets both), as the column kernel does.
 template <int MODE, bool SPECIAL, bool NEAR>
-__device__ __noinline__ double3 col_stray(const SysDev* __restrict__ sp, int si, int skip, const float* s_tab,
-                                         int owner_lane, int i) {
-  const SysDev& s = *sp;
-  float ff[6];
-  PairAcc acc;
-  acc_zero(ff, acc);
-  tile_stray<float, MODE, SPECIAL, false, NEAR>(s, si, skip, s.pice, true, s_tab, 0, nullptr, nullptr, nullptr, nullptr, ff,
-                                          acc);
-  double cmb[6], r9[9];
-  acc_warp_total<true>(ff, acc, cmb);
-  acc_to_r9<MODE, true, false>(s, cmb, acc, r9);
-  if ((int)(threadIdx.x & 31) == owner_lane) finish_atom<MODE>(s, i, r9);
-  return make_double3(r9[0], r9[1], r9[2]);
+__global__ void __launch_bounds__(kColWarps * 32)
+k_pair_col_strays(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwork, unsigned* __restrict__ ctr) {
+  const int lane = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  for (;;) {
+    int wi = 0;
+    if (lane == 0) wi = (int)atomicAdd(&ctr[0], 1u);
+    wi = __shfl_sync(FULL, wi, 0);
+    if (wi >= nwork) break;
+    const int2 wk = __ldg(&work[wi]);
+    const SysDev& s = S[wk.x];
+    const int dy = s.dims[1], dz = s.dims[2];
+    const int hx = wk.y / dy, hy = wk.y % dy;
+    const int cbase = dz * (hy + dy * hx);
+    const int a0 = __ldg(&s.cell_start[cbase]), a1 = __ldg(&s.cell_start[cbase + dz]);
+    for (int g0 = a0; g0 < a1; g0 += 32) {
+      const int si = g0 + lane;
+      int i = 0, c = 0;
+      bool stray = false;
+      if (si < a1) {
+        i = __ldg(&s.smeta[si]).x;
+        stray = col_is_stray(s, si, hx, hy, __ldg(&s.cell_of_atom[i]) - cbase);
+        if (stray) c = col_first_skip(s, i, s.pice);
+      }
+      for (unsigned m = __ballot_sync(FULL, stray); m; m &= m - 1) {
+        const int as = __ffs(m) - 1;
+        const int sk = __shfl_sync(FULL, c, as);
+        float ff[6];
+        PairAcc acc;
+        acc_zero(ff, acc);
+        tile_stray<float, MODE, SPECIAL, false, NEAR>(s, g0 + as, sk, s.pice, true, (const float*)s.ljf, 0, nullptr,
+                                                      nullptr, nullptr, nullptr, ff, acc);
+        double cmb[6], r9[9];
+        acc_warp_total<true>(ff, acc, cmb);
+        acc_to_r9<MODE, true, false>(s, cmb, acc, r9);
+        if (lane == as) finish_atom<MODE>(s, i, r9);
+      }
+    }
+  }
+  if (lane == 0 && atomicAdd(&ctr[1], 1u) == gridDim.x * (unsigned)kColWarps - 1u) {
+    ctr[0] = 0u;
+    ctr[1] = 0u;
+  }
 }
 
 template <int MODE, bool SPECIAL, bool NEAR>
@@ -2063,15 +2116,8 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
           i = mi.x;
           p4 = __ldg(&s.sxf[si]);
           zl = __ldg(&s.cell_of_atom[i]) - cbase;  // internal cell id iz + dz (iy + dy ix), this column
-          const double4 xd = ldg4(&s.sx[si]);
-          stray = (int)((xd.x - s.lo[0]) / s.d[0]) != hx || (int)((xd.y - s.lo[1]) / s.d[1]) != hy ||
-                  (int)((xd.z - s.lo[2]) / s.d[2]) != zl;
-          if (s.rbl_mode == RBMD_RBL_PHILOX && pice > 1) {
-            uint32_t o[4];
-            philox4x32_10((uint32_t)i, 0u, (uint32_t)s.st->step, kTagRblOffset, s.seed_lo, s.seed_hi, o);
-            const int nm = (int)(o[0] % (uint32_t)pice);
-            c = nm == 0 ? 0 : pice - nm;
-          }
+          stray = col_is_stray(s, si, hx, hy, zl);
+          c = col_first_skip(s, i, pice);
           int nsp = 0, spb = 0, sp0 = -1, sp1 = -1;
           float w0 = 1.0f, w1 = 1.0f;
           if (SPECIAL) {  // special partners: the first two cached, the rest read from the CSR lists
@@ -2097,18 +2143,13 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
         }
         s_f[wid][lane] = make_float4(0.0f, 0.0f, 0.0f, p4.w);
 
-        // ---- atoms outside the box: the whole warp walks each one's own neighbourhood
-        unsigned strays = __ballot_sync(FULL, valid && stray);
-        while (strays) {
-          const int as = __ffs(strays) - 1;
-          strays &= strays - 1;
-          const int sk = __shfl_sync(FULL, c, as);
-          const double3 r = col_stray<MODE, SPECIAL, NEAR>(&s, g0 + as, sk, (const float*)s.ljf, as, i);
-          if (lane == as) {
-            red0 += r.x;
-            red1 += r.y;
-            red2 += r.z;
-          }
+        // ---- an atom outside its cell: walked by k_pair_col_strays before this launch, which wrote
+        // its force
+        if (valid && stray) {
+          const double4 fs = s.f[i];
+          red0 += fs.x;
+          red1 += fs.y;
+          red2 += fs.z;
         }
 
         // ---- the chunk's own atoms, row by row
@@ -2131,9 +2172,8 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
           const float* const ntab = s.near_tab;  // RBMD_NEAR_TABLE: the reference's G table
           int wc = 0;  // block of the next selected candidate, its remaining bits and its picks
           unsigned mc = s_sel[wid][0][lane], pc = s_pk[wid][0][lane];
-          // (not unrolled: two rounds per iteration cut the instructions by 7% and force evaluations
-          // from the start ran 8% faster, but steps of the dynamics ran no faster, and the first
-          // step's launch stalled on instruction fetch)
+          // two rounds per iteration: independent pairs for the scheduler to interleave
+#pragma unroll 2
           for (int k = 0; k < rounds; ++k) {
             if (k < qn) {
               while (mc == 0u) {
@@ -2417,6 +2457,9 @@ static void go_near(const Batch& b, cudaStream_t st) {
   if constexpr (kColumn) {
     if (b.dense == 2) {
       if (b.pair.n > 0) {
+        k_pair_col_strays<MODE, SPECIAL, NEAR><<<b.col_grid, kColWarps * 32, 0, st>>>(b.sys, b.pair.d, b.pair.n,
+                                                                                      b.col_ctr + 2);
+        note_launch();
         k_pair_col<MODE, SPECIAL, NEAR><<<b.col_grid, kColWarps * 32, 0, st>>>(b.sys, b.pair.d, b.pair.n, b.col_ctr,
                                                                                band);
         note_launch();

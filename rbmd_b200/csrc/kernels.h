@@ -22,7 +22,8 @@ struct Batch {
   Work pair_cells;           // column layout: the tile kernel's cell table (energies, other modes)
   // column layout: pair.d lists every column (slot, column index), most atoms per column first;
   // the persistent column kernel's warps take them in that order from col_ctr[0] (col_ctr[1] counts
-  // the warps that are done; the last one resets both), col_grid blocks
+  // the warps that are done; the last one resets both), col_grid blocks; the stray pass before it
+  // uses col_ctr[2] and col_ctr[3] the same way
   unsigned* col_ctr = nullptr;
   int col_grid = 0;
   // uniform switches of the batch (a batch never mixes them)
