@@ -952,7 +952,8 @@ Context::BatchRec* Context::build_batch(const std::vector<System*>& group, int& 
       br->allocs.push_back(b.col_ctr);
       cudaMemsetAsync(b.col_ctr, 0, 4 * sizeof(unsigned), stream);
     }
-    b.col_grid = pair_col_grid(b.pair.n, b.ff, b.special, b.near);
+    b.col_grid = pair_col_grid(b.pair.n, b.ff, b.special, b.near, false);
+    b.stray_grid = pair_col_grid(b.pair.n, b.ff, b.special, b.near, true);
   }
   mk(wc, b.cell);
   mk(wr, b.rho);

@@ -1996,8 +1996,16 @@ __device__ inline int col_first_skip(const SysDev& s, int i, int pice) {
 // warp over its own neighbourhood and its force written (finish_atom), where the column kernel
 // reads it back.  Warps take columns from a work counter (ctr[0]; ctr[1] counts finished warps, and
 // the last one resets both), as the column kernel does.
+// resident blocks per SM the stray pass is compiled for: its walks wait on dependent loads, so it
+// runs more warps per SM than the column kernel, at the price of a few spilled registers (on the
+// saline stream 25.79 ms for both pair launches of a step, against 25.83 ms at the column kernel's
+// 4 blocks and 25.76 ms at 8)
+#ifndef RBMD_STRAY_MIN_BLOCKS
+#define RBMD_STRAY_MIN_BLOCKS 6
+#endif
+
 template <int MODE, bool SPECIAL, bool NEAR>
-__global__ void __launch_bounds__(kColWarps * 32)
+__global__ void __launch_bounds__(kColWarps * 32, RBMD_STRAY_MIN_BLOCKS)
 k_pair_col_strays(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwork, unsigned* __restrict__ ctr) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
@@ -2457,8 +2465,8 @@ static void go_near(const Batch& b, cudaStream_t st) {
   if constexpr (kColumn) {
     if (b.dense == 2) {
       if (b.pair.n > 0) {
-        k_pair_col_strays<MODE, SPECIAL, NEAR><<<b.col_grid, kColWarps * 32, 0, st>>>(b.sys, b.pair.d, b.pair.n,
-                                                                                      b.col_ctr + 2);
+        k_pair_col_strays<MODE, SPECIAL, NEAR><<<b.stray_grid, kColWarps * 32, 0, st>>>(b.sys, b.pair.d, b.pair.n,
+                                                                                        b.col_ctr + 2);
         note_launch();
         k_pair_col<MODE, SPECIAL, NEAR><<<b.col_grid, kColWarps * 32, 0, st>>>(b.sys, b.pair.d, b.pair.n, b.col_ctr,
                                                                                band);
@@ -2489,15 +2497,23 @@ static void go(const Batch& b, cudaStream_t st) {
   go_near<R, MODE, SPECIAL, VIRIAL, false>(b, st);
 }
 
-int pair_col_grid(int ncols, int ff, int special, int near) {
+int pair_col_grid(int ncols, int ff, int special, int near, bool strays) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const void* fn = ff == RBMD_FF_LJ_CUT ? (const void*)k_pair_col<kLJ_RBL, false, false>
-                   : special ? (near ? (const void*)k_pair_col<kCOUL_RBL, true, true>
-                                     : (const void*)k_pair_col<kCOUL_RBL, true, false>)
-                             : (near ? (const void*)k_pair_col<kCOUL_RBL, false, true>
-                                     : (const void*)k_pair_col<kCOUL_RBL, false, false>);
+  const void* fn;
+  if (strays)
+    fn = ff == RBMD_FF_LJ_CUT ? (const void*)k_pair_col_strays<kLJ_RBL, false, false>
+         : special ? (near ? (const void*)k_pair_col_strays<kCOUL_RBL, true, true>
+                           : (const void*)k_pair_col_strays<kCOUL_RBL, true, false>)
+                   : (near ? (const void*)k_pair_col_strays<kCOUL_RBL, false, true>
+                           : (const void*)k_pair_col_strays<kCOUL_RBL, false, false>);
+  else
+    fn = ff == RBMD_FF_LJ_CUT ? (const void*)k_pair_col<kLJ_RBL, false, false>
+         : special ? (near ? (const void*)k_pair_col<kCOUL_RBL, true, true>
+                           : (const void*)k_pair_col<kCOUL_RBL, true, false>)
+                   : (near ? (const void*)k_pair_col<kCOUL_RBL, false, true>
+                           : (const void*)k_pair_col<kCOUL_RBL, false, false>);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kColWarps * 32, 0);
   const int need = (ncols + kColWarps - 1) / kColWarps;
   return std::max(1, std::min(need, std::max(1, sms) * std::max(1, per_sm)));

@@ -23,9 +23,9 @@ struct Batch {
   // column layout: pair.d lists every column (slot, column index), most atoms per column first;
   // the persistent column kernel's warps take them in that order from col_ctr[0] (col_ctr[1] counts
   // the warps that are done; the last one resets both), col_grid blocks; the stray pass before it
-  // uses col_ctr[2] and col_ctr[3] the same way
+  // uses col_ctr[2] and col_ctr[3] the same way, stray_grid blocks
   unsigned* col_ctr = nullptr;
-  int col_grid = 0;
+  int col_grid = 0, stray_grid = 0;
   // uniform switches of the batch (a batch never mixes them)
   int ff = 0, neigh = 0, coul = 0, prec = 0, temp_ctrl = 0, special = 0;
   int has_shake = 0, has_bonded = 0;
@@ -51,7 +51,7 @@ void launch_bonded(const Batch& b, cudaStream_t s, int virial);
 void launch_pair(const Batch& b, cudaStream_t s, int virial);
 // Blocks of the persistent column kernel for `ncols` columns: resident blocks per SM x SMs of the
 // current device, fewer when the columns do not fill them (4 warps per block, a column per warp).
-int pair_col_grid(int ncols, int ff, int special, int near);
+int pair_col_grid(int ncols, int ff, int special, int near, bool strays);
 void launch_final(const Batch& b, cudaStream_t s, FinalMode mode, int virial);
 void launch_ke_thermostat(const Batch& b, cudaStream_t s);
 void launch_flush_vscale(const Batch& b, cudaStream_t s);
