@@ -77,6 +77,10 @@ struct SysState {
   // cell list.  The pair kernels that cull cells geometrically widen by the displacement and never
   // cull a recorded cell (an atom there sits on the far side of the box).
   unsigned shake_disp_bits;
+  // The farthest any atom lay outside its binned cell when the cell list was built (FP32 bits,
+  // rounded up): atoms given outside the box are binned into the clamped edge cell.  The culling
+  // margins widen by it too.
+  unsigned out_bits;
   int mig_n;
   int mig_cell[kMaxMigrated];
 };

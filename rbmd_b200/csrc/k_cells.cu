@@ -17,6 +17,7 @@ __global__ void k_cells_zero(const SysDev* __restrict__ S, const int2* __restric
   if (c < s.ncell) s.cell_count[c] = 0;
   if (c == 0) {  // a new cell list: nothing has moved since
     s.st->shake_disp_bits = 0u;
+    s.st->out_bits = 0u;
     s.st->mig_n = 0;
   }
 }
@@ -29,13 +30,16 @@ __global__ void k_cells_count(const SysDev* __restrict__ S, const int2* __restri
   const double4 p = s.x[i];
   const double pc[3] = {p.x, p.y, p.z};
   int ijk[3];
+  double out = 0.0;  // how far the atom lies outside the cell it is binned into
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     long long c = (long long)((pc[k] - s.lo[k]) / s.d[k]);  // truncation, as vtkm::Id3(Vec3f)
     c = c < 0 ? 0 : c;
     c = c > s.dims[k] - 1 ? s.dims[k] - 1 : c;
     ijk[k] = (int)c;
+    out = fmax(out, fmax(s.lo[k] + (double)c * s.d[k] - pc[k], pc[k] - (s.lo[k] + (double)(c + 1) * s.d[k])));
   }
+  if (out > 0.0) atomicMax(&s.st->out_bits, __float_as_uint(__double2float_ru(out)));  // non-negative: bits order as values
   // internal numbering is z fastest so that the 2 nc + 1 cells of a traversal row (fixed x and y
   // offsets) are contiguous in cell order; get_cells reports the reference's x-fastest ids
   const int cell = ijk[2] + s.dims[2] * (ijk[1] + s.dims[1] * ijk[0]);

@@ -745,11 +745,14 @@ k_pair2(const SysDev* __restrict__ S, const int2* __restrict__ work) {
     for (int k = 0; k < 32; k += pice) base_mask |= (1u << k);
     const R rc2 = (R)s.rc2, rs2 = (R)s.rs2;
     const int nc = s.nc, side = 2 * nc + 1, nrows = side * side;
-    // conservative culling radius: cells farther than rc from i (with a margin for atoms that
-    // moved since binning: at least the largest SHAKE displacement since the cell list was built)
-    // cannot hold a core or shell atom; cells of atoms SHAKE wrapped across the box (they sit on
-    // the far side of it) are never culled, and beyond kMaxMigrated of them nothing is
-    const double margin = fmax(0.1 * fmin(d0, fmin(d1, d2c)), 1.001 * (double)__uint_as_float(s.st->shake_disp_bits));
+    // conservative culling radius: cells farther than rc from i (with a margin for atoms outside
+    // their cell: at least the farthest an atom lay outside its binned cell plus the largest SHAKE
+    // displacement since the cell list was built) cannot hold a core or shell atom; cells of atoms
+    // SHAKE wrapped across the box (they sit on the far side of it) are never culled, and beyond
+    // kMaxMigrated of them nothing is
+    const double margin =
+        fmax(0.1 * fmin(d0, fmin(d1, d2c)), 1.001 * ((double)__uint_as_float(s.st->shake_disp_bits) +
+                                                     (double)__uint_as_float(s.st->out_bits)));
     const int mig_n = s.st->mig_n;
     const double cut2 = s.rc2;
     const double lo0 = s.lo[0], lo1 = s.lo[1], lo2 = s.lo[2];
@@ -2099,9 +2102,10 @@ k_pair_col(const SysDev* __restrict__ S, const int2* __restrict__ work, int nwor
     const float fdx = (float)s.d[0], fdy = (float)s.d[1], fdz = (float)s.d[2];
     const float frc2 = (float)s.rc2;
     // trimming margins: 1e-3 of a cell (far above the FP32 rounding of the coordinates involved) plus
-    // the largest distance SHAKE moved an atom since the cell list was built; cells of atoms it wrapped
-    // across the box are never trimmed, and beyond kMaxMigrated of them nothing is
-    const float mdisp = __uint_as_float(s.st->shake_disp_bits);
+    // the farthest an atom lay outside its binned cell (atoms given outside the box) and the largest
+    // distance SHAKE moved an atom since the cell list was built; cells of atoms it wrapped across
+    // the box are never trimmed, and beyond kMaxMigrated of them nothing is
+    const float mdisp = __uint_as_float(s.st->shake_disp_bits) + __uint_as_float(s.st->out_bits);
     const int mig_n = s.st->mig_n;
     const float mgx = 1e-3f * fdx + mdisp, mgy = 1e-3f * fdy + mdisp, mgz = 1e-3f * fdz + mdisp;
     double red0 = 0.0, red1 = 0.0, red2 = 0.0;  // this lane's atoms' forces (the RBL mean)
