@@ -565,7 +565,8 @@ def cpu_stream_rate(n_requests, steps=None, warmup=1, seconds=None, threads=None
                 strata=[dict(st, rate=r) for st, r in zip(strata, rates)], steps=done)
 
 
-PAIR_KERNELS = {"pair_col": "k_pair_col (warp per column of home cells, lane per atom over a staged row: RBL picks, LJ + erfc)",
+PAIR_KERNELS = {"pair_col": "k_pair_col (warp per column of home cells, lane per atom over a staged row: RBL picks, LJ + erfc), "
+                            "timed with the stray pass k_pair_col_strays before it",
                 "pair_tile": "k_pair_tile (warp per home cell: shared candidate batches, RBL picks, LJ + erfc)",
                 "pair_lean": "k_pair2 (warp per atom with segment tables)", "pair_atom": "k_pair (general warp per atom)"}
 
