@@ -41,3 +41,30 @@ def test_stream_strata_cover_the_stream():
     assert sum(s["requests"] for s in st) == 512 and sum(s["atoms"] for s in st) == int(sizes.sum())
     for s in st:
         assert s["lo"] <= s["size"] < s["hi"]
+
+
+def test_profiled_figures_of_the_column_kernel():
+    """The roofline fields that the bench line takes from the committed ncu summary of the column
+    kernel: all three present, and the DRAM traffic at least the algorithmic 64 B per atom."""
+    fig = bench.profiled_figures("pair_col")
+    assert fig["source"] == "profiles/k_pair_col_saline_small.md"
+    assert fig["traffic_bytes_per_atom"] >= 64.0
+    assert 0.0 < fig["issue_active_pct"] <= 100.0
+    assert fig["warp_inst_per_atom"] > 0.0
+
+
+def test_reference_arm_line():
+    """`bench.py --impl reference` on a tiny CPU sample: one JSON line with the reference arm's
+    keys -- the oracle port's throughput, its cpu_baseline and an e2e without device copies."""
+    import json
+    import subprocess
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0", "--cpu-seconds", "0.5"], capture_output=True, text=True, timeout=600,
+                       cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    assert d["impl"] == "reference" and d["unit"] == bench.UNIT and d["metric"] == bench.METRIC
+    assert d["value"] > 0 and d["higher_is_better"] is True
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"] and cb["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
